@@ -1,0 +1,193 @@
+/* tictac_b200 — B200-native WPCD solve of the elastic nucleon-deuteron
+ * AGS/Faddeev equations (the P123 / resolvent / Faddeev-solve path of Tic-tac).
+ *
+ * C-ABI: plain structs of pointers and sizes, status codes, no exceptions and
+ * no process exit.  Every entry point returns TT_OK (0) or an error code; the
+ * message of the last error on the calling thread is tt_last_error_string().
+ *
+ * Two layers:
+ *   1. drop-in entry points with the argument meaning of the reference's
+ *      three hot-path functions (host buffers in and out);
+ *   2. a run handle (tt_run_*) that performs the reference main loop's
+ *      state-space setup from key=value options and keeps each channel's
+ *      P123, A and factorisations resident in HBM for repeated solves.
+ */
+#ifndef TICTAC_B200_H
+#define TICTAC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define TT_OK 0
+#define TT_ERR_BADARG 1
+#define TT_ERR_NOMEM 2       /* HBM admission failed; nothing was left allocated */
+#define TT_ERR_CUDA 3
+#define TT_ERR_NOCONVERGE 4  /* iterative refinement hit refine_max_iter */
+#define TT_ERR_IO 5
+#define TT_ERR_UNSUPPORTED 6
+#define TT_ERR_SINGULAR 7    /* zero pivot in the LU of 1 - A G */
+
+/* ---- precision of the dense solve ---- */
+#define TT_PRECISION_FP64 0   /* complex128 LU, FP64 throughout */
+#define TT_PRECISION_MIXED 1  /* complex64 LU, BF16x3 tcgen05 trailing updates, FP64 refinement */
+#define TT_PRECISION_MIXED_SIMT 2  /* complex64 LU, FP32 CUDA-core trailing updates, FP64 refinement */
+
+/* complex128, layout-compatible with std::complex<double> */
+typedef struct tt_complex {
+  double re, im;
+} tt_complex;
+
+/* One 3N channel of the partial-wave basis.  Same fields and order as
+ * pw_3N_statespace (CPP/type_defs.h:15-29) restricted to one channel
+ * (the reference passes pw_substates, CPP/main.cpp:181-192). */
+typedef struct tt_pw_states {
+  int Nalpha;
+  int J_2N_max;
+  const int* L_2N_array;
+  const int* S_2N_array;
+  const int* J_2N_array;
+  const int* T_2N_array;
+  const int* L_1N_array;
+  const int* two_J_1N_array;
+  const int* two_J_3N_array;
+  const int* two_T_3N_array;
+  const int* P_3N_array;
+} tt_pw_states;
+
+/* Free wave-packet grid: the fields of fwp_statespace (CPP/type_defs.h:32-47)
+ * the path reads (bin boundaries). */
+typedef struct tt_fwp_states {
+  int Np_WP;
+  int Nq_WP;
+  const double* p_WP_array; /* [Np_WP+1] */
+  const double* q_WP_array; /* [Nq_WP+1] */
+} tt_fwp_states;
+
+/* Scattering wave packets, swp_statespace (CPP/type_defs.h:50-61). */
+typedef struct tt_swp_states {
+  int Np_WP;
+  int Nq_WP;
+  int num_2N_unco_states;
+  int num_2N_coup_states;
+  double E_bound;
+  const double* e_SWP_unco_array; /* [(Np+1) num_unco] */
+  const double* e_SWP_coup_array; /* [2 (Np+1) num_coup] */
+  const double* C_SWP_unco_array; /* [Np Np num_unco] row-major */
+  const double* C_SWP_coup_array; /* [4 Np Np num_coup] row-major */
+  const double* q_WP_array;       /* [Nq+1] */
+} tt_swp_states;
+
+/* Elastic on-shell indexing, channel_os_indexing (CPP/type_defs.h:77-85). */
+typedef struct tt_os_indexing {
+  int num_T_lab;
+  const int* q_com_idx_array;     /* [num_T_lab] */
+  const int* deuteron_idx_array;  /* [num_deuteron_states] */
+  int num_deuteron_states;
+} tt_os_indexing;
+
+/* The run_params fields (CPP/type_defs.h:87-123) the three functions read,
+ * plus the precision controls of this implementation. */
+typedef struct tt_run_params {
+  int Nphi;                 /* default 48 */
+  int Nx;                   /* default 48 */
+  int tensor_force;         /* default 1 */
+  int isospin_breaking_1S0; /* default 1 */
+  int production_run;       /* default 1 */
+  int precision;            /* TT_PRECISION_* (replaces solve_dense/Pade selection) */
+  double refine_tol;        /* refinement stop: max |dx|/|x| (default 1e-12) */
+  int refine_max_iter;      /* default 30 */
+} tt_run_params;
+
+void tt_run_params_default(tt_run_params* rp);
+
+typedef struct tt_solve_report {
+  double ms_A;          /* building A = C^T (2 P123) (V C) */
+  double ms_form;       /* forming 1 - A G for all energies */
+  double ms_factor;     /* LU factorisations */
+  double ms_solve;      /* triangular solves */
+  double ms_refine;     /* FP64 refinement */
+  int refine_iters;     /* max over energies */
+  double final_correction;
+  int info;             /* first zero pivot (1-based), 0 if none */
+} tt_solve_report;
+
+/* ---- layer 1: drop-in entry points ---------------------------------- */
+
+/* Replaces fill_P123_arrays (CPP/make_permutation_matrix.h:79-87,
+ * make_permutation_matrix.cpp:1297-1403) for one channel: builds P123 on the
+ * GPU and returns it in the reference's row-major COO order (sorted by
+ * row*n+col).  Callee allocates *val, *row, *col (free with tt_free).
+ * No TFC/HDF5 side files are written. */
+int tt_fill_P123_arrays(double** val, int** row, int** col, size_t* nnz, int production_run,
+                        const tt_fwp_states* fwp, const tt_pw_states* pw, const tt_run_params* rp);
+
+/* Replaces calculate_resolvent_array_in_SWP_basis (CPP/make_resolvent.h:36-40):
+ * caller-allocated G[n], n = Nalpha Nq Np, index alpha*Nq*Np + q*Np + p. */
+int tt_calculate_resolvent_array_in_SWP_basis(tt_complex* G, double E, const tt_swp_states* swp,
+                                              const tt_pw_states* pw, const tt_run_params* rp);
+
+/* Replaces solve_faddeev_equations (CPP/solve_faddeev.h:25-38) for the
+ * elastic on-shell U-matrix: U[d'*nd*nE + d*nE + j] (caller allocates
+ * nE*nd*nd), G[j*n + i] the resolvents of the nE on-shell energies, P123 in
+ * the reference's CSC form (values, int row indices, size_t column pointers
+ * [n+1]), V in the WP basis.  rp->precision selects FP64 or mixed+refined. */
+int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double* P123_val, const int* P123_row,
+                               const size_t* P123_colptr_csc, size_t P123_nnz, const double* V_WP_unco,
+                               const double* V_WP_coup, const tt_swp_states* swp, const tt_os_indexing* os,
+                               const tt_pw_states* pw, const tt_run_params* rp, tt_solve_report* report);
+
+void tt_free(void* p);
+const char* tt_last_error_string(void);
+int tt_device_count(int* count);
+
+/* ---- layer 2: run handle -------------------------------------------- */
+
+typedef struct tt_run tt_run;
+
+/* Configure a run from key=value options with the reference's keys and
+ * defaults (CPP/set_run_parameters.cpp:76-280, 577-615), e.g.
+ * "Np_WP=16", "potential_model=malfliet_tjon", "lab_energies=13".  Builds the
+ * partial-wave basis, WP grids, potential matrices, SWP states and on-shell
+ * bins on the host (CPP/main.cpp:98-378). */
+int tt_run_create(tt_run** run, int nopt, const char* const* opts);
+void tt_run_destroy(tt_run* run);
+
+/* Counts and per-channel facts. */
+int tt_run_num_channels(const tt_run* run, int* n_chn);
+int tt_run_channel_info(const tt_run* run, int chn, int* Nalpha, int* dense_dim, int* two_J_3N, int* P_3N,
+                        int* n_deuteron);
+int tt_run_num_energies(const tt_run* run, int* nE);
+int tt_run_energies(const tt_run* run, double* T_lab, double* E_com, int* q_com_idx);
+int tt_run_E_bound(const tt_run* run, double* E_bound);
+
+/* Device stages for one channel: P123 in HBM, A in HBM, resolvents. */
+int tt_run_build_P123(tt_run* run, int chn, int64_t* nnz);
+int tt_run_build_A(tt_run* run, int chn, double* ms);
+int tt_run_build_resolvent(tt_run* run, int chn);
+/* Solve all on-shell energies of the channel; U as in tt_solve_faddeev_equations. */
+int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_report* report);
+/* Release the channel's device data. */
+int tt_run_release_channel(tt_run* run, int chn);
+
+/* Host copies for checking (sizes from tt_run_channel_info / build results). */
+int tt_run_get_P123_csr(const tt_run* run, int chn, int64_t* rowptr, int32_t* col, double* val);
+int tt_run_get_A(const tt_run* run, int chn, double* A);
+int tt_run_get_G(const tt_run* run, int chn, tt_complex* G);
+/* which: 0 pw states (9 ints per alpha: L S J T l 2j 2J 2T P), 1 p_WP, 2 q_WP,
+ * 3 V_unco, 4 V_coup, 5 C_unco, 6 C_coup, 7 e_unco, 8 e_coup.  With buf NULL
+ * only *count is returned. */
+int tt_run_get_host_array(const tt_run* run, int chn, int which, void* buf, size_t* count);
+
+/* U-matrix text table in the reference's format (disk_io_routines.cpp:759-913). */
+int tt_run_write_U_table(const tt_run* run, int chn, const tt_complex* U, const char* path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TICTAC_B200_H */

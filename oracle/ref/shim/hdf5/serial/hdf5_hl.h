@@ -1,0 +1,1 @@
+#include "../../tt_hdf5_shim.h"

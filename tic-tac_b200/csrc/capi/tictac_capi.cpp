@@ -1,0 +1,561 @@
+// C-ABI of tictac_b200 (include/tictac_b200.h).
+#include "tictac_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../cuda/tt_kernels.h"
+#include "../host/tt_host.h"
+#include "../host/tt_p123.h"
+#include "../host/tt_solver.h"
+
+namespace tt {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+}  // namespace tt
+
+using namespace tt;
+
+namespace {
+
+int fail(int code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+
+struct ChannelState {
+  std::unique_ptr<ChannelSolver> solver;
+  bool have_P = false, have_A = false, have_G = false;
+};
+
+// Per-thread stream for the drop-in entry points.
+cudaStream_t default_stream() {
+  static thread_local cudaStream_t s = nullptr;
+  if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  return s;
+}
+
+PWChannel view_of(const tt_pw_states* pw) {
+  PWChannel c;
+  c.Nalpha = pw->Nalpha;
+  c.J_2N_max = pw->J_2N_max;
+  c.L_2N = pw->L_2N_array;
+  c.S_2N = pw->S_2N_array;
+  c.J_2N = pw->J_2N_array;
+  c.T_2N = pw->T_2N_array;
+  c.L_1N = pw->L_1N_array;
+  c.two_J_1N = pw->two_J_1N_array;
+  c.two_J_3N = pw->two_J_3N_array;
+  c.two_T_3N = pw->two_T_3N_array;
+  c.P_3N = pw->P_3N_array;
+  return c;
+}
+
+RunParams params_of(const tt_run_params* rp) {
+  RunParams r;
+  if (rp) {
+    r.Nphi = rp->Nphi;
+    r.Nx = rp->Nx;
+    r.tensor_force = rp->tensor_force != 0;
+    r.isospin_breaking_1S0 = rp->isospin_breaking_1S0 != 0;
+    r.production_run = rp->production_run != 0;
+    r.precision = rp->precision == TT_PRECISION_FP64 ? "fp64" : "mixed";
+    r.precision_code = rp->precision;
+    r.refine_tol = rp->refine_tol;
+    r.refine_max_iter = rp->refine_max_iter;
+  }
+  return r;
+}
+
+SWPStates swp_of(const tt_swp_states* s) {
+  SWPStates w;
+  w.Np_WP = s->Np_WP;
+  w.Nq_WP = s->Nq_WP;
+  w.n_unco = s->num_2N_unco_states;
+  w.n_coup = s->num_2N_coup_states;
+  w.E_bound = s->E_bound;
+  const size_t Np = s->Np_WP;
+  if (s->e_SWP_unco_array) w.e_unco.assign(s->e_SWP_unco_array, s->e_SWP_unco_array + (Np + 1) * w.n_unco);
+  if (s->e_SWP_coup_array) w.e_coup.assign(s->e_SWP_coup_array, s->e_SWP_coup_array + 2 * (Np + 1) * w.n_coup);
+  if (s->C_SWP_unco_array) w.C_unco.assign(s->C_SWP_unco_array, s->C_SWP_unco_array + Np * Np * w.n_unco);
+  if (s->C_SWP_coup_array) w.C_coup.assign(s->C_SWP_coup_array, s->C_SWP_coup_array + 4 * Np * Np * w.n_coup);
+  w.q_WP.assign(s->q_WP_array, s->q_WP_array + s->Nq_WP + 1);
+  return w;
+}
+
+SolveOptions options_of(const RunParams& rp, int precision) {
+  SolveOptions o;
+  o.mixed = precision == TT_PRECISION_MIXED || precision == TT_PRECISION_MIXED_SIMT;
+  o.tensor_cores = precision == TT_PRECISION_MIXED;
+  o.refine_tol = rp.refine_tol;
+  o.refine_max_iter = rp.refine_max_iter;
+  return o;
+}
+
+void fill_report(const SolveReport& r, double ms_A, tt_solve_report* out) {
+  if (!out) return;
+  out->ms_A = ms_A;
+  out->ms_form = r.ms_form;
+  out->ms_factor = r.ms_factor;
+  out->ms_solve = r.ms_solve;
+  out->ms_refine = r.ms_refine;
+  out->refine_iters = r.refine_iters;
+  out->final_correction = r.final_correction;
+  out->info = r.info;
+}
+
+}  // namespace
+
+struct tt_run {
+  RunParams rp;
+  PWStates pw;
+  FWPStates fwp;
+  std::vector<double> V_unco, V_coup;
+  SWPStates swp;
+  OnShell os;
+  std::vector<ChannelState> chn;
+  cudaStream_t stream = nullptr;
+};
+
+extern "C" {
+
+void tt_run_params_default(tt_run_params* rp) {
+  if (!rp) return;
+  rp->Nphi = 48;
+  rp->Nx = 48;
+  rp->tensor_force = 1;
+  rp->isospin_breaking_1S0 = 1;
+  rp->production_run = 1;
+  rp->precision = TT_PRECISION_MIXED;
+  rp->refine_tol = 1e-12;
+  rp->refine_max_iter = 30;
+}
+
+void tt_free(void* p) { std::free(p); }
+const char* tt_last_error_string(void) { return last_error(); }
+
+int tt_device_count(int* count) {
+  if (!count) return fail(TT_ERR_BADARG, "null count");
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+    return fail(TT_ERR_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  }
+  *count = c;
+  return TT_OK;
+}
+
+int tt_fill_P123_arrays(double** val, int** row, int** col, size_t* nnz, int production_run, const tt_fwp_states* fwp,
+                        const tt_pw_states* pw, const tt_run_params* rpp) {
+  if (!val || !row || !col || !nnz || !fwp || !pw || !rpp) return fail(TT_ERR_BADARG, "null argument");
+  RunParams rp = params_of(rpp);
+  rp.production_run = production_run != 0;
+  FWPStates f;
+  f.Np_WP = fwp->Np_WP;
+  f.Nq_WP = fwp->Nq_WP;
+  f.p_WP.assign(fwp->p_WP_array, fwp->p_WP_array + fwp->Np_WP + 1);
+  f.q_WP.assign(fwp->q_WP_array, fwp->q_WP_array + fwp->Nq_WP + 1);
+  P123Tables t;
+  std::string err;
+  if (!p123_prepare(rp, f, view_of(pw), t, &err)) return fail(TT_ERR_BADARG, err);
+  cudaStream_t st = default_stream();
+  DeviceCSR P;
+  int s = p123_build_device(t, P, st, nullptr);
+  if (s != TT_OK) return s;
+  const int n = P.n;
+  std::vector<int64_t> rowptr(n + 1);
+  if (cudaMemcpy(rowptr.data(), P.rowptr.ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(TT_ERR_CUDA, "copy of P123 row pointers failed");
+  const size_t m = (size_t)P.nnz;
+  *val = (double*)std::malloc(sizeof(double) * std::max<size_t>(m, 1));
+  *row = (int*)std::malloc(sizeof(int) * std::max<size_t>(m, 1));
+  *col = (int*)std::malloc(sizeof(int) * std::max<size_t>(m, 1));
+  if (!*val || !*row || !*col) return fail(TT_ERR_NOMEM, "host allocation for P123 failed");
+  if (m) {
+    if (cudaMemcpy(*val, P.val.ptr, sizeof(double) * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(*col, P.col.ptr, sizeof(int) * m, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(TT_ERR_CUDA, "copy of P123 failed");
+  }
+  for (int r = 0; r < n; r++)
+    for (int64_t e = rowptr[r]; e < rowptr[r + 1]; e++) (*row)[e] = r;
+  *nnz = m;
+  return TT_OK;
+}
+
+int tt_calculate_resolvent_array_in_SWP_basis(tt_complex* G, double E, const tt_swp_states* swp,
+                                              const tt_pw_states* pw, const tt_run_params* rpp) {
+  if (!G || !swp || !pw || !rpp) return fail(TT_ERR_BADARG, "null argument");
+  RunParams rp = params_of(rpp);
+  SWPStates w = swp_of(swp);
+  // only the SWP energy boundaries are needed; give the layout builder
+  // identity C/V blocks of the right size
+  if (w.C_unco.empty()) w.C_unco.assign((size_t)w.Np_WP * w.Np_WP * w.n_unco, 0.0);
+  if (w.C_coup.empty()) w.C_coup.assign((size_t)4 * w.Np_WP * w.Np_WP * w.n_coup, 0.0);
+  std::vector<double> Vu(w.C_unco.size(), 0.0), Vc(w.C_coup.size(), 0.0);
+  ChannelLayout L;
+  std::string err;
+  if (!build_channel_layout(rp, view_of(pw), w, Vu, Vc, L, &err)) return fail(TT_ERR_BADARG, err);
+  cudaStream_t st = default_stream();
+  ChannelSolver cs;
+  int s = cs.setup(L, w.q_WP, st);
+  if (s != TT_OK) return s;
+  s = cs.resolvent({E}, st);
+  if (s != TT_OK) return s;
+  if (cudaMemcpy(G, cs.G(), sizeof(tt_complex) * cs.n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(TT_ERR_CUDA, "copy of G failed");
+  return TT_OK;
+}
+
+int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double* P_val, const int* P_row,
+                               const size_t* P_colptr, size_t P_nnz, const double* V_unco, const double* V_coup,
+                               const tt_swp_states* swp, const tt_os_indexing* os, const tt_pw_states* pw,
+                               const tt_run_params* rpp, tt_solve_report* report) {
+  if (!U || !G || !P_colptr || !swp || !os || !pw || !rpp) return fail(TT_ERR_BADARG, "null argument");
+  if (P_nnz && (!P_val || !P_row)) return fail(TT_ERR_BADARG, "null P123 arrays");
+  RunParams rp = params_of(rpp);
+  SWPStates w = swp_of(swp);
+  const size_t Np = w.Np_WP;
+  std::vector<double> Vu(V_unco, V_unco + Np * Np * w.n_unco);
+  std::vector<double> Vc;
+  if (w.n_coup) Vc.assign(V_coup, V_coup + 4 * Np * Np * w.n_coup);
+  ChannelLayout L;
+  std::string err;
+  const PWChannel ch = view_of(pw);
+  if (!build_channel_layout(rp, ch, w, Vu, Vc, L, &err)) return fail(TT_ERR_BADARG, err);
+  const int n = ch.Nalpha * w.Np_WP * w.Nq_WP;
+  // CSC (column pointers, row indices) -> CSR with ascending columns
+  std::vector<int64_t> rowptr(n + 1, 0);
+  for (size_t e = 0; e < P_nnz; e++) {
+    if (P_row[e] < 0 || P_row[e] >= n) return fail(TT_ERR_BADARG, "P123 row index out of range");
+    rowptr[P_row[e] + 1]++;
+  }
+  for (int r = 0; r < n; r++) rowptr[r + 1] += rowptr[r];
+  std::vector<int32_t> col(P_nnz);
+  std::vector<double> val(P_nnz);
+  std::vector<int64_t> fillpos(rowptr.begin(), rowptr.end() - 1);
+  for (int c = 0; c < n; c++)
+    for (size_t e = P_colptr[c]; e < P_colptr[c + 1]; e++) {
+      const int64_t p = fillpos[P_row[e]]++;
+      col[p] = c;
+      val[p] = P_val[e];
+    }
+  cudaStream_t st = default_stream();
+  ChannelSolver cs;
+  int s = cs.setup(L, w.q_WP, st);
+  if (s != TT_OK) return s;
+  s = cs.set_P_host_csr(rowptr.data(), col.data(), val.data(), (int64_t)P_nnz, st);
+  if (s != TT_OK) return s;
+  double msA = 0;
+  s = cs.build_A(st, &msA);
+  if (s != TT_OK) return s;
+  // G supplied by the caller: upload into the solver through resolvent-shaped storage
+  std::vector<double> dummyE(os->num_T_lab, 0.0);
+  s = cs.resolvent(dummyE, st);
+  if (s != TT_OK) return s;
+  if (cudaMemcpy((void*)cs.G(), G, sizeof(tt_complex) * (size_t)n * os->num_T_lab, cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return fail(TT_ERR_CUDA, "upload of G failed");
+  std::vector<int> q_idx(os->q_com_idx_array, os->q_com_idx_array + os->num_T_lab);
+  std::vector<int> deut(os->deuteron_idx_array, os->deuteron_idx_array + os->num_deuteron_states);
+  std::vector<double> Uh;
+  SolveReport rep;
+  if (rpp->precision < TT_PRECISION_FP64 || rpp->precision > TT_PRECISION_MIXED_SIMT)
+    return fail(TT_ERR_BADARG, "unknown precision");
+  s = cs.solve(q_idx, deut, options_of(rp, rpp->precision), Uh, &rep, st);
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  return TT_OK;
+}
+
+// ---------------------------------------------------------------------------
+int tt_run_create(tt_run** out, int nopt, const char* const* opts) {
+  if (!out) return fail(TT_ERR_BADARG, "null run pointer");
+  *out = nullptr;
+  std::unique_ptr<tt_run> r(new tt_run());
+  std::string err;
+  for (int i = 0; i < nopt; i++) {
+    const std::string a = opts[i] ? opts[i] : "";
+    const size_t eq = a.find('=');
+    if (eq == std::string::npos) return fail(TT_ERR_BADARG, "option without '=': " + a);
+    const std::string v = a.substr(eq + 1);
+    if (v.empty()) continue;  // the reference skips empty values
+    if (!set_run_parameter(r->rp, a.substr(0, eq), v, &err)) return fail(TT_ERR_BADARG, err);
+  }
+  if (!construct_pw_states(r->rp, r->pw, &err)) return fail(TT_ERR_BADARG, err);
+  if (!make_fwp_states(r->rp, r->fwp, &err)) return fail(TT_ERR_BADARG, err);
+  if (!potential_matrices(r->rp, r->fwp, r->pw, r->V_unco, r->V_coup, &err)) return fail(TT_ERR_BADARG, err);
+  if (!make_swp_states(r->rp, r->fwp, r->pw, r->V_unco, r->V_coup, r->swp, &err)) return fail(TT_ERR_BADARG, err);
+  if (!find_on_shell_bins(r->rp, r->swp, r->os, &err)) return fail(TT_ERR_BADARG, err);
+  r->chn.resize(r->pw.N_chn_3N);
+  *out = r.release();
+  return TT_OK;
+}
+
+void tt_run_destroy(tt_run* run) {
+  if (!run) return;
+  run->chn.clear();
+  if (run->stream) cudaStreamDestroy(run->stream);
+  delete run;
+}
+
+static int check_chn(const tt_run* run, int chn) {
+  if (!run) return fail(TT_ERR_BADARG, "null run");
+  if (chn < 0 || chn >= run->pw.N_chn_3N) return fail(TT_ERR_BADARG, "channel index out of range");
+  return TT_OK;
+}
+
+static cudaStream_t run_stream(tt_run* run) {
+  if (!run->stream) cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking);
+  return run->stream;
+}
+
+int tt_run_num_channels(const tt_run* run, int* n) {
+  if (!run || !n) return fail(TT_ERR_BADARG, "null argument");
+  *n = run->pw.N_chn_3N;
+  return TT_OK;
+}
+
+int tt_run_channel_info(const tt_run* run, int chn, int* Nalpha, int* dense_dim, int* two_J, int* P, int* nd) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  const PWChannel c = channel_view(run->pw, chn);
+  if (Nalpha) *Nalpha = c.Nalpha;
+  if (dense_dim) *dense_dim = c.Nalpha * run->fwp.Np_WP * run->fwp.Nq_WP;
+  if (two_J) *two_J = c.two_J_3N[0];
+  if (P) *P = c.P_3N[0];
+  if (nd) *nd = (int)deuteron_indices(c).size();
+  return TT_OK;
+}
+
+int tt_run_num_energies(const tt_run* run, int* nE) {
+  if (!run || !nE) return fail(TT_ERR_BADARG, "null argument");
+  *nE = (int)run->os.q_com_idx.size();
+  return TT_OK;
+}
+
+int tt_run_energies(const tt_run* run, double* T_lab, double* E_com, int* q_idx) {
+  if (!run) return fail(TT_ERR_BADARG, "null run");
+  for (size_t i = 0; i < run->os.q_com_idx.size(); i++) {
+    if (T_lab) T_lab[i] = run->os.T_lab[i];
+    if (E_com) E_com[i] = run->os.E_com[i];
+    if (q_idx) q_idx[i] = run->os.q_com_idx[i];
+  }
+  return TT_OK;
+}
+
+int tt_run_E_bound(const tt_run* run, double* Eb) {
+  if (!run || !Eb) return fail(TT_ERR_BADARG, "null argument");
+  *Eb = run->swp.E_bound;
+  return TT_OK;
+}
+
+static int ensure_solver(tt_run* run, int chn) {
+  ChannelState& cs = run->chn[chn];
+  if (cs.solver) return TT_OK;
+  ChannelLayout L;
+  std::string err;
+  if (!build_channel_layout(run->rp, channel_view(run->pw, chn), run->swp, run->V_unco, run->V_coup, L, &err))
+    return fail(TT_ERR_BADARG, err);
+  cs.solver.reset(new ChannelSolver());
+  return cs.solver->setup(L, run->swp.q_WP, run_stream(run));
+}
+
+int tt_run_build_P123(tt_run* run, int chn, int64_t* nnz) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  TT_TRY(ensure_solver(run, chn));
+  P123Tables t;
+  std::string err;
+  if (!p123_prepare(run->rp, run->fwp, channel_view(run->pw, chn), t, &err)) return fail(TT_ERR_BADARG, err);
+  DeviceCSR P;
+  TT_TRY(p123_build_device(t, P, run_stream(run), nullptr));
+  if (nnz) *nnz = P.nnz;
+  TT_TRY(run->chn[chn].solver->set_P_device(std::move(P)));
+  run->chn[chn].have_P = true;
+  return TT_OK;
+}
+
+int tt_run_build_A(tt_run* run, int chn, double* ms) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!run->chn[chn].have_P) TT_TRY(tt_run_build_P123(run, chn, nullptr));
+  TT_TRY(run->chn[chn].solver->build_A(run_stream(run), ms));
+  run->chn[chn].have_A = true;
+  return TT_OK;
+}
+
+int tt_run_build_resolvent(tt_run* run, int chn) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  TT_TRY(ensure_solver(run, chn));
+  std::vector<double> E;
+  for (double e : run->os.E_com) E.push_back(e + run->swp.E_bound);  // CPP/main.cpp:391
+  TT_TRY(run->chn[chn].solver->resolvent(E, run_stream(run)));
+  run->chn[chn].have_G = true;
+  return TT_OK;
+}
+
+int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_report* report) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!U) return fail(TT_ERR_BADARG, "null U");
+  if (precision < TT_PRECISION_FP64 || precision > TT_PRECISION_MIXED_SIMT) return fail(TT_ERR_BADARG, "unknown precision");
+  double msA = 0;
+  if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
+  if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));
+  const std::vector<int> deut = deuteron_indices(channel_view(run->pw, chn));
+  std::vector<double> Uh;
+  SolveReport rep;
+  s = run->chn[chn].solver->solve(run->os.q_com_idx, deut, options_of(run->rp, precision), Uh, &rep,
+                                  run_stream(run));
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  return TT_OK;
+}
+
+int tt_run_release_channel(tt_run* run, int chn) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  run->chn[chn] = ChannelState();
+  return TT_OK;
+}
+
+int tt_run_get_P123_csr(const tt_run* run, int chn, int64_t* rowptr, int32_t* col, double* val) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!run->chn[chn].have_P) return fail(TT_ERR_BADARG, "P123 not built");
+  const DeviceCSR& P = run->chn[chn].solver->P();
+  if (rowptr && cudaMemcpy(rowptr, P.rowptr.ptr, sizeof(int64_t) * (P.n + 1), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(TT_ERR_CUDA, "copy failed");
+  if (P.nnz && col && cudaMemcpy(col, P.col.ptr, sizeof(int32_t) * P.nnz, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(TT_ERR_CUDA, "copy failed");
+  if (P.nnz && val && cudaMemcpy(val, P.val.ptr, sizeof(double) * P.nnz, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(TT_ERR_CUDA, "copy failed");
+  return TT_OK;
+}
+
+int tt_run_get_A(const tt_run* run, int chn, double* A) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!run->chn[chn].have_A || !A) return fail(TT_ERR_BADARG, "A not built");
+  const size_t n = run->chn[chn].solver->n;
+  if (cudaMemcpy(A, run->chn[chn].solver->A(), sizeof(double) * n * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(TT_ERR_CUDA, "copy failed");
+  return TT_OK;
+}
+
+int tt_run_get_G(const tt_run* run, int chn, tt_complex* G) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!run->chn[chn].have_G || !G) return fail(TT_ERR_BADARG, "resolvent not built");
+  const size_t n = run->chn[chn].solver->n, nE = run->chn[chn].solver->nE();
+  if (cudaMemcpy(G, run->chn[chn].solver->G(), sizeof(tt_complex) * n * nE, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(TT_ERR_CUDA, "copy failed");
+  return TT_OK;
+}
+
+int tt_run_get_host_array(const tt_run* run, int chn, int which, void* buf, size_t* count) {
+  if (!run || !count) return fail(TT_ERR_BADARG, "null argument");
+  auto put_d = [&](const std::vector<double>& v) {
+    *count = v.size();
+    if (buf) std::memcpy(buf, v.data(), sizeof(double) * v.size());
+    return TT_OK;
+  };
+  switch (which) {
+    case 0: {
+      int s = check_chn(run, chn);
+      if (s) return s;
+      const PWChannel c = channel_view(run->pw, chn);
+      *count = (size_t)c.Nalpha * 9;
+      if (buf) {
+        int* o = (int*)buf;
+        for (int a = 0; a < c.Nalpha; a++) {
+          const int v[9] = {c.L_2N[a], c.S_2N[a], c.J_2N[a], c.T_2N[a], c.L_1N[a],
+                            c.two_J_1N[a], c.two_J_3N[a], c.two_T_3N[a], c.P_3N[a]};
+          std::memcpy(o + 9 * a, v, sizeof(v));
+        }
+      }
+      return TT_OK;
+    }
+    case 1: return put_d(run->fwp.p_WP);
+    case 2: return put_d(run->fwp.q_WP);
+    case 3: return put_d(run->V_unco);
+    case 4: return put_d(run->V_coup);
+    case 5: return put_d(run->swp.C_unco);
+    case 6: return put_d(run->swp.C_coup);
+    case 7: return put_d(run->swp.e_unco);
+    case 8: return put_d(run->swp.e_coup);
+    default: return fail(TT_ERR_BADARG, "unknown host array");
+  }
+}
+
+int tt_run_write_U_table(const tt_run* run, int chn, const tt_complex* U, const char* path) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!U || !path) return fail(TT_ERR_BADARG, "null argument");
+  const PWChannel c = channel_view(run->pw, chn);
+  const std::vector<int> deut = deuteron_indices(c);
+  const size_t nd = deut.size(), nE = run->os.q_com_idx.size();
+  std::ofstream f(path);
+  if (!f) return fail(TT_ERR_IO, std::string("cannot open ") + path);
+  // layout of store_U_matrix_elements_txt, disk_io_routines.cpp:759-913
+  f << std::setprecision(8);
+  f << "# Elastic Nd-scattering U-matrix elements in a wave-packet, Jj-scheme representation. \n# \n";
+  f << "# The calculations below were done for: \n";
+  f << "# JP:          " << c.two_J_3N[0] << "/2" << (c.P_3N[0] == 1 ? "+" : "-") << "\n";
+  f << "# Potential:   " << run->rp.potential_model << "\n";
+  f << "# Np:          " << run->fwp.Np_WP << " \n";
+  f << "# Nq:          " << run->fwp.Nq_WP << " \n";
+  f << "# Particles:   nd-scattering\n";
+  f << "# Deuteron BE: " << run->swp.E_bound << " MeV \n# \n";
+  f << "# ################################################################################################### \n";
+  f << std::right << std::scientific << std::setprecision(16);
+  const char* h1[] = {"Name", "row-idx", "col-idx", "l'", "2*j'", "l", "2*j"};
+  f << "#";
+  for (const char* h : h1) f << std::setw(10) << h;
+  f << "\n";
+  for (size_t r = 0; r < nd; r++)
+    for (size_t cc = 0; cc < nd; cc++) {
+      f << " " << std::setw(10) << ("U" + std::to_string(r) + std::to_string(cc)) << std::setw(10) << r
+        << std::setw(10) << cc << std::setw(10) << c.L_1N[deut[r]] << std::setw(10) << c.two_J_1N[deut[r]]
+        << std::setw(10) << c.L_1N[deut[cc]] << std::setw(10) << c.two_J_1N[deut[cc]] << "\n";
+    }
+  f << "# ################################################################################################### \n";
+  auto fmt = [](double v) {
+    char b[64];
+    std::snprintf(b, sizeof(b), "%+.16e", v);
+    return std::string(b);
+  };
+  for (size_t j = 0; j < nE; j++) {
+    f << " " << std::setw(24) << run->os.T_lab[j] << std::setw(24) << run->os.E_com[j] << std::setw(10)
+      << run->os.q_com_idx[j];
+    for (size_t r = 0; r < nd; r++)
+      for (size_t cc = 0; cc < nd; cc++) {
+        const tt_complex u = U[r * nd * nE + cc * nE + j];
+        f << std::setw(50) << (fmt(u.re) + fmt(u.im) + "j");
+      }
+    f << "\n";
+  }
+  f << "# ################################################################################################### \n";
+  f << std::endl;
+  return TT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,384 @@
+// Kernels of the Faddeev-solve stage other than the LU factorisation:
+// resolvent diagonals, the dense kernel matrix A = C^T (2 P123) (V C),
+// L = 1 - A diag(G), right-hand sides and the FP64 refinement residual.
+#include <cmath>
+#include <cstring>
+
+#include "tt_kernels.h"
+
+namespace tt {
+
+constexpr double kMp_d = 938.272;
+constexpr double kMn_d = 939.565;
+
+int DeviceLayout::upload(const ChannelLayout& L, const std::vector<double>& qwp, cudaStream_t st) {
+  Nalpha = L.Nalpha;
+  Np = L.Np;
+  Nq = L.Nq;
+  n = L.Nalpha * L.Np * L.Nq;
+  TT_TRY(blk.upload(L.blk, st));
+  TT_TRY(part.upload(L.part, st));
+  TT_TRY(dim.upload(L.dim, st));
+  TT_TRY(cpl_off.upload(L.cpl_off, st));
+  TT_TRY(cpl.upload(L.cpl, st));
+  TT_TRY(blk_off.upload(L.blk_off, st));
+  TT_TRY(blk_dim.upload(L.blk_dim, st));
+  TT_TRY(C.upload(L.C, st));
+  TT_TRY(VC.upload(L.VC, st));
+  TT_TRY(e_off.upload(L.e_off, st));
+  TT_TRY(e_swp.upload(L.e_swp, st));
+  TT_TRY(q_WP.upload(qwp, st));
+  return TT_OK;
+}
+
+namespace {
+
+__device__ __forceinline__ double heaviside(double v) { return v < 0 ? 0.0 : 1.0; }
+
+// make_resolvent.cpp:14-80 (bound-continuum and continuum-continuum terms)
+__global__ void k_resolvent(int Na, int Nq, int Np, const int32_t* __restrict__ e_off,
+                            const double* __restrict__ e_swp, const double* __restrict__ qwp,
+                            const double* __restrict__ E, int nE, double2* __restrict__ G) {
+  const int n = Na * Nq * Np;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (size_t)n * nE) return;
+  const int j = (int)(tid / n), idx = (int)(tid % n);
+  const int a = idx / (Nq * Np), q = (idx / Np) % Nq, p = idx % Np;
+  const double e_lo = e_swp[e_off[a] + p], e_hi = e_swp[e_off[a] + p + 1];
+  const double q_lo = qwp[q], q_hi = qwp[q + 1];
+  const double En = E[j];
+  double re, im;
+  if (e_lo < 0) {
+    const double Eb = e_lo;
+    const double mu1 = kMn_d * (kMn_d + kMp_d + Eb) / (kMn_d + kMn_d + kMp_d + Eb);
+    const double Eq_lo = q_lo * q_lo / (2 * mu1), Eq_hi = q_hi * q_hi / (2 * mu1);
+    const double Dq = Eq_hi - Eq_lo;
+    re = log(fabs((Eq_lo + Eb - En) / (Eq_hi + Eb - En))) / (Dq);
+    im = (heaviside(Eq_hi + Eb - En) - heaviside(Eq_lo + Eb - En)) * (-M_PI) / (Dq);
+  } else {
+    const double Eb = 0;
+    const double mu1 = kMn_d * (kMn_d + kMp_d + Eb) / (kMn_d + kMn_d + kMp_d + Eb);
+    const double Eq_lo = q_lo * q_lo / (2 * mu1), Eq_hi = q_hi * q_hi / (2 * mu1);
+    const double Ep = 0.5 * (e_lo + e_hi), Eq = 0.5 * (Eq_lo + Eq_hi);
+    const double Dq = Eq_hi - Eq_lo, Dp = e_hi - e_lo;
+    const double DM = 0.5 * (Dp - Dq), DP = 0.5 * (Dp + Dq), D = Ep + Eq - En;
+    re = ((D + DM) * log(fabs(D + DM)) + (D - DM) * log(fabs(D - DM)) - (D + DP) * log(fabs(D + DP)) -
+          (D - DP) * log(fabs(D - DP))) /
+         (Dp * Dq);
+    im = ((D + DM) * heaviside(D + DM) + (D - DM) * heaviside(D - DM) - (D + DP) * heaviside(D + DP) -
+          (D - DP) * heaviside(D - DP)) *
+         M_PI / (Dp * Dq);
+  }
+  G[tid] = make_double2(re, im);
+}
+
+__device__ __forceinline__ int64_t lower_bound_col(const int32_t* __restrict__ col, int64_t lo, int64_t hi,
+                                                   int32_t key) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (col[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// B = 2 P123 (V C)_big, one warp per (row r, alpha_c); calculate_PVC_col
+// (solve_faddeev.cpp:4-48) restated row-wise.  B must be zeroed.
+__global__ void k_pvc(int Na, int Nq, int Np, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                      const double* __restrict__ val, const int32_t* __restrict__ blk,
+                      const int32_t* __restrict__ part, const int32_t* __restrict__ cpl_off,
+                      const int32_t* __restrict__ cpl, const int64_t* __restrict__ blk_off,
+                      const int32_t* __restrict__ blk_dim, const double* __restrict__ VC, double* __restrict__ B) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int n = Na * Nq * Np;
+  if (warp >= (int64_t)n * Na) return;
+  const int r = (int)(warp / Na), ac = (int)(warp % Na);
+  const int NqNp = Nq * Np;
+  const int64_t r_lo = rowptr[r], r_hi = rowptr[r + 1];
+  if (r_lo == r_hi) return;
+  const int b = blk[ac];
+  const int dimb = blk_dim[b];
+  const double* VCb = VC + blk_off[b];
+  const int part_c = part[ac];
+  double* Brow = B + (size_t)r * n + (size_t)ac * NqNp;
+  for (int t = cpl_off[ac]; t < cpl_off[ac + 1]; t++) {
+    const int aj = cpl[t];
+    const int part_j = part[aj];
+    const int64_t lo = lower_bound_col(col, r_lo, r_hi, aj * NqNp);
+    const int64_t hi = lower_bound_col(col, lo, r_hi, (aj + 1) * NqNp);
+    for (int pc0 = 0; pc0 < Np; pc0 += 32) {
+      const int pc = pc0 + lane;
+      double acc = 0.0;
+      int cur_q = -1;
+      for (int64_t e = lo; e < hi; e++) {
+        const int cj = col[e] - aj * NqNp;
+        const int q = cj / Np, pj = cj % Np;
+        if (q != cur_q) {
+          if (cur_q >= 0 && pc < Np) Brow[cur_q * Np + pc] += acc;
+          acc = 0.0;
+          cur_q = q;
+        }
+        if (pc < Np) acc += (2 * val[e]) * VCb[(size_t)(part_j * Np + pj) * dimb + part_c * Np + pc];
+      }
+      if (cur_q >= 0 && pc < Np) Brow[cur_q * Np + pc] += acc;
+    }
+  }
+}
+
+// A = C^T_big B: block (alpha_r, q) x 128 columns; calculate_CPVC_col
+// (solve_faddeev.cpp:50-181) restated as small dense products.
+template <int MAXH>
+__global__ void __launch_bounds__(256) k_ct(int Na, int Nq, int Np, const int32_t* __restrict__ blk,
+                                            const int32_t* __restrict__ part, const int32_t* __restrict__ cpl_off,
+                                            const int32_t* __restrict__ cpl, const int64_t* __restrict__ blk_off,
+                                            const int32_t* __restrict__ blk_dim, const double* __restrict__ Cm,
+                                            const double* __restrict__ B, double* __restrict__ A) {
+  extern __shared__ double sCt[];  // [ncpl][Np][Np]: Ct[pr][pi]
+  const int n = Na * Nq * Np;
+  const int ar = blockIdx.y / Nq, q = blockIdx.y % Nq;
+  const int c = blockIdx.x * 128 + (threadIdx.x & 127);
+  const int half = threadIdx.x >> 7;
+  const int b = blk[ar];
+  const int dimb = blk_dim[b];
+  const double* Cb = Cm + blk_off[b];
+  const int part_r = part[ar];
+  const int t0 = cpl_off[ar], t1 = cpl_off[ar + 1];
+  const int ncpl = t1 - t0;
+  for (int i = threadIdx.x; i < ncpl * Np * Np; i += blockDim.x) {
+    const int t = i / (Np * Np), pr = (i / Np) % Np, pi = i % Np;
+    const int ai = cpl[t0 + t];
+    // Ct(alpha_r, alpha_i)(pr, pi) = C[(part_i, pi), (part_r, pr)]
+    sCt[i] = Cb[(size_t)(part[ai] * Np + pi) * dimb + part_r * Np + pr];
+  }
+  __syncthreads();
+  if (c >= n) return;
+  double acc[MAXH];
+#pragma unroll
+  for (int h = 0; h < MAXH; h++) acc[h] = 0.0;
+  for (int t = 0; t < ncpl; t++) {
+    const int ai = cpl[t0 + t];
+    const double* Bcol = B + ((size_t)ai * Nq * Np + (size_t)q * Np) * n + c;
+    const double* Ct = sCt + t * Np * Np;
+    for (int pi = 0; pi < Np; pi++) {
+      const double bv = Bcol[(size_t)pi * n];
+#pragma unroll
+      for (int h = 0; h < MAXH; h++) {
+        const int pr = 2 * h + half;
+        if (pr < Np) acc[h] += Ct[pr * Np + pi] * bv;
+      }
+    }
+  }
+  double* Acol = A + ((size_t)ar * Nq * Np + (size_t)q * Np) * n + c;
+#pragma unroll
+  for (int h = 0; h < MAXH; h++) {
+    const int pr = 2 * h + half;
+    if (pr < Np) Acol[(size_t)pr * n] = acc[h];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T make_c(double re, double im);
+template <>
+__device__ __forceinline__ double2 make_c<double2>(double re, double im) { return make_double2(re, im); }
+template <>
+__device__ __forceinline__ float2 make_c<float2>(double re, double im) {
+  return make_float2((float)re, (float)im);
+}
+
+template <typename T>
+__global__ void k_form_L(const double* __restrict__ A, const double2* __restrict__ G, int n, T* __restrict__ L) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (size_t)n * n) return;
+  const int i = (int)(tid / n), c = (int)(tid % n);
+  const double a = A[tid];
+  const double2 g = G[c];
+  L[tid] = make_c<T>((i == c ? 1.0 : 0.0) - a * g.x, -a * g.y);
+}
+
+__global__ void k_gather_rhs(const double* __restrict__ A, int n, const int32_t* __restrict__ cols, int nrhs,
+                             double2* __restrict__ b) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (size_t)n * nrhs) return;
+  const int k = (int)(tid / n), i = (int)(tid % n);
+  b[tid] = make_double2(A[(size_t)i * n + cols[k]], 0.0);
+}
+
+// r_k = b_k - x_k + A y_k, y_k = G o x_k; warp per row, up to 8 rhs per pass.
+constexpr int RES_MAXR = 8;
+__global__ void k_residual(const double* __restrict__ A, int n, const double2* __restrict__ y,
+                           const double2* __restrict__ b, const double2* __restrict__ x, int nrhs,
+                           double2* __restrict__ r) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = (int)warp;
+  const double* Ar = A + (size_t)i * n;
+  for (int k0 = 0; k0 < nrhs; k0 += RES_MAXR) {
+    const int kn = min(RES_MAXR, nrhs - k0);
+    double sr[RES_MAXR], si[RES_MAXR];
+#pragma unroll
+    for (int k = 0; k < RES_MAXR; k++) sr[k] = si[k] = 0.0;
+    for (int c = lane; c < n; c += 32) {
+      const double a = Ar[c];
+#pragma unroll
+      for (int k = 0; k < RES_MAXR; k++) {
+        if (k < kn) {
+          const double2 yv = y[(size_t)(k0 + k) * n + c];
+          sr[k] += a * yv.x;
+          si[k] += a * yv.y;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < RES_MAXR; k++) {
+      for (int o = 16; o > 0; o >>= 1) {
+        sr[k] += __shfl_down_sync(0xffffffffu, sr[k], o);
+        si[k] += __shfl_down_sync(0xffffffffu, si[k], o);
+      }
+    }
+    if (lane == 0) {
+      for (int k = 0; k < kn; k++) {
+        const size_t o = (size_t)(k0 + k) * n + i;
+        r[o] = make_double2(b[o].x - x[o].x + sr[k], b[o].y - x[o].y + si[k]);
+      }
+    }
+  }
+}
+
+__global__ void k_hadamard(const double2* __restrict__ G, const int32_t* __restrict__ rhs_e, int n,
+                           const double2* __restrict__ x, int nrhs, double2* __restrict__ y) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (size_t)n * nrhs) return;
+  const int k = (int)(tid / n), c = (int)(tid % n);
+  const double2 g = G[(size_t)rhs_e[k] * n + c];
+  const double2 v = x[tid];
+  y[tid] = make_double2(g.x * v.x - g.y * v.y, g.x * v.y + g.y * v.x);
+}
+
+__global__ void k_axpy_norm(double2* __restrict__ x, const double2* __restrict__ d, int n, int nrhs,
+                            unsigned long long* __restrict__ dmax, unsigned long long* __restrict__ xmax) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double ad = 0.0, ax = 0.0;
+  int k = 0;
+  if (tid < (size_t)n * nrhs) {
+    k = (int)(tid / n);
+    const double2 dv = d[tid];
+    double2 xv = x[tid];
+    xv.x += dv.x;
+    xv.y += dv.y;
+    x[tid] = xv;
+    ad = fmax(fabs(dv.x), fabs(dv.y));
+    ax = fmax(fabs(xv.x), fabs(xv.y));
+  }
+  if (tid < (size_t)n * nrhs) {
+    // non-negative doubles order like their bit patterns
+    atomicMax(&dmax[k], (unsigned long long)__double_as_longlong(ad));
+    atomicMax(&xmax[k], (unsigned long long)__double_as_longlong(ax));
+  }
+}
+
+}  // namespace
+
+int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d_G, cudaStream_t st) {
+  const size_t total = (size_t)L.n * nE;
+  if (total == 0) return TT_OK;
+  k_resolvent<<<ceil_div(total, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, L.e_off.ptr, L.e_swp.ptr, L.q_WP.ptr, d_E,
+                                                    nE, reinterpret_cast<double2*>(d_G));
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, double* d_A, cudaStream_t st) {
+  const int n = L.n;
+  if (L.Np > 64) {
+    set_error("Np_WP > 64 is not supported by the A-build kernel");
+    return TT_ERR_UNSUPPORTED;
+  }
+  TT_CUDA_TRY(cudaMemsetAsync(d_B, 0, sizeof(double) * (size_t)n * n, st));
+  if (P.nnz > 0) {
+    const size_t warps = (size_t)n * L.Nalpha;
+    k_pvc<<<ceil_div(warps * 32, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
+                                                     L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr, L.blk_off.ptr,
+                                                     L.blk_dim.ptr, L.VC.ptr, d_B);
+    TT_CUDA_TRY(cudaGetLastError());
+  }
+  int max_cpl = 1;
+  // the coupling lists hold at most 2 partners per alpha for the 2N structure;
+  // shared memory is sized for 2 Np x Np blocks
+  const size_t smem = (size_t)2 * L.Np * L.Np * sizeof(double);
+  (void)max_cpl;
+  dim3 grid(ceil_div(n, 128), L.Nalpha * L.Nq);
+  if (smem > 48 * 1024) TT_CUDA_TRY(cudaFuncSetAttribute(k_ct<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_ct<32><<<grid, 256, smem, st>>>(L.Nalpha, L.Nq, L.Np, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
+                                    L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, d_B, d_A);
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+template <typename T>
+int form_L_device(const double* d_A, const double* d_G, int n, T* d_L, cudaStream_t st) {
+  const size_t total = (size_t)n * n;
+  k_form_L<T><<<ceil_div(total, 256), 256, 0, st>>>(d_A, reinterpret_cast<const double2*>(d_G), n, d_L);
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+template int form_L_device<double2>(const double*, const double*, int, double2*, cudaStream_t);
+template int form_L_device<float2>(const double*, const double*, int, float2*, cudaStream_t);
+
+int gather_rhs_device(const double* d_A, int n, const int32_t* d_cols, int nrhs, double* d_b, cudaStream_t st) {
+  k_gather_rhs<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(d_A, n, d_cols, nrhs, reinterpret_cast<double2*>(d_b));
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int hadamard_device(const double* d_G, const int32_t* d_rhs_e, int n, const double* d_x, int nrhs, double* d_y,
+                    cudaStream_t st) {
+  k_hadamard<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_G), d_rhs_e, n,
+                                                             reinterpret_cast<const double2*>(d_x), nrhs,
+                                                             reinterpret_cast<double2*>(d_y));
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int residual_multi_device(const double* d_A, int n, const double* d_y, const double* d_b, const double* d_x, int nrhs,
+                          double* d_r, cudaStream_t st) {
+  k_residual<<<ceil_div((size_t)n * 32, 256), 256, 0, st>>>(
+      d_A, n, reinterpret_cast<const double2*>(d_y), reinterpret_cast<const double2*>(d_b),
+      reinterpret_cast<const double2*>(d_x), nrhs, reinterpret_cast<double2*>(d_r));
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_ratio, cudaStream_t st) {
+  DevBuf<unsigned long long> mx;
+  TT_TRY(mx.alloc(2 * (size_t)nrhs));
+  TT_CUDA_TRY(cudaMemsetAsync(mx.ptr, 0, sizeof(unsigned long long) * 2 * nrhs, st));
+  k_axpy_norm<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<double2*>(d_x),
+                                                              reinterpret_cast<const double2*>(d_d), n, nrhs, mx.ptr,
+                                                              mx.ptr + nrhs);
+  TT_CUDA_TRY(cudaGetLastError());
+  std::vector<unsigned long long> h(2 * (size_t)nrhs);
+  TT_CUDA_TRY(cudaMemcpyAsync(h.data(), mx.ptr, sizeof(unsigned long long) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
+  TT_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int k = 0; k < nrhs; k++) {
+    double dm, xm;
+    memcpy(&dm, &h[k], 8);
+    memcpy(&xm, &h[nrhs + k], 8);
+    h_ratio[k] = xm > 0 ? dm / xm : dm;
+  }
+  return TT_OK;
+}
+
+int device_sm_count() {
+  static int sms = -1;
+  if (sms < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+}  // namespace tt

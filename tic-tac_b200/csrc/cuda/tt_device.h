@@ -1,0 +1,85 @@
+// Shared device-side utilities: error propagation, RAII device buffers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "tictac_b200.h"  // status codes
+
+namespace tt {
+
+void set_error(const std::string& msg);
+const char* last_error();
+
+#define TT_CUDA_TRY(expr)                                                                   \
+  do {                                                                                      \
+    cudaError_t _e = (expr);                                                                \
+    if (_e != cudaSuccess) {                                                                \
+      ::tt::set_error(std::string(#expr) + " failed: " + cudaGetErrorString(_e) + " at " + \
+                      __FILE__ + ":" + std::to_string(__LINE__));                           \
+      return (_e == cudaErrorMemoryAllocation) ? TT_ERR_NOMEM : TT_ERR_CUDA;   \
+    }                                                                                       \
+  } while (0)
+
+#define TT_TRY(expr)                 \
+  do {                               \
+    int _s = (expr);                 \
+    if (_s != TT_OK) return _s; \
+  } while (0)
+
+// Owning device buffer.  alloc() reports NOMEM through the status path instead
+// of faulting.
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count) { o.ptr = nullptr; o.count = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); ptr = o.ptr; count = o.count; o.ptr = nullptr; o.count = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  int alloc(size_t n) {
+    release();
+    if (n == 0) return TT_OK;
+    cudaError_t e = cudaMalloc((void**)&ptr, n * sizeof(T));
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      cudaGetLastError();
+      set_error("device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed: " +
+                cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? TT_ERR_NOMEM : TT_ERR_CUDA;
+    }
+    count = n;
+    return TT_OK;
+  }
+  int upload(const T* h, size_t n, cudaStream_t s) {
+    TT_TRY(alloc(n));
+    if (n) TT_CUDA_TRY(cudaMemcpyAsync(ptr, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    return TT_OK;
+  }
+  int upload(const std::vector<T>& v, cudaStream_t s) { return upload(v.data(), v.size(), s); }
+};
+
+// Device CSR matrix (rows sorted, columns ascending within a row).
+struct DeviceCSR {
+  int n = 0;
+  int64_t nnz = 0;
+  DevBuf<int64_t> rowptr;
+  DevBuf<int32_t> col;
+  DevBuf<double> val;
+};
+
+inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace tt

@@ -1,0 +1,82 @@
+// Device stages of the WPCD path (host-callable launchers).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "tt_device.h"
+
+namespace tt {
+
+struct P123Tables;
+
+struct P123Stats {
+  int64_t n_cells = 0;
+  int64_t n_pairs = 0;
+};
+
+// P123 of one channel in CSR on the device (p123.cu).
+int p123_build_device(const P123Tables& t, DeviceCSR& out, cudaStream_t st, P123Stats* stats);
+
+// Per-channel description of the 2N structure used by the resolvent and the
+// A = C^T (2 P123) (V C) build (host-prepared, see tt_solve_prep.cpp).
+struct ChannelLayout {
+  int Nalpha = 0, Np = 0, Nq = 0;
+  // per alpha: index of its 2N block, its part (0 = L=J-1 / T3=1/2, 1 = L=J+1 / T3=3/2), block dim (Np or 2Np)
+  std::vector<int32_t> blk, part, dim;
+  // per alpha: partners alpha' coupled through the 2N interaction (CSR)
+  std::vector<int32_t> cpl_off, cpl;
+  // per 2N block: offset (in doubles) into the C and VC arrays; dim
+  std::vector<int64_t> blk_off;
+  std::vector<int32_t> blk_dim;
+  std::vector<double> C, VC;  // row-major blocks, VC = V.C
+  // per alpha: offset into e_swp (Np+1 boundaries of its SWP energies)
+  std::vector<int32_t> e_off;
+  std::vector<double> e_swp;
+};
+
+struct DeviceLayout {
+  int Nalpha = 0, Np = 0, Nq = 0, n = 0;
+  DevBuf<int32_t> blk, part, dim, cpl_off, cpl, blk_dim, e_off;
+  DevBuf<int64_t> blk_off;
+  DevBuf<double> C, VC, e_swp;
+  DevBuf<double> q_WP;
+  int upload(const ChannelLayout& L, const std::vector<double>& q_WP, cudaStream_t st);
+};
+
+// G[j*n + i] (complex128 interleaved) for energies E[j]; make_resolvent.cpp:82-211.
+int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d_G, cudaStream_t st);
+
+// Dense A (n x n, row-major FP64) = C^T (2 P123) (V C); solve_faddeev.cpp:4-181.
+// d_B is an n x n FP64 scratch of the product 2 P123 (V C).
+int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, double* d_A, cudaStream_t st);
+
+// L = 1 - A diag(G), complex, row-major; T = double2 (complex128) or float2 (complex64).
+template <typename T>
+int form_L_device(const double* d_A, const double* d_G, int n, T* d_L, cudaStream_t st);
+
+// RHS columns b_k = A[:, cols[k]] as complex128, stored column-by-column [k][n].
+int gather_rhs_device(const double* d_A, int n, const int32_t* d_cols, int nrhs, double* d_b, cudaStream_t st);
+
+// y_k = G_{e(k)} o x_k (complex128) for nrhs right-hand sides, G stored [nE][n].
+int hadamard_device(const double* d_G, const int32_t* d_rhs_e, int n, const double* d_x, int nrhs, double* d_y,
+                    cudaStream_t st);
+// r_k = b_k - x_k + A y_k: the FP64 residual of (1 - A G) x = b, one read of A for all rhs.
+int residual_multi_device(const double* d_A, int n, const double* d_y, const double* d_b, const double* d_x, int nrhs,
+                          double* d_r, cudaStream_t st);
+
+// LU with partial pivoting, in place, row-major (lu.cu).  ipiv[k] = row swapped with k.
+template <typename T>
+int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_tensor_cores, int* info);
+// Solve L U x = P b for nrhs complex128 columns [k][n] in place using the factor of type T.
+template <typename T>
+int lu_solve_device(const T* d_LU, int n, const int32_t* d_ipiv, double* d_x, int nrhs, cudaStream_t st);
+
+// x += d ; returns max |d| / max |x| per rhs in h_ratio (host, synchronises).
+int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_dx_over_x, cudaStream_t st);
+
+// Device count of SMs, cached.
+int device_sm_count();
+
+}  // namespace tt

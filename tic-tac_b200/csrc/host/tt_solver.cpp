@@ -1,0 +1,275 @@
+// Host orchestration of the per-channel Faddeev solve.  See tt_solver.h.
+#include "tt_solver.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <map>
+
+namespace tt {
+
+namespace {
+
+struct AlphaBlock {
+  bool coupled;
+  int chn;
+  int part;
+};
+
+// 2N block and part of one partial wave (make_resolvent.cpp:118-156).
+bool alpha_block(const RunParams& rp, const PWChannel& ch, int a, AlphaBlock& out, std::string* err) {
+  const int L = ch.L_2N[a], S = ch.S_2N[a], J = ch.J_2N[a], T = ch.T_2N[a];
+  const bool state_1S0 = (S == 0 && J == 0 && L == 0);
+  const bool via_L = (rp.tensor_force && L != J && J != 0);
+  const bool via_T = (state_1S0 && rp.isospin_breaking_1S0);
+  if (via_L && via_T) {
+    if (err) *err = "isospin-breaking in coupled channels is not supported";
+    return false;
+  }
+  out.coupled = via_L || via_T;
+  out.chn = unique_2N_idx(L, S, J, T, out.coupled, rp);
+  if (via_L) out.part = (L < J) ? 0 : 1;
+  else if (via_T) out.part = (ch.two_T_3N[a] == 1) ? 0 : 1;
+  else out.part = 0;
+  return true;
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+bool build_channel_layout(const RunParams& rp, const PWChannel& ch, const SWPStates& swp,
+                          const std::vector<double>& V_unco, const std::vector<double>& V_coup, ChannelLayout& L,
+                          std::string* err) {
+  const int Na = ch.Nalpha, Np = swp.Np_WP;
+  L = ChannelLayout();
+  L.Nalpha = Na;
+  L.Np = Np;
+  L.Nq = swp.Nq_WP;
+  L.e_swp = swp.e_unco;
+  L.e_swp.insert(L.e_swp.end(), swp.e_coup.begin(), swp.e_coup.end());
+  const int e_coup_base = (int)swp.e_unco.size();
+  std::map<std::pair<int, int>, int> blocks;  // (coupled, chn) -> block index
+  for (int a = 0; a < Na; a++) {
+    AlphaBlock ab;
+    if (!alpha_block(rp, ch, a, ab, err)) return false;
+    const auto key = std::make_pair(ab.coupled ? 1 : 0, ab.chn);
+    auto it = blocks.find(key);
+    int b;
+    if (it == blocks.end()) {
+      b = (int)L.blk_dim.size();
+      blocks[key] = b;
+      const int dim = ab.coupled ? 2 * Np : Np;
+      const double* Cs = ab.coupled ? &swp.C_coup[(size_t)ab.chn * dim * dim] : &swp.C_unco[(size_t)ab.chn * dim * dim];
+      const double* Vs = ab.coupled ? &V_coup[(size_t)ab.chn * dim * dim] : &V_unco[(size_t)ab.chn * dim * dim];
+      L.blk_dim.push_back(dim);
+      L.blk_off.push_back((int64_t)L.C.size());
+      L.C.insert(L.C.end(), Cs, Cs + (size_t)dim * dim);
+      // VC = V . C (row-major), the dot_MM products of solve_faddeev.cpp:1818-1846
+      std::vector<double> vc((size_t)dim * dim, 0.0);
+      for (int i = 0; i < dim; i++)
+        for (int k = 0; k < dim; k++) {
+          const double v = Vs[(size_t)i * dim + k];
+          if (v == 0.0) continue;
+          for (int j = 0; j < dim; j++) vc[(size_t)i * dim + j] += v * Cs[(size_t)k * dim + j];
+        }
+      L.VC.insert(L.VC.end(), vc.begin(), vc.end());
+    } else {
+      b = it->second;
+    }
+    L.blk.push_back(b);
+    L.part.push_back(ab.part);
+    L.dim.push_back(L.blk_dim[b]);
+    L.e_off.push_back(ab.coupled ? e_coup_base + ab.chn * 2 * (Np + 1) + ab.part * (Np + 1) : ab.chn * (Np + 1));
+  }
+  // coupling partners (non-NULL entries of the C^T / VC pointer tables,
+  // solve_faddeev.cpp:1690-1699)
+  L.cpl_off.push_back(0);
+  for (int r = 0; r < Na; r++) {
+    int cnt = 0;
+    for (int c = 0; c < Na; c++) {
+      const bool check_T = ch.T_2N[r] == ch.T_2N[c];
+      const bool check_J = ch.J_2N[r] == ch.J_2N[c];
+      const bool check_S = ch.S_2N[r] == ch.S_2N[c];
+      const bool check_L = (rp.tensor_force && std::abs(ch.L_2N[r] - ch.L_2N[c]) <= 2) || ch.L_2N[r] == ch.L_2N[c];
+      const bool check_l = ch.L_1N[r] == ch.L_1N[c];
+      const bool check_j = ch.two_J_1N[r] == ch.two_J_1N[c];
+      if (check_T && check_J && check_S && check_L && check_l && check_j) {
+        if (L.blk[r] != L.blk[c]) {
+          if (err) *err = "inconsistent 2N block structure between coupled partial waves";
+          return false;
+        }
+        L.cpl.push_back(c);
+        cnt++;
+      }
+    }
+    if (cnt > 2) {
+      if (err) *err = "more than two coupled partial waves per 2N block";
+      return false;
+    }
+    L.cpl_off.push_back((int32_t)L.cpl.size());
+  }
+  return true;
+}
+
+int ChannelSolver::setup(const ChannelLayout& L, const std::vector<double>& q_WP, cudaStream_t st) {
+  n = L.Nalpha * L.Np * L.Nq;
+  return L_.upload(L, q_WP, st);
+}
+
+int ChannelSolver::set_P_device(DeviceCSR&& P) {
+  if (P.n != n) {
+    set_error("P123 dimension does not match the channel");
+    return TT_ERR_BADARG;
+  }
+  P_ = std::move(P);
+  return TT_OK;
+}
+
+int ChannelSolver::set_P_host_csr(const int64_t* rowptr, const int32_t* col, const double* val, int64_t nnz,
+                                  cudaStream_t st) {
+  P_.n = n;
+  P_.nnz = nnz;
+  TT_TRY(P_.rowptr.upload(rowptr, (size_t)n + 1, st));
+  TT_TRY(P_.col.upload(col, (size_t)std::max<int64_t>(nnz, 0), st));
+  TT_TRY(P_.val.upload(val, (size_t)std::max<int64_t>(nnz, 0), st));
+  return TT_OK;
+}
+
+int ChannelSolver::build_A(cudaStream_t st, double* ms) {
+  auto t0 = std::chrono::steady_clock::now();
+  TT_TRY(A_.alloc((size_t)n * n));
+  DevBuf<double> B;
+  TT_TRY(B.alloc((size_t)n * n));
+  TT_TRY(build_A_device(L_, P_, B.ptr, A_.ptr, st));
+  TT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (ms) *ms = ms_since(t0);
+  return TT_OK;
+}
+
+int ChannelSolver::resolvent(const std::vector<double>& E, cudaStream_t st) {
+  nE_ = (int)E.size();
+  DevBuf<double> dE;
+  TT_TRY(dE.upload(E, st));
+  TT_TRY(G_.alloc((size_t)2 * n * std::max(1, nE_)));
+  TT_TRY(resolvent_device(L_, dE.ptr, nE_, G_.ptr, st));
+  TT_CUDA_TRY(cudaStreamSynchronize(st));
+  return TT_OK;
+}
+
+int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
+                         std::vector<double>& U, SolveReport* rep, cudaStream_t st) {
+  const int nE = (int)q_idx.size(), nd = (int)deut.size();
+  if (nE != nE_) {
+    set_error("number of on-shell bins does not match the resolvent energies");
+    return TT_ERR_BADARG;
+  }
+  if (!A_.ptr) {
+    set_error("A has not been built");
+    return TT_ERR_BADARG;
+  }
+  U.assign((size_t)2 * nd * nd * nE, 0.0);
+  SolveReport r;
+  if (nd == 0 || nE == 0) {
+    if (rep) *rep = r;
+    return TT_OK;
+  }
+  const int Nq = L_.Nq, Np = L_.Np;
+  DevBuf<int32_t> ipiv, cols, rhs_e;
+  TT_TRY(ipiv.alloc(n));
+  DevBuf<double> b, x, y, res, d;
+  TT_TRY(b.alloc((size_t)2 * n * nd));
+  TT_TRY(x.alloc((size_t)2 * n * nd));
+  DevBuf<double2> L64;
+  DevBuf<float2> L32;
+  if (opt.mixed) {
+    TT_TRY(L32.alloc((size_t)n * n));
+    TT_TRY(y.alloc((size_t)2 * n * nd));
+    TT_TRY(res.alloc((size_t)2 * n * nd));
+  } else {
+    TT_TRY(L64.alloc((size_t)n * n));
+  }
+  for (int j = 0; j < nE; j++) {
+    std::vector<int32_t> hc(nd), he(nd, 0);
+    for (int k = 0; k < nd; k++) hc[k] = deut[k] * Nq * Np + q_idx[j] * Np + 0;
+    TT_TRY(cols.upload(hc, st));
+    TT_TRY(rhs_e.upload(he, st));
+    const double* Gj = G_.ptr + (size_t)2 * n * j;
+    auto t0 = std::chrono::steady_clock::now();
+    int info = 0;
+    if (opt.mixed) {
+      TT_TRY(form_L_device<float2>(A_.ptr, Gj, n, L32.ptr, st));
+      TT_CUDA_TRY(cudaStreamSynchronize(st));
+      r.ms_form += ms_since(t0);
+      t0 = std::chrono::steady_clock::now();
+      TT_TRY(lu_factor_device<float2>(L32.ptr, n, ipiv.ptr, st, opt.tensor_cores ? 1 : 0, &info));
+      r.ms_factor += ms_since(t0);
+    } else {
+      TT_TRY(form_L_device<double2>(A_.ptr, Gj, n, L64.ptr, st));
+      TT_CUDA_TRY(cudaStreamSynchronize(st));
+      r.ms_form += ms_since(t0);
+      t0 = std::chrono::steady_clock::now();
+      TT_TRY(lu_factor_device<double2>(L64.ptr, n, ipiv.ptr, st, 0, &info));
+      r.ms_factor += ms_since(t0);
+    }
+    if (info != 0) {
+      r.info = info;
+      set_error("zero pivot at column " + std::to_string(info) + " of the Faddeev kernel matrix");
+      if (rep) *rep = r;
+      return TT_ERR_SINGULAR;
+    }
+    t0 = std::chrono::steady_clock::now();
+    TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nd, b.ptr, st));
+    TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * 2 * n * nd, cudaMemcpyDeviceToDevice, st));
+    if (opt.mixed) TT_TRY(lu_solve_device<float2>(L32.ptr, n, ipiv.ptr, x.ptr, nd, st));
+    else TT_TRY(lu_solve_device<double2>(L64.ptr, n, ipiv.ptr, x.ptr, nd, st));
+    TT_CUDA_TRY(cudaStreamSynchronize(st));
+    r.ms_solve += ms_since(t0);
+    if (opt.mixed) {
+      // FP64 iterative refinement: r = b - (x - A (G o x)), L d = r, x += d
+      t0 = std::chrono::steady_clock::now();
+      bool converged = false;
+      int it = 0;
+      double worst = 0;
+      std::vector<double> ratio(nd);
+      for (it = 1; it <= opt.refine_max_iter; it++) {
+        TT_TRY(hadamard_device(Gj, rhs_e.ptr, n, x.ptr, nd, y.ptr, st));
+        TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nd, res.ptr, st));
+        TT_TRY(lu_solve_device<float2>(L32.ptr, n, ipiv.ptr, res.ptr, nd, st));
+        TT_TRY(axpy_norms_device(x.ptr, res.ptr, n, nd, ratio.data(), st));
+        worst = 0;
+        for (double v : ratio) worst = std::max(worst, v);
+        if (!(worst == worst)) break;  // NaN
+        if (worst <= opt.refine_tol) {
+          converged = true;
+          break;
+        }
+      }
+      r.ms_refine += ms_since(t0);
+      r.refine_iters = std::max(r.refine_iters, std::min(it, opt.refine_max_iter));
+      r.final_correction = std::max(r.final_correction, worst);
+      if (!converged) {
+        set_error("iterative refinement did not converge (last |dx|/|x| = " + std::to_string(worst) + ")");
+        if (rep) *rep = r;
+        return TT_ERR_NOCONVERGE;
+      }
+    }
+    // on-shell read-out, solve_faddeev.cpp:407-431
+    std::vector<double> hx((size_t)2 * n * nd);
+    TT_CUDA_TRY(cudaMemcpyAsync(hx.data(), x.ptr, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st));
+    TT_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int dr = 0; dr < nd; dr++)
+      for (int dc = 0; dc < nd; dc++) {
+        const size_t row = (size_t)deut[dr] * Nq * Np + (size_t)q_idx[j] * Np + 0;
+        const size_t u = (size_t)dr * nd * nE + (size_t)dc * nE + j;
+        U[2 * u + 0] = hx[2 * ((size_t)dc * n + row) + 0];
+        U[2 * u + 1] = hx[2 * ((size_t)dc * n + row) + 1];
+      }
+  }
+  if (rep) *rep = r;
+  return TT_OK;
+}
+
+}  // namespace tt

@@ -1,0 +1,56 @@
+// Per-channel device solver of the elastic AGS/Faddeev equations in the WPCD
+// basis: U = (1 - A G)^{-1} A on the on-shell deuteron columns, A = C^T (2 P123) (V C).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../cuda/tt_kernels.h"
+#include "tt_host.h"
+
+namespace tt {
+
+// 2N block structure of one channel (solve_faddeev.cpp:1588-1927, make_resolvent.cpp:109-156).
+bool build_channel_layout(const RunParams& rp, const PWChannel& ch, const SWPStates& swp,
+                          const std::vector<double>& V_unco, const std::vector<double>& V_coup, ChannelLayout& L,
+                          std::string* err);
+
+struct SolveOptions {
+  bool mixed = true;        // complex64 LU on tensor cores + FP64 refinement; false: complex128 LU
+  bool tensor_cores = true; // trailing update on tcgen05 (mixed only)
+  double refine_tol = 1e-12;
+  int refine_max_iter = 30;
+};
+
+struct SolveReport {
+  double ms_A = 0, ms_form = 0, ms_factor = 0, ms_solve = 0, ms_refine = 0;
+  int refine_iters = 0;          // max over energies
+  double final_correction = 0;   // max over rhs of |dx|/|x| at exit
+  int info = 0;                  // first zero pivot (1-based) if any
+};
+
+class ChannelSolver {
+ public:
+  int n = 0;
+  int setup(const ChannelLayout& L, const std::vector<double>& q_WP, cudaStream_t st);
+  // P123 built on the device, or uploaded from host CSR arrays
+  int set_P_device(DeviceCSR&& P);
+  int set_P_host_csr(const int64_t* rowptr, const int32_t* col, const double* val, int64_t nnz, cudaStream_t st);
+  int build_A(cudaStream_t st, double* ms = nullptr);
+  // resolvent for energies E (= E_com + E_bound) into device G [nE][n]
+  int resolvent(const std::vector<double>& E, cudaStream_t st);
+  // U[d'*nd*nE + d*nE + j] for each on-shell q bin j and deuteron states
+  int solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
+            std::vector<double>& U_interleaved, SolveReport* rep, cudaStream_t st);
+  const DeviceCSR& P() const { return P_; }
+  const double* A() const { return A_.ptr; }
+  const double* G() const { return G_.ptr; }
+  int nE() const { return nE_; }
+
+ private:
+  DeviceLayout L_;
+  DeviceCSR P_;
+  DevBuf<double> A_, G_;
+  int nE_ = 0;
+};
+
+}  // namespace tt

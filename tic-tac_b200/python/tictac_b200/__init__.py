@@ -1,0 +1,312 @@
+"""ctypes binding of the tictac_b200 C-ABI (include/tictac_b200.h).
+
+The library is the in-tree build ``tic-tac_b200/lib/libtictac_b200.so``; there
+is no Python or CPU implementation of the path behind this module.  Every call
+raises ``TicTacError`` when the library returns a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, byref, c_char_p, c_double, c_int, c_int32, c_int64, c_size_t, c_void_p
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libtictac_b200.so"))
+
+TT_OK = 0
+TT_ERR_BADARG = 1
+TT_ERR_NOMEM = 2
+TT_ERR_CUDA = 3
+TT_ERR_NOCONVERGE = 4
+TT_ERR_IO = 5
+TT_ERR_UNSUPPORTED = 6
+TT_ERR_SINGULAR = 7
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+PRECISION_MIXED_SIMT = 2
+
+EXPORTED_SYMBOLS = (
+    "tt_run_params_default", "tt_fill_P123_arrays", "tt_calculate_resolvent_array_in_SWP_basis",
+    "tt_solve_faddeev_equations", "tt_free", "tt_last_error_string", "tt_device_count", "tt_run_create",
+    "tt_run_destroy", "tt_run_num_channels", "tt_run_channel_info", "tt_run_num_energies", "tt_run_energies",
+    "tt_run_E_bound", "tt_run_build_P123", "tt_run_build_A", "tt_run_build_resolvent", "tt_run_solve",
+    "tt_run_release_channel", "tt_run_get_P123_csr", "tt_run_get_A", "tt_run_get_G", "tt_run_get_host_array",
+    "tt_run_write_U_table",
+)
+
+
+class TicTacError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"tictac_b200 error {code}: {msg}")
+        self.code = code
+
+
+class tt_pw_states(ctypes.Structure):
+    _fields_ = [("Nalpha", c_int), ("J_2N_max", c_int)] + [
+        (f, POINTER(c_int)) for f in ("L_2N_array", "S_2N_array", "J_2N_array", "T_2N_array", "L_1N_array",
+                                      "two_J_1N_array", "two_J_3N_array", "two_T_3N_array", "P_3N_array")]
+
+
+class tt_fwp_states(ctypes.Structure):
+    _fields_ = [("Np_WP", c_int), ("Nq_WP", c_int), ("p_WP_array", POINTER(c_double)),
+                ("q_WP_array", POINTER(c_double))]
+
+
+class tt_swp_states(ctypes.Structure):
+    _fields_ = [("Np_WP", c_int), ("Nq_WP", c_int), ("num_2N_unco_states", c_int), ("num_2N_coup_states", c_int),
+                ("E_bound", c_double)] + [
+        (f, POINTER(c_double)) for f in ("e_SWP_unco_array", "e_SWP_coup_array", "C_SWP_unco_array",
+                                         "C_SWP_coup_array", "q_WP_array")]
+
+
+class tt_os_indexing(ctypes.Structure):
+    _fields_ = [("num_T_lab", c_int), ("q_com_idx_array", POINTER(c_int)), ("deuteron_idx_array", POINTER(c_int)),
+                ("num_deuteron_states", c_int)]
+
+
+class tt_run_params(ctypes.Structure):
+    _fields_ = [("Nphi", c_int), ("Nx", c_int), ("tensor_force", c_int), ("isospin_breaking_1S0", c_int),
+                ("production_run", c_int), ("precision", c_int), ("refine_tol", c_double),
+                ("refine_max_iter", c_int)]
+
+
+class tt_solve_report(ctypes.Structure):
+    _fields_ = [("ms_A", c_double), ("ms_form", c_double), ("ms_factor", c_double), ("ms_solve", c_double),
+                ("ms_refine", c_double), ("refine_iters", c_int), ("final_correction", c_double), ("info", c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the in-tree shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise TicTacError(TT_ERR_UNSUPPORTED, f"{path} is missing: run __graft_entry__.build() first")
+    lib = ctypes.CDLL(path)
+    lib.tt_last_error_string.restype = c_char_p
+    lib.tt_run_destroy.restype = None
+    lib.tt_free.restype = None
+    lib.tt_run_params_default.restype = None
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != TT_OK:
+        raise TicTacError(rc, _lib.tt_last_error_string().decode(errors="replace"))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(POINTER(c_int))
+
+
+def _dptr(a):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def device_count() -> int:
+    lib = load()
+    n = c_int(0)
+    rc = lib.tt_device_count(byref(n))
+    return n.value if rc == TT_OK else 0
+
+
+def run_params(**kw) -> tt_run_params:
+    lib = load()
+    rp = tt_run_params()
+    lib.tt_run_params_default(byref(rp))
+    for k, v in kw.items():
+        setattr(rp, k, v)
+    return rp
+
+
+class PW:
+    """One channel's partial-wave table (9 ints per alpha: L S J T l 2j 2J 2T P)."""
+
+    def __init__(self, table: np.ndarray, J_2N_max: int = 1):
+        t = np.ascontiguousarray(np.asarray(table, dtype=np.int32).reshape(-1, 9))
+        self._cols = [np.ascontiguousarray(t[:, k]) for k in range(9)]
+        self.s = tt_pw_states(t.shape[0], J_2N_max, *[_iptr(c) for c in self._cols])
+        self.Nalpha = t.shape[0]
+
+
+def fill_P123_arrays(pw: PW, p_WP, q_WP, production_run=True, **rp_kw):
+    """tt_fill_P123_arrays: row-major COO (row, col, val) of P123 built on the GPU."""
+    lib = load()
+    p = np.ascontiguousarray(p_WP, dtype=np.float64)
+    q = np.ascontiguousarray(q_WP, dtype=np.float64)
+    fwp = tt_fwp_states(len(p) - 1, len(q) - 1, _dptr(p), _dptr(q))
+    rp = run_params(**rp_kw)
+    val = POINTER(c_double)()
+    row = POINTER(c_int)()
+    col = POINTER(c_int)()
+    nnz = c_size_t(0)
+    _check(lib.tt_fill_P123_arrays(byref(val), byref(row), byref(col), byref(nnz), int(production_run), byref(fwp),
+                                   byref(pw.s), byref(rp)))
+    m = nnz.value
+    try:
+        v = np.ctypeslib.as_array(val, shape=(max(m, 1),))[:m].copy()
+        r = np.ctypeslib.as_array(row, shape=(max(m, 1),))[:m].copy()
+        c = np.ctypeslib.as_array(col, shape=(max(m, 1),))[:m].copy()
+    finally:
+        lib.tt_free(ctypes.cast(val, c_void_p))
+        lib.tt_free(ctypes.cast(row, c_void_p))
+        lib.tt_free(ctypes.cast(col, c_void_p))
+    return r, c, v
+
+
+class SWP:
+    def __init__(self, Np, Nq, n_unco, n_coup, E_bound, e_unco, e_coup, C_unco, C_coup, q_WP):
+        self._keep = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else np.zeros(1)
+                      for a in (e_unco, e_coup, C_unco, C_coup, q_WP)]
+        self.s = tt_swp_states(Np, Nq, n_unco, n_coup, E_bound, *[_dptr(a) for a in self._keep])
+
+
+def resolvent(G_E: float, swp: SWP, pw: PW, **rp_kw) -> np.ndarray:
+    lib = load()
+    n = pw.Nalpha * swp.s.Np_WP * swp.s.Nq_WP
+    G = np.zeros(n, dtype=np.complex128)
+    rp = run_params(**rp_kw)
+    _check(lib.tt_calculate_resolvent_array_in_SWP_basis(G.ctypes.data_as(c_void_p), c_double(G_E), byref(swp.s),
+                                                         byref(pw.s), byref(rp)))
+    return G
+
+
+def solve_faddeev(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q_idx, deut, pw: PW, precision=PRECISION_MIXED,
+                  **rp_kw):
+    """tt_solve_faddeev_equations with the reference's CSC P123 and host arrays."""
+    lib = load()
+    G = np.ascontiguousarray(G, dtype=np.complex128)
+    Pv = np.ascontiguousarray(P_val, dtype=np.float64)
+    Pr = np.ascontiguousarray(P_row, dtype=np.int32)
+    Pc = np.ascontiguousarray(P_colptr, dtype=np.uint64)
+    Vu = np.ascontiguousarray(V_unco, dtype=np.float64)
+    Vc = np.ascontiguousarray(V_coup if V_coup is not None and len(V_coup) else np.zeros(1), dtype=np.float64)
+    qi = np.ascontiguousarray(q_idx, dtype=np.int32)
+    di = np.ascontiguousarray(deut, dtype=np.int32)
+    os_ = tt_os_indexing(len(qi), _iptr(qi), _iptr(di), len(di))
+    rp = run_params(precision=precision, **rp_kw)
+    U = np.zeros(len(qi) * len(di) * len(di), dtype=np.complex128)
+    rep = tt_solve_report()
+    _check(lib.tt_solve_faddeev_equations(U.ctypes.data_as(c_void_p), G.ctypes.data_as(c_void_p), _dptr(Pv),
+                                          _iptr(Pr), Pc.ctypes.data_as(POINTER(c_size_t)), c_size_t(len(Pv)),
+                                          _dptr(Vu), _dptr(Vc), byref(swp.s), byref(os_), byref(pw.s), byref(rp),
+                                          byref(rep)))
+    return U, rep.as_dict()
+
+
+class Run:
+    """A configured run (tt_run_*): host state-space setup from key=value options."""
+
+    def __init__(self, **opts):
+        lib = load()
+        args = [f"{k}={v}" for k, v in opts.items()]
+        arr = (c_char_p * len(args))(*[a.encode() for a in args])
+        self._h = c_void_p()
+        _check(lib.tt_run_create(byref(self._h), len(args), arr))
+        self.lib = lib
+
+    def close(self):
+        if self._h:
+            self.lib.tt_run_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_channels(self):
+        n = c_int()
+        _check(self.lib.tt_run_num_channels(self._h, byref(n)))
+        return n.value
+
+    def channel_info(self, chn):
+        v = [c_int() for _ in range(5)]
+        _check(self.lib.tt_run_channel_info(self._h, chn, *[byref(x) for x in v]))
+        return dict(zip(("Nalpha", "n", "two_J_3N", "P_3N", "n_deuteron"), [x.value for x in v]))
+
+    def energies(self):
+        nE = c_int()
+        _check(self.lib.tt_run_num_energies(self._h, byref(nE)))
+        T = np.zeros(nE.value)
+        E = np.zeros(nE.value)
+        q = np.zeros(nE.value, dtype=np.int32)
+        _check(self.lib.tt_run_energies(self._h, _dptr(T), _dptr(E), _iptr(q)))
+        return T, E, q
+
+    @property
+    def E_bound(self):
+        e = c_double()
+        _check(self.lib.tt_run_E_bound(self._h, byref(e)))
+        return e.value
+
+    def host_array(self, which, chn=0):
+        dtype = np.int32 if which == 0 else np.float64
+        cnt = c_size_t()
+        _check(self.lib.tt_run_get_host_array(self._h, chn, which, None, byref(cnt)))
+        out = np.zeros(cnt.value, dtype=dtype)
+        _check(self.lib.tt_run_get_host_array(self._h, chn, which, out.ctypes.data_as(c_void_p), byref(cnt)))
+        return out
+
+    def build_P123(self, chn):
+        nnz = c_int64()
+        _check(self.lib.tt_run_build_P123(self._h, chn, byref(nnz)))
+        return nnz.value
+
+    def P123_csr(self, chn, nnz):
+        n = self.channel_info(chn)["n"]
+        rowptr = np.zeros(n + 1, dtype=np.int64)
+        col = np.zeros(max(nnz, 1), dtype=np.int32)
+        val = np.zeros(max(nnz, 1), dtype=np.float64)
+        _check(self.lib.tt_run_get_P123_csr(self._h, chn, rowptr.ctypes.data_as(c_void_p), col.ctypes.data_as(c_void_p),
+                                            val.ctypes.data_as(c_void_p)))
+        return rowptr, col[:nnz], val[:nnz]
+
+    def build_A(self, chn):
+        ms = c_double()
+        _check(self.lib.tt_run_build_A(self._h, chn, byref(ms)))
+        return ms.value
+
+    def A(self, chn):
+        n = self.channel_info(chn)["n"]
+        out = np.zeros((n, n))
+        _check(self.lib.tt_run_get_A(self._h, chn, _dptr(out)))
+        return out
+
+    def build_resolvent(self, chn):
+        _check(self.lib.tt_run_build_resolvent(self._h, chn))
+
+    def G(self, chn):
+        n = self.channel_info(chn)["n"]
+        nE = len(self.energies()[0])
+        out = np.zeros(n * nE, dtype=np.complex128)
+        _check(self.lib.tt_run_get_G(self._h, chn, out.ctypes.data_as(c_void_p)))
+        return out.reshape(nE, n)
+
+    def solve(self, chn, precision=PRECISION_MIXED):
+        info = self.channel_info(chn)
+        nE = len(self.energies()[0])
+        nd = info["n_deuteron"]
+        U = np.zeros(nE * nd * nd, dtype=np.complex128)
+        rep = tt_solve_report()
+        _check(self.lib.tt_run_solve(self._h, chn, precision, U.ctypes.data_as(c_void_p), byref(rep)))
+        return U, rep.as_dict()
+
+    def release(self, chn):
+        _check(self.lib.tt_run_release_channel(self._h, chn))
+
+    def write_U_table(self, chn, U, path):
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        _check(self.lib.tt_run_write_U_table(self._h, chn, U.ctypes.data_as(c_void_p), path.encode()))
