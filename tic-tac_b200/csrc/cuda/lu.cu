@@ -327,6 +327,7 @@ int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_te
       }
     }
   }
+  if (use_tensor_cores) TT_TRY(tc_check_error(st));
   if (info) {
     TT_CUDA_TRY(cudaMemcpyAsync(info, d_info.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
     TT_CUDA_TRY(cudaStreamSynchronize(st));
