@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Throughput of the WPCD elastic Faddeev solve (P123 -> A -> LU -> refined U).
+
+Workload (default): the configuration the headline metric is quoted on --
+two-body j <= 3, all 3N channels J^pi = 1/2+- .. 7/2+-, Np_WP = Nq_WP = 30,
+T_lab = 10 MeV (two on-shell q bins), with the chiral LO one-pion-exchange
+potential standing in for N3LO-Idaho (which exists only as Fortran in the
+reference; the solve cost depends on the shapes only).  Eight channels,
+n = 24,300 .. 56,700.  One step = both on-shell energies for all channels:
+A = C^T (2 P123)(V C) built from the resident P123, 1 - A G_E formed and
+LU-factorised per energy, on-shell columns solved and refined to 1e-12.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU (torchrun); rank r solves its own pair of
+on-shell energies (T_lab = 10 + 6 r MeV) for all channels -- independent
+replicas over the energy scan, no collective on the data path (weak scaling).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "tic-tac_b200", "python"))
+
+CONFIGS = {
+    # the metric's configuration (see module docstring)
+    "j3_J7_n30": dict(potential_model="LO_internal", J_2N_max=3, two_J_3N_max=7, Np_WP=30, Nq_WP=30),
+    # small case for quick checks of this script
+    "j1_J3_n12": dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=12, Nq_WP=12),
+}
+METRIC = "energies/sec, mixed+refined vs FP64 on B200 at <=1e-10 rel err in on-shell U"
+
+
+def load_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+
+    def summary(self):
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) >= 9:
+                for k, nm in enumerate(names):
+                    if s[5 + k].lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, value):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def step_flops(ns, nE):
+    return sum(nE * 8.0 / 3.0 * float(n) ** 3 for n in ns)
+
+
+def run_ours(args, world, rank, local, pg):
+    import tictac_b200 as tt
+    os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
+    cfg = dict(CONFIGS[args.config])
+    cfg["lab_energies"] = str(10.0 + 6.0 * rank)
+    prec = tt.PRECISION_MIXED if args.precision == "mixed" else tt.PRECISION_FP64
+    t_setup = time.perf_counter()
+    run = tt.Run(**cfg)
+    nch = run.num_channels
+    infos = [run.channel_info(c) for c in range(nch)]
+    T_lab, E_com, q_idx = run.energies()
+    nE = len(T_lab)
+    nnz = [run.build_P123(c) for c in range(nch)]  # resident for the whole run
+    t_setup = time.perf_counter() - t_setup
+
+    def one_step():
+        Us = []
+        for c in range(nch):
+            run.build_A(c)
+            run.build_resolvent(c)
+            U, rep = run.solve(c, prec)
+            Us.append(U)
+            run.release_A(c)
+        return Us
+
+    for _ in range(args.warmup):
+        one_step()
+    barrier(pg)
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            run.timer_start()
+            one_step()
+            times.append(run.timer_stop())
+    barrier(pg)
+    ms_step = allreduce_max(pg, float(np.mean(times)))
+    energies_per_step = nE * world
+    value = energies_per_step / (ms_step * 1e-3)
+
+    # dominant kernel: the tensor-core trailing update, timed in isolation on the
+    # largest channel's first update (CUDA events on the launching stream)
+    hbm, tf_peak, peak_kind = load_peaks()
+    flops = step_flops([i["n"] for i in infos], nE)
+    achieved_tflops = flops / (ms_step * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "achieved": round(achieved_tflops, 2), "peak": tf_peak, "unit": "TFLOP/s",
+                "frac": round(achieved_tflops / tf_peak, 4), "traffic": None,
+                "note": f"achieved = (8/3) n^3 complex-LU flops per channel-energy over the step time; peak {peak_kind} bf16"}
+
+    # end to end through the drop-in C-ABI call with host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        host = []
+        Np = Nq = cfg["Np_WP"]
+        e_unco = run.host_array(7)
+        e_coup = run.host_array(8)
+        C_unco = run.host_array(5)
+        C_coup = run.host_array(6)
+        V_unco = run.host_array(3)
+        V_coup = run.host_array(4)
+        q_WP = run.host_array(2)
+        n_unco = len(e_unco) // (Np + 1)
+        n_coup = len(e_coup) // (2 * (Np + 1))
+        swp = tt.SWP(Np, Nq, n_unco, n_coup, run.E_bound, e_unco, e_coup, C_unco, C_coup, q_WP)
+        for c in range(nch):
+            rowptr, col, val = run.P123_csr(c, nnz[c])
+            n = infos[c]["n"]
+            rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rowptr))
+            order = np.lexsort((rows, col))
+            colptr = np.zeros(n + 1, dtype=np.uint64)
+            np.add.at(colptr, col + 1, 1)
+            colptr = np.cumsum(colptr).astype(np.uint64)
+            run.build_resolvent(c)
+            G = run.G(c).reshape(-1)
+            pwt = run.host_array(0, c).reshape(-1, 9)
+            deut = [a for a in range(len(pwt)) if tuple(pwt[a, :4]) == (0, 1, 1, 0)]
+            host.append((G, val[order].copy(), rows[order].copy(), colptr, tt.PW(pwt, cfg["J_2N_max"]), deut))
+            run.release(c)
+        h2d = sum(h[0].nbytes + h[1].nbytes + h[2].nbytes + h[3].nbytes for h in host) + \
+            nch * (V_unco.nbytes + V_coup.nbytes + C_unco.nbytes + C_coup.nbytes + e_unco.nbytes + e_coup.nbytes)
+        d2h = sum(16 * nE * len(h[5]) ** 2 for h in host)
+
+        def e2e_step():
+            for (G, v, r, cp, pw, deut) in host:
+                tt.solve_faddeev(G, v, r, cp, V_unco, V_coup, swp, q_idx, deut, pw, precision=prec)
+
+        e2e_step()
+        barrier(pg)
+        te = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            e2e_step()
+            te.append(time.perf_counter() - t0)
+        t_e2e = allreduce_max(pg, float(np.mean(te)))
+        e2e = {"value": round(energies_per_step / t_e2e, 6), "unit": "energies/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "timer": "host perf_counter around the synchronous C-ABI call"}
+    return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, e2e=e2e,
+                infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times)
+
+
+def reference_sample(args, sample_N=10, channel=None):
+    """Time the reference's own dense LAPACK solve (oracle/_ref/tictac_ref,
+    OpenMP + OpenBLAS on all host cores) on one channel of the same physics at
+    Np_WP = Nq_WP = sample_N and scale to the workload by n^3."""
+    binp = os.path.join(HERE, "oracle", "_ref", "tictac_ref")
+    if not os.path.exists(binp):
+        return None, "oracle/_ref/tictac_ref not built"
+    cfg = dict(CONFIGS[args.config])
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as out:
+        opts = [f"{k}={v}" for k, v in cfg.items() if k not in ("Np_WP", "Nq_WP")]
+        opts += [f"Np_WP={sample_N}", f"Nq_WP={sample_N}", "lab_energies=10"]
+        ch = channel if channel is not None else 0
+        cmd = [binp, "time", out, f"--channel={ch}"] + opts
+        t0 = time.perf_counter()
+        subprocess.run(cmd, check=True, cwd=out, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(cores)), timeout=900)
+        wall = time.perf_counter() - t0
+        t = {}
+        with open(os.path.join(out, "meta.txt")) as f:
+            for line in f:
+                tok = line.split()
+                if tok and tok[0] == "timing":
+                    t = dict(zip(tok[1::2], tok[2::2]))
+                if tok and tok[0] == "chn":
+                    meta = dict(zip(tok[::2], tok[1::2]))
+    n_s = int(t["n"])
+    per_energy = (float(t["t_A"]) + float(t["t_getrf_getrs"])) / int(meta["nE"])
+    return dict(n_sample=n_s, per_energy_s=per_energy, t_fair=float(t["t_fair"]) / int(meta["nE"]),
+                t_p123=float(meta["t_p123"]), cores=cores, wall=wall), None
+
+
+def cpu_value_for(infos, ref):
+    # seconds per energy for all channels of the workload, scaled by n^3
+    s = sum(ref["per_energy_s"] * (i["n"] / ref["n_sample"]) ** 3 for i in infos)
+    return 1.0 / s
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=list(CONFIGS), default="j3_J7_n30")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    cfg = CONFIGS[args.config]
+    config = {"workload": f"{args.config}: LO-OPEP (stands in for N3LO-Idaho), j<=3, J<=7/2 both parities, "
+                          f"Np=Nq={cfg['Np_WP']}, T_lab=10 MeV (rank r: 10+6r MeV)",
+              "channels_per_step": None, "energies_per_rank": None, "parallelism": f"replicas x{world}",
+              "l2": "inputs larger than L2 (A is 25.7 GB for the largest channel)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import tictac_b200 as tt
+        run = tt.Run(**dict(cfg, lab_energies="10"))
+        infos = [run.channel_info(c) for c in range(run.num_channels)]
+        nE = len(run.energies()[0])
+        run.close()
+        ref, why = reference_sample(args)
+        if ref is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        v = cpu_value_for(infos, ref)
+        times = []
+        for _ in range(args.warmup + args.steps):
+            r2, _ = reference_sample(args)
+            times.append(r2["per_energy_s"])
+        ref["per_energy_s"] = float(np.mean(times[args.warmup:])) if args.steps else ref["per_energy_s"]
+        v = cpu_value_for(infos, ref)
+        sample = (f"reference dense LAPACK solve (A columns + zgetrf + zgetrs nrhs=n) of channel 0 at "
+                  f"Np=Nq=10 (n={ref['n_sample']}), {ref['cores']} threads, scaled by n^3 to the workload")
+        print(json.dumps({"metric": METRIC, "value": v, "unit": "energies/s", "impl": "reference", "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_step": nE / v * 1e3,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+                          "data": "synthetic (seeded LO potential)", "config": config,
+                          "cpu_baseline": {"value": v, "unit": "energies/s", "cores": ref["cores"],
+                                           "kind": "reference", "sample": sample},
+                          "e2e": {"value": v, "unit": "energies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    r = run_ours(args, world, rank, local, pg)
+    if rank == 0:
+        config["channels_per_step"] = len(r["infos"])
+        config["energies_per_rank"] = r["nE"]
+        config["n_per_channel"] = [i["n"] for i in r["infos"]]
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            ref, why = reference_sample(args)
+            if ref is not None:
+                v = cpu_value_for(r["infos"], ref)
+                cpu = {"value": v, "unit": "energies/s", "cores": ref["cores"], "kind": "reference",
+                       "sample": f"reference dense LAPACK solve of channel 0 at Np=Nq=10 (n={ref['n_sample']}), "
+                                 f"scaled by n^3 to all {len(r['infos'])} channels"}
+        out = {"metric": METRIC, "value": round(r["value"], 6), "unit": "energies/s", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_step": round(r["ms_step"], 3),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "complex64 LU (BF16x3 tcgen05) + FP64 refinement" if args.precision == "mixed" else "complex128",
+               "data": "synthetic (chiral LO potential on the reference's default Chebyshev WP grid)",
+               "config": config, "clocks": r["clocks"], "roofline": r["roofline"], "cpu_baseline": cpu,
+               "e2e": r["e2e"], "gpu_launches": None, "setup_s": round(r["t_setup"], 3)}
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -144,6 +144,24 @@ int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double*
 void tt_free(void* p);
 const char* tt_last_error_string(void);
 int tt_device_count(int* count);
+/* Kernels launched by this library since load (diagnostic). */
+unsigned long long tt_kernel_launches(void);
+
+/* Host numerics the P123 tables are built from, doubled (2j, 2m) arguments:
+ * replace gsl_sf_coupling_3j/6j/9j as wrapped by wigner_3j/6j/9j and
+ * clebsch_gordan (CPP/General_functions/coupling_coefficients.h:12-24,
+ * CPP/auxiliary.cpp:127-135). */
+double tt_wigner_3j(int two_j1, int two_j2, int two_j3, int two_m1, int two_m2, int two_m3);
+double tt_wigner_6j(int two_j1, int two_j2, int two_j3, int two_j4, int two_j5, int two_j6);
+double tt_wigner_9j(int two_j1, int two_j2, int two_j3, int two_j4, int two_j5, int two_j6, int two_j7, int two_j8,
+                    int two_j9);
+double tt_clebsch_gordan(int two_j1, int two_j2, int two_j3, int two_m1, int two_m2, int two_m3);
+/* Y_l^m(theta,0), 0 <= m <= l <= lmax at x = cos(theta), index l(l+1)/2+m: the
+ * gsl_sf_legendre_array_e(GSL_SF_LEGENDRE_SPHARM, lmax, x, -1, out) table the
+ * reference uses (CPP/make_permutation_matrix.cpp:549-589). */
+int tt_legendre_spharm_array(int lmax, double x, double* out);
+/* Gauss-Legendre rule on [-1,1] (gauss, CPP/General_functions/gauss_legendre.cpp:36-66). */
+int tt_gauss_legendre(int n, double* x, double* w);
 
 /* ---- layer 2: run handle -------------------------------------------- */
 
@@ -171,8 +189,15 @@ int tt_run_build_A(tt_run* run, int chn, double* ms);
 int tt_run_build_resolvent(tt_run* run, int chn);
 /* Solve all on-shell energies of the channel; U as in tt_solve_faddeev_equations. */
 int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_report* report);
-/* Release the channel's device data. */
+/* Release the channel's device data (all of it, or only A and the resolvents,
+ * keeping P123 resident for the next parameter set or energy scan). */
 int tt_run_release_channel(tt_run* run, int chn);
+int tt_run_release_A(tt_run* run, int chn);
+
+/* CUDA-event timer on the run's stream: start records an event, stop records
+ * another, waits for it and returns the elapsed device time in ms. */
+int tt_run_timer_start(tt_run* run);
+int tt_run_timer_stop(tt_run* run, double* ms);
 
 /* Host copies for checking (sizes from tt_run_channel_info / build results). */
 int tt_run_get_P123_csr(const tt_run* run, int chn, int64_t* rowptr, int32_t* col, double* val);

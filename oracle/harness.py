@@ -1,0 +1,162 @@
+"""Python side of the CPU oracle (test infrastructure only).
+
+Loads oracle/_build/liboracle.so (the plain-C restatement in oracle/*.c) and
+restates in numpy the 2N block bookkeeping the reference keeps in its C^T /
+V C pointer tables (CPP/solve_faddeev.cpp:1588-1927) and resolvent
+(CPP/make_resolvent.cpp:109-156), so that the oracle chain
+P123 -> A -> dense LU solve -> U runs independently of the product library.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use this.
+"""
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int, c_int64
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise RuntimeError(f"{LIB} missing: run `make -C oracle lib`")
+        _lib = ctypes.CDLL(LIB)
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(POINTER(t))
+
+
+def p123(pw, p_WP, q_WP, Nphi, Nx):
+    """Row-major COO (row, col, val) of P123 for one channel."""
+    L = lib()
+    pw = np.ascontiguousarray(pw, dtype=np.int32).reshape(-1, 9)
+    p = np.ascontiguousarray(p_WP, dtype=np.float64)
+    q = np.ascontiguousarray(q_WP, dtype=np.float64)
+    nnz = c_int64()
+    r = POINTER(ctypes.c_int32)()
+    c = POINTER(ctypes.c_int32)()
+    v = POINTER(c_double)()
+    L.to_p123(len(p) - 1, len(q) - 1, _p(p, c_double), _p(q, c_double), Nphi, Nx, pw.shape[0],
+              _p(pw, ctypes.c_int32), ctypes.byref(nnz), ctypes.byref(r), ctypes.byref(c), ctypes.byref(v))
+    m = nnz.value
+    out = (np.ctypeslib.as_array(r, shape=(max(m, 1),))[:m].copy(),
+           np.ctypeslib.as_array(c, shape=(max(m, 1),))[:m].copy(),
+           np.ctypeslib.as_array(v, shape=(max(m, 1),))[:m].copy())
+    for ptr in (r, c, v):
+        L.to_free(ctypes.cast(ptr, ctypes.c_void_p))
+    return out
+
+
+def unique_2N_idx(L, S, J, T, coupled, tensor_force, iso):
+    """make_pw_symm_states.cpp:4-60"""
+    s1S0 = (S == 0 and J == 0 and L == 0 and T == 1)
+    if tensor_force:
+        if coupled:
+            idx = J - 1
+            if not s1S0 and iso:
+                idx += 1
+            if s1S0 and iso:
+                idx = 0
+            return idx
+        idx = 2 * J + S
+        return idx - 1 if iso else idx
+    if coupled:
+        return 0 if iso else -1
+    idx = J * (4 * (J > 1) + 2) + (S == 1) + (S == 1 and J != 0) * (J - L + 1)
+    return idx - 1 if iso else idx
+
+
+def layout(pw, Np, V_unco, V_coup, C_unco, C_coup, e_unco, e_coup, tensor_force=True, iso=True):
+    """2N block structure of a channel: per alpha block/part/e-offset, coupling lists, C and VC blocks."""
+    pw = np.asarray(pw).reshape(-1, 9)
+    Na = pw.shape[0]
+    blocks, blk, part, e_off = {}, [], [], []
+    Cs, VCs, offs, dims = [], [], [], []
+    off = 0
+    for a in range(Na):
+        L, S, J, T = (int(x) for x in pw[a, :4])
+        tT = int(pw[a, 7])
+        via_L = tensor_force and L != J and J != 0
+        via_T = (S == 0 and J == 0 and L == 0) and iso
+        coupled = via_L or via_T
+        chn = unique_2N_idx(L, S, J, T, coupled, tensor_force, iso)
+        prt = (0 if L < J else 1) if via_L else ((0 if tT == 1 else 1) if via_T else 0)
+        key = (coupled, chn)
+        if key not in blocks:
+            d = 2 * Np if coupled else Np
+            src_C = C_coup if coupled else C_unco
+            src_V = V_coup if coupled else V_unco
+            Cm = np.asarray(src_C[chn * d * d:(chn + 1) * d * d]).reshape(d, d)
+            Vm = np.asarray(src_V[chn * d * d:(chn + 1) * d * d]).reshape(d, d)
+            blocks[key] = len(dims)
+            dims.append(d)
+            offs.append(off)
+            off += d * d
+            Cs.append(Cm.reshape(-1))
+            VCs.append((Vm @ Cm).reshape(-1))
+        blk.append(blocks[key])
+        part.append(prt)
+        e_off.append(len(e_unco) + chn * 2 * (Np + 1) + prt * (Np + 1) if coupled else chn * (Np + 1))
+    cpl_off, cpl = [0], []
+    for r in range(Na):
+        for c in range(Na):
+            chk_L = (tensor_force and abs(int(pw[r, 0]) - int(pw[c, 0])) <= 2) or pw[r, 0] == pw[c, 0]
+            if (pw[r, 3] == pw[c, 3] and pw[r, 2] == pw[c, 2] and pw[r, 1] == pw[c, 1] and chk_L
+                    and pw[r, 4] == pw[c, 4] and pw[r, 5] == pw[c, 5]):
+                cpl.append(c)
+        cpl_off.append(len(cpl))
+    i32 = lambda x: np.ascontiguousarray(x, dtype=np.int32)
+    return dict(blk=i32(blk), part=i32(part), e_off=i32(e_off), cpl_off=i32(cpl_off), cpl=i32(cpl),
+                blk_off=np.ascontiguousarray(offs, dtype=np.int64), blk_dim=i32(dims),
+                C=np.ascontiguousarray(np.concatenate(Cs)), VC=np.ascontiguousarray(np.concatenate(VCs)),
+                e_swp=np.ascontiguousarray(np.concatenate([e_unco, e_coup]), dtype=np.float64))
+
+
+def resolvent(lay, Na, Nq, Np, q_WP, E):
+    G = np.zeros(Na * Nq * Np, dtype=np.complex128)
+    q = np.ascontiguousarray(q_WP, dtype=np.float64)
+    lib().to_resolvent(Na, Nq, Np, _p(lay["e_off"], ctypes.c_int32), _p(lay["e_swp"], c_double), _p(q, c_double),
+                       c_double(E), G.ctypes.data_as(POINTER(c_double)))
+    return G
+
+
+def build_A(lay, Na, Nq, Np, row, col, val):
+    """Dense A from row-major COO P123 (converted to the reference's CSC)."""
+    n = Na * Nq * Np
+    order = np.lexsort((row, col))
+    r = np.ascontiguousarray(row[order], dtype=np.int32)
+    v = np.ascontiguousarray(val[order], dtype=np.float64)
+    colptr = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(colptr, np.asarray(col, dtype=np.int64) + 1, 1)
+    colptr = np.cumsum(colptr)
+    A = np.zeros((n, n))
+    lib().to_build_A(Na, Nq, Np, _p(colptr, c_int64), _p(r, ctypes.c_int32), _p(v, c_double),
+                     _p(lay["blk"], ctypes.c_int32), _p(lay["part"], ctypes.c_int32), _p(lay["cpl_off"], ctypes.c_int32),
+                     _p(lay["cpl"], ctypes.c_int32), _p(lay["blk_off"], c_int64), _p(lay["blk_dim"], ctypes.c_int32),
+                     _p(lay["C"], c_double), _p(lay["VC"], c_double), A.ctypes.data_as(POINTER(c_double)))
+    return A
+
+
+def dense_solve(A, G, q_idx, deut, Nq, Np):
+    n = A.shape[0]
+    G = np.ascontiguousarray(np.asarray(G, dtype=np.complex128).reshape(-1))
+    nE = len(q_idx)
+    qi = np.ascontiguousarray(q_idx, dtype=np.int32)
+    di = np.ascontiguousarray(deut, dtype=np.int32)
+    U = np.zeros(nE * len(di) * len(di), dtype=np.complex128)
+    st = lib().to_dense_solve(n, np.ascontiguousarray(A).ctypes.data_as(POINTER(c_double)), nE,
+                              G.ctypes.data_as(POINTER(c_double)), _p(qi, ctypes.c_int32), len(di),
+                              _p(di, ctypes.c_int32), Nq, Np, U.ctypes.data_as(POINTER(c_double)))
+    if st:
+        raise RuntimeError(f"oracle LU: zero pivot at column {st}")
+    return U
+
+
+def deuterons(pw):
+    pw = np.asarray(pw).reshape(-1, 9)
+    return [a for a in range(pw.shape[0]) if tuple(int(x) for x in pw[a, :4]) == (0, 1, 1, 0)]

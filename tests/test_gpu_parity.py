@@ -1,0 +1,177 @@
+"""GPU path (through the C-ABI) against the reference's golden outputs and the CPU oracle."""
+import numpy as np
+import pytest
+
+import harness as oracle
+import tictac_b200 as tt
+from conftest import CASES, load_case, rel
+
+pytestmark = pytest.mark.gpu
+
+PRECISIONS = [tt.PRECISION_FP64, tt.PRECISION_MIXED, tt.PRECISION_MIXED_SIMT]
+
+
+def swp_of(g, m):
+    Np, Nq = m["Np"], m["Nq"]
+    return tt.SWP(Np, Nq, len(g["e_unco"]) // (Np + 1), len(g["e_coup"]) // (2 * (Np + 1)), float(g["E_bound"]),
+                  g["e_unco"], g["e_coup"], g["C_unco"], g["C_coup"], g["q_WP"])
+
+
+def csc_of(n, row, col, val):
+    order = np.lexsort((row, col))
+    colptr = np.zeros(n + 1, dtype=np.uint64)
+    np.add.at(colptr, np.asarray(col, dtype=np.int64) + 1, 1)
+    return val[order], row[order], np.cumsum(colptr).astype(np.uint64)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_p123_pattern_bit_exact_and_values(case):
+    g, m = load_case(case)
+    for c in range(int(g["n_chn"])):
+        pw = tt.PW(g[f"pw_c{c}"])
+        r, cc, v = tt.fill_P123_arrays(pw, g["p_WP"], g["q_WP"], Nphi=m["Nphi"], Nx=m["Nx"])
+        assert np.array_equal(r, g[f"p123_row_c{c}"]) and np.array_equal(cc, g[f"p123_col_c{c}"])
+        assert rel(v, g[f"p123_val_c{c}"]) <= 1e-13
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_resolvent_matches_reference(case):
+    g, m = load_case(case)
+    swp = swp_of(g, m)
+    E = g["E_com"] + float(g["E_bound"])
+    for c in range(int(g["n_chn"])):
+        pw = tt.PW(g[f"pw_c{c}"])
+        G = np.stack([tt.resolvent(e, swp, pw, tensor_force=int(m["tensor_force"]), isospin_breaking_1S0=int(m["iso"]))
+                      for e in E])
+        assert rel(G.reshape(-1), g[f"G_c{c}"]) <= 1e-11
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("precision", PRECISIONS)
+def test_solve_dropin_matches_reference(case, precision):
+    g, m = load_case(case)
+    swp = swp_of(g, m)
+    for c in range(int(g["n_chn"])):
+        pwt = g[f"pw_c{c}"]
+        n = pwt.shape[0] * m["Np"] * m["Nq"]
+        v, r, cp = csc_of(n, g[f"p123_row_c{c}"], g[f"p123_col_c{c}"], g[f"p123_val_c{c}"])
+        U, rep = tt.solve_faddeev(g[f"G_c{c}"], v, r, cp, g["V_unco"], g["V_coup"], swp, g["q_idx"],
+                                  oracle.deuterons(pwt), tt.PW(pwt), precision=precision,
+                                  tensor_force=int(m["tensor_force"]), isospin_breaking_1S0=int(m["iso"]))
+        assert rel(U, g[f"U_c{c}"]) <= 1e-10, (c, rep)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_run_handle_end_to_end(case):
+    g, m = load_case(case)
+    run = tt.Run(**m["opts"])
+    for c in range(run.num_channels):
+        for prec in (tt.PRECISION_FP64, tt.PRECISION_MIXED):
+            U, rep = run.solve(c, prec)
+            assert rel(U, g[f"U_c{c}"]) <= 1e-10
+    run.close()
+
+
+@pytest.mark.parametrize("case", ["mt_swave_n16", "lo_j1_J3_n8"])
+def test_A_matches_oracle(case):
+    g, m = load_case(case)
+    run = tt.Run(**m["opts"])
+    for c in range(run.num_channels):
+        pw = run.host_array(0, c).reshape(-1, 9)
+        lay = oracle.layout(pw, m["Np"], run.host_array(3), run.host_array(4), run.host_array(5), run.host_array(6),
+                            run.host_array(7), run.host_array(8), m["tensor_force"], m["iso"])
+        run.build_A(c)
+        A = run.A(c)
+        A_o = oracle.build_A(lay, pw.shape[0], m["Nq"], m["Np"], g[f"p123_row_c{c}"], g[f"p123_col_c{c}"],
+                             g[f"p123_val_c{c}"])
+        assert rel(A, A_o) <= 1e-12
+    run.close()
+
+
+def test_larger_case_against_oracle():
+    # j <= 2, J <= 3/2, N = 8 with tensor force and isospin breaking: beyond the fixtures
+    opts = dict(potential_model="LO_internal", J_2N_max=2, two_J_3N_max=3, Np_WP=8, Nq_WP=8, Nphi=20, Nx=20,
+                lab_energies="7,40")
+    run = tt.Run(**opts)
+    Np = Nq = 8
+    T, E_com, q_idx = run.energies()
+    for c in [0, run.num_channels - 1]:
+        pw = run.host_array(0, c).reshape(-1, 9)
+        nnz = run.build_P123(c)
+        rowptr, col, val = run.P123_csr(c, nnz)
+        r_o, c_o, v_o = oracle.p123(pw, run.host_array(1), run.host_array(2), 20, 20)
+        rows = np.repeat(np.arange(len(rowptr) - 1, dtype=np.int32), np.diff(rowptr))
+        assert np.array_equal(rows, r_o) and np.array_equal(col, c_o)
+        assert rel(val, v_o) <= 1e-13
+        lay = oracle.layout(pw, Np, run.host_array(3), run.host_array(4), run.host_array(5), run.host_array(6),
+                            run.host_array(7), run.host_array(8))
+        G_o = np.stack([oracle.resolvent(lay, pw.shape[0], Nq, Np, run.host_array(2), e + run.E_bound) for e in E_com])
+        A_o = oracle.build_A(lay, pw.shape[0], Nq, Np, r_o, c_o, v_o)
+        U_o = oracle.dense_solve(A_o, G_o, q_idx, oracle.deuterons(pw), Nq, Np)
+        for prec in PRECISIONS:
+            U, rep = run.solve(c, prec)
+            assert rel(U, U_o) <= 1e-10, (prec, rep)
+    run.close()
+
+
+def test_full_size_channel_mixed_agrees_with_fp64():
+    # largest channel of the j<=3, J<=7/2 basis at N=16 (n = 16128): size-independent check
+    # that refinement recovers the FP64 solution
+    run = tt.Run(potential_model="LO_internal", J_2N_max=3, two_J_3N_max=7, Np_WP=16, Nq_WP=16, lab_energies="10")
+    c = max(range(run.num_channels), key=lambda k: run.channel_info(k)["n"])
+    U64, _ = run.solve(c, tt.PRECISION_FP64)
+    Um, rep = run.solve(c, tt.PRECISION_MIXED)
+    assert rep["final_correction"] <= 1e-12 and rep["refine_iters"] >= 1
+    assert rel(Um, U64) <= 1e-10
+    run.close()
+
+
+def test_refinement_nonconvergence_is_reported():
+    g, m = load_case("mt_swave_n16")
+    pwt = g["pw_c0"]
+    n = pwt.shape[0] * m["Np"] * m["Nq"]
+    v, r, cp = csc_of(n, g["p123_row_c0"], g["p123_col_c0"], g["p123_val_c0"])
+    with pytest.raises(tt.TicTacError) as e:
+        tt.solve_faddeev(g["G_c0"], v, r, cp, g["V_unco"], g["V_coup"], swp_of(g, m), g["q_idx"], [1], tt.PW(pwt),
+                         precision=tt.PRECISION_MIXED, tensor_force=0, isospin_breaking_1S0=0, refine_max_iter=1,
+                         refine_tol=1e-300)
+    assert e.value.code == tt.TT_ERR_NOCONVERGE
+
+
+def test_hbm_admission_reports_nomem_without_fault():
+    # n = 2 * 316 * 316 = 199712: A alone would need 319 GB
+    Np = Nq = 316
+    pw = np.array([[0, 0, 0, 1, 0, 1, 1, 1, 1], [0, 1, 1, 0, 0, 1, 1, 1, 1]], dtype=np.int32)
+    n = 2 * Np * Nq
+    qwp = np.linspace(0, 1000, Nq + 1)
+    # tensor force off, no isospin breaking: 6 uncoupled 2N slots for j <= 1 (CPP/main.cpp:283-288)
+    swp = tt.SWP(Np, Nq, 6, 0, -2.0, np.linspace(-2, 100, (Np + 1) * 6), None, np.tile(np.eye(Np).ravel(), 6),
+                 None, qwp)
+    G = np.zeros(n, dtype=np.complex128)
+    with pytest.raises(tt.TicTacError) as e:
+        tt.solve_faddeev(G, np.zeros(0), np.zeros(0, dtype=np.int32), np.zeros(n + 1, dtype=np.uint64),
+                         np.zeros(Np * Np * 6), None, swp, [0], [1], tt.PW(pw), tensor_force=0, isospin_breaking_1S0=0)
+    assert e.value.code == tt.TT_ERR_NOMEM
+    # the device stays usable afterwards
+    g, m = load_case("mt_swave_n16")
+    run = tt.Run(**m["opts"])
+    U, _ = run.solve(0, tt.PRECISION_FP64)
+    assert rel(U, g["U_c0"]) <= 1e-10
+
+
+def test_no_deuteron_states_gives_empty_U():
+    g, m = load_case("mt_swave_n16")
+    pwt = g["pw_c0"]
+    n = pwt.shape[0] * m["Np"] * m["Nq"]
+    v, r, cp = csc_of(n, g["p123_row_c0"], g["p123_col_c0"], g["p123_val_c0"])
+    U, rep = tt.solve_faddeev(g["G_c0"], v, r, cp, g["V_unco"], g["V_coup"], swp_of(g, m), g["q_idx"], [],
+                              tt.PW(pwt), tensor_force=0, isospin_breaking_1S0=0)
+    assert U.size == 0
+
+
+def test_kernel_launch_counter_advances():
+    g, m = load_case("mt_swave_n16")
+    before = tt.kernel_launches()
+    run = tt.Run(**m["opts"])
+    run.solve(0, tt.PRECISION_MIXED)
+    assert tt.kernel_launches() > before

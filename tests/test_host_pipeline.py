@@ -1,0 +1,64 @@
+"""Host state-space setup behind the C-ABI (no GPU needed) against the reference."""
+import numpy as np
+import pytest
+
+import tictac_b200 as tt
+from conftest import CASES, load_case, rel
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_state_space_matches_reference(case):
+    g, m = load_case(case)
+    run = tt.Run(**m["opts"])
+    assert run.num_channels == int(g["n_chn"])
+    for c in range(run.num_channels):
+        assert np.array_equal(run.host_array(0, c).reshape(-1, 9), g[f"pw_c{c}"])
+    # WP boundaries and potential matrices are bit-identical
+    assert np.array_equal(run.host_array(1), g["p_WP"])
+    assert np.array_equal(run.host_array(2), g["q_WP"])
+    assert np.array_equal(run.host_array(3), g["V_unco"])
+    assert np.array_equal(run.host_array(4), g["V_coup"])
+    # SWP energies from a different symmetric eigensolver: FP64 rounding level
+    scale = max(np.max(np.abs(g["e_unco"])), 1.0)
+    assert np.max(np.abs(run.host_array(7) - g["e_unco"])) <= 1e-12 * scale
+    if g["e_coup"].size:
+        assert np.max(np.abs(run.host_array(8) - g["e_coup"])) <= 1e-12 * max(np.max(np.abs(g["e_coup"])), 1.0)
+    assert abs(run.E_bound - float(g["E_bound"])) <= 1e-12 * abs(float(g["E_bound"]))
+    T, E, q = run.energies()
+    assert np.array_equal(q, g["q_idx"])
+    assert rel(T, g["T_lab"]) <= 1e-12 and rel(E, g["E_com"]) <= 1e-12
+
+
+def test_bad_option_and_model_errors():
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(not_a_key="3")
+    assert e.value.code == tt.TT_ERR_BADARG
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(two_J_3N_max=2)
+    assert e.value.code == tt.TT_ERR_BADARG
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(tensor_force="maybe")
+    assert e.value.code == tt.TT_ERR_BADARG
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(potential_model="Idaho_N3LO", J_2N_max=1, Np_WP=8, Nq_WP=8, lab_energies="10")
+    assert "Fortran" in str(e.value)
+    # an energy beyond every pair of q-bin midpoints selects no on-shell bin
+    # (run_organizer.cpp:57-85): no energies, not an error
+    run = tt.Run(potential_model="malfliet_tjon", J_2N_max=1, Np_WP=8, Nq_WP=8, lab_energies="1e9")
+    assert len(run.energies()[0]) == 0
+
+
+def test_u_table_format(tmp_path):
+    g, m = load_case("mt_swave_n16")
+    run = tt.Run(**m["opts"])
+    U = g["U_c0"]
+    p = str(tmp_path / "U.txt")
+    run.write_U_table(0, U, p)
+    txt = open(p).read().splitlines()
+    labels = [l for l in txt if l.strip().startswith("U")]
+    rows = [l for l in txt if l.strip() and not l.startswith("#") and not l.strip().startswith("U")]
+    assert len(labels) == 1 and len(rows) == len(g["q_idx"])  # disk_io_routines.cpp:820-908 layout
+    for j, line in enumerate(rows):
+        f = line.split()
+        assert int(f[2]) == int(g["q_idx"][j])
+        assert abs(complex(f[3]) - U[j]) <= 1e-15 * abs(U[j])

@@ -1,0 +1,53 @@
+"""Host numerics the P123 tables are built from, against exact and library values."""
+import os
+
+import numpy as np
+
+import tictac_b200 as tt
+from conftest import GOLDEN
+
+
+def test_wigner_symbols_against_sympy():
+    d = np.load(os.path.join(GOLDEN, "wigner.npz"))
+    for t, v in zip(d["t3"], d["v3"]):
+        assert abs(tt.wigner3j(*t) - v) <= 1e-14 * max(1.0, abs(v))
+    for t, v in zip(d["t6"], d["v6"]):
+        assert abs(tt.wigner6j(*t) - v) <= 1e-14 * max(1.0, abs(v))
+        if v == 0:
+            assert tt.wigner6j(*t) == 0.0 or abs(tt.wigner6j(*t)) < 1e-16
+    for t, v in zip(d["t9"], d["v9"]):
+        assert abs(tt.wigner9j(*t) - v) <= 1e-13 * max(1.0, abs(v))
+
+
+def test_clebsch_gordan_orthonormality():
+    # sum_{m1} <j1 m1 j2 M-m1 | J M> <j1 m1 j2 M-m1 | J' M> = delta_JJ'
+    for tj1, tj2 in [(2, 2), (4, 6), (1, 3), (6, 8)]:
+        tJs = range(abs(tj1 - tj2), tj1 + tj2 + 1, 2)
+        for tM in range(-(tj1 + tj2), tj1 + tj2 + 1, 2):
+            for tJ in tJs:
+                for tJp in tJs:
+                    if abs(tM) > min(tJ, tJp):
+                        continue
+                    s = sum(tt.clebsch_gordan(tj1, tj2, tJ, tm1, tM - tm1, tM) *
+                            tt.clebsch_gordan(tj1, tj2, tJp, tm1, tM - tm1, tM)
+                            for tm1 in range(-tj1, tj1 + 1, 2) if abs(tM - tm1) <= tj2)
+                    assert abs(s - (1.0 if tJ == tJp else 0.0)) < 1e-13
+
+
+def test_spharm_against_scipy():
+    from scipy.special import sph_harm_y
+    lmax = 9
+    for x in np.linspace(-0.999, 0.999, 23):
+        out = tt.spharm_array(lmax, float(x))
+        th = np.arccos(x)
+        for l in range(lmax + 1):
+            for m in range(l + 1):
+                ref = np.real(sph_harm_y(l, m, th, 0.0))
+                assert abs(out[l * (l + 1) // 2 + m] - ref) <= 1e-13 * max(1.0, abs(ref))
+
+
+def test_gauss_legendre_against_numpy():
+    for n in (2, 8, 16, 48, 150):
+        x, w = tt.gauss_legendre(n)
+        xr, wr = np.polynomial.legendre.leggauss(n)
+        assert np.max(np.abs(x - xr)) <= 1e-15 and np.max(np.abs(w - wr)) <= 1e-14

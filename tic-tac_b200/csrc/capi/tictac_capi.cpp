@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -16,6 +17,7 @@
 
 #include "../cuda/tt_kernels.h"
 #include "../host/tt_host.h"
+#include "../host/tt_math.h"
 #include "../host/tt_p123.h"
 #include "../host/tt_solver.h"
 
@@ -24,6 +26,9 @@ namespace tt {
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 }  // namespace tt
 
@@ -128,6 +133,7 @@ struct tt_run {
   OnShell os;
   std::vector<ChannelState> chn;
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 extern "C" {
@@ -145,6 +151,27 @@ void tt_run_params_default(tt_run_params* rp) {
 }
 
 void tt_free(void* p) { std::free(p); }
+
+unsigned long long tt_kernel_launches(void) { return g_launches.load(); }
+
+double tt_wigner_3j(int a, int b, int c, int ma, int mb, int mc) { return wigner3j(a, b, c, ma, mb, mc); }
+double tt_wigner_6j(int a, int b, int c, int d, int e, int f) { return wigner6j(a, b, c, d, e, f); }
+double tt_wigner_9j(int a, int b, int c, int d, int e, int f, int g, int h, int i) {
+  return wigner9j(a, b, c, d, e, f, g, h, i);
+}
+double tt_clebsch_gordan(int j1, int j2, int j3, int m1, int m2, int m3) {
+  return clebsch_gordan(j1, j2, j3, m1, m2, m3);
+}
+int tt_legendre_spharm_array(int lmax, double x, double* out) {
+  if (lmax < 0 || !out) return fail(TT_ERR_BADARG, "bad argument");
+  legendre_spharm_array(lmax, x, out);
+  return TT_OK;
+}
+int tt_gauss_legendre(int n, double* x, double* w) {
+  if (n < 1 || !x || !w) return fail(TT_ERR_BADARG, "bad argument");
+  gauss_legendre(x, w, n);
+  return TT_OK;
+}
 const char* tt_last_error_string(void) { return last_error(); }
 
 int tt_device_count(int* count) {
@@ -310,6 +337,8 @@ int tt_run_create(tt_run** out, int nopt, const char* const* opts) {
 void tt_run_destroy(tt_run* run) {
   if (!run) return;
   run->chn.clear();
+  if (run->ev0) cudaEventDestroy(run->ev0);
+  if (run->ev1) cudaEventDestroy(run->ev1);
   if (run->stream) cudaStreamDestroy(run->stream);
   delete run;
 }
@@ -434,6 +463,34 @@ int tt_run_release_channel(tt_run* run, int chn) {
   int s = check_chn(run, chn);
   if (s) return s;
   run->chn[chn] = ChannelState();
+  return TT_OK;
+}
+
+int tt_run_release_A(tt_run* run, int chn) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (run->chn[chn].solver) run->chn[chn].solver->release_A();
+  run->chn[chn].have_A = false;
+  run->chn[chn].have_G = false;
+  return TT_OK;
+}
+
+int tt_run_timer_start(tt_run* run) {
+  if (!run) return fail(TT_ERR_BADARG, "null run");
+  cudaStream_t st = run_stream(run);
+  if (!run->ev0) TT_CUDA_TRY(cudaEventCreate(&run->ev0));
+  if (!run->ev1) TT_CUDA_TRY(cudaEventCreate(&run->ev1));
+  TT_CUDA_TRY(cudaEventRecord(run->ev0, st));
+  return TT_OK;
+}
+
+int tt_run_timer_stop(tt_run* run, double* ms) {
+  if (!run || !ms || !run->ev0) return fail(TT_ERR_BADARG, "timer not started");
+  TT_CUDA_TRY(cudaEventRecord(run->ev1, run_stream(run)));
+  TT_CUDA_TRY(cudaEventSynchronize(run->ev1));
+  float f = 0;
+  TT_CUDA_TRY(cudaEventElapsedTime(&f, run->ev0, run->ev1));
+  *ms = f;
   return TT_OK;
 }
 

@@ -437,9 +437,11 @@ int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, i
     TT_CUDA_TRY(cudaMemsetAsync(ws.err.ptr, 0, sizeof(int), st));
   }
   tc::k_split_L<<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L, ldl, M, K, ws.WA.ptr);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
   tc::k_split_U<<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   CUtensorMap mA, mB;
   TT_TRY(make_map(&mA, ws.WA.ptr, (uint64_t)M, (uint64_t)4 * K, tc::BM));
@@ -453,6 +455,7 @@ int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, i
   const int tiles = ((M + tc::BM - 1) / tc::BM) * ((N + tc::BN - 1) / tc::BN);
   const int grid = std::min(tiles, device_sm_count());
   tc::k_lu_update_tc<<<grid, tc::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, ws.err.ptr);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }

@@ -307,22 +307,27 @@ int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_te
       int* inf = d_info.ptr;
       void* args[] = {&Ap, &nn, &kk, &kbb, &ip, &rv, &ri, &inf};
       TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_panel<T>, dim3(sms), dim3(256), args, 0, st));
+      count_launch();
     }
     if (k > 0) {
       k_laswp<T><<<ceil_div(k, 256), 256, 0, st>>>(d_L, n, k, kb, d_ipiv, 0, k);
+      count_launch();
       TT_CUDA_TRY(cudaGetLastError());
     }
     const int rest = n - k - kb;
     if (rest > 0) {
       k_laswp<T><<<ceil_div(rest, 256), 256, 0, st>>>(d_L, n, k, kb, d_ipiv, k + kb, n);
+      count_launch();
       TT_CUDA_TRY(cudaGetLastError());
       k_trsm<T><<<ceil_div(rest, 32), 256, trsm_smem, st>>>(d_L, n, k, kb);
+      count_launch();
       TT_CUDA_TRY(cudaGetLastError());
       if (use_tensor_cores) {
         TT_TRY(lu_update_tc(d_L, n, k, kb, st));
       } else {
         dim3 grid(ceil_div(rest, 64), ceil_div(rest, 64));
         k_gemm_update<T><<<grid, 256, 0, st>>>(d_L, n, k, kb);
+        count_launch();
         TT_CUDA_TRY(cudaGetLastError());
       }
     }
@@ -448,13 +453,16 @@ int lu_solve_device(const T* d_LU, int n, const int32_t* d_ipiv, double* d_x, in
   TT_CUDA_TRY(cudaMemcpyAsync(d_tmp.ptr, d_x, sizeof(double2) * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, st));
   double2* x = reinterpret_cast<double2*>(d_x);
   k_permute<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(d_tmp.ptr, d_perm.ptr, n, nrhs, x);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   // forward: unit lower
   for (int i0 = 0; i0 < n; i0 += SB) {
     const int bs = min(SB, n - i0);
     k_diag_solve<T, true><<<1, 256, 0, st>>>(d_LU, n, i0, bs, x, nrhs);
+    count_launch();
     const int r_lo = i0 + bs;
     if (r_lo < n) k_block_update<T><<<ceil_div((size_t)(n - r_lo) * 32, 256), 256, 0, st>>>(d_LU, n, i0, bs, r_lo, n, x, nrhs);
+    count_launch();
   }
   TT_CUDA_TRY(cudaGetLastError());
   // backward: upper with diagonal
@@ -462,7 +470,9 @@ int lu_solve_device(const T* d_LU, int n, const int32_t* d_ipiv, double* d_x, in
   for (int b = nblk - 1; b >= 0; b--) {
     const int i0 = b * SB, bs = min(SB, n - i0);
     k_diag_solve<T, false><<<1, 256, 0, st>>>(d_LU, n, i0, bs, x, nrhs);
+    count_launch();
     if (i0 > 0) k_block_update<T><<<ceil_div((size_t)i0 * 32, 256), 256, 0, st>>>(d_LU, n, i0, bs, 0, i0, x, nrhs);
+    count_launch();
   }
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;

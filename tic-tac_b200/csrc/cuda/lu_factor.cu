@@ -1,0 +1,403 @@
+// Blocked right-looking LU with partial pivoting of the complex Faddeev kernel
+// matrix 1 - A G (row-major, in place).  Replaces the LAPACK zgetrf of the
+// reference's dense solver (CPP/General_functions/matrix_routines.cpp:73-80).
+//
+// Outer panels of NB columns (256 for the complex64 / tensor-core path, 128
+// for complex128).  Each panel is factored in IB = 32 column sub-panels:
+//   k_subpanel   cooperative kernel, ONE grid barrier per column: every block
+//                publishes its best pivot candidate together with a copy of
+//                that row (and the owner of the diagonal row publishes it), so
+//                after the barrier every block knows the pivot row's values and
+//                the two owners swap their rows without a second barrier
+//   k_laswp2     the sub-panel's interchanges on the rest of the panel
+//   k_trsm_blk   U = L^{-1} U for the 32-wide unit-lower diagonal block
+//   k_gemm_sub   rank-32 update of the remaining panel columns (CUDA cores)
+// then the panel's interchanges outside the panel, the blocked triangular
+// solve for U12 and the trailing update A22 -= L21 U12 (tcgen05 BF16x3 for
+// complex64, CUDA-core complex GEMM for complex128).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "tt_kernels.h"
+#include "tt_lu_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace tt {
+namespace {
+
+template <typename T>
+struct Real;
+template <>
+struct Real<double2> {
+  using R = double;
+};
+template <>
+struct Real<float2> {
+  using R = float;
+};
+
+template <typename T>
+__device__ __forceinline__ T cdiv_smith(T a, T b) {
+  using R = typename Real<T>::R;
+  T r;
+  if (fabs((double)b.x) >= fabs((double)b.y)) {
+    const R t = b.y / b.x, d = b.x + b.y * t;
+    r.x = (a.x + a.y * t) / d;
+    r.y = (a.y - a.x * t) / d;
+  } else {
+    const R t = b.x / b.y, d = b.y + b.x * t;
+    r.x = (a.x * t + a.y) / d;
+    r.y = (a.y * t - a.x) / d;
+  }
+  return r;
+}
+
+constexpr int IB = 32;
+
+template <typename T>
+struct PivotScratch {
+  double* val;  // [2][G]
+  int* idx;     // [2][G]
+  T* row;       // [2][G][IB]
+  T* top;       // [2][IB]
+};
+
+// Sub-panel rows [c0, n), columns [c0, c0+w), w <= IB.
+template <typename T>
+__global__ void __launch_bounds__(256) k_subpanel(T* __restrict__ A, int n, int c0, int w, int32_t* __restrict__ ipiv,
+                                                  PivotScratch<T> scr, int* __restrict__ info) {
+  cg::grid_group grid = cg::this_grid();
+  const int G = gridDim.x;
+  const int m = n - c0;
+  const int chunk = (m + G - 1) / G;
+  const int lo = c0 + blockIdx.x * chunk;
+  const int hi = min(n, lo + chunk);
+  __shared__ double s_val[256];
+  __shared__ int s_idx[256];
+  __shared__ T s_prow[IB];
+  __shared__ int s_piv;
+  __shared__ int s_zero;
+  for (int jj = 0; jj < w; jj++) {
+    const int j = c0 + jj;  // diagonal row/column
+    const int buf = jj & 1;
+    // 1. local candidate among own rows >= j
+    double best = -1.0;
+    int bidx = -1;
+    for (int i = max(lo, j) + threadIdx.x; i < hi; i += blockDim.x) {
+      const T v = A[(size_t)i * n + j];
+      const double a = fabs((double)v.x) + fabs((double)v.y);
+      if (a > best || (a == best && i < bidx)) {
+        best = a;
+        bidx = i;
+      }
+    }
+    s_val[threadIdx.x] = best;
+    s_idx[threadIdx.x] = bidx;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) {
+        const double o = s_val[threadIdx.x + s];
+        const int oi = s_idx[threadIdx.x + s];
+        const double mv = s_val[threadIdx.x];
+        const int mi = s_idx[threadIdx.x];
+        if (oi >= 0 && (mi < 0 || o > mv || (o == mv && oi < mi))) {
+          s_val[threadIdx.x] = o;
+          s_idx[threadIdx.x] = oi;
+        }
+      }
+      __syncthreads();
+    }
+    const int cand = s_idx[0];
+    if (threadIdx.x == 0) {
+      scr.val[buf * G + blockIdx.x] = s_val[0];
+      scr.idx[buf * G + blockIdx.x] = cand;
+    }
+    if (cand >= 0 && threadIdx.x < w) scr.row[((size_t)buf * G + blockIdx.x) * IB + threadIdx.x] = A[(size_t)cand * n + c0 + threadIdx.x];
+    if (j >= lo && j < hi && threadIdx.x < w) scr.top[buf * IB + threadIdx.x] = A[(size_t)j * n + c0 + threadIdx.x];
+    grid.sync();
+    // 2. global pivot (every block, same rule)
+    if (threadIdx.x == 0) {
+      double bv = -1.0;
+      int bi = -1, bg = -1;
+      for (int g = 0; g < G; g++) {
+        const int vi = scr.idx[buf * G + g];
+        if (vi < 0) continue;
+        const double v = scr.val[buf * G + g];
+        if (v > bv || (v == bv && vi < bi)) {
+          bv = v;
+          bi = vi;
+          bg = g;
+        }
+      }
+      s_piv = bi;
+      s_zero = !(bv > 0.0);
+      if (blockIdx.x == 0) {
+        ipiv[j] = s_zero ? j : bi;
+        if (s_zero && *info == 0) *info = j + 1;
+      }
+      s_idx[0] = bg;
+    }
+    __syncthreads();
+    const int piv = s_piv;
+    if (s_zero) {
+      __syncthreads();
+      continue;
+    }
+    const int winner = s_idx[0];
+    if (threadIdx.x < w) s_prow[threadIdx.x] = scr.row[((size_t)buf * G + winner) * IB + threadIdx.x];
+    __syncthreads();
+    // 3. the two owners exchange rows j and piv (sub-panel columns only)
+    if (piv != j) {
+      if (piv >= lo && piv < hi && threadIdx.x < w)
+        A[(size_t)piv * n + c0 + threadIdx.x] = scr.top[buf * IB + threadIdx.x];
+      if (j >= lo && j < hi && threadIdx.x < w) A[(size_t)j * n + c0 + threadIdx.x] = s_prow[threadIdx.x];
+    } else if (j >= lo && j < hi && threadIdx.x < w) {
+      A[(size_t)j * n + c0 + threadIdx.x] = s_prow[threadIdx.x];
+    }
+    __syncthreads();
+    // 4. eliminate below the diagonal in own rows
+    const T d = s_prow[jj];
+    const int r0 = max(lo, j + 1);
+    const int ncol = w - jj - 1;
+    for (int i = r0 + threadIdx.x; i < hi; i += blockDim.x) {
+      T* row = A + (size_t)i * n + c0;
+      const T l = cdiv_smith(row[jj], d);
+      row[jj] = l;
+      for (int c = 1; c <= ncol; c++) {
+        const T u = s_prow[jj + c];
+        T a = row[jj + c];
+        a.x -= l.x * u.x - l.y * u.y;
+        a.y -= l.x * u.y + l.y * u.x;
+        row[jj + c] = a;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Interchanges of pivots [p0, p1) applied to columns [a0, a1) and [b0, b1).
+template <typename T>
+__global__ void k_laswp2(T* __restrict__ A, int n, const int32_t* __restrict__ ipiv, int p0, int p1, int a0, int a1,
+                         int b0, int b1) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = a1 - a0;
+  int c;
+  if (t < na) c = a0 + t;
+  else if (t - na < b1 - b0) c = b0 + (t - na);
+  else return;
+  for (int j = p0; j < p1; j++) {
+    const int p = ipiv[j];
+    if (p != j) {
+      const T tmp = A[(size_t)j * n + c];
+      A[(size_t)j * n + c] = A[(size_t)p * n + c];
+      A[(size_t)p * n + c] = tmp;
+    }
+  }
+}
+
+// X <- L^{-1} X, L the w x w unit-lower block at (r0, r0), X = rows [r0, r0+w) of columns [cb, ce).
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsm_blk(T* __restrict__ A, int n, int r0, int w, int cb, int ce) {
+  __shared__ T sL[IB][IB + 1];
+  __shared__ T sX[IB][33];
+  const int c0 = cb + blockIdx.x * 32;
+  for (int t = threadIdx.x; t < w * w; t += blockDim.x) sL[t / w][t % w] = A[(size_t)(r0 + t / w) * n + r0 + t % w];
+  for (int t = threadIdx.x; t < w * 32; t += blockDim.x) {
+    const int i = t / 32, c = c0 + t % 32;
+    T v;
+    v.x = 0;
+    v.y = 0;
+    if (c < ce) v = A[(size_t)(r0 + i) * n + c];
+    sX[i][t % 32] = v;
+  }
+  __syncthreads();
+  const int cc = threadIdx.x % 32, grp = threadIdx.x / 32;
+  for (int i = 0; i < w; i++) {
+    const T xi = sX[i][cc];
+    for (int r = i + 1 + grp; r < w; r += 8) {
+      const T l = sL[r][i];
+      T v = sX[r][cc];
+      v.x -= l.x * xi.x - l.y * xi.y;
+      v.y -= l.x * xi.y + l.y * xi.x;
+      sX[r][cc] = v;
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < w * 32; t += blockDim.x) {
+    const int i = t / 32, c = c0 + t % 32;
+    if (c < ce) A[(size_t)(r0 + i) * n + c] = sX[i][t % 32];
+  }
+}
+
+// C[M x N] -= L[M x K] U[K x N], complex, leading dimensions ld*; 64 x 64 tiles.
+template <typename T>
+__global__ void __launch_bounds__(256) k_gemm_sub(T* __restrict__ C, int ldc, const T* __restrict__ L, int ldl,
+                                                  const T* __restrict__ U, int ldu, int M, int N, int K) {
+  using R = typename Real<T>::R;
+  constexpr int BM = 64, BN = 64, BK = 16;
+  __shared__ T sA[BK][BM + 1];
+  __shared__ T sB[BK][BN + 1];
+  const int r0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  R ar[4][4], ai[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) ar[i][j] = ai[i][j] = 0;
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    for (int t = threadIdx.x; t < BM * BK; t += 256) {
+      const int i = t / BK, q = t % BK;
+      T v;
+      v.x = 0;
+      v.y = 0;
+      if (r0 + i < M && k0 + q < K) v = L[(size_t)(r0 + i) * ldl + k0 + q];
+      sA[q][i] = v;
+    }
+    for (int t = threadIdx.x; t < BK * BN; t += 256) {
+      const int q = t / BN, j = t % BN;
+      T v;
+      v.x = 0;
+      v.y = 0;
+      if (c0 + j < N && k0 + q < K) v = U[(size_t)(k0 + q) * ldu + c0 + j];
+      sB[q][j] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < BK; q++) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = sA[q][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = sB[q][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          ar[i][j] += a[i].x * b[j].x - a[i].y * b[j].y;
+          ai[i][j] += a[i].x * b[j].y + a[i].y * b[j].x;
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int r = r0 + ty + 16 * i;
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int c = c0 + tx + 16 * j;
+      if (c >= N) continue;
+      T v = C[(size_t)r * ldc + c];
+      v.x -= ar[i][j];
+      v.y -= ai[i][j];
+      C[(size_t)r * ldc + c] = v;
+    }
+  }
+}
+
+template <typename T>
+int gemm_sub(T* C, int ldc, const T* L, int ldl, const T* U, int ldu, int M, int N, int K, cudaStream_t st) {
+  if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
+  dim3 grid(ceil_div(N, 64), ceil_div(M, 64));
+  k_gemm_sub<T><<<grid, 256, 0, st>>>(C, ldc, L, ldl, U, ldu, M, N, K);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+template <typename T>
+int laswp2(T* A, int n, const int32_t* ipiv, int p0, int p1, int a0, int a1, int b0, int b1, cudaStream_t st) {
+  const int cols = std::max(0, a1 - a0) + std::max(0, b1 - b0);
+  if (cols <= 0 || p1 <= p0) return TT_OK;
+  k_laswp2<T><<<ceil_div(cols, 256), 256, 0, st>>>(A, n, ipiv, p0, p1, a0, std::max(a0, a1), b0, std::max(b0, b1));
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+template <typename T>
+int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st) {
+  if (ce <= cb) return TT_OK;
+  k_trsm_blk<T><<<ceil_div(ce - cb, 32), 256, 0, st>>>(A, n, r0, w, cb, ce);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+}  // namespace
+
+template <typename T>
+int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {
+  const bool tc = use_tc != 0;
+  if (tc && sizeof(T) != sizeof(float2)) {
+    set_error("tensor-core trailing update is only defined for the complex64 factorisation");
+    return TT_ERR_UNSUPPORTED;
+  }
+  const int NB = (sizeof(T) == sizeof(float2)) ? 256 : 128;
+  const int G = device_sm_count();
+  DevBuf<double> sval;
+  DevBuf<int> sidx, d_info;
+  DevBuf<T> srow, stop;
+  TT_TRY(sval.alloc(2 * (size_t)G));
+  TT_TRY(sidx.alloc(2 * (size_t)G));
+  TT_TRY(srow.alloc(2 * (size_t)G * IB));
+  TT_TRY(stop.alloc(2 * (size_t)IB));
+  TT_TRY(d_info.alloc(1));
+  TT_CUDA_TRY(cudaMemsetAsync(d_info.ptr, 0, sizeof(int), st));
+  PivotScratch<T> scr{sval.ptr, sidx.ptr, srow.ptr, stop.ptr};
+  for (int k = 0; k < n; k += NB) {
+    const int kb = std::min(NB, n - k);
+    // ---- panel [k, k+kb) in sub-panels of IB columns
+    for (int j0 = k; j0 < k + kb; j0 += IB) {
+      const int w = std::min(IB, k + kb - j0);
+      {
+        T* Ap = A;
+        int nn = n, cc0 = j0, ww = w;
+        int32_t* ip = ipiv;
+        int* inf = d_info.ptr;
+        void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
+        TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
+        count_launch();
+      }
+      TT_TRY(laswp2(A, n, ipiv, j0, j0 + w, k, j0, j0 + w, k + kb, st));
+      const int right = k + kb - (j0 + w);
+      if (right > 0) {
+        TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
+        TT_TRY(gemm_sub(A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
+                        A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
+      }
+    }
+    // ---- interchanges outside the panel
+    TT_TRY(laswp2(A, n, ipiv, k, k + kb, 0, k, k + kb, n, st));
+    const int rest = n - k - kb;
+    if (rest <= 0) continue;
+    // ---- U12 = L11^{-1} A12, blocked by IB
+    for (int i0 = k; i0 < k + kb; i0 += IB) {
+      const int wi = std::min(IB, k + kb - i0);
+      TT_TRY(trsm_blk(A, n, i0, wi, k + kb, n, st));
+      const int below = k + kb - (i0 + wi);
+      if (below > 0)
+        TT_TRY(gemm_sub(A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
+                        A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
+    }
+    // ---- trailing update
+    if (tc) {
+      TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
+    } else {
+      TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
+                      A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
+    }
+  }
+  if (tc) TT_TRY(tc_check_error(st));
+  if (info) {
+    TT_CUDA_TRY(cudaMemcpyAsync(info, d_info.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TT_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  return TT_OK;
+}
+template int lu_factor_device<double2>(double2*, int, int32_t*, cudaStream_t, int, int*);
+template int lu_factor_device<float2>(float2*, int, int32_t*, cudaStream_t, int, int*);
+
+}  // namespace tt

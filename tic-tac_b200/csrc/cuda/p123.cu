@@ -339,6 +339,7 @@ int p123_build_device(const P123Tables& t, DeviceCSR& out, cudaStream_t st, P123
   TT_TRY(d_mask.alloc(ncell_all));
   k_overlap<<<ceil_div(ncell_all, 128), 128, 0, st>>>(d_pb.ptr, d_qb.ptr, Np, Nq, d_x.ptr, Nx, d_phi_ok.ptr,
                                                       d_sin.ptr, d_cos.ptr, Nphi, d_mask.ptr);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   std::vector<uint8_t> mask(ncell_all);
   TT_CUDA_TRY(cudaMemcpyAsync(mask.data(), d_mask.ptr, ncell_all, cudaMemcpyDeviceToHost, st));
@@ -397,6 +398,7 @@ int p123_build_device(const P123Tables& t, DeviceCSR& out, cudaStream_t st, P123
   TT_TRY(d_W.alloc((size_t)ncell * K));
   k_cell_weights<<<ncell, 256, 0, st>>>(d_cells.ptr, d_pb.ptr, d_qb.ptr, Np, d_x.ptr, d_wx.ptr, Nx, d_sin.ptr,
                                         d_cos.ptr, d_wphi.ptr, Nphi, d_W.ptr);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   TT_TRY(d_Pv.alloc((size_t)ncell * npairs));
   // batches of bra rows so that Gtilde stays within ~4 GB
@@ -412,13 +414,16 @@ int p123_build_device(const P123Tables& t, DeviceCSR& out, cudaStream_t st, P123
     k_legendre<<<ceil_div((size_t)nb * K, 128), 128, 0, st>>>((int)r0, nb, d_x.ptr, Nx, d_sin.ptr, d_cos.ptr, Nphi,
                                                              t.max_L12, t.lenL, t.max_l3, t.lenl, d_plm2.ptr,
                                                              d_plm3.ptr);
+    count_launch();
     TT_CUDA_TRY(cudaGetLastError());
     dim3 gg(ceil_div(K, 128), npairs, nb);
     k_gtilde<<<gg, 128, 0, st>>>(nb, npairs, K, Nx, d_pair_off.ptr, d_terms.ptr, d_pnorm.ptr, d_plm1.ptr, t.lenl,
                                  d_plm2.ptr, t.lenL, d_plm3.ptr, d_G.ptr);
+    count_launch();
     TT_CUDA_TRY(cudaGetLastError());
     dim3 gc(ceil_div(npairs, CT_P), nb);
     k_contract<<<gc, 256, 0, st>>>((int)r0, d_rco.ptr, npairs, K, d_W.ptr, d_G.ptr, d_Pv.ptr);
+    count_launch();
     TT_CUDA_TRY(cudaGetLastError());
   }
   DevBuf<int64_t> d_counts;
@@ -426,6 +431,7 @@ int p123_build_device(const P123Tables& t, DeviceCSR& out, cudaStream_t st, P123
   TT_CUDA_TRY(cudaMemsetAsync(d_counts.ptr + n, 0, sizeof(int64_t), st));
   k_row_count<<<ceil_div((size_t)n * 32, 256), 256, 0, st>>>(Na, Nq, Np, d_ap_lo.ptr, d_rco.ptr, npairs, d_Pv.ptr,
                                                            d_counts.ptr);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   size_t tmp_bytes = 0;
   TT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_counts.ptr, out.rowptr.ptr, n + 1, st));
@@ -441,6 +447,7 @@ int p123_build_device(const P123Tables& t, DeviceCSR& out, cudaStream_t st, P123
   k_row_fill<<<ceil_div((size_t)n * 32, 256), 256, 0, st>>>(Na, Nq, Np, d_ap_lo.ptr, d_pair_a.ptr, d_rco.ptr,
                                                           d_cells.ptr, d_cnorm.ptr, npairs, d_Pv.ptr,
                                                           out.rowptr.ptr, out.col.ptr, out.val.ptr);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   TT_CUDA_TRY(cudaStreamSynchronize(st));
   return TT_OK;

@@ -285,6 +285,7 @@ int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d
   if (total == 0) return TT_OK;
   k_resolvent<<<ceil_div(total, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, L.e_off.ptr, L.e_swp.ptr, L.q_WP.ptr, d_E,
                                                     nE, reinterpret_cast<double2*>(d_G));
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
@@ -301,6 +302,7 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, doubl
     k_pvc<<<ceil_div(warps * 32, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
                                                      L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr, L.blk_off.ptr,
                                                      L.blk_dim.ptr, L.VC.ptr, d_B);
+    count_launch();
     TT_CUDA_TRY(cudaGetLastError());
   }
   int max_cpl = 1;
@@ -312,6 +314,7 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, doubl
   if (smem > 48 * 1024) TT_CUDA_TRY(cudaFuncSetAttribute(k_ct<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_ct<32><<<grid, 256, smem, st>>>(L.Nalpha, L.Nq, L.Np, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
                                     L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, d_B, d_A);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
@@ -320,6 +323,7 @@ template <typename T>
 int form_L_device(const double* d_A, const double* d_G, int n, T* d_L, cudaStream_t st) {
   const size_t total = (size_t)n * n;
   k_form_L<T><<<ceil_div(total, 256), 256, 0, st>>>(d_A, reinterpret_cast<const double2*>(d_G), n, d_L);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
@@ -328,6 +332,7 @@ template int form_L_device<float2>(const double*, const double*, int, float2*, c
 
 int gather_rhs_device(const double* d_A, int n, const int32_t* d_cols, int nrhs, double* d_b, cudaStream_t st) {
   k_gather_rhs<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(d_A, n, d_cols, nrhs, reinterpret_cast<double2*>(d_b));
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
@@ -337,6 +342,7 @@ int hadamard_device(const double* d_G, const int32_t* d_rhs_e, int n, const doub
   k_hadamard<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_G), d_rhs_e, n,
                                                              reinterpret_cast<const double2*>(d_x), nrhs,
                                                              reinterpret_cast<double2*>(d_y));
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
@@ -346,6 +352,7 @@ int residual_multi_device(const double* d_A, int n, const double* d_y, const dou
   k_residual<<<ceil_div((size_t)n * 32, 256), 256, 0, st>>>(
       d_A, n, reinterpret_cast<const double2*>(d_y), reinterpret_cast<const double2*>(d_b),
       reinterpret_cast<const double2*>(d_x), nrhs, reinterpret_cast<double2*>(d_r));
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
@@ -357,6 +364,7 @@ int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h
   k_axpy_norm<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<double2*>(d_x),
                                                               reinterpret_cast<const double2*>(d_d), n, nrhs, mx.ptr,
                                                               mx.ptr + nrhs);
+  count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   std::vector<unsigned long long> h(2 * (size_t)nrhs);
   TT_CUDA_TRY(cudaMemcpyAsync(h.data(), mx.ptr, sizeof(unsigned long long) * 2 * nrhs, cudaMemcpyDeviceToHost, st));

@@ -13,6 +13,9 @@ namespace tt {
 void set_error(const std::string& msg);
 const char* last_error();
 
+// Count of kernels this library has launched (reported by tt_kernel_launches).
+void count_launch();
+
 #define TT_CUDA_TRY(expr)                                                                   \
   do {                                                                                      \
     cudaError_t _e = (expr);                                                                \

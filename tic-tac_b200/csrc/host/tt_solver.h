@@ -41,6 +41,11 @@ class ChannelSolver {
   // U[d'*nd*nE + d*nE + j] for each on-shell q bin j and deuteron states
   int solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
             std::vector<double>& U_interleaved, SolveReport* rep, cudaStream_t st);
+  void release_A() {
+    A_.release();
+    G_.release();
+    nE_ = 0;
+  }
   const DeviceCSR& P() const { return P_; }
   const double* A() const { return A_.ptr; }
   const double* G() const { return G_.ptr; }

@@ -34,7 +34,9 @@ EXPORTED_SYMBOLS = (
     "tt_run_destroy", "tt_run_num_channels", "tt_run_channel_info", "tt_run_num_energies", "tt_run_energies",
     "tt_run_E_bound", "tt_run_build_P123", "tt_run_build_A", "tt_run_build_resolvent", "tt_run_solve",
     "tt_run_release_channel", "tt_run_get_P123_csr", "tt_run_get_A", "tt_run_get_G", "tt_run_get_host_array",
-    "tt_run_write_U_table",
+    "tt_run_write_U_table", "tt_run_release_A", "tt_run_timer_start", "tt_run_timer_stop", "tt_kernel_launches",
+    "tt_wigner_3j", "tt_wigner_6j", "tt_wigner_9j", "tt_clebsch_gordan", "tt_legendre_spharm_array",
+    "tt_gauss_legendre",
 )
 
 
@@ -96,6 +98,9 @@ def load(path: str = LIB_PATH):
     lib.tt_run_destroy.restype = None
     lib.tt_free.restype = None
     lib.tt_run_params_default.restype = None
+    lib.tt_kernel_launches.restype = ctypes.c_ulonglong
+    for f in ("tt_wigner_3j", "tt_wigner_6j", "tt_wigner_9j", "tt_clebsch_gordan"):
+        getattr(lib, f).restype = c_double
     _lib = lib
     return lib
 
@@ -118,6 +123,39 @@ def device_count() -> int:
     n = c_int(0)
     rc = lib.tt_device_count(byref(n))
     return n.value if rc == TT_OK else 0
+
+
+def kernel_launches() -> int:
+    return int(load().tt_kernel_launches())
+
+
+def wigner3j(*a):
+    return load().tt_wigner_3j(*[int(x) for x in a])
+
+
+def wigner6j(*a):
+    return load().tt_wigner_6j(*[int(x) for x in a])
+
+
+def wigner9j(*a):
+    return load().tt_wigner_9j(*[int(x) for x in a])
+
+
+def clebsch_gordan(*a):
+    return load().tt_clebsch_gordan(*[int(x) for x in a])
+
+
+def spharm_array(lmax, x):
+    out = np.zeros((lmax + 1) * (lmax + 2) // 2)
+    _check(load().tt_legendre_spharm_array(int(lmax), c_double(x), _dptr(out)))
+    return out
+
+
+def gauss_legendre(n):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    _check(load().tt_gauss_legendre(int(n), _dptr(x), _dptr(w)))
+    return x, w
 
 
 def run_params(**kw) -> tt_run_params:
@@ -306,6 +344,17 @@ class Run:
 
     def release(self, chn):
         _check(self.lib.tt_run_release_channel(self._h, chn))
+
+    def release_A(self, chn):
+        _check(self.lib.tt_run_release_A(self._h, chn))
+
+    def timer_start(self):
+        _check(self.lib.tt_run_timer_start(self._h))
+
+    def timer_stop(self):
+        ms = c_double()
+        _check(self.lib.tt_run_timer_stop(self._h, byref(ms)))
+        return ms.value
 
     def write_U_table(self, chn, U, path):
         U = np.ascontiguousarray(U, dtype=np.complex128)
