@@ -6,16 +6,18 @@
 // product is accumulated in FP32 in tensor memory as
 //   Re += Lr.Ur - Li.Ui ,  Im += Lr.Ui + Li.Ur
 // with every real product taken as hi.hi + hi.lo + lo.hi (BF16x3), i.e. 12
-// tcgen05.mma (kind::f16, M=128, N=64, K=16) per 16-deep k step; the negative
-// terms use the instruction descriptor's negate-A bit.
+// tcgen05.mma (kind::f16, M=128, N=128, K=16) per 16-deep k step; the
+// negative terms use the instruction descriptor's negate-A bit.
 //
-// Kernel organisation (one CTA per SM, persistent over 128 x 64 output tiles):
+// Kernel organisation (one CTA per SM, persistent over 128 x 128 output tiles):
 //   warp 0      TMA producer: cp.async.bulk.tensor loads of the bf16 parts of
-//               L (4 x 16 KB) and U^T (4 x 8 KB) per 64-deep k chunk into a
-//               2-stage ring of 128B-swizzled shared memory
+//               L (4 x 8 KB) and U^T (4 x 8 KB) per 32-deep k chunk into a
+//               3-stage ring of 64B-swizzled shared memory
 //   warp 1      MMA issuer (one elected thread), accumulators double-buffered
-//               in TMEM (2 x (64 Re + 64 Im) columns)
-//   warps 2..5  epilogue: tcgen05.ld of the accumulators, C -= acc in place
+//               in TMEM (2 x (128 Re + 128 Im) columns = all 512)
+//   warps 2..9  epilogue: tcgen05.ld of a 32-row x 16-column accumulator
+//               slice, staged through swizzled shared memory, then a
+//               coalesced C -= acc read-modify-write
 // Every mbarrier wait is bounded in time; on expiry the kernel records an
 // error code, drains its own copies in flight, frees TMEM and returns.
 #include <cuda.h>
@@ -31,14 +33,16 @@ namespace tt {
 namespace tc {
 
 constexpr int BM = 128;           // rows per tile (MMA M)
-constexpr int BN = 64;            // complex columns per tile (MMA N)
-constexpr int KC = 64;            // k elements per chunk (128 B of bf16 = one swizzle row)
-constexpr int STAGES = 2;
-constexpr int A_PART_BYTES = BM * KC * 2;  // 16 KB
+constexpr int BN = 128;           // complex columns per tile (MMA N)
+constexpr int KC = 32;            // k elements per chunk (64 B of bf16 = one swizzle row)
+constexpr int STAGES = 3;
+constexpr int A_PART_BYTES = BM * KC * 2;  // 8 KB
 constexpr int B_PART_BYTES = BN * KC * 2;  // 8 KB
-constexpr int STAGE_BYTES = 4 * A_PART_BYTES + 4 * B_PART_BYTES;  // 96 KB
-constexpr int TMEM_COLS = 256;    // 2 accumulators x (BN re + BN im)
-constexpr int NUM_THREADS = 192;  // 6 warps
+constexpr int STAGE_BYTES = 4 * A_PART_BYTES + 4 * B_PART_BYTES;  // 64 KB
+constexpr int TMEM_COLS = 512;    // 2 accumulators x (BN re + BN im)
+constexpr int EPI_WARPS = 8;
+constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;  // producer, MMA, epilogue
+constexpr int EPI_STAGE_BYTES = 32 * 16 * 8;      // 32 rows x 16 complex per epilogue warp
 constexpr uint64_t WAIT_NS = 2000000000ull;  // 2 s bound on any single wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -91,18 +95,18 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// K-major, 128B-swizzled operand: rows of 128 B, 8-row atoms 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// K-major, 64B-swizzled operand: rows of 64 B, 8-row atoms 512 B apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);  // start address
   d |= (uint64_t)1 << 16;                    // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;          // stride byte offset: next 8-row atom
+  d |= (uint64_t)(512 >> 4) << 32;           // stride byte offset: next 8-row atom
   d |= (uint64_t)1 << 46;                    // descriptor version for tcgen05
-  d |= (uint64_t)2 << 61;                    // SWIZZLE_128B
+  d |= (uint64_t)4 << 61;                    // SWIZZLE_64B
   return d;
 }
 
-// kind::f16 instruction descriptor: D f32, A/B bf16, K-major, M=128, N=64.
+// kind::f16 instruction descriptor: D f32, A/B bf16, K-major, M=128, N=128.
 __host__ __device__ constexpr uint32_t idesc_bf16(bool negA) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((negA ? 1u : 0u) << 13) | ((uint32_t)(BN >> 3) << 17) |
          ((uint32_t)(BM >> 4) << 24);
@@ -159,7 +163,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                    int ldc, int M, int N, int K, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+  float2* epi_stage = (float2*)(smem + STAGES * STAGE_BYTES);
+  uint64_t* full = (uint64_t*)(smem + STAGES * STAGE_BYTES + EPI_WARPS * EPI_STAGE_BYTES);
   uint64_t* empty = full + STAGES;
   uint64_t* acc_full = empty + STAGES;
   uint64_t* acc_empty = acc_full + 2;
@@ -177,7 +182,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+      mbar_init(&acc_empty[b], EPI_WARPS);  // one arrival per epilogue warp
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -252,8 +257,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
           for (int ks = 0; ks < KC / 16; ks++) {
 #pragma unroll
             for (int q = 0; q < 12; q++) {
-              const uint64_t ad = sw128_desc(a0 + ta[q] * A_PART_BYTES + ks * 32);
-              const uint64_t bd = sw128_desc(b0 + tb[q] * B_PART_BYTES + ks * 32);
+              const uint64_t ad = sw64_desc(a0 + ta[q] * A_PART_BYTES + ks * 32);
+              const uint64_t bd = sw64_desc(b0 + tb[q] * B_PART_BYTES + ks * 32);
               const bool first = (kc == 0 && ks == 0 && (q == 0 || q == 6));
               const bool neg = (q >= 3 && q < 6);
               umma(q < 6 ? d_re : d_im, ad, bd, neg ? id_neg : id_pos, first ? 0u : 1u);
@@ -266,9 +271,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       }
     }
   } else {
-    // ---------------- epilogue (warps 2..5 -> TMEM lane quarters 2,3,0,1)
+    // ---------------- epilogue (warps 2..9): warp w reads TMEM lane quarter
+    // w % 4 (the hardware lane-access rule) and column half (w - 2) / 4
     const int quarter = warp & 3;
-    const int row_in_tile = quarter * 32 + lane;
+    const int half = (warp - 2) >> 2;
+    float2* stage = epi_stage + (size_t)(warp - 2) * (32 * 16);
     int local = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, local++) {
       int tm, tn;
@@ -277,25 +284,35 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       const uint32_t aph = (uint32_t)(local >> 1) & 1u;
       if (!mbar_wait(&acc_full[ab], aph, err, 4)) break;
       tc_fence_after();
-      const int row = tm * BM + row_in_tile;
       const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16) + ab * (2 * BN);
-#pragma unroll
-      for (int c0 = 0; c0 < BN; c0 += 16) {
+      const int row0 = tm * BM + quarter * 32;
+#pragma unroll 1
+      for (int cc = 0; cc < BN / 2; cc += 16) {
+        const int col = half * (BN / 2) + cc;
         float re[16], im[16];
-        tmem_ld16(lane_addr + c0, re);
-        tmem_ld16(lane_addr + BN + c0, im);
-        if (row < M) {
-          float2* crow = C + (size_t)row * ldc + (size_t)tn * BN + c0;
+        tmem_ld16(lane_addr + col, re);
+        tmem_ld16(lane_addr + BN + col, im);
+        // stage this thread's row (row = lane) with an XOR swizzle on the column
 #pragma unroll
-          for (int j = 0; j < 16; j++) {
-            if (tn * BN + c0 + j < N) {
-              float2 v = crow[j];
-              v.x -= re[j];
-              v.y -= im[j];
-              crow[j] = v;
-            }
-          }
+        for (int j = 0; j < 16; j++) stage[lane * 16 + (j ^ (lane & 15))] = make_float2(re[j], im[j]);
+        __syncwarp();
+        // coalesced read-modify-write: two rows of 16 complex per instruction
+        const int gcol0 = tn * BN + col;
+        float2 cv[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int idx = i * 32 + lane, r = idx >> 4, c = idx & 15;
+          const int grow = row0 + r, gcol = gcol0 + c;
+          cv[i] = (grow < M && gcol < N) ? C[(size_t)grow * ldc + gcol] : make_float2(0.f, 0.f);
         }
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int idx = i * 32 + lane, r = idx >> 4, c = idx & 15;
+          const int grow = row0 + r, gcol = gcol0 + c;
+          const float2 a = stage[r * 16 + (c ^ (r & 15))];
+          if (grow < M && gcol < N) C[(size_t)grow * ldc + gcol] = make_float2(cv[i].x - a.x, cv[i].y - a.y);
+        }
+        __syncwarp();
       }
       tc_fence_before();
       __syncwarp();
@@ -381,7 +398,7 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 2D bf16 tensor [rows][cols] row-major, box = 64 cols (128 B) x box_rows, 128B swizzle.
+// 2D bf16 tensor [rows][cols] row-major, box = 32 cols (64 B) x box_rows, 64B swizzle.
 int make_map(CUtensorMap* map, void* base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) {
@@ -393,7 +410,7 @@ int make_map(CUtensorMap* map, void* base, uint64_t rows, uint64_t cols, uint32_
   const cuuint32_t box[2] = {tc::KC, box_rows};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
@@ -419,7 +436,7 @@ int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, i
                 cudaStream_t st) {
   if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
   if (K % tc::KC != 0) {
-    set_error("tensor-core update needs K to be a multiple of 64");
+    set_error("tensor-core update needs K to be a multiple of 32");
     return TT_ERR_BADARG;
   }
   TCWorkspace& ws = workspace();
@@ -446,7 +463,7 @@ int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, i
   CUtensorMap mA, mB;
   TT_TRY(make_map(&mA, ws.WA.ptr, (uint64_t)M, (uint64_t)4 * K, tc::BM));
   TT_TRY(make_map(&mB, ws.WB.ptr, (uint64_t)N, (uint64_t)4 * K, tc::BN));
-  const size_t smem = (size_t)tc::STAGES * tc::STAGE_BYTES + 1024 + 256;
+  const size_t smem = (size_t)tc::STAGES * tc::STAGE_BYTES + tc::EPI_WARPS * tc::EPI_STAGE_BYTES + 1024 + 128;
   static bool attr = false;
   if (!attr) {
     TT_CUDA_TRY(cudaFuncSetAttribute(tc::k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -55,6 +55,8 @@ __device__ __forceinline__ T cdiv_smith(T a, T b) {
 }
 
 constexpr int IB = 32;
+constexpr int SP = IB + 1;                     // shared-memory row stride of a staged sub-panel
+constexpr size_t kSubpanelSmem = 220 * 1024;  // bound on one block's staged sub-panel rows
 
 template <typename T>
 struct PivotScratch {
@@ -77,8 +79,10 @@ __global__ void __launch_bounds__(256) k_subpanel(T* __restrict__ A, int n, int 
   __shared__ double s_val[256];
   __shared__ int s_idx[256];
   __shared__ T s_prow[IB];
+  __shared__ int s_grp[256];
   __shared__ int s_piv;
   __shared__ int s_zero;
+  __shared__ int s_win;
   for (int jj = 0; jj < w; jj++) {
     const int j = c0 + jj;  // diagonal row/column
     const int buf = jj & 1;
@@ -117,35 +121,55 @@ __global__ void __launch_bounds__(256) k_subpanel(T* __restrict__ A, int n, int 
     if (cand >= 0 && threadIdx.x < w) scr.row[((size_t)buf * G + blockIdx.x) * IB + threadIdx.x] = A[(size_t)cand * n + c0 + threadIdx.x];
     if (j >= lo && j < hi && threadIdx.x < w) scr.top[buf * IB + threadIdx.x] = A[(size_t)j * n + c0 + threadIdx.x];
     grid.sync();
-    // 2. global pivot (every block, same rule)
-    if (threadIdx.x == 0) {
-      double bv = -1.0;
-      int bi = -1, bg = -1;
-      for (int g = 0; g < G; g++) {
-        const int vi = scr.idx[buf * G + g];
-        if (vi < 0) continue;
-        const double v = scr.val[buf * G + g];
-        if (v > bv || (v == bv && vi < bi)) {
-          bv = v;
-          bi = vi;
-          bg = g;
+    // 2. global pivot: every block reduces the G candidates in parallel (same rule everywhere)
+    {
+      double v = -1.0;
+      int vi = -1, vg = -1;
+      for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        const int ci = scr.idx[buf * G + g];
+        if (ci < 0) continue;
+        const double cv = scr.val[buf * G + g];
+        if (vi < 0 || cv > v || (cv == v && ci < vi)) {
+          v = cv;
+          vi = ci;
+          vg = g;
         }
       }
-      s_piv = bi;
-      s_zero = !(bv > 0.0);
-      if (blockIdx.x == 0) {
-        ipiv[j] = s_zero ? j : bi;
-        if (s_zero && *info == 0) *info = j + 1;
+      s_val[threadIdx.x] = v;
+      s_idx[threadIdx.x] = vi;
+      s_grp[threadIdx.x] = vg;
+      __syncthreads();
+      for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+          const double o = s_val[threadIdx.x + s];
+          const int oi = s_idx[threadIdx.x + s];
+          const double mv = s_val[threadIdx.x];
+          const int mi = s_idx[threadIdx.x];
+          if (oi >= 0 && (mi < 0 || o > mv || (o == mv && oi < mi))) {
+            s_val[threadIdx.x] = o;
+            s_idx[threadIdx.x] = oi;
+            s_grp[threadIdx.x] = s_grp[threadIdx.x + s];
+          }
+        }
+        __syncthreads();
       }
-      s_idx[0] = bg;
+      if (threadIdx.x == 0) {
+        s_piv = s_idx[0];
+        s_zero = !(s_val[0] > 0.0);
+        if (blockIdx.x == 0) {
+          ipiv[j] = s_zero ? j : s_idx[0];
+          if (s_zero && *info == 0) *info = j + 1;
+        }
+        s_win = s_grp[0];
+      }
+      __syncthreads();
     }
-    __syncthreads();
     const int piv = s_piv;
     if (s_zero) {
       __syncthreads();
       continue;
     }
-    const int winner = s_idx[0];
+    const int winner = s_win;
     if (threadIdx.x < w) s_prow[threadIdx.x] = scr.row[((size_t)buf * G + winner) * IB + threadIdx.x];
     __syncthreads();
     // 3. the two owners exchange rows j and piv (sub-panel columns only)
@@ -174,6 +198,149 @@ __global__ void __launch_bounds__(256) k_subpanel(T* __restrict__ A, int n, int 
       }
     }
     __syncthreads();
+  }
+}
+
+// Same algorithm with each block's rows of the sub-panel resident in shared
+// memory for all w columns: one coalesced load and one store per element,
+// everything else (pivot search, swaps, elimination) in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) k_subpanel_smem(T* __restrict__ A, int n, int c0, int w,
+                                                       int32_t* __restrict__ ipiv, PivotScratch<T> scr,
+                                                       int* __restrict__ info) {
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ unsigned char sp_raw[];
+  T* sA = reinterpret_cast<T*>(sp_raw);  // [chunk][SP], padded against bank conflicts
+  const int G = gridDim.x;
+  const int m = n - c0;
+  const int chunk = (m + G - 1) / G;
+  const int lo = c0 + blockIdx.x * chunk;
+  const int hi = min(n, lo + chunk);
+  const int nr = max(0, hi - lo);
+  __shared__ double s_val[256];
+  __shared__ int s_idx[256];
+  __shared__ int s_grp[256];
+  __shared__ T s_prow[IB];
+  __shared__ T s_l[1];
+  __shared__ int s_piv, s_zero, s_win;
+  for (int t = threadIdx.x; t < nr * w; t += blockDim.x) {
+    const int r = t / w, c = t % w;
+    sA[r * SP + c] = A[(size_t)(lo + r) * n + c0 + c];
+  }
+  __syncthreads();
+  for (int jj = 0; jj < w; jj++) {
+    const int j = c0 + jj;
+    const int buf = jj & 1;
+    double best = -1.0;
+    int bidx = -1;
+    for (int r = max(0, j - lo) + threadIdx.x; r < nr; r += blockDim.x) {
+      const T v = sA[r * SP + jj];
+      const double a = fabs((double)v.x) + fabs((double)v.y);
+      if (a > best) {
+        best = a;
+        bidx = lo + r;
+      }
+    }
+    s_val[threadIdx.x] = best;
+    s_idx[threadIdx.x] = bidx;
+    __syncthreads();
+    for (int sft = blockDim.x / 2; sft > 0; sft >>= 1) {
+      if (threadIdx.x < sft) {
+        const double o = s_val[threadIdx.x + sft];
+        const int oi = s_idx[threadIdx.x + sft];
+        const double mv = s_val[threadIdx.x];
+        const int mi = s_idx[threadIdx.x];
+        if (oi >= 0 && (mi < 0 || o > mv || (o == mv && oi < mi))) {
+          s_val[threadIdx.x] = o;
+          s_idx[threadIdx.x] = oi;
+        }
+      }
+      __syncthreads();
+    }
+    const int cand = s_idx[0];
+    if (threadIdx.x == 0) {
+      scr.val[buf * G + blockIdx.x] = s_val[0];
+      scr.idx[buf * G + blockIdx.x] = cand;
+    }
+    if (cand >= 0 && threadIdx.x < w) scr.row[((size_t)buf * G + blockIdx.x) * IB + threadIdx.x] = sA[(cand - lo) * SP + threadIdx.x];
+    if (j >= lo && j < hi && threadIdx.x < w) scr.top[buf * IB + threadIdx.x] = sA[(j - lo) * SP + threadIdx.x];
+    grid.sync();
+    {
+      double v = -1.0;
+      int vi = -1, vg = -1;
+      for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        const int ci = scr.idx[buf * G + g];
+        if (ci < 0) continue;
+        const double cv = scr.val[buf * G + g];
+        if (vi < 0 || cv > v || (cv == v && ci < vi)) {
+          v = cv;
+          vi = ci;
+          vg = g;
+        }
+      }
+      s_val[threadIdx.x] = v;
+      s_idx[threadIdx.x] = vi;
+      s_grp[threadIdx.x] = vg;
+      __syncthreads();
+      for (int sft = blockDim.x / 2; sft > 0; sft >>= 1) {
+        if (threadIdx.x < sft) {
+          const double o = s_val[threadIdx.x + sft];
+          const int oi = s_idx[threadIdx.x + sft];
+          const double mv = s_val[threadIdx.x];
+          const int mi = s_idx[threadIdx.x];
+          if (oi >= 0 && (mi < 0 || o > mv || (o == mv && oi < mi))) {
+            s_val[threadIdx.x] = o;
+            s_idx[threadIdx.x] = oi;
+            s_grp[threadIdx.x] = s_grp[threadIdx.x + sft];
+          }
+        }
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) {
+        s_piv = s_idx[0];
+        s_zero = !(s_val[0] > 0.0);
+        if (blockIdx.x == 0) {
+          ipiv[j] = s_zero ? j : s_idx[0];
+          if (s_zero && *info == 0) *info = j + 1;
+        }
+        s_win = s_grp[0];
+      }
+      __syncthreads();
+    }
+    if (s_zero) {
+      __syncthreads();
+      continue;
+    }
+    const int piv = s_piv;
+    if (threadIdx.x < w) s_prow[threadIdx.x] = scr.row[((size_t)buf * G + s_win) * IB + threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x < w) {
+      if (piv != j && piv >= lo && piv < hi) sA[(piv - lo) * SP + threadIdx.x] = scr.top[buf * IB + threadIdx.x];
+      if (j >= lo && j < hi) sA[(j - lo) * SP + threadIdx.x] = s_prow[threadIdx.x];
+    }
+    __syncthreads();
+    // multipliers, then the rank-1 update of the remaining sub-panel columns
+    const T d = s_prow[jj];
+    const int r0 = max(0, j + 1 - lo);
+    for (int r = r0 + threadIdx.x; r < nr; r += blockDim.x) sA[r * SP + jj] = cdiv_smith(sA[r * SP + jj], d);
+    __syncthreads();
+    const int ncol = w - jj - 1;
+    if (ncol > 0) {
+      for (int t = threadIdx.x; t < (nr - r0) * ncol; t += blockDim.x) {
+        const int r = r0 + t / ncol, c = jj + 1 + t % ncol;
+        const T l = sA[r * SP + jj];
+        const T u = s_prow[c];
+        T a = sA[r * SP + c];
+        a.x -= l.x * u.x - l.y * u.y;
+        a.y -= l.x * u.y + l.y * u.x;
+        sA[r * SP + c] = a;
+      }
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < nr * w; t += blockDim.x) {
+    const int r = t / w, c = t % w;
+    A[(size_t)(lo + r) * n + c0 + c] = sA[r * SP + c];
   }
 }
 
@@ -347,6 +514,11 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
   TT_TRY(d_info.alloc(1));
   TT_CUDA_TRY(cudaMemsetAsync(d_info.ptr, 0, sizeof(int), st));
   PivotScratch<T> scr{sval.ptr, sidx.ptr, srow.ptr, stop.ptr};
+  static bool smem_attr = false;
+  if (!smem_attr) {
+    TT_CUDA_TRY(cudaFuncSetAttribute(k_subpanel_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubpanelSmem));
+    smem_attr = true;
+  }
   for (int k = 0; k < n; k += NB) {
     const int kb = std::min(NB, n - k);
     // ---- panel [k, k+kb) in sub-panels of IB columns
@@ -358,7 +530,13 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
         int32_t* ip = ipiv;
         int* inf = d_info.ptr;
         void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
-        TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
+        const size_t chunk = (size_t)(n - j0 + G - 1) / G;
+        const size_t smem = chunk * SP * sizeof(T);
+        if (smem <= kSubpanelSmem) {
+          TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel_smem<T>, dim3(G), dim3(256), args, smem, st));
+        } else {
+          TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
+        }
         count_launch();
       }
       TT_TRY(laswp2(A, n, ipiv, j0, j0 + w, k, j0, j0 + w, k + kb, st));

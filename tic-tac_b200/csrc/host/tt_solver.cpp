@@ -177,9 +177,10 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     return TT_OK;
   }
   const int Nq = L_.Nq, Np = L_.Np;
-  DevBuf<int32_t> ipiv, cols, rhs_e;
+  DevBuf<int32_t> ipiv, cols, rhs_e, perm_d;
   TT_TRY(ipiv.alloc(n));
-  DevBuf<double> b, x, y, res, d;
+  DevBuf<double> b, x, y, res, d, tmp;
+  TT_TRY(tmp.alloc((size_t)2 * n * nd));
   TT_TRY(b.alloc((size_t)2 * n * nd));
   TT_TRY(x.alloc((size_t)2 * n * nd));
   DevBuf<double2> L64;
@@ -221,10 +222,13 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       return TT_ERR_SINGULAR;
     }
     t0 = std::chrono::steady_clock::now();
+    std::vector<int32_t> perm;
+    TT_TRY(lu_permutation(ipiv.ptr, n, perm, st));
+    TT_TRY(perm_d.upload(perm, st));
     TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nd, b.ptr, st));
     TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * 2 * n * nd, cudaMemcpyDeviceToDevice, st));
-    if (opt.mixed) TT_TRY(lu_solve_device<float2>(L32.ptr, n, ipiv.ptr, x.ptr, nd, st));
-    else TT_TRY(lu_solve_device<double2>(L64.ptr, n, ipiv.ptr, x.ptr, nd, st));
+    if (opt.mixed) TT_TRY(lu_solve_device<float2>(L32.ptr, n, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+    else TT_TRY(lu_solve_device<double2>(L64.ptr, n, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
     TT_CUDA_TRY(cudaStreamSynchronize(st));
     r.ms_solve += ms_since(t0);
     if (opt.mixed) {
@@ -237,7 +241,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       for (it = 1; it <= opt.refine_max_iter; it++) {
         TT_TRY(hadamard_device(Gj, rhs_e.ptr, n, x.ptr, nd, y.ptr, st));
         TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nd, res.ptr, st));
-        TT_TRY(lu_solve_device<float2>(L32.ptr, n, ipiv.ptr, res.ptr, nd, st));
+        TT_TRY(lu_solve_device<float2>(L32.ptr, n, perm_d.ptr, res.ptr, tmp.ptr, nd, st));
         TT_TRY(axpy_norms_device(x.ptr, res.ptr, n, nd, ratio.data(), st));
         worst = 0;
         for (double v : ratio) worst = std::max(worst, v);
