@@ -131,6 +131,28 @@ int tt_fill_P123_arrays(double** val, int** row, int** col, size_t* nnz, int pro
 int tt_calculate_resolvent_array_in_SWP_basis(tt_complex* G, double E, const tt_swp_states* swp,
                                               const tt_pw_states* pw, const tt_run_params* rp);
 
+/* No counterpart in the reference.  The resolvent of
+ * tt_calculate_resolvent_array_in_SWP_basis for nE energies E[j] (host array),
+ * written to G_dev[j*n + i] in DEVICE memory the caller owns, on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream), without any device
+ * allocation: for callers whose device memory is all held by their own pool
+ * (a caching allocator, a pre-reserved arena) and that cannot let a library
+ * cudaMalloc.  The lookup tables are staged in a fixed static device scratch
+ * of TT_RESOLVENT_NOALLOC_SCRATCH_BYTES:
+ *   4 Nalpha + 8 [(Np+1)(num_unco + 2 num_coup)] + 8 (Nq+1) + 8 nE bytes,
+ *   each part rounded up to 256,
+ * and larger inputs are rejected with TT_ERR_UNSUPPORTED before any device work.
+ * The first call on each device looks up the scratch address with
+ * cudaGetSymbolAddress (that device current) and loads the module there:
+ * make it before any stream capture.  Nothing has to be zeroed beforehand;
+ * every call rewrites the tables it reads.  Calls that overlap in time on one
+ * device (other streams or host threads) share the scratch and race:
+ * serialise them.  Returns when the work is queued on `stream`. */
+#define TT_RESOLVENT_NOALLOC_SCRATCH_BYTES (256u * 1024u)
+int tt_calculate_resolvent_array_in_SWP_basis_noalloc(tt_complex* G_dev, const double* E, int nE,
+                                                      const tt_swp_states* swp, const tt_pw_states* pw,
+                                                      const tt_run_params* rp, void* stream);
+
 /* Replaces solve_faddeev_equations (CPP/solve_faddeev.h:25-38) for the
  * elastic on-shell U-matrix: U[d'*nd*nE + d*nE + j] (caller allocates
  * nE*nd*nd), G[j*n + i] the resolvents of the nE on-shell energies, P123 in

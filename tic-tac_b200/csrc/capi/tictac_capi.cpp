@@ -248,6 +248,21 @@ int tt_calculate_resolvent_array_in_SWP_basis(tt_complex* G, double E, const tt_
   return TT_OK;
 }
 
+int tt_calculate_resolvent_array_in_SWP_basis_noalloc(tt_complex* G_dev, const double* E, int nE,
+                                                      const tt_swp_states* swp, const tt_pw_states* pw,
+                                                      const tt_run_params* rpp, void* stream) {
+  if (!G_dev || !swp || !pw || !rpp || (nE > 0 && !E) || !swp->q_WP_array) return fail(TT_ERR_BADARG, "null argument");
+  if (nE < 0 || swp->Np_WP < 1 || swp->Nq_WP < 1 || pw->Nalpha < 0 || swp->num_2N_unco_states < 0 ||
+      swp->num_2N_coup_states < 0)
+    return fail(TT_ERR_BADARG, "negative or empty size");
+  if ((swp->num_2N_unco_states && !swp->e_SWP_unco_array) || (swp->num_2N_coup_states && !swp->e_SWP_coup_array))
+    return fail(TT_ERR_BADARG, "null SWP energy array");
+  const RunParams rp = params_of(rpp);
+  return resolvent_noalloc(rp, view_of(pw), swp->Np_WP, swp->Nq_WP, swp->num_2N_unco_states, swp->num_2N_coup_states,
+                           swp->e_SWP_unco_array, swp->e_SWP_coup_array, swp->q_WP_array, E, nE,
+                           reinterpret_cast<double*>(G_dev), static_cast<cudaStream_t>(stream));
+}
+
 int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double* P_val, const int* P_row,
                                const size_t* P_colptr, size_t P_nnz, const double* V_unco, const double* V_coup,
                                const tt_swp_states* swp, const tt_os_indexing* os, const tt_pw_states* pw,

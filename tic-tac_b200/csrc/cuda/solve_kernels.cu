@@ -290,6 +290,17 @@ int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d
   return TT_OK;
 }
 
+int resolvent_device_tables(int Na, int Nq, int Np, const int32_t* e_off, const double* e_swp, const double* q_WP,
+                            const double* d_E, int nE, double* d_G, cudaStream_t st) {
+  const size_t total = (size_t)Na * Nq * Np * nE;
+  if (total == 0) return TT_OK;
+  k_resolvent<<<ceil_div(total, 256), 256, 0, st>>>(Na, Nq, Np, e_off, e_swp, q_WP, d_E, nE,
+                                                    reinterpret_cast<double2*>(d_G));
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
 int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, double* d_A, cudaStream_t st) {
   const int n = L.n;
   if (L.Np > 64) {

@@ -48,6 +48,11 @@ struct DeviceLayout {
 // G[j*n + i] (complex128 interleaved) for energies E[j]; make_resolvent.cpp:82-211.
 int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d_G, cudaStream_t st);
 
+// Same kernel on tables the caller placed in device memory: e_off[Na],
+// e_swp (SWP energy boundaries), q_WP[Nq+1], E[nE].
+int resolvent_device_tables(int Na, int Nq, int Np, const int32_t* e_off, const double* e_swp, const double* q_WP,
+                            const double* d_E, int nE, double* d_G, cudaStream_t st);
+
 // Dense A (n x n, row-major FP64) = C^T (2 P123) (V C); solve_faddeev.cpp:4-181.
 // d_B is an n x n FP64 scratch of the product 2 P123 (V C).
 int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, double* d_A, cudaStream_t st);

@@ -40,6 +40,20 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
+bool channel_energy_offsets(const RunParams& rp, const PWChannel& ch, int Np, int n_unco, int n_coup,
+                            int32_t* e_off, std::string* err) {
+  for (int a = 0; a < ch.Nalpha; a++) {
+    AlphaBlock ab;
+    if (!alpha_block(rp, ch, a, ab, err)) return false;
+    if (ab.chn < 0 || ab.chn >= (ab.coupled ? n_coup : n_unco)) {
+      if (err) *err = "partial wave maps to a 2N channel outside the SWP state arrays";
+      return false;
+    }
+    e_off[a] = ab.coupled ? n_unco * (Np + 1) + ab.chn * 2 * (Np + 1) + ab.part * (Np + 1) : ab.chn * (Np + 1);
+  }
+  return true;
+}
+
 bool build_channel_layout(const RunParams& rp, const PWChannel& ch, const SWPStates& swp,
                           const std::vector<double>& V_unco, const std::vector<double>& V_coup, ChannelLayout& L,
                           std::string* err) {

@@ -14,6 +14,19 @@ bool build_channel_layout(const RunParams& rp, const PWChannel& ch, const SWPSta
                           const std::vector<double>& V_unco, const std::vector<double>& V_coup, ChannelLayout& L,
                           std::string* err);
 
+// Per-alpha offsets into the SWP energy table e_unco ++ e_coup (the e_off of
+// build_channel_layout), written to e_off[Nalpha]; checks each 2N index
+// against the n_unco / n_coup slots.  Allocates nothing.
+bool channel_energy_offsets(const RunParams& rp, const PWChannel& ch, int Np, int n_unco, int n_coup,
+                            int32_t* e_off, std::string* err);
+
+// Resolvent for nE energies into caller-owned device memory d_G [nE][n] with
+// the tables staged in a static device array (no device allocation); defined
+// in the CUDA sources.  TT_ERR_UNSUPPORTED when the tables exceed it.
+int resolvent_noalloc(const RunParams& rp, const PWChannel& ch, int Np, int Nq, int n_unco, int n_coup,
+                      const double* e_unco, const double* e_coup, const double* q_WP, const double* E, int nE,
+                      double* d_G, cudaStream_t st);
+
 struct SolveOptions {
   bool mixed = true;        // complex64 LU on tensor cores + FP64 refinement; false: complex128 LU
   bool tensor_cores = true; // trailing update on tcgen05 (mixed only)

@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = (
     "tt_run_release_channel", "tt_run_get_P123_csr", "tt_run_get_A", "tt_run_get_G", "tt_run_get_host_array",
     "tt_run_write_U_table", "tt_run_release_A", "tt_run_timer_start", "tt_run_timer_stop", "tt_kernel_launches",
     "tt_wigner_3j", "tt_wigner_6j", "tt_wigner_9j", "tt_clebsch_gordan", "tt_legendre_spharm_array",
-    "tt_gauss_legendre",
+    "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc",
 )
 
 
@@ -217,6 +217,18 @@ def resolvent(G_E: float, swp: SWP, pw: PW, **rp_kw) -> np.ndarray:
     _check(lib.tt_calculate_resolvent_array_in_SWP_basis(G.ctypes.data_as(c_void_p), c_double(G_E), byref(swp.s),
                                                          byref(pw.s), byref(rp)))
     return G
+
+
+def resolvent_noalloc(G_dev_ptr: int, energies, swp: SWP, pw: PW, stream: int = 0, **rp_kw) -> None:
+    """tt_calculate_resolvent_array_in_SWP_basis_noalloc: resolvents of all
+    `energies` into the caller's device buffer at address G_dev_ptr
+    (complex128 [nE][n]), queued on `stream` (a cudaStream_t handle)."""
+    lib = load()
+    E = np.ascontiguousarray(energies, dtype=np.float64)
+    rp = run_params(**rp_kw)
+    _check(lib.tt_calculate_resolvent_array_in_SWP_basis_noalloc(
+        c_void_p(G_dev_ptr), E.ctypes.data_as(c_void_p), ctypes.c_int(len(E)), byref(swp.s), byref(pw.s), byref(rp),
+        c_void_p(stream)))
 
 
 def solve_faddeev(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q_idx, deut, pw: PW, precision=PRECISION_MIXED,
