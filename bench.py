@@ -33,6 +33,8 @@ sys.path.insert(0, os.path.join(HERE, "tic-tac_b200", "python"))
 CONFIGS = {
     # the metric's configuration (see module docstring)
     "j3_J7_n30": dict(potential_model="LO_internal", J_2N_max=3, two_J_3N_max=7, Np_WP=30, Nq_WP=30),
+    # same basis at Np=Nq=12 (largest channel n = 9072, ~0.7 GB per matrix): profiler captures
+    "j3_J7_n12": dict(potential_model="LO_internal", J_2N_max=3, two_J_3N_max=7, Np_WP=12, Nq_WP=12),
     # small case for quick checks of this script
     "j1_J3_n12": dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=12, Nq_WP=12),
 }
@@ -44,8 +46,9 @@ def load_peaks():
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
-    return 6650.0, 1590.0, "fallback"
+        return (d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0),
+                "measured")
+    return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 class ClockSampler:
@@ -132,6 +135,51 @@ def step_flops(ns, nE):
     return sum(nE * 8.0 / 3.0 * float(n) ** 3 for n in ns)
 
 
+# DRAM traffic of the tensor-core update per algorithmic byte (C read + written
+# as complex64, L and U panels read once), from the ncu capture of that kernel
+# in profiles/k_lu_update_tc.md; scales the bench's mean launch to a traffic figure.
+TC_TRAFFIC_PER_ALGO_BYTE = None
+
+
+def roofline_of(kern, timed_ms, ms_step, ns, nE):
+    """Roofline of the dominant kernel class over the timed region: algorithmic
+    flops (or bytes) per launch over the CUDA-event time per launch."""
+    hbm, tf_burst, tf_sust, peak_kind = load_peaks()
+    kernels = {}
+    for name, k in kern.items():
+        if k["launches"]:
+            kernels[name] = {"launches": k["launches"], "ms": round(k["ms"], 3),
+                             "share_of_timed": round(k["ms"] / timed_ms, 4),
+                             "tflops": round(k["flops"] / (k["ms"] * 1e-3) / 1e12, 2) if k["ms"] else None,
+                             "gbs": round(k["bytes"] / (k["ms"] * 1e-3) / 1e9, 1) if k["ms"] else None}
+    dom = max(kern, key=lambda nm: kern[nm]["ms"])
+    k = kern[dom]
+    if k["launches"] == 0:
+        return None, kernels
+    per_launch_s = k["ms"] * 1e-3 / k["launches"]
+    if dom == "tc_update":
+        # complex64 product in BF16x3: 3 bf16 tensor products per fp32-accurate
+        # product, so the tensor roofline for algorithmic flops is peak / 3;
+        # the kernel runs inside a seconds-long step -> sustained figure
+        achieved = k["flops"] / k["launches"] / per_launch_s / 1e12
+        peak = tf_sust / 3.0
+        traffic = None
+        if TC_TRAFFIC_PER_ALGO_BYTE:
+            traffic = TC_TRAFFIC_PER_ALGO_BYTE * k["bytes"] / k["launches"]
+        roof = {"bound": "tensor", "achieved": round(achieved, 2), "peak": round(peak, 1), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": "k_lu_update_tc (complex64 trailing update C -= L U, BF16x3 on tcgen05)",
+                "flops_per_launch": k["flops"] / k["launches"], "ms_per_launch": round(per_launch_s * 1e3, 3),
+                "peak_source": f"{peak_kind} bf16_tflops_sustained {tf_sust} / 3 (BF16x3 split factor)"}
+    else:
+        achieved = k["bytes"] / k["launches"] / per_launch_s / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "traffic": None, "kernel": dom,
+                "peak_source": f"{peak_kind} hbm_gbs"}
+    roof["step_lu_tflops"] = round(step_flops(ns, nE) / (ms_step * 1e-3) / 1e12, 2)
+    return roof, kernels
+
+
 def run_ours(args, world, rank, local, pg):
     import tictac_b200 as tt
     os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
@@ -140,16 +188,17 @@ def run_ours(args, world, rank, local, pg):
     prec = tt.PRECISION_MIXED if args.precision == "mixed" else tt.PRECISION_FP64
     t_setup = time.perf_counter()
     run = tt.Run(**cfg)
-    nch = run.num_channels
-    infos = [run.channel_info(c) for c in range(nch)]
+    chans = [int(c) for c in args.channels.split(",")] if args.channels else list(range(run.num_channels))
+    nch = len(chans)
+    infos = [run.channel_info(c) for c in chans]
     T_lab, E_com, q_idx = run.energies()
     nE = len(T_lab)
-    nnz = [run.build_P123(c) for c in range(nch)]  # resident for the whole run
+    nnz = [run.build_P123(c) for c in chans]  # resident for the whole run
     t_setup = time.perf_counter() - t_setup
 
     def one_step():
         Us = []
-        for c in range(nch):
+        for c in chans:
             run.build_A(c)
             run.build_resolvent(c)
             U, rep = run.solve(c, prec)
@@ -161,24 +210,20 @@ def run_ours(args, world, rank, local, pg):
         one_step()
     barrier(pg)
     times = []
+    launches0 = tt.kernel_launches()
+    tt.profile_begin()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             run.timer_start()
             one_step()
             times.append(run.timer_stop())
+    kern = tt.profile_end()
+    launches = tt.kernel_launches() - launches0
     barrier(pg)
     ms_step = allreduce_max(pg, float(np.mean(times)))
     energies_per_step = nE * world
     value = energies_per_step / (ms_step * 1e-3)
-
-    # dominant kernel: the tensor-core trailing update, timed in isolation on the
-    # largest channel's first update (CUDA events on the launching stream)
-    hbm, tf_peak, peak_kind = load_peaks()
-    flops = step_flops([i["n"] for i in infos], nE)
-    achieved_tflops = flops / (ms_step * 1e-3) / 1e12
-    roofline = {"bound": "tensor", "achieved": round(achieved_tflops, 2), "peak": tf_peak, "unit": "TFLOP/s",
-                "frac": round(achieved_tflops / tf_peak, 4), "traffic": None,
-                "note": f"achieved = (8/3) n^3 complex-LU flops per channel-energy over the step time; peak {peak_kind} bf16"}
+    roofline, kernels = roofline_of(kern, float(np.sum(times)), ms_step, [i["n"] for i in infos], nE)
 
     # end to end through the drop-in C-ABI call with host buffers
     e2e = None
@@ -195,9 +240,9 @@ def run_ours(args, world, rank, local, pg):
         n_unco = len(e_unco) // (Np + 1)
         n_coup = len(e_coup) // (2 * (Np + 1))
         swp = tt.SWP(Np, Nq, n_unco, n_coup, run.E_bound, e_unco, e_coup, C_unco, C_coup, q_WP)
-        for c in range(nch):
-            rowptr, col, val = run.P123_csr(c, nnz[c])
-            n = infos[c]["n"]
+        for i, c in enumerate(chans):
+            rowptr, col, val = run.P123_csr(c, nnz[i])
+            n = infos[i]["n"]
             rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rowptr))
             order = np.lexsort((rows, col))
             colptr = np.zeros(n + 1, dtype=np.uint64)
@@ -209,6 +254,21 @@ def run_ours(args, world, rank, local, pg):
             deut = [a for a in range(len(pwt)) if tuple(pwt[a, :4]) == (0, 1, 1, 0)]
             host.append((G, val[order].copy(), rows[order].copy(), colptr, tt.PW(pwt, cfg["J_2N_max"]), deut))
             run.release(c)
+        # inputs live in pinned host memory, as a caller streaming channels would keep them
+        import torch
+
+        pinned = []
+
+        def pin(a):
+            a = np.ascontiguousarray(a)
+            t = torch.empty(max(1, a.nbytes), dtype=torch.uint8, pin_memory=True)
+            v = t.numpy()[:a.nbytes].view(a.dtype).reshape(a.shape)
+            v[...] = a
+            pinned.append(t)
+            return v
+
+        host = [tuple(pin(x) if isinstance(x, np.ndarray) else x for x in h) for h in host]
+        V_unco, V_coup = pin(V_unco), pin(V_coup)
         h2d = sum(h[0].nbytes + h[1].nbytes + h[2].nbytes + h[3].nbytes for h in host) + \
             nch * (V_unco.nbytes + V_coup.nbytes + C_unco.nbytes + C_coup.nbytes + e_unco.nbytes + e_coup.nbytes)
         d2h = sum(16 * nE * len(h[5]) ** 2 for h in host)
@@ -227,11 +287,30 @@ def run_ours(args, world, rank, local, pg):
         t_e2e = allreduce_max(pg, float(np.mean(te)))
         e2e = {"value": round(energies_per_step / t_e2e, 6), "unit": "energies/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "timer": "host perf_counter around the synchronous C-ABI call"}
-    return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, e2e=e2e,
-                infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times)
+    # the metric's comparison: mixed+refined against the plain FP64 solve on the
+    # smallest channel (same inputs, same energies), outside the timed region
+    fp64 = None
+    if args.fp64_check and prec == tt.PRECISION_MIXED:
+        i = min(range(nch), key=lambda k: infos[k]["n"])
+        c = chans[i]
+        run.build_A(c)
+        run.build_resolvent(c)
+        Um, rm = run.solve(c, tt.PRECISION_MIXED)
+        U64, r64 = run.solve(c, tt.PRECISION_FP64)
+        run.release_A(c)
+        t_m = rm["ms_form"] + rm["ms_factor"] + rm["ms_solve"] + rm["ms_refine"]
+        t_64 = r64["ms_form"] + r64["ms_factor"] + r64["ms_solve"] + r64["ms_refine"]
+        fp64 = {"channel": c, "n": infos[i]["n"], "mixed_ms": round(t_m, 1), "fp64_ms": round(t_64, 1),
+                "speedup": round(t_64 / t_m, 2), "refine_iters": rm["refine_iters"],
+                "max_rel_diff_U": float(np.max(np.abs(Um - U64)) / np.max(np.abs(U64)))}
+    return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, kernels=kernels, e2e=e2e,
+                infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times, launches=launches, fp64=fp64)
 
 
-def reference_sample(args, sample_N=10, channel=None):
+REF_SAMPLE_N = 12
+
+
+def reference_sample(args, sample_N=REF_SAMPLE_N, channel=None):
     """Time the reference's own dense LAPACK solve (oracle/_ref/tictac_ref,
     OpenMP + OpenBLAS on all host cores) on one channel of the same physics at
     Np_WP = Nq_WP = sample_N and scale to the workload by n^3."""
@@ -272,13 +351,15 @@ def cpu_value_for(infos, ref):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=list(CONFIGS), default="j3_J7_n30")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp64-check", type=int, default=1, help="time FP64 vs mixed on the smallest channel")
+    ap.add_argument("--channels", default="", help="comma list of channel indices to step (default: all)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     cfg = CONFIGS[args.config]
@@ -295,19 +376,19 @@ def main():
         infos = [run.channel_info(c) for c in range(run.num_channels)]
         nE = len(run.energies()[0])
         run.close()
-        ref, why = reference_sample(args)
-        if ref is None:
-            print(json.dumps({"impl": "reference", "unavailable": why}))
-            return
-        v = cpu_value_for(infos, ref)
-        times = []
-        for _ in range(args.warmup + args.steps):
-            r2, _ = reference_sample(args)
-            times.append(r2["per_energy_s"])
-        ref["per_energy_s"] = float(np.mean(times[args.warmup:])) if args.steps else ref["per_energy_s"]
+        samples = []
+        for _ in range(args.warmup + max(1, args.steps)):
+            r2, why = reference_sample(args)
+            if r2 is None:
+                print(json.dumps({"impl": "reference", "unavailable": why}))
+                return
+            samples.append(r2)
+        ref = dict(samples[-1])
+        ref["per_energy_s"] = float(np.mean([x["per_energy_s"] for x in samples[args.warmup:]]))
         v = cpu_value_for(infos, ref)
         sample = (f"reference dense LAPACK solve (A columns + zgetrf + zgetrs nrhs=n) of channel 0 at "
-                  f"Np=Nq=10 (n={ref['n_sample']}), {ref['cores']} threads, scaled by n^3 to the workload")
+                  f"Np=Nq={REF_SAMPLE_N} (n={ref['n_sample']}), T_lab=10 MeV, {ref['cores']} threads, "
+                  f"extrapolated by n^3 to every channel of the workload")
         print(json.dumps({"metric": METRIC, "value": v, "unit": "energies/s", "impl": "reference", "n_gpus": world,
                           "steps": args.steps, "warmup": args.warmup, "ms_step": nE / v * 1e3,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
@@ -328,7 +409,7 @@ def main():
             if ref is not None:
                 v = cpu_value_for(r["infos"], ref)
                 cpu = {"value": v, "unit": "energies/s", "cores": ref["cores"], "kind": "reference",
-                       "sample": f"reference dense LAPACK solve of channel 0 at Np=Nq=10 (n={ref['n_sample']}), "
+                       "sample": f"reference dense LAPACK solve of channel 0 at Np=Nq={REF_SAMPLE_N} (n={ref['n_sample']}), "
                                  f"scaled by n^3 to all {len(r['infos'])} channels"}
         out = {"metric": METRIC, "value": round(r["value"], 6), "unit": "energies/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_step": round(r["ms_step"], 3),
@@ -336,7 +417,9 @@ def main():
                "dtype": "complex64 LU (BF16x3 tcgen05) + FP64 refinement" if args.precision == "mixed" else "complex128",
                "data": "synthetic (chiral LO potential on the reference's default Chebyshev WP grid)",
                "config": config, "clocks": r["clocks"], "roofline": r["roofline"], "cpu_baseline": cpu,
-               "e2e": r["e2e"], "gpu_launches": None, "setup_s": round(r["t_setup"], 3)}
+               "e2e": r["e2e"], "gpu_launches": int(r["launches"]),
+               "channel_solves_per_s": round(len(r["infos"]) * r["nE"] * world / (r["ms_step"] * 1e-3), 4),
+               "kernels": r["kernels"], "fp64_comparison": r["fp64"], "setup_s": round(r["t_setup"], 3)}
         print(json.dumps(out))
     if pg is not None:
         pg.destroy_process_group()

@@ -169,6 +169,33 @@ int tt_device_count(int* count);
 /* Kernels launched by this library since load (diagnostic). */
 unsigned long long tt_kernel_launches(void);
 
+/* Kernel timing over a region (diagnostic; no counterpart in the reference).
+ * Between tt_profile_begin and tt_profile_end every launch of the kernel
+ * classes below is bracketed by CUDA events on its own stream; end waits for
+ * them and tt_profile_read returns, per class, the launches, the summed event
+ * time and the algorithmic flops and bytes booked for those launches:
+ *   TC_UPDATE  trailing update C -= L U of the complex64 LU on tcgen05, 8 M N K flops
+ *   SUBPANEL   pivoted factorisation of an m x w sub-panel (w <= 32): 4 m w^2 flops,
+ *              2 m w sizeof(elem) bytes (panel read and written once)
+ *   TRSV       forward + backward substitution, LU read once: n^2 sizeof(elem) bytes
+ *   RESIDUAL   FP64 refinement residual b - x + A (G o x), A read once: 8 n^2 bytes
+ *   A_BUILD    A = C^T (2 P123)(V C) */
+#define TT_PROF_TC_UPDATE 0
+#define TT_PROF_SUBPANEL 1
+#define TT_PROF_TRSV 2
+#define TT_PROF_RESIDUAL 3
+#define TT_PROF_A_BUILD 4
+#define TT_PROF_COUNT 5
+typedef struct tt_kernel_profile {
+  unsigned long long launches;
+  double ms;
+  double flops;
+  double bytes;
+} tt_kernel_profile;
+int tt_profile_begin(void);
+int tt_profile_end(void);
+int tt_profile_read(int kernel_class, tt_kernel_profile* out);
+
 /* Host numerics the P123 tables are built from, doubled (2j, 2m) arguments:
  * replace gsl_sf_coupling_3j/6j/9j as wrapped by wigner_3j/6j/9j and
  * clebsch_gordan (CPP/General_functions/coupling_coefficients.h:12-24,

@@ -159,6 +159,7 @@ int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cud
 template <typename T>
 int lu_solve_device(const T* d_LU, int n, const int32_t* d_perm, double* d_x, double* d_tmp, int nrhs,
                     cudaStream_t st) {
+  ProfScope prof(TT_PROF_TRSV, st, 8.0 * n * (double)n * nrhs, (double)n * n * sizeof(T));
   TT_CUDA_TRY(cudaMemcpyAsync(d_tmp, d_x, sizeof(double2) * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, st));
   double2* x = reinterpret_cast<double2*>(d_x);
   k_permute<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_tmp), d_perm, n,

@@ -532,6 +532,8 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
         void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
         const size_t chunk = (size_t)(n - j0 + G - 1) / G;
         const size_t smem = chunk * SP * sizeof(T);
+        const double mrows = n - j0;
+        ProfScope prof(TT_PROF_SUBPANEL, st, 4.0 * mrows * w * w, 2.0 * mrows * w * sizeof(T));
         if (smem <= kSubpanelSmem) {
           TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel_smem<T>, dim3(G), dim3(256), args, smem, st));
         } else {

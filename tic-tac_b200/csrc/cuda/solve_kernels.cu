@@ -307,6 +307,11 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, doubl
     set_error("Np_WP > 64 is not supported by the A-build kernel");
     return TT_ERR_UNSUPPORTED;
   }
+  // SpMM 2 k Np nnz + block product 2 k Np n^2 flops (k = mean coupled partners);
+  // CSR read once, B written, read, A written
+  const double kcpl = L.Nalpha ? (double)L.cpl.count / L.Nalpha : 0.0;
+  ProfScope prof(TT_PROF_A_BUILD, st, 2.0 * kcpl * L.Np * ((double)P.nnz + (double)n * n),
+                 12.0 * (double)P.nnz + 24.0 * (double)n * n);
   TT_CUDA_TRY(cudaMemsetAsync(d_B, 0, sizeof(double) * (size_t)n * n, st));
   if (P.nnz > 0) {
     const size_t warps = (size_t)n * L.Nalpha;
@@ -316,11 +321,9 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, doubl
     count_launch();
     TT_CUDA_TRY(cudaGetLastError());
   }
-  int max_cpl = 1;
   // the coupling lists hold at most 2 partners per alpha for the 2N structure;
   // shared memory is sized for 2 Np x Np blocks
   const size_t smem = (size_t)2 * L.Np * L.Np * sizeof(double);
-  (void)max_cpl;
   dim3 grid(ceil_div(n, 128), L.Nalpha * L.Nq);
   if (smem > 48 * 1024) TT_CUDA_TRY(cudaFuncSetAttribute(k_ct<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_ct<32><<<grid, 256, smem, st>>>(L.Nalpha, L.Nq, L.Np, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
@@ -360,6 +363,8 @@ int hadamard_device(const double* d_G, const int32_t* d_rhs_e, int n, const doub
 
 int residual_multi_device(const double* d_A, int n, const double* d_y, const double* d_b, const double* d_x, int nrhs,
                           double* d_r, cudaStream_t st) {
+  ProfScope prof(TT_PROF_RESIDUAL, st, 4.0 * n * (double)n * nrhs,
+                 8.0 * n * (double)n * ((nrhs + RES_MAXR - 1) / RES_MAXR));
   k_residual<<<ceil_div((size_t)n * 32, 256), 256, 0, st>>>(
       d_A, n, reinterpret_cast<const double2*>(d_y), reinterpret_cast<const double2*>(d_b),
       reinterpret_cast<const double2*>(d_x), nrhs, reinterpret_cast<double2*>(d_r));

@@ -16,6 +16,22 @@ const char* last_error();
 // Count of kernels this library has launched (reported by tt_kernel_launches).
 void count_launch();
 
+// Optional per-kernel-class timing, off unless tt_profile_begin() was called:
+// a ProfScope brackets its launches with CUDA events on the launching stream
+// and books the scope's algorithmic flops and bytes (TT_PROF_* classes).
+struct ProfScope {
+  ProfScope(int kernel_class, cudaStream_t st, double flops, double bytes);
+  ~ProfScope();
+  ProfScope(const ProfScope&) = delete;
+  ProfScope& operator=(const ProfScope&) = delete;
+
+ private:
+  int cls_ = -1;
+  long ev0_ = -1;
+  cudaStream_t st_ = nullptr;
+  double flops_ = 0, bytes_ = 0;
+};
+
 #define TT_CUDA_TRY(expr)                                                                   \
   do {                                                                                      \
     cudaError_t _e = (expr);                                                                \

@@ -36,8 +36,11 @@ EXPORTED_SYMBOLS = (
     "tt_run_release_channel", "tt_run_get_P123_csr", "tt_run_get_A", "tt_run_get_G", "tt_run_get_host_array",
     "tt_run_write_U_table", "tt_run_release_A", "tt_run_timer_start", "tt_run_timer_stop", "tt_kernel_launches",
     "tt_wigner_3j", "tt_wigner_6j", "tt_wigner_9j", "tt_clebsch_gordan", "tt_legendre_spharm_array",
-    "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc",
+    "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc", "tt_profile_begin", "tt_profile_end",
+    "tt_profile_read",
 )
+
+PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build")
 
 
 class TicTacError(RuntimeError):
@@ -217,6 +220,27 @@ def resolvent(G_E: float, swp: SWP, pw: PW, **rp_kw) -> np.ndarray:
     _check(lib.tt_calculate_resolvent_array_in_SWP_basis(G.ctypes.data_as(c_void_p), c_double(G_E), byref(swp.s),
                                                          byref(pw.s), byref(rp)))
     return G
+
+
+class tt_kernel_profile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_ulonglong), ("ms", c_double), ("flops", c_double), ("bytes", c_double)]
+
+
+def profile_begin() -> None:
+    """Start event timing of the kernel classes in PROFILE_CLASSES."""
+    _check(load().tt_profile_begin())
+
+
+def profile_end() -> dict:
+    """Stop timing; {class: {launches, ms, flops, bytes}} over the region."""
+    lib = load()
+    _check(lib.tt_profile_end())
+    out = {}
+    for i, name in enumerate(PROFILE_CLASSES):
+        p = tt_kernel_profile()
+        _check(lib.tt_profile_read(i, byref(p)))
+        out[name] = {"launches": int(p.launches), "ms": p.ms, "flops": p.flops, "bytes": p.bytes}
+    return out
 
 
 def resolvent_noalloc(G_dev_ptr: int, energies, swp: SWP, pw: PW, stream: int = 0, **rp_kw) -> None:
