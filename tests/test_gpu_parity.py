@@ -114,6 +114,30 @@ def test_larger_case_against_oracle():
     run.close()
 
 
+@pytest.mark.parametrize("Np,Nq", [(9, 7), (11, 3)])
+def test_ragged_block_sizes_against_oracle(Np, Nq):
+    # n = Nalpha * Np * Nq (363 .. 945) is no multiple of the 32/64/128-row
+    # blocks of the factorisation and the substitutions: partial blocks everywhere
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=Np, Nq_WP=Nq, Nphi=16, Nx=16,
+                lab_energies="12")
+    run = tt.Run(**opts)
+    T, E_com, q_idx = run.energies()
+    for c in range(run.num_channels):
+        pw = run.host_array(0, c).reshape(-1, 9)
+        nnz = run.build_P123(c)
+        rowptr, col, val = run.P123_csr(c, nnz)
+        lay = oracle.layout(pw, Np, run.host_array(3), run.host_array(4), run.host_array(5), run.host_array(6),
+                            run.host_array(7), run.host_array(8))
+        rows = np.repeat(np.arange(len(rowptr) - 1, dtype=np.int32), np.diff(rowptr))
+        G_o = np.stack([oracle.resolvent(lay, pw.shape[0], Nq, Np, run.host_array(2), e + run.E_bound) for e in E_com])
+        A_o = oracle.build_A(lay, pw.shape[0], Nq, Np, rows, col, val)
+        U_o = oracle.dense_solve(A_o, G_o, q_idx, oracle.deuterons(pw), Nq, Np)
+        for prec in PRECISIONS:
+            U, rep = run.solve(c, prec)
+            assert rel(U, U_o) <= 1e-10, (c, prec, rep)
+    run.close()
+
+
 def test_full_size_channel_mixed_agrees_with_fp64():
     # largest channel of the j<=3, J<=7/2 basis at N=16 (n = 16128): size-independent check
     # that refinement recovers the FP64 solution

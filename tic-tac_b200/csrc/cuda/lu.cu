@@ -1,14 +1,24 @@
 // Triangular solves with the LU factor of lu_factor.cu (the zgetrs half of the
 // reference's LAPACK solve, General_functions/matrix_routines.cpp:73-80), for a
 // few right-hand sides at a time: forward substitution with the unit lower
-// factor and back substitution with the upper factor, in FP64 arithmetic on a
-// complex128 or complex64 factor.
+// factor and back substitution with the upper factor.
+//
+// The factor is read once per substitution, as a stream: after each
+// factorisation the 64 x 64 diagonal blocks of L and U are inverted (one CTA
+// per block, in shared memory) and multiplied into the neighbouring
+// off-diagonal block; each substitution is then one cooperative kernel with
+// one grid barrier per block column (k_trsv).
 
+#include <cooperative_groups.h>
+
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
 #include "tt_kernels.h"
 #include "tt_lu_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace tt {
 
@@ -23,6 +33,9 @@ struct CT<float2> {
   using R = float;
 };
 
+constexpr int TSB = 64;       // diagonal block of the substitution (both element types)
+constexpr int TLD = TSB + 1;  // padded shared-memory row of a 64 x 64 tile
+
 template <typename T>
 __device__ __forceinline__ T cmul(T a, T b) {
   T r;
@@ -31,24 +44,22 @@ __device__ __forceinline__ T cmul(T a, T b) {
   return r;
 }
 template <typename T>
-__device__ __forceinline__ T cdiv(T a, T b) {
+__device__ __forceinline__ T crecip(T b) {
   using R = typename CT<T>::R;
-  // Smith's algorithm
+  // Smith's algorithm for 1 / b
   T r;
   if (fabs((double)b.x) >= fabs((double)b.y)) {
     const R t = b.y / b.x, d = b.x + b.y * t;
-    r.x = (a.x + a.y * t) / d;
-    r.y = (a.y - a.x * t) / d;
+    r.x = R(1) / d;
+    r.y = -t / d;
   } else {
     const R t = b.x / b.y, d = b.y + b.x * t;
-    r.x = (a.x * t + a.y) / d;
-    r.y = (a.y * t - a.x) / d;
+    r.x = t / d;
+    r.y = R(-1) / d;
   }
   return r;
 }
 
-// ---------------------------------------------------------------------------
-// Triangular solves on nrhs complex128 columns x[k][n].
 __global__ void k_permute(const double2* __restrict__ b, const int32_t* __restrict__ perm, int n, int nrhs,
                           double2* __restrict__ x) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -57,85 +68,387 @@ __global__ void k_permute(const double2* __restrict__ b, const int32_t* __restri
   x[t] = b[(size_t)k * n + perm[i]];
 }
 
-constexpr int SB = 64;  // substitution block
-
-// diagonal block solve, one CTA; the bs x bs block is staged in shared memory
-// first; lower: unit diagonal, forward; upper: backward with the diagonal
-template <typename T, bool LOWER>
-__global__ void __launch_bounds__(256) k_diag_solve(const T* __restrict__ A, int n, int i0, int bs,
-                                                     double2* __restrict__ x, int nrhs) {
-  extern __shared__ unsigned char dsm[];
-  T* sA = reinterpret_cast<T*>(dsm);  // [bs][bs]
-  __shared__ double2 sx[SB][8];
-  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) sA[t] = A[(size_t)(i0 + t / bs) * n + i0 + t % bs];
-  for (int k0 = 0; k0 < nrhs; k0 += 8) {
-    const int kn = min(8, nrhs - k0);
-    for (int t = threadIdx.x; t < bs * kn; t += blockDim.x) {
-      const int i = t / kn, k = t % kn;
-      sx[i][k] = x[(size_t)(k0 + k) * n + i0 + i];
-    }
-    __syncthreads();
-    for (int s = 0; s < bs; s++) {
-      const int i = LOWER ? s : bs - 1 - s;
-      if (!LOWER) {
-        if (threadIdx.x < kn) {
-          const T d = sA[i * bs + i];
-          const double dr = d.x, di = d.y;
-          const double2 v = sx[i][threadIdx.x];
-          const double den = dr * dr + di * di;
-          sx[i][threadIdx.x] = make_double2((v.x * dr + v.y * di) / den, (v.y * dr - v.x * di) / den);
+// ---------------------------------------------------------------------------
+// Inverses of the diagonal blocks: inv[b] (64 x 64, row-major) of the unit lower
+// (UPPER = false) or upper (UPPER = true) block b of the factor.  Rows and
+// columns past n are the identity.  In place in shared memory, right-looking:
+// lower, j ascending: X[r][c] -= L[r][j] X[j][c] for r > j, c <= j;
+// upper, j descending: row j is scaled by 1/U[j][j], then
+// X[r][c] -= U[r][j] X[j][c] for r < j, c >= j.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(512) k_inv_diag(const T* __restrict__ LU, int n, T* __restrict__ inv) {
+  extern __shared__ unsigned char ism[];
+  T* M = reinterpret_cast<T*>(ism);  // [TSB][TLD]
+  __shared__ T col[TSB];
+  const int b = blockIdx.x, r0 = b * TSB, bs = min(TSB, n - r0);
+  const T zero = {0, 0}, one = {1, 0};
+  for (int t = threadIdx.x; t < TSB * TSB; t += blockDim.x) {
+    const int r = t / TSB, c = t % TSB;
+    T v = (r == c) ? one : zero;
+    if (r < bs && c < bs && (UPPER ? c >= r : c < r)) v = LU[(size_t)(r0 + r) * n + r0 + c];
+    M[r * TLD + c] = v;
+  }
+  __syncthreads();
+  if (!UPPER) {
+    for (int j = 0; j + 1 < bs; j++) {
+      for (int r = j + 1 + threadIdx.x; r < bs; r += blockDim.x) col[r] = M[r * TLD + j];
+      __syncthreads();
+      const int w = j + 1, cnt = (bs - 1 - j) * w;
+      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const int r = j + 1 + t / w, c = t % w;
+        const T l = col[r];
+        if (c == j) {
+          M[r * TLD + j] = T{-l.x, -l.y};
+        } else {
+          const T p = cmul(l, M[j * TLD + c]);
+          T v = M[r * TLD + c];
+          v.x -= p.x;
+          v.y -= p.y;
+          M[r * TLD + c] = v;
         }
-        __syncthreads();
-      }
-      for (int t = threadIdx.x; t < bs * kn; t += blockDim.x) {
-        const int r = t / kn, k = t % kn;
-        const bool active = LOWER ? (r > i) : (r < i);
-        if (!active) continue;
-        const T l = sA[r * bs + i];
-        const double2 xi = sx[i][k];
-        double2 v = sx[r][k];
-        v.x -= (double)l.x * xi.x - (double)l.y * xi.y;
-        v.y -= (double)l.x * xi.y + (double)l.y * xi.x;
-        sx[r][k] = v;
       }
       __syncthreads();
     }
-    for (int t = threadIdx.x; t < bs * kn; t += blockDim.x) {
-      const int i = t / kn, k = t % kn;
-      x[(size_t)(k0 + k) * n + i0 + i] = sx[i][k];
+  } else {
+    for (int j = bs - 1; j >= 0; j--) {
+      const T d = crecip(M[j * TLD + j]);
+      __syncthreads();
+      for (int c = j + 1 + threadIdx.x; c < bs; c += blockDim.x) M[j * TLD + c] = cmul(M[j * TLD + c], d);
+      if (threadIdx.x == 0) M[j * TLD + j] = d;
+      for (int r = threadIdx.x; r < j; r += blockDim.x) col[r] = M[r * TLD + j];
+      __syncthreads();
+      const int w = bs - j, cnt = j * w;
+      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const int r = t / w, c = j + t % w;
+        const T u = col[r];
+        if (c == j) {
+          const T p = cmul(u, d);
+          M[r * TLD + j] = T{-p.x, -p.y};
+        } else {
+          const T p = cmul(u, M[j * TLD + c]);
+          T v = M[r * TLD + c];
+          v.x -= p.x;
+          v.y -= p.y;
+          M[r * TLD + c] = v;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
+  }
+  T* out = inv + (size_t)b * TSB * TSB;
+  for (int t = threadIdx.x; t < TSB * TSB; t += blockDim.x) {
+    const int r = t / TSB, c = t % TSB;
+    const bool keep = r < bs && c < bs && (UPPER ? c >= r : c < r);
+    out[t] = keep ? M[r * TLD + c] : ((r == c) ? one : zero);
   }
 }
 
-// rows outside the solved block: x[r] -= A[r, i0:i0+bs] x[i0:i0+bs]; warp per row
+// M[b] = inv[b] LU[b, prev(b)] for the blocks after the first in sweep order
+// (prev = b-1 forward, b+1 backward): the product that carries the solved
+// previous block into block b, so that x_b = inv[b] x_b - M[b] x_prev.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(512) k_prev_mul(const T* __restrict__ LU, int n, const T* __restrict__ inv,
+                                                  T* __restrict__ Mo) {
+  extern __shared__ unsigned char psm[];
+  T* sI = reinterpret_cast<T*>(psm);  // [TSB][TLD]
+  T* sT = sI + TSB * TLD;             // [TSB][TLD]
+  const int nb = (n + TSB - 1) / TSB, b = blockIdx.x;
+  const int prev = UPPER ? b + 1 : b - 1;
+  if (prev < 0 || prev >= nb) return;
+  const int r0 = b * TSB, rows = min(TSB, n - r0), c0 = prev * TSB, cols = min(TSB, n - c0);
+  for (int t = threadIdx.x; t < TSB * TSB; t += blockDim.x) {
+    const int r = t / TSB, c = t % TSB;
+    sI[r * TLD + c] = inv[(size_t)b * TSB * TSB + t];
+    sT[r * TLD + c] = (r < rows && c < cols) ? LU[(size_t)(r0 + r) * n + c0 + c] : T{0, 0};
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < TSB * TSB; t += blockDim.x) {
+    const int r = t / TSB, c = t % TSB;
+    T acc = {0, 0};
+    for (int u = 0; u < TSB; u++) {
+      const T p = cmul(sI[r * TLD + u], sT[u * TLD + c]);
+      acc.x += p.x;
+      acc.y += p.y;
+    }
+    Mo[(size_t)b * TSB * TSB + t] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One substitution (forward with L when !UPPER, backward with U when UPPER)
+// for kn <= RHS right-hand sides x[k][n], cooperative, one grid barrier per
+// block column.  Blocks are visited in sweep order q = 0, 1, .. (block q for
+// the forward sweep, block nb-1-q for the backward one).  Arithmetic is in the
+// factor's precision (FP32 for the complex64 factor, whose solves only feed the
+// FP64-residual refinement; FP64 for the complex128 factor); x stays complex128.
+//  - CTA 0 owns the serial chain: at step s it solves block q = s+1,
+//    x_{s+1} = inv[s+1] x_{s+1} - M[s+1] x_s, one 64 x 128 product with both
+//    tiles already in shared memory (cp.async issued a step ahead, during the
+//    barrier), and writes the solved block to x.
+//  - Blocks q >= 2 are owned round-robin by CTAs 1..G-1, which keep their rows
+//    of x in shared memory for the whole sweep: at step s every owner applies
+//    block column s to its unsolved blocks (q >= s+2) and publishes block s+2
+//    to x, which CTA 0 reads at the next step.  Lanes own columns: each lane
+//    holds its two entries of x_s in registers, and the factor tiles go from
+//    global memory straight into 3 (complex64) or 2 (complex128) register
+//    buffers used round-robin, each refilled as soon as it is applied, so the
+//    loads run ahead across the barriers (the factor does not depend on x).  x is never read-modify-written in global
+//    memory.
+constexpr int RHS = 4;
+constexpr int TRSV_THREADS = 512;
+
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, int bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if (bytes == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// 64 x 64 block b of a [nb][64][64] array into dst[TSB][TLD]; no commit
 template <typename T>
-__global__ void k_block_update(const T* __restrict__ A, int n, int i0, int bs, int r_lo, int r_hi,
-                               double2* __restrict__ x, int nrhs) {
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const int r = r_lo + (int)warp;
-  if (r >= r_hi) return;
-  const T* Ar = A + (size_t)r * n + i0;
-  for (int k = 0; k < nrhs; k++) {
-    double sr = 0, si = 0;
-    const double2* xb = x + (size_t)k * n + i0;
-    for (int c = lane; c < bs; c += 32) {
-      const T a = Ar[c];
-      const double2 v = xb[c];
-      sr += (double)a.x * v.x - (double)a.y * v.y;
-      si += (double)a.x * v.y + (double)a.y * v.x;
+__device__ __forceinline__ void tile_async(const T* __restrict__ src, int b, T* dst) {
+  for (int t = threadIdx.x; t < TSB * TSB; t += blockDim.x)
+    cp_async_elem(&dst[(t / TSB) * TLD + t % TSB], src + (size_t)b * TSB * TSB + t, sizeof(T));
+}
+
+// reduce 16 values over the 32 lanes of a warp: a butterfly that halves the
+// values each round (8+4+2+1 shuffles) and a final pair sum; value lane >> 1
+// ends complete in lanes 2i and 2i+1
+template <typename C>
+__device__ __forceinline__ C butterfly16(C (&acc)[16], int lane) {
+#pragma unroll
+  for (int o = 16, m = 8; m >= 1; o >>= 1, m >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int j = 0; j < m; j++) {
+      const C send = up ? acc[j] : acc[j + m];
+      const C keep = up ? acc[j + m] : acc[j];
+      acc[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      sr += __shfl_down_sync(0xffffffffu, sr, o);
-      si += __shfl_down_sync(0xffffffffu, si, o);
+  }
+  return acc[0] + __shfl_xor_sync(0xffffffffu, acc[0], 1);
+}
+
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(const T* __restrict__ LU, const T* __restrict__ inv,
+                                                         const T* __restrict__ Mp, int n, double2* __restrict__ x,
+                                                         int kn, int own_max) {
+  using C = typename CT<T>::R;
+  constexpr int TILE = TSB * TLD;
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ __align__(16) unsigned char tsm[];
+  T* tI = reinterpret_cast<T*>(tsm);                         // CTA 0: inverse tile
+  T* tM = tI + TILE;                                         // CTA 0: M tile
+  T* xo = reinterpret_cast<T*>(tsm + 2 * TILE * sizeof(T));  // owners: [own_max][RHS][TSB]
+  __shared__ T xs[RHS][TSB];   // CTA 0: solved block of this step
+  __shared__ T bsh[RHS][TSB];  // CTA 0: published rows of the block being solved
+  __shared__ T ysh[RHS][TSB];  // CTA 0: its solution
+  const int nb = (n + TSB - 1) / TSB;
+  const int G = gridDim.x;  // >= 2
+  const bool lead = blockIdx.x == 0;
+  auto blk = [&](int q) { return UPPER ? nb - 1 - q : q; };
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  auto ld_x = [&](int k, int r) -> T {
+    const double2 v = x[(size_t)k * n + r];
+    return T{(C)v.x, (C)v.y};
+  };
+  // CTA 0: out = tI . bsh - tM . xs for rows warp*4 .. +3 (two pairs), lanes
+  // over the columns lane and lane+32, to ysh and to x rows [r0, r0+rows)
+  auto lead_solve = [&](int r0, int rows) {
+#pragma unroll
+    for (int hp = 0; hp < 2; hp++) {
+      C acc[16];
+#pragma unroll
+      for (int hh = 0; hh < 2; hh++) {
+        const int r = warp * 4 + hp * 2 + hh;
+        const T i0 = tI[r * TLD + lane], i1 = tI[r * TLD + lane + 32];
+        const T m0 = tM[r * TLD + lane], m1 = tM[r * TLD + lane + 32];
+#pragma unroll
+        for (int k = 0; k < RHS; k++) {
+          C sr = 0, si = 0;
+          if (k < kn) {
+            const T b0 = bsh[k][lane], b1 = bsh[k][lane + 32], y0 = xs[k][lane], y1 = xs[k][lane + 32];
+            sr = i0.x * b0.x - i0.y * b0.y + i1.x * b1.x - i1.y * b1.y -
+                 (m0.x * y0.x - m0.y * y0.y + m1.x * y1.x - m1.y * y1.y);
+            si = i0.x * b0.y + i0.y * b0.x + i1.x * b1.y + i1.y * b1.x -
+                 (m0.x * y0.y + m0.y * y0.x + m1.x * y1.y + m1.y * y1.x);
+          }
+          acc[(hh * RHS + k) * 2 + 0] = sr;
+          acc[(hh * RHS + k) * 2 + 1] = si;
+        }
+      }
+      const C v = butterfly16<C>(acc, lane);
+      const int idx = lane >> 1, hh = idx >> 3, k = (idx >> 1) & 3, part = idx & 1;
+      const int r = warp * 4 + hp * 2 + hh;
+      if ((lane & 1) == 0 && k < kn) {
+        reinterpret_cast<C*>(&ysh[k][r])[part] = v;
+        if (r < rows) reinterpret_cast<double*>(x + (size_t)k * n + r0 + r)[part] = (double)v;
+      }
+
     }
-    if (lane == 0) {
-      double2 v = x[(size_t)k * n + r];
-      v.x -= sr;
-      v.y -= si;
-      x[(size_t)k * n + r] = v;
+  };
+
+  // owners: item iterator over (step, owned slot) in consumption order
+  const int me = (int)blockIdx.x - 1;
+  auto first_slot = [&](int s) { return s > me ? (s - me + (G - 1) - 1) / (G - 1) : 0; };
+  auto live = [&](int j) { return j < own_max && 2 + me + j * (G - 1) < nb; };
+  int ps = 0, pj = 0;
+  // tile of the next item: rows warp*4+h (h < 4), columns lane + 32 e (e < 2)
+  auto load_item = [&](T(&dst)[8]) {
+    // past the last item of step ps: the next step's first slot, if live; the
+    // first slot only moves forward with the step, so a step without items
+    // means that no later step has any
+    if (ps + 1 < nb && !live(pj)) {
+      ps++;
+      pj = first_slot(ps);
+      if (!live(pj)) ps = nb - 1;
     }
+    if (ps + 1 < nb) {
+      const int q = 2 + me + pj * (G - 1);
+      const int r0 = blk(q) * TSB + warp * 4, c0 = blk(ps) * TSB, csz = min(TSB, n - c0);
+#pragma unroll
+      for (int h = 0; h < 4; h++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int r = r0 + h, c = lane + 32 * e;
+          dst[h * 2 + e] = (r < n && c < csz) ? LU[(size_t)r * n + c0 + c] : T{0, 0};
+        }
+      pj++;
+    } else {
+#pragma unroll
+      for (int u = 0; u < 8; u++) dst[u] = T{0, 0};
+    }
+    // keep the loads here, ahead of their use: without this the compiler may
+    // sink them to the apply that consumes the buffer and lose the prefetch
+    asm volatile("" ::: "memory");
+  };
+  // three tiles in flight for complex64, two for complex128 (register budget)
+  constexpr bool DEEP = sizeof(T) == 8;
+  constexpr int NBUF = DEEP ? 3 : 2;
+  T a0[8], a1[8], a2[DEEP ? 8 : 1];
+  int slot = 0;  // buffer holding the next item to apply
+
+  if (lead) {
+    // first block: x_0 = inv[0] x_0
+    tile_async<T>(inv, blk(0), tI);
+    cp_async_commit();
+    const int r0 = blk(0) * TSB, bsz = min(TSB, n - r0);
+    for (int e = t; e < TSB * RHS; e += blockDim.x) {
+      const int k = e / TSB, r = e % TSB;
+      bsh[k][r] = (k < kn && r < bsz) ? ld_x(k, r0 + r) : T{0, 0};
+      xs[k][r] = T{0, 0};
+    }
+    for (int e = t; e < TILE; e += blockDim.x) tM[e] = T{0, 0};
+    cp_async_wait_all();
+    __syncthreads();
+    lead_solve(r0, bsz);
+    __syncthreads();
+    for (int e = t; e < TSB * RHS; e += blockDim.x) xs[e / TSB][e % TSB] = ysh[e / TSB][e % TSB];
+    if (nb > 1) {
+      tile_async<T>(inv, blk(1), tI);
+      tile_async<T>(Mp, blk(1), tM);
+      cp_async_commit();
+    }
+  } else {
+    for (int j = 0; j < own_max; j++) {
+      const int q = 2 + me + j * (G - 1);
+      const int r0 = q < nb ? blk(q) * TSB : 0, bsz = q < nb ? min(TSB, n - r0) : 0;
+      for (int e = t; e < TSB * RHS; e += blockDim.x) {
+        const int k = e / TSB, r = e % TSB;
+        xo[((size_t)j * RHS + k) * TSB + r] = (k < kn && r < bsz) ? ld_x(k, r0 + r) : T{0, 0};
+      }
+    }
+    pj = first_slot(0);
+    load_item(a0);
+    load_item(a1);
+    if constexpr (DEEP) load_item(a2);
+  }
+  grid.sync();
+  for (int s = 0; s + 1 < nb; s++) {
+    const int c0 = blk(s) * TSB, csz = min(TSB, n - c0);
+    if (lead) {
+      const int nr0 = blk(s + 1) * TSB, nsz = min(TSB, n - nr0);
+      for (int e = t; e < TSB * RHS; e += blockDim.x) {
+        const int k = e / TSB, r = e % TSB;
+        bsh[k][r] = (k < kn && r < nsz) ? ld_x(k, nr0 + r) : T{0, 0};
+      }
+      cp_async_wait_all();
+      __syncthreads();
+      lead_solve(nr0, nsz);
+      __syncthreads();
+      for (int e = t; e < TSB * RHS; e += blockDim.x) xs[e / TSB][e % TSB] = ysh[e / TSB][e % TSB];
+      if (s + 2 < nb) {
+        tile_async<T>(inv, blk(s + 2), tI);
+        tile_async<T>(Mp, blk(s + 2), tM);
+        cp_async_commit();
+      }
+    } else {
+      // this lane's entries of x_s
+      T xv[RHS][2];
+#pragma unroll
+      for (int k = 0; k < RHS; k++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int c = lane + 32 * e;
+          xv[k][e] = (k < kn && c < csz) ? ld_x(k, c0 + c) : T{0, 0};
+        }
+      auto apply = [&](const T(&a)[8], int j) {
+#pragma unroll
+        for (int hp = 0; hp < 2; hp++) {
+          C acc[16];
+#pragma unroll
+          for (int hh = 0; hh < 2; hh++) {
+            const int h = hp * 2 + hh;
+#pragma unroll
+            for (int k = 0; k < RHS; k++) {
+              const T p0 = a[h * 2], p1 = a[h * 2 + 1], v0 = xv[k][0], v1 = xv[k][1];
+              acc[(hh * RHS + k) * 2 + 0] = p0.x * v0.x - p0.y * v0.y + p1.x * v1.x - p1.y * v1.y;
+              acc[(hh * RHS + k) * 2 + 1] = p0.x * v0.y + p0.y * v0.x + p1.x * v1.y + p1.y * v1.x;
+            }
+          }
+          const C v = butterfly16<C>(acc, lane);
+          const int idx = lane >> 1, hh = idx >> 3, k = (idx >> 1) & 3, part = idx & 1;
+          const int row = warp * 4 + hp * 2 + hh;
+          if ((lane & 1) == 0 && k < kn) reinterpret_cast<C*>(&xo[((size_t)j * RHS + k) * TSB + row])[part] -= v;
+        }
+      };
+      // buffers are consumed and refilled in place (a register copy of a tile
+      // whose load is still in flight would wait for it)
+      // not unrolled: three inlined copies of the tile step are already large
+#pragma unroll 1
+      for (int j = first_slot(s); live(j); j++) {
+        if (slot == 0) {
+          apply(a0, j);
+          load_item(a0);
+        } else if (slot == 1) {
+          apply(a1, j);
+          load_item(a1);
+        } else {
+          if constexpr (DEEP) {
+            apply(a2, j);
+            load_item(a2);
+          }
+        }
+        slot = slot + 1 == NBUF ? 0 : slot + 1;
+      }
+      // publish block s+2 if owned here
+      const int qp = s + 2;
+      if (qp < nb && (qp - 2) % (G - 1) == me) {
+        __syncthreads();
+        const int j = (qp - 2) / (G - 1), r0 = blk(qp) * TSB, bsz = min(TSB, n - r0);
+        for (int e = t; e < TSB * RHS; e += blockDim.x) {
+          const int k = e / TSB, r = e % TSB;
+          if (k < kn && r < bsz) {
+            const T v = xo[((size_t)j * RHS + k) * TSB + r];
+            x[(size_t)k * n + r0 + r] = make_double2((double)v.x, (double)v.y);
+          }
+        }
+      }
+    }
+    grid.sync();
   }
 }
 
@@ -157,8 +470,65 @@ int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cud
 }
 
 template <typename T>
-int lu_solve_device(const T* d_LU, int n, const int32_t* d_perm, double* d_x, double* d_tmp, int nrhs,
-                    cudaStream_t st) {
+int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st) {
+  const int nb = (n + TSB - 1) / TSB;
+  const size_t need = (size_t)nb * TSB * TSB;
+  if (blk.invL.count < need) {
+    TT_TRY(blk.invL.alloc(need));
+    TT_TRY(blk.invU.alloc(need));
+    TT_TRY(blk.mL.alloc(need));
+    TT_TRY(blk.mU.alloc(need));
+  }
+  blk.n = n;
+  const size_t smem = (size_t)TSB * TLD * sizeof(T);
+  static bool attr = false;
+  if (!attr) {
+    TT_CUDA_TRY(cudaFuncSetAttribute(k_inv_diag<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TT_CUDA_TRY(cudaFuncSetAttribute(k_inv_diag<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TT_CUDA_TRY(
+        cudaFuncSetAttribute(k_prev_mul<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem)));
+    TT_CUDA_TRY(
+        cudaFuncSetAttribute(k_prev_mul<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem)));
+    attr = true;
+  }
+  k_inv_diag<T, false><<<nb, 512, smem, st>>>(d_LU, n, blk.invL.ptr);
+  count_launch();
+  k_inv_diag<T, true><<<nb, 512, smem, st>>>(d_LU, n, blk.invU.ptr);
+  count_launch();
+  k_prev_mul<T, false><<<nb, 512, 2 * smem, st>>>(d_LU, n, blk.invL.ptr, blk.mL.ptr);
+  count_launch();
+  k_prev_mul<T, true><<<nb, 512, 2 * smem, st>>>(d_LU, n, blk.invU.ptr, blk.mU.ptr);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+template int lu_trsv_prepare<double2>(const double2*, int, TrsvBlocks<double2>&, cudaStream_t);
+template int lu_trsv_prepare<float2>(const float2*, int, TrsvBlocks<float2>&, cudaStream_t);
+
+template <typename T>
+int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_t* d_perm, double* d_x,
+                    double* d_tmp, int nrhs, cudaStream_t st) {
+  if (n <= 0 || nrhs <= 0) return TT_OK;
+  if (blk.n != n || !blk.invL.ptr) {
+    set_error("triangular solve called without the inverted diagonal blocks of this factor");
+    return TT_ERR_BADARG;
+  }
+  const int G = std::max(2, device_sm_count());
+  const int nb = (n + TSB - 1) / TSB;
+  int own_max = std::max(1, (nb - 2 + (G - 1) - 1) / (G - 1));
+  const size_t smem = (size_t)2 * TSB * TLD * sizeof(T) + (size_t)own_max * RHS * TSB * sizeof(T);
+  constexpr size_t kMaxSmem = 212 * 1024;  // + up to 12 KB static, within the 227 KB per CTA
+  if (smem > kMaxSmem) {
+    set_error("triangular solve: n = " + std::to_string(n) + " needs " + std::to_string(smem) +
+              " bytes of shared memory per CTA (limit " + std::to_string(kMaxSmem) + ")");
+    return TT_ERR_UNSUPPORTED;
+  }
+  static bool attr = false;
+  if (!attr) {
+    TT_CUDA_TRY(cudaFuncSetAttribute(k_trsv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+    TT_CUDA_TRY(cudaFuncSetAttribute(k_trsv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+    attr = true;
+  }
   ProfScope prof(TT_PROF_TRSV, st, 8.0 * n * (double)n * nrhs, (double)n * n * sizeof(T));
   TT_CUDA_TRY(cudaMemcpyAsync(d_tmp, d_x, sizeof(double2) * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, st));
   double2* x = reinterpret_cast<double2*>(d_x);
@@ -166,40 +536,27 @@ int lu_solve_device(const T* d_LU, int n, const int32_t* d_perm, double* d_x, do
                                                             nrhs, x);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
-  const size_t dsm = (size_t)SB * SB * sizeof(T);
-  static bool attr_set = false;
-  if (!attr_set) {
-    TT_CUDA_TRY(cudaFuncSetAttribute(k_diag_solve<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
-    TT_CUDA_TRY(cudaFuncSetAttribute(k_diag_solve<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
-    attr_set = true;
-  }
-  // forward: unit lower
-  for (int i0 = 0; i0 < n; i0 += SB) {
-    const int bs = min(SB, n - i0);
-    k_diag_solve<T, true><<<1, 256, (size_t)bs * bs * sizeof(T), st>>>(d_LU, n, i0, bs, x, nrhs);
+  for (int k0 = 0; k0 < nrhs; k0 += RHS) {
+    int kn = std::min(RHS, nrhs - k0);
+    double2* xk = x + (size_t)k0 * n;
+    const T* LUp = d_LU;
+    int nn = n;
+    const T* invL = blk.invL.ptr;
+    const T* invU = blk.invU.ptr;
+    const T* mL = blk.mL.ptr;
+    const T* mU = blk.mU.ptr;
+    void* argsL[] = {&LUp, &invL, &mL, &nn, &xk, &kn, &own_max};
+    TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trsv<T, false>, dim3(G), dim3(TRSV_THREADS), argsL, smem, st));
     count_launch();
-    const int r_lo = i0 + bs;
-    if (r_lo < n) {
-      k_block_update<T><<<ceil_div((size_t)(n - r_lo) * 32, 256), 256, 0, st>>>(d_LU, n, i0, bs, r_lo, n, x, nrhs);
-      count_launch();
-    }
-  }
-  TT_CUDA_TRY(cudaGetLastError());
-  // backward: upper with diagonal
-  const int nblk = (n + SB - 1) / SB;
-  for (int b = nblk - 1; b >= 0; b--) {
-    const int i0 = b * SB, bs = min(SB, n - i0);
-    k_diag_solve<T, false><<<1, 256, (size_t)bs * bs * sizeof(T), st>>>(d_LU, n, i0, bs, x, nrhs);
+    void* argsU[] = {&LUp, &invU, &mU, &nn, &xk, &kn, &own_max};
+    TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trsv<T, true>, dim3(G), dim3(TRSV_THREADS), argsU, smem, st));
     count_launch();
-    if (i0 > 0) {
-      k_block_update<T><<<ceil_div((size_t)i0 * 32, 256), 256, 0, st>>>(d_LU, n, i0, bs, 0, i0, x, nrhs);
-      count_launch();
-    }
   }
-  TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
-template int lu_solve_device<double2>(const double2*, int, const int32_t*, double*, double*, int, cudaStream_t);
-template int lu_solve_device<float2>(const float2*, int, const int32_t*, double*, double*, int, cudaStream_t);
+template int lu_solve_device<double2>(const double2*, int, const TrsvBlocks<double2>&, const int32_t*, double*,
+                                      double*, int, cudaStream_t);
+template int lu_solve_device<float2>(const float2*, int, const TrsvBlocks<float2>&, const int32_t*, double*,
+                                     double*, int, cudaStream_t);
 
 }  // namespace tt

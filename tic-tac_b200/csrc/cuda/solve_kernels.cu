@@ -205,43 +205,73 @@ __global__ void k_gather_rhs(const double* __restrict__ A, int n, const int32_t*
 }
 
 // r_k = b_k - x_k + A y_k, y_k = G o x_k; warp per row, up to 8 rhs per pass.
-constexpr int RES_MAXR = 8;
-__global__ void k_residual(const double* __restrict__ A, int n, const double2* __restrict__ y,
-                           const double2* __restrict__ b, const double2* __restrict__ x, int nrhs,
-                           double2* __restrict__ r) {
+constexpr int RES_MAXR = 4;
+// r_k = b_k - x_k + A y_k for up to RES_MAXR right-hand sides per pass; each
+// warp takes RES_ROWS rows so that every y element fetched serves 4 rows of A,
+// and each lane keeps 4 rows x 4 columns of A in flight.
+constexpr int RES_ROWS = 4;
+__global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, int n, const double2* __restrict__ y,
+                                                  const double2* __restrict__ b, const double2* __restrict__ x,
+                                                  int nrhs, double2* __restrict__ r) {
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int i = (int)warp;
-  const double* Ar = A + (size_t)i * n;
+  const int64_t r0 = warp * RES_ROWS;
+  if (r0 >= n) return;
+  const int nr = (int)min((int64_t)RES_ROWS, (int64_t)n - r0);
+  const double* Ar[RES_ROWS];
+#pragma unroll
+  for (int h = 0; h < RES_ROWS; h++) Ar[h] = A + (size_t)(r0 + min(h, nr - 1)) * n;
   for (int k0 = 0; k0 < nrhs; k0 += RES_MAXR) {
     const int kn = min(RES_MAXR, nrhs - k0);
-    double sr[RES_MAXR], si[RES_MAXR];
+    double sr[RES_ROWS][RES_MAXR], si[RES_ROWS][RES_MAXR];
 #pragma unroll
-    for (int k = 0; k < RES_MAXR; k++) sr[k] = si[k] = 0.0;
-    for (int c = lane; c < n; c += 32) {
-      const double a = Ar[c];
+    for (int h = 0; h < RES_ROWS; h++)
 #pragma unroll
-      for (int k = 0; k < RES_MAXR; k++) {
-        if (k < kn) {
-          const double2 yv = y[(size_t)(k0 + k) * n + c];
-          sr[k] += a * yv.x;
-          si[k] += a * yv.y;
+      for (int k = 0; k < RES_MAXR; k++) sr[h][k] = si[h][k] = 0.0;
+    for (int c0 = 0; c0 < n; c0 += 128) {
+      double a[RES_ROWS][4];
+#pragma unroll
+      for (int h = 0; h < RES_ROWS; h++)
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int c = c0 + lane + 32 * u;
+          a[h][u] = c < n ? __ldg(Ar[h] + c) : 0.0;
+        }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int c = c0 + lane + 32 * u;
+        if (c >= n) break;
+#pragma unroll
+        for (int k = 0; k < RES_MAXR; k++) {
+          if (k >= kn) break;
+          const double2 yv = __ldg(y + (size_t)(k0 + k) * n + c);
+#pragma unroll
+          for (int h = 0; h < RES_ROWS; h++) {
+            sr[h][k] += a[h][u] * yv.x;
+            si[h][k] += a[h][u] * yv.y;
+          }
         }
       }
     }
 #pragma unroll
-    for (int k = 0; k < RES_MAXR; k++) {
-      for (int o = 16; o > 0; o >>= 1) {
-        sr[k] += __shfl_down_sync(0xffffffffu, sr[k], o);
-        si[k] += __shfl_down_sync(0xffffffffu, si[k], o);
+    for (int h = 0; h < RES_ROWS; h++)
+#pragma unroll
+      for (int k = 0; k < RES_MAXR; k++) {
+        for (int o = 16; o > 0; o >>= 1) {
+          sr[h][k] += __shfl_xor_sync(0xffffffffu, sr[h][k], o);
+          si[h][k] += __shfl_xor_sync(0xffffffffu, si[h][k], o);
+        }
       }
-    }
     if (lane == 0) {
-      for (int k = 0; k < kn; k++) {
-        const size_t o = (size_t)(k0 + k) * n + i;
-        r[o] = make_double2(b[o].x - x[o].x + sr[k], b[o].y - x[o].y + si[k]);
-      }
+#pragma unroll
+      for (int h = 0; h < RES_ROWS; h++)
+#pragma unroll
+        for (int k = 0; k < RES_MAXR; k++) {
+          if (h < nr && k < kn) {
+            const size_t o = (size_t)(k0 + k) * n + r0 + h;
+            r[o] = make_double2(b[o].x - x[o].x + sr[h][k], b[o].y - x[o].y + si[h][k]);
+          }
+        }
     }
   }
 }
@@ -365,7 +395,7 @@ int residual_multi_device(const double* d_A, int n, const double* d_y, const dou
                           double* d_r, cudaStream_t st) {
   ProfScope prof(TT_PROF_RESIDUAL, st, 4.0 * n * (double)n * nrhs,
                  8.0 * n * (double)n * ((nrhs + RES_MAXR - 1) / RES_MAXR));
-  k_residual<<<ceil_div((size_t)n * 32, 256), 256, 0, st>>>(
+  k_residual<<<ceil_div(ceil_div((size_t)n, RES_ROWS) * 32, 256), 256, 0, st>>>(
       d_A, n, reinterpret_cast<const double2*>(d_y), reinterpret_cast<const double2*>(d_b),
       reinterpret_cast<const double2*>(d_x), nrhs, reinterpret_cast<double2*>(d_r));
   count_launch();

@@ -76,11 +76,22 @@ template <typename T>
 int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_tensor_cores, int* info);
 // Row permutation of the interchange sequence ipiv (host, once per factorisation).
 int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cudaStream_t st);
+// Inverted diagonal blocks of one LU factor (unit lower and upper) and their
+// products with the neighbouring off-diagonal blocks, made by lu_trsv_prepare
+// after each factorisation and read by every solve with it.
+template <typename T>
+struct TrsvBlocks {
+  DevBuf<T> invL, invU;  // inverted 64 x 64 diagonal blocks
+  DevBuf<T> mL, mU;      // inv[b] times the block that carries the previous solved block into b
+  int n = 0;
+};
+template <typename T>
+int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st);
 // Solve L U x = P b for nrhs complex128 columns [k][n] in place using the factor
 // of type T; d_perm from lu_permutation (uploaded), d_tmp scratch of 2 n nrhs doubles.
 template <typename T>
-int lu_solve_device(const T* d_LU, int n, const int32_t* d_perm, double* d_x, double* d_tmp, int nrhs,
-                    cudaStream_t st);
+int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_t* d_perm, double* d_x,
+                    double* d_tmp, int nrhs, cudaStream_t st);
 
 // x += d ; returns max |d| / max |x| per rhs in h_ratio (host, synchronises).
 int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_dx_over_x, cudaStream_t st);

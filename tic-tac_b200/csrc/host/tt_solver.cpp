@@ -199,6 +199,8 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
   TT_TRY(x.alloc((size_t)2 * n * nd));
   DevBuf<double2> L64;
   DevBuf<float2> L32;
+  TrsvBlocks<double2> tb64;
+  TrsvBlocks<float2> tb32;
   if (opt.mixed) {
     TT_TRY(L32.alloc((size_t)n * n));
     TT_TRY(y.alloc((size_t)2 * n * nd));
@@ -241,8 +243,13 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     TT_TRY(perm_d.upload(perm, st));
     TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nd, b.ptr, st));
     TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * 2 * n * nd, cudaMemcpyDeviceToDevice, st));
-    if (opt.mixed) TT_TRY(lu_solve_device<float2>(L32.ptr, n, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
-    else TT_TRY(lu_solve_device<double2>(L64.ptr, n, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+    if (opt.mixed) {
+      TT_TRY(lu_trsv_prepare<float2>(L32.ptr, n, tb32, st));
+      TT_TRY(lu_solve_device<float2>(L32.ptr, n, tb32, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+    } else {
+      TT_TRY(lu_trsv_prepare<double2>(L64.ptr, n, tb64, st));
+      TT_TRY(lu_solve_device<double2>(L64.ptr, n, tb64, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+    }
     TT_CUDA_TRY(cudaStreamSynchronize(st));
     r.ms_solve += ms_since(t0);
     if (opt.mixed) {
@@ -255,7 +262,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       for (it = 1; it <= opt.refine_max_iter; it++) {
         TT_TRY(hadamard_device(Gj, rhs_e.ptr, n, x.ptr, nd, y.ptr, st));
         TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nd, res.ptr, st));
-        TT_TRY(lu_solve_device<float2>(L32.ptr, n, perm_d.ptr, res.ptr, tmp.ptr, nd, st));
+        TT_TRY(lu_solve_device<float2>(L32.ptr, n, tb32, perm_d.ptr, res.ptr, tmp.ptr, nd, st));
         TT_TRY(axpy_norms_device(x.ptr, res.ptr, n, nd, ratio.data(), st));
         worst = 0;
         for (double v : ratio) worst = std::max(worst, v);
