@@ -136,9 +136,12 @@ def step_flops(ns, nE):
 
 
 # DRAM traffic of the tensor-core update per algorithmic byte (C read + written
-# as complex64, L and U panels read once), from the ncu capture of that kernel
-# in profiles/k_lu_update_tc.md; scales the bench's mean launch to a traffic figure.
-TC_TRAFFIC_PER_ALGO_BYTE = None
+# as complex64, L and U panels read once): dram__bytes_read.sum +
+# dram__bytes_write.sum over 16 M N + 8 (M + N) K for two launches (M = N = 7536
+# and 7280, K = 256) of the n = 9072 capture in profiles/k_lu_update_tc_n9072.md
+# (926.4 / 939.5 MB and 861.2 / 877.8 MB); traffic grows with the tile count, so
+# the ratio scales the bench's mean launch to a per-launch traffic figure.
+TC_TRAFFIC_PER_ALGO_BYTE = 0.984
 
 
 def roofline_of(kern, timed_ms, ms_step, ns, nE):
