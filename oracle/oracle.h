@@ -2,7 +2,7 @@
  * algorithm, used ONLY as the checker in tests/, by __graft_entry__.smoke() and
  * as bench.py's cpu_baseline.  Never linked into or called by the product.
  *
- * Parity pinning: tests/test_oracle.py checks every function here against the
+ * Parity pinning: tests/test_oracle_golden.py checks every function here against the
  * golden fixtures produced by the reference's own code (tests/golden/). */
 #ifndef TT_ORACLE_H
 #define TT_ORACLE_H
