@@ -114,6 +114,8 @@ typedef struct tt_solve_report {
   int refine_iters;     /* max over energies */
   double final_correction;
   int info;             /* first zero pivot (1-based), 0 if none */
+  double ms_adjoint;    /* adjoint: transposed solves, their refinement, parameter products */
+  int adjoint_refine_iters;
 } tt_solve_report;
 
 /* ---- layer 1: drop-in entry points ---------------------------------- */
@@ -162,6 +164,22 @@ int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double*
                                const size_t* P123_colptr_csc, size_t P123_nnz, const double* V_WP_unco,
                                const double* V_WP_coup, const tt_swp_states* swp, const tt_os_indexing* os,
                                const tt_pw_states* pw, const tt_run_params* rp, tt_solve_report* report);
+
+/* Adjoint of tt_solve_faddeev_equations (no counterpart in the reference):
+ * besides U, the derivatives dU/dtheta_k for n_theta perturbations of the
+ * potential, given as dV/dtheta_k in the layout of V_WP_unco / V_WP_coup
+ * ([n_theta][Np Np num_unco] and [n_theta][4 Np Np num_coup]).  Per energy
+ * one transposed solve with the same LU factors gives lambda = (1 - A G)^-T e
+ * for the on-shell rows, and dU[d'][d] = lambda_d'^T dA (e_d + G x_d) with
+ * dA = C^T (2 P123)(dV C); the mixed-precision path refines lambda in FP64.
+ * dU_dtheta[k*nE*nd*nd + d'*nd*nE + d*nE + j] (caller allocates).
+ * At most 4 deuteron states per channel. */
+int tt_solve_faddeev_adjoint(tt_complex* U, tt_complex* dU_dtheta, int n_theta, const double* dV_WP_unco_dtheta,
+                             const double* dV_WP_coup_dtheta, const tt_complex* G, const double* P123_val,
+                             const int* P123_row, const size_t* P123_colptr_csc, size_t P123_nnz,
+                             const double* V_WP_unco, const double* V_WP_coup, const tt_swp_states* swp,
+                             const tt_os_indexing* os, const tt_pw_states* pw, const tt_run_params* rp,
+                             tt_solve_report* report);
 
 void tt_free(void* p);
 const char* tt_last_error_string(void);
@@ -240,6 +258,18 @@ int tt_run_build_resolvent(tt_run* run, int chn);
 int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_report* report);
 /* Release the channel's device data (all of it, or only A and the resolvents,
  * keeping P123 resident for the next parameter set or energy scan). */
+/* tt_run_solve plus dU/dtheta (see tt_solve_faddeev_adjoint), for dV/dtheta
+ * arrays over all 2N channels of the run (sizes as tt_run_get_host_array
+ * which = 3 and 4). */
+int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const double* dV_WP_unco_dtheta,
+                         const double* dV_WP_coup_dtheta, tt_complex* U, tt_complex* dU_dtheta,
+                         tt_solve_report* report);
+/* Low-energy constants of the run's potential that the option lec_offsets
+ * moves (LO_internal: C_1S0, C_3S1; none for malfliet_tjon), their values,
+ * and dV/dLEC_k in the WP basis for all 2N channels (the potential is linear
+ * in these contacts, so the central difference is exact up to rounding). */
+int tt_run_num_lecs(const tt_run* run, int* n_lecs, double* values);
+int tt_run_lec_derivative(const tt_run* run, int k, double* dV_WP_unco, double* dV_WP_coup);
 int tt_run_release_channel(tt_run* run, int chn);
 int tt_run_release_A(tt_run* run, int chn);
 

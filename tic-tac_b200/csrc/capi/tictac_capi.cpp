@@ -120,6 +120,103 @@ void fill_report(const SolveReport& r, double ms_A, tt_solve_report* out) {
   out->refine_iters = r.refine_iters;
   out->final_correction = r.final_correction;
   out->info = r.info;
+  out->ms_adjoint = r.ms_adjoint;
+  out->adjoint_refine_iters = r.adjoint_refine_iters;
+}
+
+// dV_k C blocks (layout of ChannelLayout::VC) of n_theta potential derivatives
+int dvc_blocks(const RunParams& rp, const PWChannel& ch, const SWPStates& w, int n_theta, const double* dVu,
+               const double* dVc, std::vector<double>& out, size_t& per) {
+  const size_t Np = w.Np_WP, nu = Np * Np * w.n_unco, nc = 4 * Np * Np * w.n_coup;
+  out.clear();
+  per = 0;
+  for (int k = 0; k < n_theta; k++) {
+    std::vector<double> Vu(dVu + k * nu, dVu + (k + 1) * nu), Vc;
+    if (nc) Vc.assign(dVc + k * nc, dVc + (k + 1) * nc);
+    ChannelLayout Lk;
+    std::string err;
+    if (!build_channel_layout(rp, ch, w, Vu, Vc, Lk, &err)) return fail(TT_ERR_BADARG, err);
+    per = Lk.VC.size();
+    out.insert(out.end(), Lk.VC.begin(), Lk.VC.end());
+  }
+  return TT_OK;
+}
+
+// tt_solve_faddeev_equations, with the adjoint when n_theta > 0
+int dropin_solve(tt_complex* U, tt_complex* dU, int n_theta, const double* dVu, const double* dVc,
+                 const tt_complex* G, const double* P_val, const int* P_row, const size_t* P_colptr, size_t P_nnz,
+                 const double* V_unco, const double* V_coup, const tt_swp_states* swp, const tt_os_indexing* os,
+                 const tt_pw_states* pw, const tt_run_params* rpp, tt_solve_report* report) {
+  if (!U || !G || !P_colptr || !swp || !os || !pw || !rpp) return fail(TT_ERR_BADARG, "null argument");
+  if (P_nnz && (!P_val || !P_row)) return fail(TT_ERR_BADARG, "null P123 arrays");
+  if (n_theta < 0 || (n_theta > 0 && (!dU || !dVu || (swp->num_2N_coup_states && !dVc))))
+    return fail(TT_ERR_BADARG, "null or negative adjoint arguments");
+  RunParams rp = params_of(rpp);
+  SWPStates w = swp_of(swp);
+  const size_t Np = w.Np_WP;
+  std::vector<double> Vu(V_unco, V_unco + Np * Np * w.n_unco);
+  std::vector<double> Vc;
+  if (w.n_coup) Vc.assign(V_coup, V_coup + 4 * Np * Np * w.n_coup);
+  ChannelLayout L;
+  std::string err;
+  const PWChannel ch = view_of(pw);
+  if (!build_channel_layout(rp, ch, w, Vu, Vc, L, &err)) return fail(TT_ERR_BADARG, err);
+  const int n = ch.Nalpha * w.Np_WP * w.Nq_WP;
+  // CSC (column pointers, row indices) -> CSR with ascending columns
+  std::vector<int64_t> rowptr(n + 1, 0);
+  for (size_t e = 0; e < P_nnz; e++) {
+    if (P_row[e] < 0 || P_row[e] >= n) return fail(TT_ERR_BADARG, "P123 row index out of range");
+    rowptr[P_row[e] + 1]++;
+  }
+  for (int r = 0; r < n; r++) rowptr[r + 1] += rowptr[r];
+  std::vector<int32_t> col(P_nnz);
+  std::vector<double> val(P_nnz);
+  std::vector<int64_t> fillpos(rowptr.begin(), rowptr.end() - 1);
+  for (int c = 0; c < n; c++)
+    for (size_t e = P_colptr[c]; e < P_colptr[c + 1]; e++) {
+      const int64_t p = fillpos[P_row[e]]++;
+      col[p] = c;
+      val[p] = P_val[e];
+    }
+  cudaStream_t st = default_stream();
+  ChannelSolver cs;
+  int s = cs.setup(L, w.q_WP, st);
+  if (s != TT_OK) return s;
+  s = cs.set_P_host_csr(rowptr.data(), col.data(), val.data(), (int64_t)P_nnz, st);
+  if (s != TT_OK) return s;
+  double msA = 0;
+  s = cs.build_A(st, &msA);
+  if (s != TT_OK) return s;
+  // G supplied by the caller: upload into the solver through resolvent-shaped storage
+  std::vector<double> dummyE(os->num_T_lab, 0.0);
+  s = cs.resolvent(dummyE, st);
+  if (s != TT_OK) return s;
+  if (cudaMemcpy((void*)cs.G(), G, sizeof(tt_complex) * (size_t)n * os->num_T_lab, cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return fail(TT_ERR_CUDA, "upload of G failed");
+  std::vector<int> q_idx(os->q_com_idx_array, os->q_com_idx_array + os->num_T_lab);
+  std::vector<int> deut(os->deuteron_idx_array, os->deuteron_idx_array + os->num_deuteron_states);
+  std::vector<double> Uh, dUh, dvc;
+  SolveReport rep;
+  if (rpp->precision < TT_PRECISION_FP64 || rpp->precision > TT_PRECISION_MIXED_SIMT)
+    return fail(TT_ERR_BADARG, "unknown precision");
+  AdjointRequest adj;
+  DevBuf<double> d_dvc;
+  if (n_theta > 0) {
+    size_t per = 0;
+    TT_TRY(dvc_blocks(rp, ch, w, n_theta, dVu, dVc, dvc, per));
+    TT_TRY(d_dvc.upload(dvc, st));
+    adj.n_theta = n_theta;
+    adj.d_dVC = d_dvc.ptr;
+    adj.vc_count = per;
+    adj.dU = &dUh;
+  }
+  s = cs.solve(q_idx, deut, options_of(rp, rpp->precision), Uh, &rep, st, n_theta > 0 ? &adj : nullptr);
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  if (n_theta > 0) std::memcpy(dU, dUh.data(), sizeof(double) * dUh.size());
+  return TT_OK;
 }
 
 }  // namespace
@@ -267,62 +364,17 @@ int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double*
                                const size_t* P_colptr, size_t P_nnz, const double* V_unco, const double* V_coup,
                                const tt_swp_states* swp, const tt_os_indexing* os, const tt_pw_states* pw,
                                const tt_run_params* rpp, tt_solve_report* report) {
-  if (!U || !G || !P_colptr || !swp || !os || !pw || !rpp) return fail(TT_ERR_BADARG, "null argument");
-  if (P_nnz && (!P_val || !P_row)) return fail(TT_ERR_BADARG, "null P123 arrays");
-  RunParams rp = params_of(rpp);
-  SWPStates w = swp_of(swp);
-  const size_t Np = w.Np_WP;
-  std::vector<double> Vu(V_unco, V_unco + Np * Np * w.n_unco);
-  std::vector<double> Vc;
-  if (w.n_coup) Vc.assign(V_coup, V_coup + 4 * Np * Np * w.n_coup);
-  ChannelLayout L;
-  std::string err;
-  const PWChannel ch = view_of(pw);
-  if (!build_channel_layout(rp, ch, w, Vu, Vc, L, &err)) return fail(TT_ERR_BADARG, err);
-  const int n = ch.Nalpha * w.Np_WP * w.Nq_WP;
-  // CSC (column pointers, row indices) -> CSR with ascending columns
-  std::vector<int64_t> rowptr(n + 1, 0);
-  for (size_t e = 0; e < P_nnz; e++) {
-    if (P_row[e] < 0 || P_row[e] >= n) return fail(TT_ERR_BADARG, "P123 row index out of range");
-    rowptr[P_row[e] + 1]++;
-  }
-  for (int r = 0; r < n; r++) rowptr[r + 1] += rowptr[r];
-  std::vector<int32_t> col(P_nnz);
-  std::vector<double> val(P_nnz);
-  std::vector<int64_t> fillpos(rowptr.begin(), rowptr.end() - 1);
-  for (int c = 0; c < n; c++)
-    for (size_t e = P_colptr[c]; e < P_colptr[c + 1]; e++) {
-      const int64_t p = fillpos[P_row[e]]++;
-      col[p] = c;
-      val[p] = P_val[e];
-    }
-  cudaStream_t st = default_stream();
-  ChannelSolver cs;
-  int s = cs.setup(L, w.q_WP, st);
-  if (s != TT_OK) return s;
-  s = cs.set_P_host_csr(rowptr.data(), col.data(), val.data(), (int64_t)P_nnz, st);
-  if (s != TT_OK) return s;
-  double msA = 0;
-  s = cs.build_A(st, &msA);
-  if (s != TT_OK) return s;
-  // G supplied by the caller: upload into the solver through resolvent-shaped storage
-  std::vector<double> dummyE(os->num_T_lab, 0.0);
-  s = cs.resolvent(dummyE, st);
-  if (s != TT_OK) return s;
-  if (cudaMemcpy((void*)cs.G(), G, sizeof(tt_complex) * (size_t)n * os->num_T_lab, cudaMemcpyHostToDevice) !=
-      cudaSuccess)
-    return fail(TT_ERR_CUDA, "upload of G failed");
-  std::vector<int> q_idx(os->q_com_idx_array, os->q_com_idx_array + os->num_T_lab);
-  std::vector<int> deut(os->deuteron_idx_array, os->deuteron_idx_array + os->num_deuteron_states);
-  std::vector<double> Uh;
-  SolveReport rep;
-  if (rpp->precision < TT_PRECISION_FP64 || rpp->precision > TT_PRECISION_MIXED_SIMT)
-    return fail(TT_ERR_BADARG, "unknown precision");
-  s = cs.solve(q_idx, deut, options_of(rp, rpp->precision), Uh, &rep, st);
-  fill_report(rep, msA, report);
-  if (s != TT_OK) return s;
-  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
-  return TT_OK;
+  return dropin_solve(U, nullptr, 0, nullptr, nullptr, G, P_val, P_row, P_colptr, P_nnz, V_unco, V_coup, swp, os, pw,
+                      rpp, report);
+}
+
+int tt_solve_faddeev_adjoint(tt_complex* U, tt_complex* dU, int n_theta, const double* dVu, const double* dVc,
+                             const tt_complex* G, const double* P_val, const int* P_row, const size_t* P_colptr,
+                             size_t P_nnz, const double* V_unco, const double* V_coup, const tt_swp_states* swp,
+                             const tt_os_indexing* os, const tt_pw_states* pw, const tt_run_params* rpp,
+                             tt_solve_report* report) {
+  return dropin_solve(U, dU, n_theta, dVu, dVc, G, P_val, P_row, P_colptr, P_nnz, V_unco, V_coup, swp, os, pw, rpp,
+                      report);
 }
 
 // ---------------------------------------------------------------------------
@@ -471,6 +523,71 @@ int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_re
   fill_report(rep, msA, report);
   if (s != TT_OK) return s;
   std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  return TT_OK;
+}
+
+int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const double* dVu, const double* dVc,
+                         tt_complex* U, tt_complex* dU, tt_solve_report* report) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!U || n_theta < 0 || (n_theta > 0 && (!dU || !dVu || (run->swp.n_coup && !dVc))))
+    return fail(TT_ERR_BADARG, "null or negative argument");
+  if (precision < TT_PRECISION_FP64 || precision > TT_PRECISION_MIXED_SIMT) return fail(TT_ERR_BADARG, "unknown precision");
+  double msA = 0;
+  if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
+  if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));
+  const PWChannel ch = channel_view(run->pw, chn);
+  const std::vector<int> deut = deuteron_indices(ch);
+  std::vector<double> Uh, dUh, dvc;
+  AdjointRequest adj;
+  DevBuf<double> d_dvc;
+  if (n_theta > 0) {
+    size_t per = 0;
+    TT_TRY(dvc_blocks(run->rp, ch, run->swp, n_theta, dVu, dVc, dvc, per));
+    TT_TRY(d_dvc.upload(dvc, run_stream(run)));
+    adj.n_theta = n_theta;
+    adj.d_dVC = d_dvc.ptr;
+    adj.vc_count = per;
+    adj.dU = &dUh;
+  }
+  SolveReport rep;
+  s = run->chn[chn].solver->solve(run->os.q_com_idx, deut, options_of(run->rp, precision), Uh, &rep,
+                                  run_stream(run), n_theta > 0 ? &adj : nullptr);
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  if (n_theta > 0) std::memcpy(dU, dUh.data(), sizeof(double) * dUh.size());
+  return TT_OK;
+}
+
+int tt_run_num_lecs(const tt_run* run, int* n_lecs, double* values) {
+  if (!run || !n_lecs) return fail(TT_ERR_BADARG, "null argument");
+  *n_lecs = num_lecs(run->rp.potential_model);
+  if (values) {
+    const std::vector<double> v = nominal_lecs(run->rp.potential_model);
+    for (int k = 0; k < *n_lecs; k++)
+      values[k] = v[k] + (k < (int)run->rp.lec_offsets.size() ? run->rp.lec_offsets[k] : 0.0);
+  }
+  return TT_OK;
+}
+
+int tt_run_lec_derivative(const tt_run* run, int k, double* dVu, double* dVc) {
+  if (!run || !dVu || (run->swp.n_coup && !dVc)) return fail(TT_ERR_BADARG, "null argument");
+  const int nl = num_lecs(run->rp.potential_model);
+  if (k < 0 || k >= nl) return fail(TT_ERR_BADARG, "LEC index out of range");
+  const std::vector<double> nom = nominal_lecs(run->rp.potential_model);
+  // V is linear in the contact constants: any step gives the exact derivative
+  const double h = std::max(std::fabs(nom[k]), 1e-6);
+  std::vector<double> up[2], uc[2];
+  for (int sgn = 0; sgn < 2; sgn++) {
+    RunParams rp = run->rp;
+    rp.lec_offsets.resize(nl, 0.0);
+    rp.lec_offsets[k] += sgn == 0 ? h : -h;
+    std::string err;
+    if (!potential_matrices(rp, run->fwp, run->pw, up[sgn], uc[sgn], &err)) return fail(TT_ERR_BADARG, err);
+  }
+  for (size_t i = 0; i < up[0].size(); i++) dVu[i] = (up[0][i] - up[1][i]) / (2 * h);
+  for (size_t i = 0; i < uc[0].size(); i++) dVc[i] = (uc[0][i] - uc[1][i]) / (2 * h);
   return TT_OK;
 }
 

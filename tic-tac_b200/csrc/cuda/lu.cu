@@ -68,29 +68,52 @@ __global__ void k_permute(const double2* __restrict__ b, const int32_t* __restri
   x[t] = b[(size_t)k * n + perm[i]];
 }
 
+// x[perm[i]] = w[i]: the row interchanges applied backwards (transposed solves)
+__global__ void k_permute_inv(const double2* __restrict__ w, const int32_t* __restrict__ perm, int n, int nrhs,
+                              double2* __restrict__ x) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * nrhs) return;
+  const int k = (int)(t / n), i = (int)(t % n);
+  x[(size_t)k * n + perm[i]] = w[t];
+}
+
 // ---------------------------------------------------------------------------
-// Inverses of the diagonal blocks: inv[b] (64 x 64, row-major) of the unit lower
-// (UPPER = false) or upper (UPPER = true) block b of the factor.  Rows and
-// columns past n are the identity.  In place in shared memory, right-looking:
-// lower, j ascending: X[r][c] -= L[r][j] X[j][c] for r > j, c <= j;
-// upper, j descending: row j is scaled by 1/U[j][j], then
+// Inverses of the diagonal blocks: inv[b] (64 x 64, row-major) of the lower
+// (UPPER = false) or upper (UPPER = true) triangle of block b of the factor,
+// with a unit diagonal (UNIT) or the stored one.  The factor of L U keeps the
+// unit lower and the upper triangle; its transpose (for transposed solves)
+// keeps the non-unit lower and the unit upper triangle.  Rows and columns past
+// n are the identity.  In place in shared memory, right-looking, row j being
+// final when step j starts:
+// lower, j ascending: row j is scaled by 1/D[j][j], then
+// X[r][c] -= L[r][j] X[j][c] for r > j, c <= j;
+// upper, j descending: row j is scaled by 1/D[j][j], then
 // X[r][c] -= U[r][j] X[j][c] for r < j, c >= j.
-template <typename T, bool UPPER>
+template <typename T, bool UPPER, bool UNIT>
 __global__ void __launch_bounds__(512) k_inv_diag(const T* __restrict__ LU, int n, T* __restrict__ inv) {
   extern __shared__ unsigned char ism[];
   T* M = reinterpret_cast<T*>(ism);  // [TSB][TLD]
   __shared__ T col[TSB];
   const int b = blockIdx.x, r0 = b * TSB, bs = min(TSB, n - r0);
   const T zero = {0, 0}, one = {1, 0};
+  // stored entries of the triangle (the diagonal only when it is not unit)
+  auto stored = [](int r, int c) { return UPPER ? (UNIT ? c > r : c >= r) : (UNIT ? c < r : c <= r); };
   for (int t = threadIdx.x; t < TSB * TSB; t += blockDim.x) {
     const int r = t / TSB, c = t % TSB;
     T v = (r == c) ? one : zero;
-    if (r < bs && c < bs && (UPPER ? c >= r : c < r)) v = LU[(size_t)(r0 + r) * n + r0 + c];
+    if (r < bs && c < bs && stored(r, c)) v = LU[(size_t)(r0 + r) * n + r0 + c];
     M[r * TLD + c] = v;
   }
   __syncthreads();
   if (!UPPER) {
-    for (int j = 0; j + 1 < bs; j++) {
+    for (int j = 0; j < bs; j++) {
+      T d = one;
+      if (!UNIT) {
+        d = crecip(M[j * TLD + j]);
+        __syncthreads();
+        for (int c = threadIdx.x; c < j; c += blockDim.x) M[j * TLD + c] = cmul(M[j * TLD + c], d);
+        if (threadIdx.x == 0) M[j * TLD + j] = d;
+      }
       for (int r = j + 1 + threadIdx.x; r < bs; r += blockDim.x) col[r] = M[r * TLD + j];
       __syncthreads();
       const int w = j + 1, cnt = (bs - 1 - j) * w;
@@ -98,7 +121,8 @@ __global__ void __launch_bounds__(512) k_inv_diag(const T* __restrict__ LU, int 
         const int r = j + 1 + t / w, c = t % w;
         const T l = col[r];
         if (c == j) {
-          M[r * TLD + j] = T{-l.x, -l.y};
+          const T p = cmul(l, d);
+          M[r * TLD + j] = T{-p.x, -p.y};
         } else {
           const T p = cmul(l, M[j * TLD + c]);
           T v = M[r * TLD + c];
@@ -111,10 +135,13 @@ __global__ void __launch_bounds__(512) k_inv_diag(const T* __restrict__ LU, int 
     }
   } else {
     for (int j = bs - 1; j >= 0; j--) {
-      const T d = crecip(M[j * TLD + j]);
-      __syncthreads();
-      for (int c = j + 1 + threadIdx.x; c < bs; c += blockDim.x) M[j * TLD + c] = cmul(M[j * TLD + c], d);
-      if (threadIdx.x == 0) M[j * TLD + j] = d;
+      T d = one;
+      if (!UNIT) {
+        d = crecip(M[j * TLD + j]);
+        __syncthreads();
+        for (int c = j + 1 + threadIdx.x; c < bs; c += blockDim.x) M[j * TLD + c] = cmul(M[j * TLD + c], d);
+        if (threadIdx.x == 0) M[j * TLD + j] = d;
+      }
       for (int r = threadIdx.x; r < j; r += blockDim.x) col[r] = M[r * TLD + j];
       __syncthreads();
       const int w = bs - j, cnt = j * w;
@@ -138,7 +165,7 @@ __global__ void __launch_bounds__(512) k_inv_diag(const T* __restrict__ LU, int 
   T* out = inv + (size_t)b * TSB * TSB;
   for (int t = threadIdx.x; t < TSB * TSB; t += blockDim.x) {
     const int r = t / TSB, c = t % TSB;
-    const bool keep = r < bs && c < bs && (UPPER ? c >= r : c < r);
+    const bool keep = r < bs && c < bs && (UPPER ? c >= r : c <= r);
     out[t] = keep ? M[r * TLD + c] : ((r == c) ? one : zero);
   }
 }
@@ -470,7 +497,7 @@ int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cud
 }
 
 template <typename T>
-int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st) {
+int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st, bool transposed) {
   const int nb = (n + TSB - 1) / TSB;
   const size_t need = (size_t)nb * TSB * TSB;
   if (blk.invL.count < need) {
@@ -483,18 +510,31 @@ int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st) {
   const size_t smem = (size_t)TSB * TLD * sizeof(T);
   static bool attr = false;
   if (!attr) {
-    TT_CUDA_TRY(cudaFuncSetAttribute(k_inv_diag<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TT_CUDA_TRY(cudaFuncSetAttribute(k_inv_diag<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TT_CUDA_TRY(
+        cudaFuncSetAttribute(k_inv_diag<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TT_CUDA_TRY(
+        cudaFuncSetAttribute(k_inv_diag<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TT_CUDA_TRY(
+        cudaFuncSetAttribute(k_inv_diag<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TT_CUDA_TRY(
+        cudaFuncSetAttribute(k_inv_diag<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     TT_CUDA_TRY(
         cudaFuncSetAttribute(k_prev_mul<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem)));
     TT_CUDA_TRY(
         cudaFuncSetAttribute(k_prev_mul<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem)));
     attr = true;
   }
-  k_inv_diag<T, false><<<nb, 512, smem, st>>>(d_LU, n, blk.invL.ptr);
-  count_launch();
-  k_inv_diag<T, true><<<nb, 512, smem, st>>>(d_LU, n, blk.invU.ptr);
-  count_launch();
+  if (!transposed) {
+    k_inv_diag<T, false, true><<<nb, 512, smem, st>>>(d_LU, n, blk.invL.ptr);
+    count_launch();
+    k_inv_diag<T, true, false><<<nb, 512, smem, st>>>(d_LU, n, blk.invU.ptr);
+    count_launch();
+  } else {
+    k_inv_diag<T, false, false><<<nb, 512, smem, st>>>(d_LU, n, blk.invL.ptr);
+    count_launch();
+    k_inv_diag<T, true, true><<<nb, 512, smem, st>>>(d_LU, n, blk.invU.ptr);
+    count_launch();
+  }
   k_prev_mul<T, false><<<nb, 512, 2 * smem, st>>>(d_LU, n, blk.invL.ptr, blk.mL.ptr);
   count_launch();
   k_prev_mul<T, true><<<nb, 512, 2 * smem, st>>>(d_LU, n, blk.invU.ptr, blk.mU.ptr);
@@ -502,13 +542,12 @@ int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st) {
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
-template int lu_trsv_prepare<double2>(const double2*, int, TrsvBlocks<double2>&, cudaStream_t);
-template int lu_trsv_prepare<float2>(const float2*, int, TrsvBlocks<float2>&, cudaStream_t);
+template int lu_trsv_prepare<double2>(const double2*, int, TrsvBlocks<double2>&, cudaStream_t, bool);
+template int lu_trsv_prepare<float2>(const float2*, int, TrsvBlocks<float2>&, cudaStream_t, bool);
 
+// forward then backward substitution sweep over x [k][n] in place
 template <typename T>
-int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_t* d_perm, double* d_x,
-                    double* d_tmp, int nrhs, cudaStream_t st) {
-  if (n <= 0 || nrhs <= 0) return TT_OK;
+int trsv_sweeps(const T* d_LU, int n, const TrsvBlocks<T>& blk, double2* x, int nrhs, cudaStream_t st) {
   if (blk.n != n || !blk.invL.ptr) {
     set_error("triangular solve called without the inverted diagonal blocks of this factor");
     return TT_ERR_BADARG;
@@ -529,13 +568,6 @@ int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_
     TT_CUDA_TRY(cudaFuncSetAttribute(k_trsv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
     attr = true;
   }
-  ProfScope prof(TT_PROF_TRSV, st, 8.0 * n * (double)n * nrhs, (double)n * n * sizeof(T));
-  TT_CUDA_TRY(cudaMemcpyAsync(d_tmp, d_x, sizeof(double2) * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, st));
-  double2* x = reinterpret_cast<double2*>(d_x);
-  k_permute<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_tmp), d_perm, n,
-                                                            nrhs, x);
-  count_launch();
-  TT_CUDA_TRY(cudaGetLastError());
   for (int k0 = 0; k0 < nrhs; k0 += RHS) {
     int kn = std::min(RHS, nrhs - k0);
     double2* xk = x + (size_t)k0 * n;
@@ -554,6 +586,39 @@ int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_
   }
   return TT_OK;
 }
+
+template <typename T>
+int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_t* d_perm, double* d_x,
+                    double* d_tmp, int nrhs, cudaStream_t st) {
+  if (n <= 0 || nrhs <= 0) return TT_OK;
+  ProfScope prof(TT_PROF_TRSV, st, 8.0 * n * (double)n * nrhs, (double)n * n * sizeof(T));
+  TT_CUDA_TRY(cudaMemcpyAsync(d_tmp, d_x, sizeof(double2) * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, st));
+  double2* x = reinterpret_cast<double2*>(d_x);
+  k_permute<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_tmp), d_perm, n,
+                                                            nrhs, x);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return trsv_sweeps<T>(d_LU, n, blk, x, nrhs, st);
+}
+
+template <typename T>
+int lu_solve_transposed_device(const T* d_LUt, int n, const TrsvBlocks<T>& blkT, const int32_t* d_perm, double* d_x,
+                               double* d_tmp, int nrhs, cudaStream_t st) {
+  if (n <= 0 || nrhs <= 0) return TT_OK;
+  ProfScope prof(TT_PROF_TRSV, st, 8.0 * n * (double)n * nrhs, (double)n * n * sizeof(T));
+  double2* x = reinterpret_cast<double2*>(d_x);
+  TT_TRY(trsv_sweeps<T>(d_LUt, n, blkT, x, nrhs, st));
+  TT_CUDA_TRY(cudaMemcpyAsync(d_tmp, d_x, sizeof(double2) * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, st));
+  k_permute_inv<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_tmp), d_perm, n,
+                                                                nrhs, x);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+template int lu_solve_transposed_device<double2>(const double2*, int, const TrsvBlocks<double2>&, const int32_t*,
+                                                 double*, double*, int, cudaStream_t);
+template int lu_solve_transposed_device<float2>(const float2*, int, const TrsvBlocks<float2>&, const int32_t*,
+                                                double*, double*, int, cudaStream_t);
 template int lu_solve_device<double2>(const double2*, int, const TrsvBlocks<double2>&, const int32_t*, double*,
                                       double*, int, cudaStream_t);
 template int lu_solve_device<float2>(const float2*, int, const TrsvBlocks<float2>&, const int32_t*, double*,

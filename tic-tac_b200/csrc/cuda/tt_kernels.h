@@ -85,13 +85,42 @@ struct TrsvBlocks {
   DevBuf<T> mL, mU;      // inv[b] times the block that carries the previous solved block into b
   int n = 0;
 };
+// transposed = true: d_LU holds the transpose of a factor (non-unit lower,
+// unit upper), for lu_solve_transposed_device.
 template <typename T>
-int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st);
+int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st, bool transposed = false);
 // Solve L U x = P b for nrhs complex128 columns [k][n] in place using the factor
 // of type T; d_perm from lu_permutation (uploaded), d_tmp scratch of 2 n nrhs doubles.
 template <typename T>
 int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_t* d_perm, double* d_x,
                     double* d_tmp, int nrhs, cudaStream_t st);
+
+// Solve (P^T L U)^T x = b, i.e. transposed systems of the same factor, for
+// nrhs complex128 columns [k][n] in place: d_LUt is the transpose of the
+// factor (transpose_device) with blkT from lu_trsv_prepare(..., true).
+template <typename T>
+int lu_solve_transposed_device(const T* d_LUt, int n, const TrsvBlocks<T>& blkT, const int32_t* d_perm, double* d_x,
+                               double* d_tmp, int nrhs, cudaStream_t st);
+
+// Adjoint pieces (adjoint.cu); vectors are complex128 [k][n].
+template <typename T>
+int transpose_device(const T* in, int n, T* out, cudaStream_t st);
+// y_k = A^T v_k, k < nrhs <= 4
+int gemv_t_device(const double* d_A, int n, const double* d_v, int nrhs, double* d_y, cudaStream_t st);
+// r_k = e_{rows[k]} - lam_k + G o y_k
+int residual_t_device(const double* d_lam, const double* d_y, const double* d_G, const int32_t* d_rows, int n,
+                      int nrhs, double* d_r, cudaStream_t st);
+int unit_rhs_device(const int32_t* d_rows, int n, int nrhs, double* d_x, cudaStream_t st);
+// w_k = e_{rows[k]} + G o x_k
+int make_w_device(const double* d_x, const double* d_G, const int32_t* d_rows, int n, int nrhs, double* d_w,
+                  cudaStream_t st);
+// out_k = OP(X) in_k with X in the layout of C / VC (one block per 2N channel)
+int block_apply_device(const DeviceLayout& L, const double* d_X, const double* d_in, int nrhs, double* d_out,
+                       cudaStream_t st);
+// g_k = 2 P^T u_k
+int spmv_t_device(const DeviceCSR& P, const double* d_u, int nrhs, double* d_g, cudaStream_t st);
+// out[a nb + b] = sum_i g_a[i] h_b[i], complex, na, nb <= 4
+int bilinear_device(int n, const double* d_g, int na, const double* d_h, int nb, double* d_out, cudaStream_t st);
 
 // x += d ; returns max |d| / max |x| per rhs in h_ratio (host, synchronises).
 int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_dx_over_x, cudaStream_t st);

@@ -57,6 +57,9 @@ struct RunParams {
   double refine_tol = 1e-12;
   int refine_max_iter = 30;
   std::vector<double> lab_energies; // set directly or read from energy_input_file
+  // additive offsets to the potential's low-energy constants, in the model's
+  // order (LO_internal: C_1S0, C_3S1 in MeV^-2; malfliet_tjon has none)
+  std::vector<double> lec_offsets;
 };
 
 // Sets one key=value option. Returns false (with message) on unknown key or bad value.
@@ -147,6 +150,11 @@ class Potential {
   // Varray[6] as in Interactions/potential_model.h:21
   virtual void V(double qi, double qo, bool coupled, int S, int J, int T, int Tz, double* Varray) = 0;
 };
-Potential* make_potential(const std::string& name, std::string* err);
+Potential* make_potential(const std::string& name, std::string* err,
+                          const std::vector<double>& lec_offsets = std::vector<double>());
+// Number of low-energy constants of a model that lec_offsets can move.
+int num_lecs(const std::string& name);
+// Nominal values of those constants (same order).
+std::vector<double> nominal_lecs(const std::string& name);
 
 }  // namespace tt

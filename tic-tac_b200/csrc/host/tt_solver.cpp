@@ -173,8 +173,75 @@ int ChannelSolver::resolvent(const std::vector<double>& E, cudaStream_t st) {
   return TT_OK;
 }
 
+int ChannelSolver::adjoint_energy(int j, int nE, int nd, const double* Gj, const int32_t* d_rows, const int32_t* d_perm,
+                                  double* tmp, const double* x, const SolveOptions& opt, const void* F, void* Ft,
+                                  TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT,
+                                  double* rT, double* u, double* g, double* w, double* h, double* dots,
+                                  const AdjointRequest& adj, SolveReport& r, cudaStream_t st) {
+  auto t0 = std::chrono::steady_clock::now();
+  // lambda_d' = (1 - A G)^{-T} e_d' with the transposed factor
+  auto solve_t = [&](double* v) -> int {
+    if (opt.mixed)
+      return lu_solve_transposed_device<float2>(static_cast<const float2*>(Ft), n, tbT32, d_perm, v, tmp, nd, st);
+    return lu_solve_transposed_device<double2>(static_cast<const double2*>(Ft), n, tbT64, d_perm, v, tmp, nd, st);
+  };
+  if (opt.mixed) {
+    TT_TRY(transpose_device<float2>(static_cast<const float2*>(F), n, static_cast<float2*>(Ft), st));
+    TT_TRY(lu_trsv_prepare<float2>(static_cast<const float2*>(Ft), n, tbT32, st, true));
+  } else {
+    TT_TRY(transpose_device<double2>(static_cast<const double2*>(F), n, static_cast<double2*>(Ft), st));
+    TT_TRY(lu_trsv_prepare<double2>(static_cast<const double2*>(Ft), n, tbT64, st, true));
+  }
+  TT_TRY(unit_rhs_device(d_rows, n, nd, lam, st));
+  TT_TRY(solve_t(lam));
+  if (opt.mixed) {
+    // FP64 refinement: r = e - (lambda - G o (A^T lambda)), solve, lambda += r
+    bool converged = false;
+    int it = 0;
+    double worst = 0;
+    std::vector<double> ratio(nd);
+    for (it = 1; it <= opt.refine_max_iter; it++) {
+      TT_TRY(gemv_t_device(A_.ptr, n, lam, nd, yT, st));
+      TT_TRY(residual_t_device(lam, yT, Gj, d_rows, n, nd, rT, st));
+      TT_TRY(solve_t(rT));
+      TT_TRY(axpy_norms_device(lam, rT, n, nd, ratio.data(), st));
+      worst = 0;
+      for (double v : ratio) worst = std::max(worst, v);
+      if (!(worst == worst)) break;
+      if (worst <= opt.refine_tol) {
+        converged = true;
+        break;
+      }
+    }
+    r.adjoint_refine_iters = std::max(r.adjoint_refine_iters, std::min(it, opt.refine_max_iter));
+    if (!converged) {
+      set_error("refinement of the adjoint solve did not converge (last |dx|/|x| = " + std::to_string(worst) + ")");
+      return TT_ERR_NOCONVERGE;
+    }
+  }
+  // g = 2 P123^T OP(C) lambda, w = e + G o x
+  TT_TRY(block_apply_device(L_, L_.C.ptr, lam, nd, u, st));
+  TT_TRY(spmv_t_device(P_, u, nd, g, st));
+  TT_TRY(make_w_device(x, Gj, d_rows, n, nd, w, st));
+  std::vector<double> hd((size_t)2 * nd * nd);
+  for (int k = 0; k < adj.n_theta; k++) {
+    TT_TRY(block_apply_device(L_, adj.d_dVC + (size_t)k * adj.vc_count, w, nd, h, st));
+    TT_TRY(bilinear_device(n, g, nd, h, nd, dots, st));
+    TT_CUDA_TRY(cudaMemcpyAsync(hd.data(), dots, sizeof(double) * hd.size(), cudaMemcpyDeviceToHost, st));
+    TT_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int dr = 0; dr < nd; dr++)
+      for (int dc = 0; dc < nd; dc++) {
+        const size_t o = (size_t)k * nd * nd * nE + (size_t)dr * nd * nE + (size_t)dc * nE + j;
+        (*adj.dU)[2 * o + 0] = hd[2 * (dr * nd + dc) + 0];
+        (*adj.dU)[2 * o + 1] = hd[2 * (dr * nd + dc) + 1];
+      }
+  }
+  r.ms_adjoint += ms_since(t0);
+  return TT_OK;
+}
+
 int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
-                         std::vector<double>& U, SolveReport* rep, cudaStream_t st) {
+                         std::vector<double>& U, SolveReport* rep, cudaStream_t st, const AdjointRequest* adj) {
   const int nE = (int)q_idx.size(), nd = (int)deut.size();
   if (nE != nE_) {
     set_error("number of on-shell bins does not match the resolvent energies");
@@ -185,6 +252,17 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     return TT_ERR_BADARG;
   }
   U.assign((size_t)2 * nd * nd * nE, 0.0);
+  if (adj) {
+    if (!adj->dU || (adj->n_theta > 0 && !adj->d_dVC)) {
+      set_error("adjoint request without output or derivative blocks");
+      return TT_ERR_BADARG;
+    }
+    if (nd > 4) {
+      set_error("the adjoint handles at most 4 deuteron states per channel");
+      return TT_ERR_UNSUPPORTED;
+    }
+    adj->dU->assign((size_t)adj->n_theta * 2 * nd * nd * nE, 0.0);
+  }
   SolveReport r;
   if (nd == 0 || nE == 0) {
     if (rep) *rep = r;
@@ -199,8 +277,18 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
   TT_TRY(x.alloc((size_t)2 * n * nd));
   DevBuf<double2> L64;
   DevBuf<float2> L32;
-  TrsvBlocks<double2> tb64;
-  TrsvBlocks<float2> tb32;
+  TrsvBlocks<double2> tb64, tbT64;
+  TrsvBlocks<float2> tb32, tbT32;
+  // adjoint: transposed factor and the vectors of lambda, its refinement and the products
+  DevBuf<double2> Ft64;
+  DevBuf<float2> Ft32;
+  DevBuf<double> lam, yT, rT, u, g, w, h, dots;
+  if (adj && adj->n_theta > 0) {
+    if (opt.mixed) TT_TRY(Ft32.alloc((size_t)n * n));
+    else TT_TRY(Ft64.alloc((size_t)n * n));
+    for (DevBuf<double>* b : {&lam, &yT, &rT, &u, &g, &w, &h}) TT_TRY(b->alloc((size_t)2 * n * nd));
+    TT_TRY(dots.alloc((size_t)2 * nd * nd));
+  }
   if (opt.mixed) {
     TT_TRY(L32.alloc((size_t)n * n));
     TT_TRY(y.alloc((size_t)2 * n * nd));
@@ -281,6 +369,11 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
         return TT_ERR_NOCONVERGE;
       }
     }
+    if (adj && adj->n_theta > 0) TT_TRY(adjoint_energy(j, nE, nd, Gj, cols.ptr, perm_d.ptr, tmp.ptr, x.ptr, opt,
+                                                      opt.mixed ? (const void*)L32.ptr : (const void*)L64.ptr,
+                                                      opt.mixed ? (void*)Ft32.ptr : (void*)Ft64.ptr, tbT32, tbT64,
+                                                      lam.ptr, yT.ptr, rT.ptr, u.ptr, g.ptr, w.ptr, h.ptr, dots.ptr,
+                                                      *adj, r, st));
     // on-shell read-out, solve_faddeev.cpp:407-431
     std::vector<double> hx((size_t)2 * n * nd);
     TT_CUDA_TRY(cudaMemcpyAsync(hx.data(), x.ptr, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st));

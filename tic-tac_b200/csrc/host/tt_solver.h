@@ -39,6 +39,18 @@ struct SolveReport {
   int refine_iters = 0;          // max over energies
   double final_correction = 0;   // max over rhs of |dx|/|x| at exit
   int info = 0;                  // first zero pivot (1-based) if any
+  double ms_adjoint = 0;         // transposed solves, their refinement and the parameter products
+  int adjoint_refine_iters = 0;  // max over energies
+};
+
+// Parameter derivatives wanted from a solve: dV/dtheta_k C for k < n_theta,
+// each in the layout of ChannelLayout::VC (one block per 2N channel), on the
+// device.  dU receives [n_theta][nd][nd][nE] interleaved complex.
+struct AdjointRequest {
+  int n_theta = 0;
+  const double* d_dVC = nullptr;  // n_theta * vc_count doubles
+  size_t vc_count = 0;
+  std::vector<double>* dU = nullptr;
 };
 
 class ChannelSolver {
@@ -53,7 +65,8 @@ class ChannelSolver {
   int resolvent(const std::vector<double>& E, cudaStream_t st);
   // U[d'*nd*nE + d*nE + j] for each on-shell q bin j and deuteron states
   int solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
-            std::vector<double>& U_interleaved, SolveReport* rep, cudaStream_t st);
+            std::vector<double>& U_interleaved, SolveReport* rep, cudaStream_t st,
+            const AdjointRequest* adj = nullptr);
   void release_A() {
     A_.release();
     G_.release();
@@ -61,10 +74,16 @@ class ChannelSolver {
   }
   const DeviceCSR& P() const { return P_; }
   const double* A() const { return A_.ptr; }
+  const DeviceLayout& layout() const { return L_; }
   const double* G() const { return G_.ptr; }
   int nE() const { return nE_; }
 
  private:
+  int adjoint_energy(int j, int nE, int nd, const double* Gj, const int32_t* d_rows, const int32_t* d_perm,
+                     double* tmp, const double* x, const SolveOptions& opt, const void* F, void* Ft,
+                     TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT, double* rT,
+                     double* u, double* g, double* w, double* h, double* dots, const AdjointRequest& adj,
+                     SolveReport& r, cudaStream_t st);
   DeviceLayout L_;
   DeviceCSR P_;
   DevBuf<double> A_, G_;

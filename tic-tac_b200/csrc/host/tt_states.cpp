@@ -60,6 +60,11 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       std::stringstream ss(value);
       std::string tok;
       while (std::getline(ss, tok, ',')) if (!tok.empty()) rp.lab_energies.push_back(std::stod(tok));
+    } else if (key == "lec_offsets") {
+      rp.lec_offsets.clear();
+      std::stringstream ss(value);
+      std::string tok;
+      while (std::getline(ss, tok, ',')) if (!tok.empty()) rp.lec_offsets.push_back(std::stod(tok));
     } else if (key == "subfolder" || key == "P123_omp_num_threads" || key == "P123_recovery" ||
                key == "include_breakup_channels" || key == "parameter_walk" || key == "parameter_file" ||
                key == "PSI_start" || key == "PSI_end" || key == "p_grid_filename" || key == "q_grid_filename") {

@@ -39,7 +39,7 @@ class MalflietTjon : public Potential {
 // and the chiral LO contact terms (Interactions/chiral_LO_internal.cpp:27-68).
 class ChiralLO : public Potential {
  public:
-  ChiralLO() : z_(kNz), wz_(kNz) {
+  explicit ChiralLO(double c1s0 = kC1S0, double c3s1 = kC3S1) : c1s0_(c1s0), c3s1_(c3s1), z_(kNz), wz_(kNz) {
     gauss_legendre(z_.data(), wz_.data(), kNz);
     // Legendre values P_l(z_i) for l = 0..kJmax+1 by the Bonnet recurrence
     // (General_functions/legendre.cpp:155-178).
@@ -55,8 +55,8 @@ class ChiralLO : public Potential {
   void V(double qi, double qo, bool, int, int J, int, int, double* Varray) override {
     for (int k = 0; k < 6; k++) Varray[k] = 0;
     opep(qi, qo, J, Varray);
-    if (J == 0) Varray[0] += kC1S0;
-    else if (J == 1) Varray[2] += kC3S1;
+    if (J == 0) Varray[0] += c1s0_;
+    else if (J == 1) Varray[2] += c3s1_;
     const double M = kMN;
     const double Epi = std::sqrt(M * M + qi * qi);
     const double Epo = std::sqrt(M * M + qo * qo);
@@ -75,6 +75,7 @@ class ChiralLO : public Potential {
  private:
   static constexpr int kNz = 150;
   static constexpr int kJmax = 100;
+  double c1s0_, c3s1_;  // contact LECs of the 1S0 and 3S1 waves
   std::vector<double> z_, wz_, pl_;
 
   static int iso_fac(int L, int S) {
@@ -123,9 +124,25 @@ class ChiralLO : public Potential {
   }
 };
 
-Potential* make_potential(const std::string& name, std::string* err) {
+int num_lecs(const std::string& name) { return name == "LO_internal" ? 2 : 0; }
+
+std::vector<double> nominal_lecs(const std::string& name) {
+  if (name == "LO_internal") return {kC1S0, kC3S1};
+  return {};
+}
+
+Potential* make_potential(const std::string& name, std::string* err, const std::vector<double>& lec_offsets) {
+  if ((int)lec_offsets.size() > num_lecs(name)) {
+    if (err) *err = "potential model '" + name + "' has " + std::to_string(num_lecs(name)) + " adjustable constants, " +
+                    std::to_string(lec_offsets.size()) + " offsets given";
+    return nullptr;
+  }
   if (name == "malfliet_tjon") return new MalflietTjon();
-  if (name == "LO_internal") return new ChiralLO();
+  if (name == "LO_internal") {
+    const double d0 = lec_offsets.size() > 0 ? lec_offsets[0] : 0.0;
+    const double d1 = lec_offsets.size() > 1 ? lec_offsets[1] : 0.0;
+    return new ChiralLO(kC1S0 + d0, kC3S1 + d1);
+  }
   if (err)
     *err = "potential model '" + name +
            "' is not available: the chiral N2LOopt/Idaho_N3LO and Nijmegen models exist only as Fortran in the "
@@ -152,7 +169,7 @@ static double extract_element(int L, int Lp, int J, int S, bool coupled, const d
 
 bool potential_matrices(const RunParams& rp, const FWPStates& fwp, const PWStates& pw,
                         std::vector<double>& V_unco, std::vector<double>& V_coup, std::string* err) {
-  std::unique_ptr<Potential> pot(make_potential(rp.potential_model, err));
+  std::unique_ptr<Potential> pot(make_potential(rp.potential_model, err, rp.lec_offsets));
   if (!pot) return false;
   int n_unco = 0, n_coup = 0;
   count_2N_channels(rp, n_unco, n_coup);

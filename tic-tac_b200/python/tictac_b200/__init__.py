@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "tt_run_write_U_table", "tt_run_release_A", "tt_run_timer_start", "tt_run_timer_stop", "tt_kernel_launches",
     "tt_wigner_3j", "tt_wigner_6j", "tt_wigner_9j", "tt_clebsch_gordan", "tt_legendre_spharm_array",
     "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc", "tt_profile_begin", "tt_profile_end",
-    "tt_profile_read",
+    "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build")
@@ -80,7 +80,8 @@ class tt_run_params(ctypes.Structure):
 
 class tt_solve_report(ctypes.Structure):
     _fields_ = [("ms_A", c_double), ("ms_form", c_double), ("ms_factor", c_double), ("ms_solve", c_double),
-                ("ms_refine", c_double), ("refine_iters", c_int), ("final_correction", c_double), ("info", c_int)]
+                ("ms_refine", c_double), ("refine_iters", c_int), ("final_correction", c_double), ("info", c_int),
+                ("ms_adjoint", c_double), ("adjoint_refine_iters", c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -278,6 +279,37 @@ def solve_faddeev(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q_idx, de
     return U, rep.as_dict()
 
 
+def solve_faddeev_adjoint(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q_idx, deut, pw: PW, dV_unco, dV_coup,
+                          precision=PRECISION_MIXED, **rp_kw):
+    """tt_solve_faddeev_adjoint: U and dU/dtheta_k for the potential derivatives
+    dV_unco [n_theta][...], dV_coup [n_theta][...] (layout of V_unco / V_coup),
+    with the wave-packet basis and the resolvent held fixed.  Returns U,
+    dU [n_theta][nE*nd*nd] and the solve report."""
+    lib = load()
+    G = np.ascontiguousarray(G, dtype=np.complex128)
+    Pv = np.ascontiguousarray(P_val, dtype=np.float64)
+    Pr = np.ascontiguousarray(P_row, dtype=np.int32)
+    Pc = np.ascontiguousarray(P_colptr, dtype=np.uint64)
+    Vu = np.ascontiguousarray(V_unco, dtype=np.float64)
+    Vc = np.ascontiguousarray(V_coup if V_coup is not None and len(V_coup) else np.zeros(1), dtype=np.float64)
+    dVu = np.ascontiguousarray(dV_unco, dtype=np.float64)
+    n_theta = dVu.shape[0]
+    dVc = np.ascontiguousarray(dV_coup if dV_coup is not None and np.size(dV_coup) else np.zeros((n_theta, 1)),
+                               dtype=np.float64)
+    qi = np.ascontiguousarray(q_idx, dtype=np.int32)
+    di = np.ascontiguousarray(deut, dtype=np.int32)
+    os_ = tt_os_indexing(len(qi), _iptr(qi), _iptr(di), len(di))
+    rp = run_params(precision=precision, **rp_kw)
+    U = np.zeros(len(qi) * len(di) * len(di), dtype=np.complex128)
+    dU = np.zeros((n_theta, U.size), dtype=np.complex128)
+    rep = tt_solve_report()
+    _check(lib.tt_solve_faddeev_adjoint(U.ctypes.data_as(c_void_p), dU.ctypes.data_as(c_void_p), ctypes.c_int(n_theta),
+                                        _dptr(dVu), _dptr(dVc), G.ctypes.data_as(c_void_p), _dptr(Pv), _iptr(Pr),
+                                        Pc.ctypes.data_as(POINTER(c_size_t)), c_size_t(len(Pv)), _dptr(Vu), _dptr(Vc),
+                                        byref(swp.s), byref(os_), byref(pw.s), byref(rp), byref(rep)))
+    return U, dU, rep.as_dict()
+
+
 class Run:
     """A configured run (tt_run_*): host state-space setup from key=value options."""
 
@@ -377,6 +409,39 @@ class Run:
         rep = tt_solve_report()
         _check(self.lib.tt_run_solve(self._h, chn, precision, U.ctypes.data_as(c_void_p), byref(rep)))
         return U, rep.as_dict()
+
+    def solve_adjoint(self, chn, dV_unco, dV_coup, precision=PRECISION_MIXED):
+        """U and dU/dtheta_k for potential derivatives over all 2N channels of the
+        run ([n_theta][...] in the layout of host_array(3) / host_array(4)), the
+        wave-packet basis and the resolvent held fixed."""
+        info = self.channel_info(chn)
+        nE = len(self.energies()[0])
+        nd = info["n_deuteron"]
+        dVu = np.ascontiguousarray(dV_unco, dtype=np.float64)
+        n_theta = dVu.shape[0]
+        dVc = np.ascontiguousarray(dV_coup if dV_coup is not None and np.size(dV_coup) else np.zeros((n_theta, 1)),
+                                   dtype=np.float64)
+        U = np.zeros(nE * nd * nd, dtype=np.complex128)
+        dU = np.zeros((n_theta, U.size), dtype=np.complex128)
+        rep = tt_solve_report()
+        _check(self.lib.tt_run_solve_adjoint(self._h, chn, precision, ctypes.c_int(n_theta), _dptr(dVu), _dptr(dVc),
+                                             U.ctypes.data_as(c_void_p), dU.ctypes.data_as(c_void_p), byref(rep)))
+        return U, dU, rep.as_dict()
+
+    def lecs(self):
+        """Values of the potential's adjustable low-energy constants."""
+        n = ctypes.c_int()
+        _check(self.lib.tt_run_num_lecs(self._h, byref(n), None))
+        v = np.zeros(max(1, n.value))
+        _check(self.lib.tt_run_num_lecs(self._h, byref(n), _dptr(v)))
+        return v[:n.value]
+
+    def lec_derivative(self, k):
+        """dV/dLEC_k in the WP basis for all 2N channels (uncoupled, coupled)."""
+        dVu = np.zeros_like(self.host_array(3))
+        dVc = np.zeros(max(1, self.host_array(4).size))
+        _check(self.lib.tt_run_lec_derivative(self._h, k, _dptr(dVu), _dptr(dVc)))
+        return dVu, dVc[:self.host_array(4).size]
 
     def release(self, chn):
         _check(self.lib.tt_run_release_channel(self._h, chn))
