@@ -300,12 +300,25 @@ def run_ours(args, world, rank, local, pg):
         run.build_resolvent(c)
         Um, rm = run.solve(c, tt.PRECISION_MIXED)
         U64, r64 = run.solve(c, tt.PRECISION_FP64)
-        run.release_A(c)
         t_m = rm["ms_form"] + rm["ms_factor"] + rm["ms_solve"] + rm["ms_refine"]
         t_64 = r64["ms_form"] + r64["ms_factor"] + r64["ms_solve"] + r64["ms_refine"]
         fp64 = {"channel": c, "n": infos[i]["n"], "mixed_ms": round(t_m, 1), "fp64_ms": round(t_64, 1),
                 "speedup": round(t_64 / t_m, 2), "refine_iters": rm["refine_iters"],
                 "max_rel_diff_U": float(np.max(np.abs(Um - U64)) / np.max(np.abs(U64)))}
+        # adjoint: dU/dLEC for the potential's contact constants on the same channel
+        nl = len(run.lecs())
+        if nl:
+            dV = [run.lec_derivative(k) for k in range(nl)]
+            Ua, dU, ra = run.solve_adjoint(c, np.stack([d[0] for d in dV]), np.stack([d[1] for d in dV]),
+                                           tt.PRECISION_MIXED)
+            run.release_A(c)
+            t_f = ra["ms_form"] + ra["ms_factor"] + ra["ms_solve"] + ra["ms_refine"]
+            fp64["adjoint"] = {"n_theta": nl, "forward_ms": round(t_f, 1), "adjoint_ms": round(ra["ms_adjoint"], 1),
+                               "adjoint_over_forward": round(ra["ms_adjoint"] / t_f, 3),
+                               "adjoint_refine_iters": ra["adjoint_refine_iters"],
+                               "max_abs_dU_dLEC": float(np.max(np.abs(dU)))}
+        else:
+            run.release_A(c)
     return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, kernels=kernels, e2e=e2e,
                 infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times, launches=launches, fp64=fp64)
 
