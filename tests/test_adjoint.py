@@ -140,3 +140,40 @@ def test_adjoint_run_handle_lec_gradients():
                 fd = (Up - Um) / (2 * h)
                 assert rel(dU[k], fd) <= FD_TOL, (c, prec, k, rel(dU[k], fd))
     run.close()
+
+
+@pytest.mark.gpu
+def test_torch_autograd_wrapper():
+    import torch
+
+    from tictac_b200.autograd import u_of_theta
+
+    g, m = load_case("lo_j1_J3_n8")
+    Np = m["Np"]
+    c = 0
+    pwt = g[f"pw_c{c}"]
+    n = pwt.shape[0] * Np * m["Nq"]
+    v, r, cp = csc_of(n, g[f"p123_row_c{c}"], g[f"p123_col_c{c}"], g[f"p123_val_c{c}"])
+    rng = np.random.default_rng(3)
+    dVu = np.stack([symmetric_blocks(rng, g["V_unco"], Np) for _ in range(3)])
+    dVc = np.stack([symmetric_blocks(rng, g["V_coup"], 2 * Np) for _ in range(3)])
+    problem = dict(G=g[f"G_c{c}"], P_val=v, P_row=r, P_colptr=cp, V_unco=g["V_unco"], V_coup=g["V_coup"],
+                   swp=swp_of(g, m), q_idx=g["q_idx"], deut=oracle.deuterons(pwt), pw=tt.PW(pwt), dV_unco=dVu,
+                   dV_coup=dVc, precision=tt.PRECISION_FP64,
+                   rp=dict(tensor_force=int(m["tensor_force"]), isospin_breaking_1S0=int(m["iso"])))
+    theta = torch.zeros(3, dtype=torch.float64, requires_grad=True)
+    loss = (u_of_theta(theta, problem).abs() ** 2).sum()
+    loss.backward()
+    # d/dtheta sum |U|^2 = 2 Re(sum conj(U) dU/dtheta), dU from the same adjoint
+    U, dU, _ = tt.solve_faddeev_adjoint(problem["G"], v, r, cp, g["V_unco"], g["V_coup"], problem["swp"],
+                                        g["q_idx"], problem["deut"], problem["pw"], dVu, dVc,
+                                        precision=tt.PRECISION_FP64, **problem["rp"])
+    ref = 2 * np.real(np.conj(U)[None, :] * dU).sum(axis=1)
+    assert np.allclose(theta.grad.numpy(), ref, rtol=1e-12, atol=0)
+    # and against a central difference of the loss
+    h = 1e-5
+    for k in range(3):
+        e = torch.zeros(3, dtype=torch.float64)
+        e[k] = h
+        fd = ((u_of_theta(e, problem).abs() ** 2).sum() - (u_of_theta(-e, problem).abs() ** 2).sum()) / (2 * h)
+        assert abs(fd.item() - theta.grad[k].item()) <= 1e-6 * abs(theta.grad[k].item())

@@ -493,6 +493,18 @@ int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st) {
   return TT_OK;
 }
 
+// C -= L U inside the panel: on the tensor cores when the factorisation uses
+// them and K is a multiple of their 32-wide k-chunk, else on the CUDA cores
+template <typename T>
+int panel_gemm_sub(bool tc, T* C, int ldc, const T* L, int ldl, const T* U, int ldu, int M, int N, int K,
+                   cudaStream_t st) {
+  if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
+  if (tc && K % 32 == 0)
+    return tc_gemm_sub(reinterpret_cast<float2*>(C), ldc, reinterpret_cast<const float2*>(L), ldl,
+                       reinterpret_cast<const float2*>(U), ldu, M, N, K, st);
+  return gemm_sub(C, ldc, L, ldl, U, ldu, M, N, K, st);
+}
+
 }  // namespace
 
 template <typename T>
@@ -545,8 +557,8 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
       const int right = k + kb - (j0 + w);
       if (right > 0) {
         TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
-        TT_TRY(gemm_sub(A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
-                        A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
+        TT_TRY(panel_gemm_sub(tc, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
+                              A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
       }
     }
     // ---- interchanges outside the panel
@@ -559,8 +571,8 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
       TT_TRY(trsm_blk(A, n, i0, wi, k + kb, n, st));
       const int below = k + kb - (i0 + wi);
       if (below > 0)
-        TT_TRY(gemm_sub(A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
-                        A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
+        TT_TRY(panel_gemm_sub(tc, A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
+                              A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
     }
     // ---- trailing update
     if (tc) {
