@@ -514,7 +514,7 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
     set_error("tensor-core trailing update is only defined for the complex64 factorisation");
     return TT_ERR_UNSUPPORTED;
   }
-  const int NB = (sizeof(T) == sizeof(float2)) ? 256 : 128;
+  const int NB = (sizeof(T) == sizeof(float2)) ? 512 : 128;
   const int G = device_sm_count();
   DevBuf<double> sval;
   DevBuf<int> sidx, d_info;
