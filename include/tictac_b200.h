@@ -99,7 +99,7 @@ typedef struct tt_run_params {
   int isospin_breaking_1S0; /* default 1 */
   int production_run;       /* default 1 */
   int precision;            /* TT_PRECISION_* (replaces solve_dense/Pade selection) */
-  double refine_tol;        /* refinement stop: max |dx|/|x| (default 1e-12) */
+  double refine_tol;        /* refinement stop: estimated remaining max |dx|/|x| (default 1e-12) */
   int refine_max_iter;      /* default 30 */
 } tt_run_params;
 
@@ -112,7 +112,8 @@ typedef struct tt_solve_report {
   double ms_solve;      /* triangular solves */
   double ms_refine;     /* FP64 refinement */
   int refine_iters;     /* max over energies */
-  double final_correction;
+  double final_correction; /* estimated remaining relative error at exit: the last max|dx|/max|x|, or, once two
+                              corrections contract by rho < 1/2, that times rho / (1 - rho); max over rhs/energies */
   int info;             /* first zero pivot (1-based), 0 if none */
   double ms_adjoint;    /* adjoint: transposed solves, their refinement, parameter products */
   int adjoint_refine_iters;

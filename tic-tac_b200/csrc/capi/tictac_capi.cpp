@@ -162,27 +162,14 @@ int dropin_solve(tt_complex* U, tt_complex* dU, int n_theta, const double* dVu, 
   const PWChannel ch = view_of(pw);
   if (!build_channel_layout(rp, ch, w, Vu, Vc, L, &err)) return fail(TT_ERR_BADARG, err);
   const int n = ch.Nalpha * w.Np_WP * w.Nq_WP;
-  // CSC (column pointers, row indices) -> CSR with ascending columns
-  std::vector<int64_t> rowptr(n + 1, 0);
-  for (size_t e = 0; e < P_nnz; e++) {
-    if (P_row[e] < 0 || P_row[e] >= n) return fail(TT_ERR_BADARG, "P123 row index out of range");
-    rowptr[P_row[e] + 1]++;
-  }
-  for (int r = 0; r < n; r++) rowptr[r + 1] += rowptr[r];
-  std::vector<int32_t> col(P_nnz);
-  std::vector<double> val(P_nnz);
-  std::vector<int64_t> fillpos(rowptr.begin(), rowptr.end() - 1);
-  for (int c = 0; c < n; c++)
-    for (size_t e = P_colptr[c]; e < P_colptr[c + 1]; e++) {
-      const int64_t p = fillpos[P_row[e]]++;
-      col[p] = c;
-      val[p] = P_val[e];
-    }
+  if (P_colptr[n] != P_nnz) return fail(TT_ERR_BADARG, "P123 column pointers do not end at nnz");
   cudaStream_t st = default_stream();
   ChannelSolver cs;
   int s = cs.setup(L, w.q_WP, st);
   if (s != TT_OK) return s;
-  s = cs.set_P_host_csr(rowptr.data(), col.data(), val.data(), (int64_t)P_nnz, st);
+  // CSC -> CSR on the device
+  static_assert(sizeof(size_t) == sizeof(uint64_t), "size_t column pointers");
+  s = cs.set_P_host_csc(P_val, P_row, reinterpret_cast<const uint64_t*>(P_colptr), (int64_t)P_nnz, st);
   if (s != TT_OK) return s;
   double msA = 0;
   s = cs.build_A(st, &msA);

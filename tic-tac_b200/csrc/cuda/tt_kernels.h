@@ -102,6 +102,11 @@ template <typename T>
 int lu_solve_transposed_device(const T* d_LUt, int n, const TrsvBlocks<T>& blkT, const int32_t* d_perm, double* d_x,
                                double* d_tmp, int nrhs, cudaStream_t st);
 
+// P123 from the reference's host CSC (values, int rows, size_t column pointers)
+// to device CSR with ascending columns per row (csr_build.cu).
+int csc_to_csr_device(const double* h_val, const int32_t* h_row, const uint64_t* h_colptr, int64_t nnz, int n,
+                      DeviceCSR& out, cudaStream_t st);
+
 // Adjoint pieces (adjoint.cu); vectors are complex128 [k][n].
 template <typename T>
 int transpose_device(const T* in, int n, T* out, cudaStream_t st);

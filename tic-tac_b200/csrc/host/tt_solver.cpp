@@ -34,6 +34,26 @@ bool alpha_block(const RunParams& rp, const PWChannel& ch, int a, AlphaBlock& ou
   return true;
 }
 
+// Remaining relative error after a refinement step, per right-hand side: the
+// last correction |dx|/|x| = c, or, once two corrections contract by
+// rho = c / c_prev < 1/2, the rest of the geometric series c rho / (1 - rho).
+// Returns the worst over the right-hand sides.
+double refine_error_estimate(const std::vector<double>& cur, std::vector<double>& prev, bool have_prev) {
+  double worst = 0;
+  for (size_t k = 0; k < cur.size(); k++) {
+    double e = cur[k];
+    if (have_prev && prev[k] > 0 && cur[k] < 0.5 * prev[k]) {
+      const double rho = cur[k] / prev[k];
+      e = std::min(e, cur[k] * rho / (1 - rho));
+    }
+    if (!(cur[k] == cur[k])) e = cur[k];  // NaN stays NaN
+    worst = std::max(worst, e);
+    if (!(e == e)) worst = e;
+  }
+  prev = cur;
+  return worst;
+}
+
 double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -152,6 +172,11 @@ int ChannelSolver::set_P_host_csr(const int64_t* rowptr, const int32_t* col, con
   return TT_OK;
 }
 
+int ChannelSolver::set_P_host_csc(const double* val, const int32_t* row, const uint64_t* colptr, int64_t nnz,
+                                  cudaStream_t st) {
+  return csc_to_csr_device(val, row, colptr, nnz, n, P_, st);
+}
+
 int ChannelSolver::build_A(cudaStream_t st, double* ms) {
   auto t0 = std::chrono::steady_clock::now();
   TT_TRY(A_.alloc((size_t)n * n));
@@ -199,14 +224,13 @@ int ChannelSolver::adjoint_energy(int j, int nE, int nd, const double* Gj, const
     bool converged = false;
     int it = 0;
     double worst = 0;
-    std::vector<double> ratio(nd);
+    std::vector<double> ratio(nd), prev(nd, 0.0);
     for (it = 1; it <= opt.refine_max_iter; it++) {
       TT_TRY(gemv_t_device(A_.ptr, n, lam, nd, yT, st));
       TT_TRY(residual_t_device(lam, yT, Gj, d_rows, n, nd, rT, st));
       TT_TRY(solve_t(rT));
       TT_TRY(axpy_norms_device(lam, rT, n, nd, ratio.data(), st));
-      worst = 0;
-      for (double v : ratio) worst = std::max(worst, v);
+      worst = refine_error_estimate(ratio, prev, it > 1);
       if (!(worst == worst)) break;
       if (worst <= opt.refine_tol) {
         converged = true;
@@ -346,14 +370,13 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       bool converged = false;
       int it = 0;
       double worst = 0;
-      std::vector<double> ratio(nd);
+      std::vector<double> ratio(nd), prev(nd, 0.0);
       for (it = 1; it <= opt.refine_max_iter; it++) {
         TT_TRY(hadamard_device(Gj, rhs_e.ptr, n, x.ptr, nd, y.ptr, st));
         TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nd, res.ptr, st));
         TT_TRY(lu_solve_device<float2>(L32.ptr, n, tb32, perm_d.ptr, res.ptr, tmp.ptr, nd, st));
         TT_TRY(axpy_norms_device(x.ptr, res.ptr, n, nd, ratio.data(), st));
-        worst = 0;
-        for (double v : ratio) worst = std::max(worst, v);
+        worst = refine_error_estimate(ratio, prev, it > 1);
         if (!(worst == worst)) break;  // NaN
         if (worst <= opt.refine_tol) {
           converged = true;

@@ -60,6 +60,8 @@ class ChannelSolver {
   // P123 built on the device, or uploaded from host CSR arrays
   int set_P_device(DeviceCSR&& P);
   int set_P_host_csr(const int64_t* rowptr, const int32_t* col, const double* val, int64_t nnz, cudaStream_t st);
+  // the reference's CSC form, converted on the device
+  int set_P_host_csc(const double* val, const int32_t* row, const uint64_t* colptr, int64_t nnz, cudaStream_t st);
   int build_A(cudaStream_t st, double* ms = nullptr);
   // resolvent for energies E (= E_com + E_bound) into device G [nE][n]
   int resolvent(const std::vector<double>& E, cudaStream_t st);
