@@ -311,14 +311,16 @@ def run_ours(args, world, rank, local, pg):
             dV = [run.lec_derivative(k) for k in range(nl)]
             Ua, dU, ra = run.solve_adjoint(c, np.stack([d[0] for d in dV]), np.stack([d[1] for d in dV]),
                                            tt.PRECISION_MIXED)
-            run.release_A(c)
             t_f = ra["ms_form"] + ra["ms_factor"] + ra["ms_solve"] + ra["ms_refine"]
             fp64["adjoint"] = {"n_theta": nl, "forward_ms": round(t_f, 1), "adjoint_ms": round(ra["ms_adjoint"], 1),
                                "adjoint_over_forward": round(ra["ms_adjoint"] / t_f, 3),
                                "adjoint_refine_iters": ra["adjoint_refine_iters"],
                                "max_abs_dU_dLEC": float(np.max(np.abs(dU)))}
-        else:
-            run.release_A(c)
+        # the reference's production path: Pade-resummed Neumann series (about 1e-6)
+        Up, rpd = run.solve(c, tt.PRECISION_PADE)
+        fp64["pade"] = {"ms": round(rpd["ms_solve"], 1), "order": rpd["refine_iters"],
+                        "max_rel_diff_U_vs_fp64": float(np.max(np.abs(Up - U64)) / np.max(np.abs(U64)))}
+        run.release_A(c)
     return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, kernels=kernels, e2e=e2e,
                 infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times, launches=launches, fp64=fp64)
 

@@ -36,6 +36,9 @@ extern "C" {
 #define TT_PRECISION_FP64 0   /* complex128 LU, FP64 throughout */
 #define TT_PRECISION_MIXED 1  /* complex64 LU, BF16x3 tcgen05 trailing updates, FP64 refinement */
 #define TT_PRECISION_MIXED_SIMT 2  /* complex64 LU, FP32 CUDA-core trailing updates, FP64 refinement */
+#define TT_PRECISION_PADE 3   /* the reference's production default (solve_dense = false): Pade-resummed Neumann
+                                 series A (G A)^n on the resident FP64 A, stopped by the reference's criteria
+                                 (about 1e-6 relative); report.refine_iters = highest [N/N] order formed */
 
 /* complex128, layout-compatible with std::complex<double> */
 typedef struct tt_complex {

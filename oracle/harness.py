@@ -160,3 +160,78 @@ def dense_solve(A, G, q_idx, deut, Nq, Np):
 def deuterons(pw):
     pw = np.asarray(pw).reshape(-1, 9)
     return [a for a in range(pw.shape[0]) if tuple(int(x) for x in pw[a, :4]) == (0, 1, 1, 0)]
+
+
+# ---------------------------------------------------------------------------
+# Pade-resummed Neumann series of the reference's default production solver
+# (pade_method_solve, CPP/solve_faddeev.cpp:440-1444; pade_approximant,
+# :271-296; determinant, CPP/General_functions/matrix_routines.cpp:82-101),
+# restated in numpy.  Row r = d_row*nE + j of the on-shell rows; a_n for
+# element (d_row, d_col, j) = (A (G_j A)^n)[row(d_row, j), col(d_col, j)].
+
+NM_MAX = 14
+
+
+def pade_approximant(a, N, M, z=1.0):
+    """[N/M] Pade approximant at z from the series coefficients a[0..N+M]."""
+    P = np.zeros((M + 1, M + 1), dtype=np.complex128)
+    Q = np.zeros((M + 1, M + 1), dtype=np.complex128)
+    for r in range(M):
+        for c in range(M + 1):
+            P[r, c] = Q[r, c] = a[N - M + 1 + r + c]
+    for c in range(M + 1):
+        Q[M, c] = z ** (M - c)
+        P[M, c] = sum(a[j - (M - c)] * z ** j for j in range(M - c, N + 1))
+    return np.linalg.det(P) / np.linalg.det(Q)
+
+
+def pade_solve(A, G, q_idx, deut, Nq, Np):
+    n = A.shape[0]
+    G = np.asarray(G, dtype=np.complex128).reshape(len(q_idx), n)
+    nE, nd = len(q_idx), len(deut)
+    rows = [deut[d] * Nq * Np + q_idx[j] * Np for d in range(nd) for j in range(nE)]
+    R = A[rows, :].astype(np.complex128)  # n = 0 rows
+    nel = nd * nd * nE
+    a = np.zeros((nel, 2 * NM_MAX + 1), dtype=np.complex128)
+    pa = np.zeros((nel, NM_MAX + 1), dtype=np.complex128)
+    conv = np.zeros(nel, dtype=bool)
+    best = np.zeros(nel, dtype=int)
+
+    def el(dr, dc, j):
+        return dr * nd * nE + dc * nE + j
+
+    def extract(nterm):
+        for dr in range(nd):
+            for dc in range(nd):
+                for j in range(nE):
+                    e = el(dr, dc, j)
+                    if not conv[e]:
+                        a[e, nterm] = R[dr * nE + j, deut[dc] * Nq * Np + q_idx[j] * Np]
+
+    extract(0)
+    for NM in range(NM_MAX + 1):
+        if conv.all():
+            break
+        for nterm in (2 * NM - 1, 2 * NM):
+            if nterm <= 0:
+                continue
+            for dr in range(nd):
+                for j in range(nE):
+                    R[dr * nE + j] = (R[dr * nE + j] * G[j]) @ A
+            extract(nterm)
+        for e in range(nel):
+            if conv[e]:
+                continue
+            pa[e, NM] = pade_approximant(a[e], NM, NM)
+            idx_best, min_diff = 0, 1.0
+            for prev in range(NM):
+                d = abs(pa[e, prev] - pa[e, prev - 1])  # index -1 reads the last slot, as in the reference
+                if min_diff > d > 1e-15:
+                    idx_best, min_diff = prev, d
+            d = abs(pa[e, NM] - pa[e, NM - 1])
+            if min_diff > d > 1e-15:
+                idx_best, min_diff = NM, d
+            if NM == NM_MAX or NM - idx_best > 4 or min_diff < 1e-6 * abs(pa[e, idx_best]) or min_diff < 1e-7:
+                conv[e] = True
+                best[e] = idx_best
+    return np.array([pa[e, best[e]] for e in range(nel)])

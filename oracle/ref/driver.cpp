@@ -3,7 +3,7 @@
 // P123, resolvent and the dense LAPACK Faddeev solve, and writes every stage
 // as raw binary arrays so the tests can compare them with the GPU path.
 //
-//   tictac_ref dump <outdir> [--solver=reference|replica] key=value ...
+//   tictac_ref dump <outdir> [--solver=reference|replica|pade] key=value ...
 //   tictac_ref time <outdir> [--channel=k] [--sample_cols=m] key=value ...
 //
 // Extra keys understood here (stripped before the reference's parser sees them):
@@ -148,7 +148,9 @@ int main(int argc, char** argv) {
   }
   keep_args.push_back("output_folder=" + g_out);
   keep_args.push_back("P123_folder=" + g_out);
-  keep_args.push_back("solve_dense=true");
+  // --solver=pade runs the reference's default production path (Pade-resummed
+  // Neumann series, solve_faddeev.cpp:440-1444) through its own dispatcher
+  keep_args.push_back(solver == "pade" ? "solve_dense=false" : "solve_dense=true");
   std::vector<char*> av;
   for (auto& s : keep_args) av.push_back(&s[0]);
   int ac = (int)av.size();
@@ -252,7 +254,7 @@ int main(int argc, char** argv) {
     dump("G" + tag, G.data(), G.size());
 
     std::vector<cdouble> U(nE * nd * nd + 1);
-    if (mode == "dump" && solver == "reference") {
+    if (mode == "dump" && (solver == "reference" || solver == "pade")) {
       solve_faddeev_equations(U.data(), nullptr, G.data(), val, row, colptr.data(), nnz, Vu.data(), Vc.data(), swp, os,
                               sub, "_ref", rp);
     } else {

@@ -6,7 +6,9 @@ configurations and packs every stage it dumps (partial-wave tables, WP
 boundaries, V, C, SWP energies, P123 in the reference's row-major COO order,
 resolvents, on-shell U) into one .npz per case.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [--pade]
+
+(--pade regenerates only the Pade fixtures <case>_pade.npz.)
 
 Test infrastructure only; the product never reads these files.
 """
@@ -89,8 +91,31 @@ def run_case(name, opts):
               "nnz", [ch["nnz"] for ch in meta["channels"]])
 
 
+def run_pade(name, opts):
+    """U of the reference's default production path (Pade-resummed Neumann
+    series, CPP/solve_faddeev.cpp:440-1444) for the same case, written to
+    <name>_pade.npz as U_pade_c<k>."""
+    with tempfile.TemporaryDirectory() as out:
+        args = [REF_BIN, "dump", out, "--solver=pade"] + [f"{k}={v}" for k, v in opts.items()]
+        subprocess.run(args, check=True, cwd=out, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 4)))
+        meta = read_meta(os.path.join(out, "meta.txt"))
+        data = {}
+        for ch in meta["channels"]:
+            c = ch["chn"]
+            data[f"U_pade_c{c}"] = np.fromfile(os.path.join(out, f"U_c{c}.bin"), dtype=np.complex128)
+        np.savez_compressed(os.path.join(HERE, f"{name}_pade.npz"), **data)
+        print(name, "pade channels", len(meta["channels"]))
+
+
+PADE_CASES = ["mt_swave_n16", "lo_j1_J3_n8"]
+
 if __name__ == "__main__":
     if not os.path.exists(REF_BIN):
         sys.exit(f"{REF_BIN} missing: run `make -C oracle ref` first")
+    only_pade = "--pade" in sys.argv
     for name, opts in CASES.items():
-        run_case(name, opts)
+        if not only_pade:
+            run_case(name, opts)
+        if name in PADE_CASES:
+            run_pade(name, opts)

@@ -4,7 +4,7 @@ import pytest
 
 import harness as oracle
 import tictac_b200 as tt
-from conftest import CASES, load_case, rel
+from conftest import CASES, GOLDEN, load_case, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -135,6 +135,21 @@ def test_ragged_block_sizes_against_oracle(Np, Nq):
         for prec in PRECISIONS:
             U, rep = run.solve(c, prec)
             assert rel(U, U_o) <= 1e-10, (c, prec, rep)
+    run.close()
+
+
+@pytest.mark.parametrize("case", ["mt_swave_n16", "lo_j1_J3_n8"])
+def test_pade_path_matches_reference_pade(case):
+    # TT_PRECISION_PADE against the reference's own Pade output and its dense
+    # solve, at the method's accuracy (its stopping rule is 1e-6 relative)
+    g, m = load_case(case)
+    p = np.load(f"{GOLDEN}/{case}_pade.npz")
+    run = tt.Run(**m["opts"])
+    for c in range(run.num_channels):
+        U, rep = run.solve(c, tt.PRECISION_PADE)
+        assert rel(U, p[f"U_pade_c{c}"]) <= 1e-5, (c, rep)
+        assert rel(U, g[f"U_c{c}"]) <= 1e-5, (c, rep)
+        assert 1 <= rep["refine_iters"] <= 14
     run.close()
 
 

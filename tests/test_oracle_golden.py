@@ -4,7 +4,9 @@ import numpy as np
 import pytest
 
 import harness as oracle
-from conftest import CASES, load_case, rel
+import os
+
+from conftest import CASES, GOLDEN, load_case, rel
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -37,3 +39,21 @@ def test_oracle_empty_channel_edge():
     G = np.zeros((1, A.shape[0]), dtype=np.complex128)
     U = oracle.dense_solve(A, G, g["q_idx"][:1], [], m["Nq"], m["Np"])
     assert U.size == 0
+
+
+@pytest.mark.parametrize("case", ["mt_swave_n16", "lo_j1_J3_n8"])
+def test_oracle_pade_matches_reference_pade(case):
+    # the reference's default production path (Pade-resummed Neumann series);
+    # high-order Pade ratios amplify 1e-15 differences in the coefficients to
+    # about 1e-7, so the method is compared at its own accuracy
+    g, m = load_case(case)
+    p = np.load(os.path.join(GOLDEN, f"{case}_pade.npz"))
+    for c in range(int(g["n_chn"])):
+        pw = g[f"pw_c{c}"]
+        lay = oracle.layout(pw, m["Np"], g["V_unco"], g["V_coup"], g["C_unco"], g["C_coup"], g["e_unco"], g["e_coup"],
+                            m["tensor_force"], m["iso"])
+        A = oracle.build_A(lay, pw.shape[0], m["Nq"], m["Np"], g[f"p123_row_c{c}"], g[f"p123_col_c{c}"],
+                           g[f"p123_val_c{c}"])
+        U = oracle.pade_solve(A, g[f"G_c{c}"], g["q_idx"], oracle.deuterons(pw), m["Nq"], m["Np"])
+        assert rel(U, p[f"U_pade_c{c}"]) <= 1e-5
+        assert rel(U, g[f"U_c{c}"]) <= 1e-5

@@ -105,6 +105,7 @@ SolveOptions options_of(const RunParams& rp, int precision) {
   SolveOptions o;
   o.mixed = precision == TT_PRECISION_MIXED || precision == TT_PRECISION_MIXED_SIMT;
   o.tensor_cores = precision == TT_PRECISION_MIXED;
+  o.pade = precision == TT_PRECISION_PADE;
   o.refine_tol = rp.refine_tol;
   o.refine_max_iter = rp.refine_max_iter;
   return o;
@@ -185,7 +186,7 @@ int dropin_solve(tt_complex* U, tt_complex* dU, int n_theta, const double* dVu, 
   std::vector<int> deut(os->deuteron_idx_array, os->deuteron_idx_array + os->num_deuteron_states);
   std::vector<double> Uh, dUh, dvc;
   SolveReport rep;
-  if (rpp->precision < TT_PRECISION_FP64 || rpp->precision > TT_PRECISION_MIXED_SIMT)
+  if (rpp->precision < TT_PRECISION_FP64 || rpp->precision > TT_PRECISION_PADE)
     return fail(TT_ERR_BADARG, "unknown precision");
   AdjointRequest adj;
   DevBuf<double> d_dvc;
@@ -498,7 +499,7 @@ int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_re
   int s = check_chn(run, chn);
   if (s) return s;
   if (!U) return fail(TT_ERR_BADARG, "null U");
-  if (precision < TT_PRECISION_FP64 || precision > TT_PRECISION_MIXED_SIMT) return fail(TT_ERR_BADARG, "unknown precision");
+  if (precision < TT_PRECISION_FP64 || precision > TT_PRECISION_PADE) return fail(TT_ERR_BADARG, "unknown precision");
   double msA = 0;
   if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
   if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));
@@ -519,7 +520,7 @@ int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const
   if (s) return s;
   if (!U || n_theta < 0 || (n_theta > 0 && (!dU || !dVu || (run->swp.n_coup && !dVc))))
     return fail(TT_ERR_BADARG, "null or negative argument");
-  if (precision < TT_PRECISION_FP64 || precision > TT_PRECISION_MIXED_SIMT) return fail(TT_ERR_BADARG, "unknown precision");
+  if (precision < TT_PRECISION_FP64 || precision > TT_PRECISION_PADE) return fail(TT_ERR_BADARG, "unknown precision");
   double msA = 0;
   if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
   if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));

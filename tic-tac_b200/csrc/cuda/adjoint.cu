@@ -30,33 +30,41 @@ __global__ void k_transpose(const T* __restrict__ in, int n, T* __restrict__ out
   }
 }
 
-// y_k += A^T v_k for k < nrhs <= 4: CTA = 256 columns x 256 rows of A, one
-// column per thread (coalesced rows), partial sums added atomically
+// y_k += A^T v_k for k < nrhs <= GT_MAXV: CTA = 256 columns x 256 rows of A,
+// one column per thread (coalesced rows), partial sums added atomically
 constexpr int GT_ROWS = 256;
+constexpr int GT_MAXV = 8;
 __global__ void __launch_bounds__(256) k_gemv_t(const double* __restrict__ A, int n, const double2* __restrict__ v,
                                                 int nrhs, double2* __restrict__ y) {
-  __shared__ double2 sv[4][GT_ROWS];
+  __shared__ double2 sv[GT_MAXV][GT_ROWS];
   const int c = blockIdx.x * 256 + threadIdx.x;
   const int r0 = blockIdx.y * GT_ROWS, rn = min(GT_ROWS, n - r0);
-  for (int t = threadIdx.x; t < 4 * GT_ROWS; t += blockDim.x) {
+  for (int t = threadIdx.x; t < GT_MAXV * GT_ROWS; t += blockDim.x) {
     const int k = t / GT_ROWS, i = t % GT_ROWS;
     sv[k][i] = (k < nrhs && i < rn) ? v[(size_t)k * n + r0 + i] : make_double2(0, 0);
   }
   __syncthreads();
   if (c >= n) return;
-  double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+  double ar[GT_MAXV], ai[GT_MAXV];
+#pragma unroll
+  for (int k = 0; k < GT_MAXV; k++) ar[k] = ai[k] = 0;
   const double* Ac = A + (size_t)r0 * n + c;
   for (int i = 0; i < rn; i++) {
     const double a = Ac[(size_t)i * n];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      ar[k] += a * sv[k][i].x;
-      ai[k] += a * sv[k][i].y;
+    for (int k = 0; k < GT_MAXV; k++) {
+      if (k < nrhs) {
+        ar[k] += a * sv[k][i].x;
+        ai[k] += a * sv[k][i].y;
+      }
     }
   }
-  for (int k = 0; k < nrhs; k++) {
-    atomicAdd(&y[(size_t)k * n + c].x, ar[k]);
-    atomicAdd(&y[(size_t)k * n + c].y, ai[k]);
+#pragma unroll
+  for (int k = 0; k < GT_MAXV; k++) {
+    if (k < nrhs) {
+      atomicAdd(&y[(size_t)k * n + c].x, ar[k]);
+      atomicAdd(&y[(size_t)k * n + c].y, ai[k]);
+    }
   }
 }
 
@@ -180,7 +188,60 @@ __global__ void __launch_bounds__(256) k_bilinear(int n, const double2* __restri
   }
 }
 
+// R[k][c] = A[rows[k] n + c] (complex, zero imaginary part)
+__global__ void k_gather_rows(const double* __restrict__ A, int n, const int32_t* __restrict__ rows, int nrows,
+                              double2* __restrict__ R) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * nrows) return;
+  const int k = (int)(t / n), c = (int)(t % n);
+  R[t] = make_double2(A[(size_t)rows[k] * n + c], 0.0);
+}
+
+// V[k][c] = R[k][c] G[e[k]][c]
+__global__ void k_scale_rows(const double2* __restrict__ R, const double2* __restrict__ G,
+                             const int32_t* __restrict__ e, int n, int nrows, double2* __restrict__ V) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * nrows) return;
+  const int k = (int)(t / n), c = (int)(t % n);
+  const double2 r = R[t], g = G[(size_t)e[k] * n + c];
+  V[t] = make_double2(r.x * g.x - r.y * g.y, r.x * g.y + r.y * g.x);
+}
+
+// out[i] = R[src_row[i]][src_col[i]]
+__global__ void k_pick(const double2* __restrict__ R, int n, const int32_t* __restrict__ src_row,
+                       const int32_t* __restrict__ src_col, int m, double2* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] = R[(size_t)src_row[i] * n + src_col[i]];
+}
+
 }  // namespace
+
+int gather_rows_device(const double* d_A, int n, const int32_t* d_rows, int nrows, double* d_R, cudaStream_t st) {
+  k_gather_rows<<<ceil_div((size_t)n * nrows, 256), 256, 0, st>>>(d_A, n, d_rows, nrows, reinterpret_cast<double2*>(d_R));
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int scale_rows_device(const double* d_R, const double* d_G, const int32_t* d_e, int n, int nrows, double* d_V,
+                      cudaStream_t st) {
+  k_scale_rows<<<ceil_div((size_t)n * nrows, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_R),
+                                                                 reinterpret_cast<const double2*>(d_G), d_e, n, nrows,
+                                                                 reinterpret_cast<double2*>(d_V));
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int pick_device(const double* d_R, int n, const int32_t* d_row, const int32_t* d_col, int m, double* d_out,
+                cudaStream_t st) {
+  if (m <= 0) return TT_OK;
+  k_pick<<<ceil_div(m, 128), 128, 0, st>>>(reinterpret_cast<const double2*>(d_R), n, d_row, d_col, m,
+                                           reinterpret_cast<double2*>(d_out));
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
 
 template <typename T>
 int transpose_device(const T* in, int n, T* out, cudaStream_t st) {
@@ -194,8 +255,8 @@ template int transpose_device<float2>(const float2*, int, float2*, cudaStream_t)
 template int transpose_device<double2>(const double2*, int, double2*, cudaStream_t);
 
 int gemv_t_device(const double* d_A, int n, const double* d_v, int nrhs, double* d_y, cudaStream_t st) {
-  if (nrhs > 4) {
-    set_error("A^T products take at most 4 vectors per call");
+  if (nrhs > GT_MAXV) {
+    set_error("A^T products take at most 8 vectors per call");
     return TT_ERR_BADARG;
   }
   ProfScope prof(TT_PROF_RESIDUAL, st, 4.0 * n * (double)n * nrhs, 8.0 * n * (double)n);

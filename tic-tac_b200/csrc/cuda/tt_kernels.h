@@ -110,8 +110,15 @@ int csc_to_csr_device(const double* h_val, const int32_t* h_row, const uint64_t*
 // Adjoint pieces (adjoint.cu); vectors are complex128 [k][n].
 template <typename T>
 int transpose_device(const T* in, int n, T* out, cudaStream_t st);
-// y_k = A^T v_k, k < nrhs <= 4
+// y_k = A^T v_k, k < nrhs <= 8
 int gemv_t_device(const double* d_A, int n, const double* d_v, int nrhs, double* d_y, cudaStream_t st);
+// Pade path (adjoint.cu): R[k] = A[rows[k], :] as complex; V[k] = R[k] o G[e[k]];
+// out[i] = R[row[i]][col[i]]
+int gather_rows_device(const double* d_A, int n, const int32_t* d_rows, int nrows, double* d_R, cudaStream_t st);
+int scale_rows_device(const double* d_R, const double* d_G, const int32_t* d_e, int n, int nrows, double* d_V,
+                      cudaStream_t st);
+int pick_device(const double* d_R, int n, const int32_t* d_row, const int32_t* d_col, int m, double* d_out,
+                cudaStream_t st);
 // r_k = e_{rows[k]} - lam_k + G o y_k
 int residual_t_device(const double* d_lam, const double* d_y, const double* d_G, const int32_t* d_rows, int n,
                       int nrhs, double* d_r, cudaStream_t st);

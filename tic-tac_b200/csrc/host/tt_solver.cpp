@@ -2,6 +2,7 @@
 #include "tt_solver.h"
 
 #include <chrono>
+#include <complex>
 #include <cmath>
 #include <cstdlib>
 #include <map>
@@ -198,6 +199,154 @@ int ChannelSolver::resolvent(const std::vector<double>& E, cudaStream_t st) {
   return TT_OK;
 }
 
+namespace {
+
+using cd = std::complex<double>;
+
+// Determinant by LU with partial pivoting, pivots chosen by |re| + |im| as
+// LAPACK's zgetrf does (determinant, CPP/General_functions/matrix_routines.cpp:82-101).
+cd determinant(std::vector<cd> a, int n) {
+  cd det = 1.0;
+  for (int k = 0; k < n; k++) {
+    int p = k;
+    double best = -1;
+    for (int i = k; i < n; i++) {
+      const double v = std::fabs(a[i * n + k].real()) + std::fabs(a[i * n + k].imag());
+      if (v > best) {
+        best = v;
+        p = i;
+      }
+    }
+    if (a[p * n + k] == cd(0.0)) return 0.0;
+    if (p != k) {
+      for (int c = 0; c < n; c++) std::swap(a[k * n + c], a[p * n + c]);
+      det = -det;
+    }
+    det *= a[k * n + k];
+    for (int i = k + 1; i < n; i++) {
+      const cd l = a[i * n + k] / a[k * n + k];
+      for (int c = k + 1; c < n; c++) a[i * n + c] -= l * a[k * n + c];
+    }
+  }
+  return det;
+}
+
+// [N/M] Pade approximant at z of the series with coefficients a[0 .. N+M]
+// (pade_approximant, CPP/solve_faddeev.cpp:271-296)
+cd pade_approximant(const cd* a, int N, int M, cd z) {
+  std::vector<cd> P((M + 1) * (M + 1)), Q((M + 1) * (M + 1));
+  for (int r = 0; r < M; r++)
+    for (int c = 0; c < M + 1; c++) P[r * (M + 1) + c] = Q[r * (M + 1) + c] = a[N - M + 1 + r + c];
+  for (int c = 0; c < M + 1; c++) {
+    Q[M * (M + 1) + c] = std::pow(z, M - c);
+    cd s = 0.0;
+    for (int j = M - c; j < N + 1; j++) s += a[j - (M - c)] * std::pow(z, j);
+    P[M * (M + 1) + c] = s;
+  }
+  return determinant(P, M + 1) / determinant(Q, M + 1);
+}
+
+}  // namespace
+
+// The reference's production solver (pade_method_solve,
+// CPP/solve_faddeev.cpp:440-1444): on-shell rows r_0 = A[row, :] and
+// r_{n+1} = (r_n o G_j) A give the Neumann coefficients a_n of
+// U = sum_n A (G A)^n; [N/N] Pade approximants at z = 1 for N = 0 .. 14 are
+// formed as two new terms arrive, and an element stops at the first of the
+// reference's criteria (N = 14; no better difference in the last 4 orders;
+// smallest difference of consecutive approximants < 1e-6 |best| or < 1e-7).
+int ChannelSolver::solve_pade(const std::vector<int>& q_idx, const std::vector<int>& deut, std::vector<double>& U,
+                              SolveReport& r, cudaStream_t st) {
+  constexpr int NM_MAX = 14, NTERMS = 2 * NM_MAX + 1;
+  auto t0 = std::chrono::steady_clock::now();
+  const int nE = (int)q_idx.size(), nd = (int)deut.size();
+  const int Nq = L_.Nq, Np = L_.Np;
+  const int nrows = nd * nE, nel = nd * nd * nE;
+  std::vector<int32_t> rows(nrows), erow(nrows), prow(nel), pcol(nel);
+  for (int d = 0; d < nd; d++)
+    for (int j = 0; j < nE; j++) {
+      rows[d * nE + j] = deut[d] * Nq * Np + q_idx[j] * Np;
+      erow[d * nE + j] = j;
+    }
+  for (int dr = 0; dr < nd; dr++)
+    for (int dc = 0; dc < nd; dc++)
+      for (int j = 0; j < nE; j++) {
+        const int e = dr * nd * nE + dc * nE + j;
+        prow[e] = dr * nE + j;
+        pcol[e] = deut[dc] * Nq * Np + q_idx[j] * Np;
+      }
+  DevBuf<int32_t> d_rows, d_erow, d_prow, d_pcol;
+  DevBuf<double> R, V, picked;
+  TT_TRY(d_rows.upload(rows, st));
+  TT_TRY(d_erow.upload(erow, st));
+  TT_TRY(d_prow.upload(prow, st));
+  TT_TRY(d_pcol.upload(pcol, st));
+  TT_TRY(R.alloc((size_t)2 * n * nrows));
+  TT_TRY(V.alloc((size_t)2 * n * nrows));
+  TT_TRY(picked.alloc((size_t)2 * nel));
+  std::vector<cd> a((size_t)nel * NTERMS, 0.0), pa((size_t)nel * (NM_MAX + 1), 0.0), hv(nel);
+  std::vector<char> conv(nel, 0);
+  std::vector<int> best(nel, 0);
+  auto extract = [&](int term) -> int {
+    TT_TRY(pick_device(R.ptr, n, d_prow.ptr, d_pcol.ptr, nel, picked.ptr, st));
+    TT_CUDA_TRY(cudaMemcpyAsync(hv.data(), picked.ptr, sizeof(cd) * nel, cudaMemcpyDeviceToHost, st));
+    TT_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int e = 0; e < nel; e++)
+      if (!conv[e]) a[(size_t)e * NTERMS + term] = hv[e];
+    return TT_OK;
+  };
+  TT_TRY(gather_rows_device(A_.ptr, n, d_rows.ptr, nrows, R.ptr, st));
+  TT_TRY(extract(0));
+  int nconv = 0, top = 0;
+  double worst_diff = 0;
+  for (int NM = 0; NM <= NM_MAX && nconv < nel; NM++) {
+    top = NM;
+    for (int term = 2 * NM - 1; term <= 2 * NM; term++) {
+      if (term <= 0) continue;
+      TT_TRY(scale_rows_device(R.ptr, G_.ptr, d_erow.ptr, n, nrows, V.ptr, st));
+      for (int k0 = 0; k0 < nrows; k0 += 8)
+        TT_TRY(gemv_t_device(A_.ptr, n, V.ptr + (size_t)2 * n * k0, std::min(8, nrows - k0),
+                             R.ptr + (size_t)2 * n * k0, st));
+      TT_TRY(extract(term));
+    }
+    for (int e = 0; e < nel; e++) {
+      if (conv[e]) continue;
+      cd* p = &pa[(size_t)e * (NM_MAX + 1)];
+      p[NM] = pade_approximant(&a[(size_t)e * NTERMS], NM, NM, 1.0);
+      int idx_best = 0;
+      double min_diff = 1;
+      for (int prev = 0; prev < NM; prev++) {
+        // the reference compares approximant 0 with the slot before it, zero here
+        const double d = std::abs(p[prev] - (prev > 0 ? p[prev - 1] : cd(0.0)));
+        if (d < min_diff && d > 1e-15) {
+          idx_best = prev;
+          min_diff = d;
+        }
+      }
+      const double d = std::abs(p[NM] - (NM > 0 ? p[NM - 1] : cd(0.0)));
+      if (d < min_diff && d > 1e-15) {
+        idx_best = NM;
+        min_diff = d;
+      }
+      if (NM == NM_MAX || NM - idx_best > 4 || min_diff < 1e-6 * std::abs(p[idx_best]) || min_diff < 1e-7) {
+        conv[e] = 1;
+        best[e] = idx_best;
+        nconv++;
+        worst_diff = std::max(worst_diff, min_diff / std::max(1e-300, std::abs(p[idx_best])));
+      }
+    }
+  }
+  for (int e = 0; e < nel; e++) {
+    const cd v = pa[(size_t)e * (NM_MAX + 1) + best[e]];
+    U[2 * e + 0] = v.real();
+    U[2 * e + 1] = v.imag();
+  }
+  r.ms_solve += ms_since(t0);
+  r.refine_iters = top;           // highest [N/N] order formed
+  r.final_correction = worst_diff;  // largest relative difference of consecutive approximants at the choice
+  return TT_OK;
+}
+
 int ChannelSolver::adjoint_energy(int j, int nE, int nd, const double* Gj, const int32_t* d_rows, const int32_t* d_perm,
                                   double* tmp, const double* x, const SolveOptions& opt, const void* F, void* Ft,
                                   TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT,
@@ -291,6 +440,15 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
   if (nd == 0 || nE == 0) {
     if (rep) *rep = r;
     return TT_OK;
+  }
+  if (opt.pade) {
+    if (adj) {
+      set_error("the adjoint needs the LU path; the Pade series has no stored factors");
+      return TT_ERR_UNSUPPORTED;
+    }
+    const int s = solve_pade(q_idx, deut, U, r, st);
+    if (rep) *rep = r;
+    return s;
   }
   const int Nq = L_.Nq, Np = L_.Np;
   DevBuf<int32_t> ipiv, cols, rhs_e, perm_d;

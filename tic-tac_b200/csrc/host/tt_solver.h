@@ -30,6 +30,7 @@ int resolvent_noalloc(const RunParams& rp, const PWChannel& ch, int Np, int Nq, 
 struct SolveOptions {
   bool mixed = true;        // complex64 LU on tensor cores + FP64 refinement; false: complex128 LU
   bool tensor_cores = true; // trailing update on tcgen05 (mixed only)
+  bool pade = false;        // Pade-resummed Neumann series on the resident A instead of an LU
   double refine_tol = 1e-12;
   int refine_max_iter = 30;
 };
@@ -81,6 +82,8 @@ class ChannelSolver {
   int nE() const { return nE_; }
 
  private:
+  int solve_pade(const std::vector<int>& q_idx, const std::vector<int>& deut, std::vector<double>& U,
+                 SolveReport& r, cudaStream_t st);
   int adjoint_energy(int j, int nE, int nd, const double* Gj, const int32_t* d_rows, const int32_t* d_perm,
                      double* tmp, const double* x, const SolveOptions& opt, const void* F, void* Ft,
                      TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT, double* rT,

@@ -27,6 +27,7 @@ TT_ERR_SINGULAR = 7
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRECISION_MIXED_SIMT = 2
+PRECISION_PADE = 3
 
 EXPORTED_SYMBOLS = (
     "tt_run_params_default", "tt_fill_P123_arrays", "tt_calculate_resolvent_array_in_SWP_basis",
