@@ -394,6 +394,9 @@ def main():
         infos = [run.channel_info(c) for c in range(run.num_channels)]
         nE = len(run.energies()[0])
         run.close()
+        config["channels_per_step"] = len(infos)
+        config["energies_per_rank"] = nE
+        config["n_per_channel"] = [i["n"] for i in infos]
         samples = []
         for _ in range(args.warmup + max(1, args.steps)):
             r2, why = reference_sample(args)
