@@ -215,11 +215,9 @@ __global__ void __launch_bounds__(512) k_prev_mul(const T* __restrict__ LU, int 
 //  - Blocks q >= 2 are owned round-robin by CTAs 1..G-1, which keep their rows
 //    of x in shared memory for the whole sweep: at step s every owner applies
 //    block column s to its unsolved blocks (q >= s+2) and publishes block s+2
-//    to x, which CTA 0 reads at the next step.  Lanes own columns: each lane
-//    holds its two entries of x_s in registers, and the factor tiles go from
-//    global memory straight into 3 (complex64) or 2 (complex128) register
-//    buffers used round-robin, each refilled as soon as it is applied, so the
-//    loads run ahead across the barriers (the factor does not depend on x).  x is never read-modify-written in global
+//    to x, which CTA 0 reads at the next step.  Eight lanes share a row (four
+//    rows per warp) against x_s staged in shared memory, and the next owned
+//    tile is loaded while the current one is applied.  x is never read-modify-written in global
 //    memory.
 constexpr int RHS = 4;
 constexpr int TRSV_THREADS = 512;
@@ -318,45 +316,10 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(const T* __restrict__ 
     }
   };
 
-  // owners: item iterator over (step, owned slot) in consumption order
+  // owners: slots j of block q = 2 + me + j (G-1)
   const int me = (int)blockIdx.x - 1;
   auto first_slot = [&](int s) { return s > me ? (s - me + (G - 1) - 1) / (G - 1) : 0; };
   auto live = [&](int j) { return j < own_max && 2 + me + j * (G - 1) < nb; };
-  int ps = 0, pj = 0;
-  // tile of the next item: rows warp*4+h (h < 4), columns lane + 32 e (e < 2)
-  auto load_item = [&](T(&dst)[8]) {
-    // past the last item of step ps: the next step's first slot, if live; the
-    // first slot only moves forward with the step, so a step without items
-    // means that no later step has any
-    if (ps + 1 < nb && !live(pj)) {
-      ps++;
-      pj = first_slot(ps);
-      if (!live(pj)) ps = nb - 1;
-    }
-    if (ps + 1 < nb) {
-      const int q = 2 + me + pj * (G - 1);
-      const int r0 = blk(q) * TSB + warp * 4, c0 = blk(ps) * TSB, csz = min(TSB, n - c0);
-#pragma unroll
-      for (int h = 0; h < 4; h++)
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int r = r0 + h, c = lane + 32 * e;
-          dst[h * 2 + e] = (r < n && c < csz) ? LU[(size_t)r * n + c0 + c] : T{0, 0};
-        }
-      pj++;
-    } else {
-#pragma unroll
-      for (int u = 0; u < 8; u++) dst[u] = T{0, 0};
-    }
-    // keep the loads here, ahead of their use: without this the compiler may
-    // sink them to the apply that consumes the buffer and lose the prefetch
-    asm volatile("" ::: "memory");
-  };
-  // three tiles in flight for complex64, two for complex128 (register budget)
-  constexpr bool DEEP = sizeof(T) == 8;
-  constexpr int NBUF = DEEP ? 3 : 2;
-  T a0[8], a1[8], a2[DEEP ? 8 : 1];
-  int slot = 0;  // buffer holding the next item to apply
 
   if (lead) {
     // first block: x_0 = inv[0] x_0
@@ -388,10 +351,6 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(const T* __restrict__ 
         xo[((size_t)j * RHS + k) * TSB + r] = (k < kn && r < bsz) ? ld_x(k, r0 + r) : T{0, 0};
       }
     }
-    pj = first_slot(0);
-    load_item(a0);
-    load_item(a1);
-    if constexpr (DEEP) load_item(a2);
   }
   grid.sync();
   for (int s = 0; s + 1 < nb; s++) {
@@ -413,53 +372,56 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(const T* __restrict__ 
         cp_async_commit();
       }
     } else {
-      // this lane's entries of x_s
-      T xv[RHS][2];
+      for (int e = t; e < TSB * RHS; e += blockDim.x) {
+        const int k = e / TSB, r = e % TSB;
+        xs[k][r] = (k < kn && r < csz) ? ld_x(k, c0 + r) : T{0, 0};
+      }
+      __syncthreads();
+      // 8 lanes per row, 4 rows per warp: x_s from shared memory, the next
+      // owned tile loaded while this one is applied
+      const int sub = lane >> 3, sl = lane & 7, row = warp * 4 + sub;
+      T a[8], an[8];
+      auto load8 = [&](int j, T(&dst)[8]) {
+        const int r = blk(2 + me + j * (G - 1)) * TSB + row;
 #pragma unroll
-      for (int k = 0; k < RHS; k++)
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int c = lane + 32 * e;
-          xv[k][e] = (k < kn && c < csz) ? ld_x(k, c0 + c) : T{0, 0};
-        }
-      auto apply = [&](const T(&a)[8], int j) {
-#pragma unroll
-        for (int hp = 0; hp < 2; hp++) {
-          C acc[16];
-#pragma unroll
-          for (int hh = 0; hh < 2; hh++) {
-            const int h = hp * 2 + hh;
-#pragma unroll
-            for (int k = 0; k < RHS; k++) {
-              const T p0 = a[h * 2], p1 = a[h * 2 + 1], v0 = xv[k][0], v1 = xv[k][1];
-              acc[(hh * RHS + k) * 2 + 0] = p0.x * v0.x - p0.y * v0.y + p1.x * v1.x - p1.y * v1.y;
-              acc[(hh * RHS + k) * 2 + 1] = p0.x * v0.y + p0.y * v0.x + p1.x * v1.y + p1.y * v1.x;
-            }
-          }
-          const C v = butterfly16<C>(acc, lane);
-          const int idx = lane >> 1, hh = idx >> 3, k = (idx >> 1) & 3, part = idx & 1;
-          const int row = warp * 4 + hp * 2 + hh;
-          if ((lane & 1) == 0 && k < kn) reinterpret_cast<C*>(&xo[((size_t)j * RHS + k) * TSB + row])[part] -= v;
+        for (int u = 0; u < 8; u++) {
+          const int c = sl + 8 * u;
+          dst[u] = (r < n && c < csz) ? LU[(size_t)r * n + c0 + c] : T{0, 0};
         }
       };
-      // buffers are consumed and refilled in place (a register copy of a tile
-      // whose load is still in flight would wait for it)
-      // not unrolled: three inlined copies of the tile step are already large
-#pragma unroll 1
-      for (int j = first_slot(s); live(j); j++) {
-        if (slot == 0) {
-          apply(a0, j);
-          load_item(a0);
-        } else if (slot == 1) {
-          apply(a1, j);
-          load_item(a1);
-        } else {
-          if constexpr (DEEP) {
-            apply(a2, j);
-            load_item(a2);
+      // complex128 tiles are not double-buffered: two would not fit in registers
+      constexpr bool PF = sizeof(T) == sizeof(float2);
+      const int j0 = first_slot(s);
+      if (PF && live(j0)) load8(j0, a);
+      for (int j = j0; live(j); j++) {
+        const bool more = PF && live(j + 1);
+        if (more) load8(j + 1, an);
+        if (!PF) load8(j, a);
+#pragma unroll
+        for (int k = 0; k < RHS; k++) {
+          if (k >= kn) break;
+          C sr = 0, si = 0;
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const T v = xs[k][sl + 8 * u];
+            sr += a[u].x * v.x - a[u].y * v.y;
+            si += a[u].x * v.y + a[u].y * v.x;
+          }
+#pragma unroll
+          for (int o = 4; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+          }
+          if (sl == 0) {
+            T& d = xo[((size_t)j * RHS + k) * TSB + row];
+            d.x -= sr;
+            d.y -= si;
           }
         }
-        slot = slot + 1 == NBUF ? 0 : slot + 1;
+        if (more) {
+#pragma unroll
+          for (int u = 0; u < 8; u++) a[u] = an[u];
+        }
       }
       // publish block s+2 if owned here
       const int qp = s + 2;
