@@ -2,16 +2,19 @@
 // matrix 1 - A G (row-major, in place).  Replaces the LAPACK zgetrf of the
 // reference's dense solver (CPP/General_functions/matrix_routines.cpp:73-80).
 //
-// Outer panels of NB columns (256 for the complex64 / tensor-core path, 128
+// Outer panels of NB columns (512 for the complex64 / tensor-core path, 128
 // for complex128).  Each panel is factored in IB = 32 column sub-panels:
-//   k_subpanel   cooperative kernel, ONE grid barrier per column: every block
-//                publishes its best pivot candidate together with a copy of
-//                that row (and the owner of the diagonal row publishes it), so
-//                after the barrier every block knows the pivot row's values and
-//                the two owners swap their rows without a second barrier
+//   k_subpanel_smem  cooperative kernel with each block's rows in shared
+//                memory, ONE grid barrier per column: every block posts its
+//                best pivot candidate as a packed 64-bit key (atomicMax) and a
+//                copy of that row (the owner of the diagonal row posts it too),
+//                so after the barrier every block reads the key and the pivot
+//                row and the two owners swap their rows without a second
+//                barrier (k_subpanel: the same from global memory, for
+//                sub-panels too tall for shared memory)
 //   k_laswp2     the sub-panel's interchanges on the rest of the panel
 //   k_trsm_blk   U = L^{-1} U for the 32-wide unit-lower diagonal block
-//   k_gemm_sub   rank-32 update of the remaining panel columns (CUDA cores)
+//   tc_gemm_sub / k_gemm_sub  rank-32 update of the remaining panel columns
 // then the panel's interchanges outside the panel, the blocked triangular
 // solve for U12 and the trailing update A22 -= L21 U12 (tcgen05 BF16x3 for
 // complex64, CUDA-core complex GEMM for complex128).
@@ -57,13 +60,15 @@ __device__ __forceinline__ T cdiv_smith(T a, T b) {
 constexpr int IB = 32;
 constexpr int SP = IB + 1;                     // shared-memory row stride of a staged sub-panel
 constexpr size_t kSubpanelSmem = 220 * 1024;  // bound on one block's staged sub-panel rows
+constexpr int SP_THREADS = 512;               // threads of the shared-memory sub-panel kernel
 
 template <typename T>
 struct PivotScratch {
-  double* val;  // [2][G]
-  int* idx;     // [2][G]
-  T* row;       // [2][G][IB]
-  T* top;       // [2][IB]
+  double* val;              // [2][G]
+  int* idx;                 // [2][G]
+  T* row;                   // [2][G][IB]
+  T* top;                   // [2][IB]
+  unsigned long long* key;  // [n], zero before the factorization: column j's packed pivot
 };
 
 // Sub-panel rows [c0, n), columns [c0, c0+w), w <= IB.
@@ -201,147 +206,188 @@ __global__ void __launch_bounds__(256) k_subpanel(T* __restrict__ A, int n, int 
   }
 }
 
+// (value, row) pivot candidates: larger |re| + |im| wins, ties go to the lower
+// row, as in LAPACK's izamax; row < 0 marks "no candidate"
+template <typename V>
+__device__ __forceinline__ bool cand_better(V v, int i, V bv, int bi) {
+  return i >= 0 && (bi < 0 || v > bv || (v == bv && i < bi));
+}
+// best of lanes [0, W) into lane 0 (W a power of two <= 32)
+template <int W, typename V>
+__device__ __forceinline__ void warp_argmax(V& v, int& i) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) {
+    const V ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (cand_better(ov, oi, v, i)) {
+      v = ov;
+      i = oi;
+    }
+  }
+}
+// A candidate packed so that a larger key is the better candidate: the top 44
+// bits of the non-negative double magnitude (exact for FP32 magnitudes;
+// complex128 magnitudes that agree to 2^-32 relative count as equal), then
+// the complement of the row offset (lower row wins ties).  0 = no candidate.
+__device__ __forceinline__ unsigned long long pivot_key(double v, int off) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v) >> 20;
+  return (b << 20) | (unsigned long long)(0xFFFFF - off);
+}
+
 // Same algorithm with each block's rows of the sub-panel resident in shared
-// memory for all w columns: one coalesced load and one store per element,
-// everything else (pivot search, swaps, elimination) in shared memory.
+// memory for all w columns: one coalesced load and one store per element.
+// Warps own rows and lanes own columns.  One pass per column applies the
+// multipliers (times the pivot's reciprocal, as LAPACK's zgetf2 scales),
+// updates the remaining columns and tracks the next column's candidate.  The
+// pivot is chosen through one 64-bit atomicMax per block on the column's key,
+// so after the grid barrier each block reads one word, then the winner's
+// published row: one grid barrier, two dependent L2 reads and two block
+// barriers per column.  Row offsets below 2^20 - 1 (checked by the caller).
 template <typename T>
-__global__ void __launch_bounds__(256) k_subpanel_smem(T* __restrict__ A, int n, int c0, int w,
-                                                       int32_t* __restrict__ ipiv, PivotScratch<T> scr,
-                                                       int* __restrict__ info) {
+__global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(T* __restrict__ A, int n, int c0, int w,
+                                                              int32_t* __restrict__ ipiv, PivotScratch<T> scr,
+                                                              int* __restrict__ info) {
   cg::grid_group grid = cg::this_grid();
   extern __shared__ unsigned char sp_raw[];
-  T* sA = reinterpret_cast<T*>(sp_raw);  // [chunk][SP], padded against bank conflicts
+  T* sA = reinterpret_cast<T*>(sp_raw);  // [chunk][SP]
+  using R = typename Real<T>::R;
+  constexpr int NW = SP_THREADS / 32;
   const int G = gridDim.x;
   const int m = n - c0;
   const int chunk = (m + G - 1) / G;
   const int lo = c0 + blockIdx.x * chunk;
   const int hi = min(n, lo + chunk);
   const int nr = max(0, hi - lo);
-  __shared__ double s_val[256];
-  __shared__ int s_idx[256];
-  __shared__ int s_grp[256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ R s_wv[NW];
+  __shared__ int s_wi[NW];
   __shared__ T s_prow[IB];
-  __shared__ T s_l[1];
-  __shared__ int s_piv, s_zero, s_win;
-  for (int t = threadIdx.x; t < nr * w; t += blockDim.x) {
-    const int r = t / w, c = t % w;
-    sA[r * SP + c] = A[(size_t)(lo + r) * n + c0 + c];
-  }
+  __shared__ int s_zero;
+  for (int r = warp; r < nr; r += NW)
+    if (lane < w) sA[r * SP + lane] = A[(size_t)(lo + r) * n + c0 + lane];
   __syncthreads();
+  // this block's candidate for column jc: warp 0 reduces the warps' and posts
+  // it, with a copy of the candidate row (and of the diagonal row, if held here)
+  auto publish = [&](int jc, R best, int bidx) {
+    if (lane == jc) {
+      s_wv[warp] = best;
+      s_wi[warp] = bidx;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      R v = lane < NW ? s_wv[lane] : R(-1);
+      int i = lane < NW ? s_wi[lane] : -1;
+      warp_argmax<NW>(v, i);
+      i = __shfl_sync(0xffffffffu, i, 0);  // lanes >= NW reduced only among themselves
+      const int buf = jc & 1, j = c0 + jc;
+      if (lane == 0 && i >= 0) atomicMax(&scr.key[j], pivot_key((double)v, i - c0));
+      if (i >= 0 && lane < w) scr.row[((size_t)buf * G + blockIdx.x) * IB + lane] = sA[(i - lo) * SP + lane];
+      if (j >= lo && j < hi && lane < w) scr.top[buf * IB + lane] = sA[(j - lo) * SP + lane];
+    }
+  };
+  // candidate of column jc over its rows without an update (first column, or
+  // after a zero pivot)
+  auto scan = [&](int jc) {
+    R best = -1;
+    int bidx = -1;
+    for (int r = max(0, c0 + jc - lo) + warp; r < nr; r += NW) {
+      if (lane == jc) {
+        const T v = sA[r * SP + jc];
+        const R a = fabs(v.x) + fabs(v.y);
+        if (a > best) {
+          best = a;
+          bidx = lo + r;
+        }
+      }
+    }
+    publish(jc, best, bidx);
+  };
+  scan(0);
   for (int jj = 0; jj < w; jj++) {
     const int j = c0 + jj;
     const int buf = jj & 1;
-    double best = -1.0;
-    int bidx = -1;
-    for (int r = max(0, j - lo) + threadIdx.x; r < nr; r += blockDim.x) {
-      const T v = sA[r * SP + jj];
-      const double a = fabs((double)v.x) + fabs((double)v.y);
-      if (a > best) {
-        best = a;
-        bidx = lo + r;
-      }
-    }
-    s_val[threadIdx.x] = best;
-    s_idx[threadIdx.x] = bidx;
-    __syncthreads();
-    for (int sft = blockDim.x / 2; sft > 0; sft >>= 1) {
-      if (threadIdx.x < sft) {
-        const double o = s_val[threadIdx.x + sft];
-        const int oi = s_idx[threadIdx.x + sft];
-        const double mv = s_val[threadIdx.x];
-        const int mi = s_idx[threadIdx.x];
-        if (oi >= 0 && (mi < 0 || o > mv || (o == mv && oi < mi))) {
-          s_val[threadIdx.x] = o;
-          s_idx[threadIdx.x] = oi;
-        }
-      }
-      __syncthreads();
-    }
-    const int cand = s_idx[0];
-    if (threadIdx.x == 0) {
-      scr.val[buf * G + blockIdx.x] = s_val[0];
-      scr.idx[buf * G + blockIdx.x] = cand;
-    }
-    if (cand >= 0 && threadIdx.x < w) scr.row[((size_t)buf * G + blockIdx.x) * IB + threadIdx.x] = sA[(cand - lo) * SP + threadIdx.x];
-    if (j >= lo && j < hi && threadIdx.x < w) scr.top[buf * IB + threadIdx.x] = sA[(j - lo) * SP + threadIdx.x];
     grid.sync();
-    {
-      double v = -1.0;
-      int vi = -1, vg = -1;
-      for (int g = threadIdx.x; g < G; g += blockDim.x) {
-        const int ci = scr.idx[buf * G + g];
-        if (ci < 0) continue;
-        const double cv = scr.val[buf * G + g];
-        if (vi < 0 || cv > v || (cv == v && ci < vi)) {
-          v = cv;
-          vi = ci;
-          vg = g;
-        }
-      }
-      s_val[threadIdx.x] = v;
-      s_idx[threadIdx.x] = vi;
-      s_grp[threadIdx.x] = vg;
-      __syncthreads();
-      for (int sft = blockDim.x / 2; sft > 0; sft >>= 1) {
-        if (threadIdx.x < sft) {
-          const double o = s_val[threadIdx.x + sft];
-          const int oi = s_idx[threadIdx.x + sft];
-          const double mv = s_val[threadIdx.x];
-          const int mi = s_idx[threadIdx.x];
-          if (oi >= 0 && (mi < 0 || o > mv || (o == mv && oi < mi))) {
-            s_val[threadIdx.x] = o;
-            s_idx[threadIdx.x] = oi;
-            s_grp[threadIdx.x] = s_grp[threadIdx.x + sft];
-          }
-        }
-        __syncthreads();
-      }
-      if (threadIdx.x == 0) {
-        s_piv = s_idx[0];
-        s_zero = !(s_val[0] > 0.0);
+    // warp 0: the column's pivot, then the winner's row and the diagonal row
+    if (warp == 0) {
+      unsigned long long k = 0;
+      if (lane == 0) k = __ldcg(&scr.key[j]);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      const bool zero = (k >> 20) == 0;
+      const int piv = zero ? j : c0 + (0xFFFFF - (int)(k & 0xFFFFF));
+      if (lane == 0) {
+        s_zero = zero;
         if (blockIdx.x == 0) {
-          ipiv[j] = s_zero ? j : s_idx[0];
-          if (s_zero && *info == 0) *info = j + 1;
+          ipiv[j] = piv;
+          if (zero && *info == 0) *info = j + 1;
         }
-        s_win = s_grp[0];
       }
-      __syncthreads();
+      if (!zero && lane < w) {
+        const int owner = (piv - c0) / chunk;
+        const T pr = scr.row[((size_t)buf * G + owner) * IB + lane];
+        const T tp = scr.top[buf * IB + lane];
+        s_prow[lane] = pr;
+        if (piv != j && piv >= lo && piv < hi) sA[(piv - lo) * SP + lane] = tp;
+        if (j >= lo && j < hi) sA[(j - lo) * SP + lane] = pr;
+      }
     }
+    __syncthreads();
     if (s_zero) {
-      __syncthreads();
+      // singular column: nothing to eliminate; the next column's candidate
+      if (jj + 1 < w) scan(jj + 1);
       continue;
     }
-    const int piv = s_piv;
-    if (threadIdx.x < w) s_prow[threadIdx.x] = scr.row[((size_t)buf * G + s_win) * IB + threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x < w) {
-      if (piv != j && piv >= lo && piv < hi) sA[(piv - lo) * SP + threadIdx.x] = scr.top[buf * IB + threadIdx.x];
-      if (j >= lo && j < hi) sA[(j - lo) * SP + threadIdx.x] = s_prow[threadIdx.x];
-    }
-    __syncthreads();
-    // multipliers, then the rank-1 update of the remaining sub-panel columns
     const T d = s_prow[jj];
-    const int r0 = max(0, j + 1 - lo);
-    for (int r = r0 + threadIdx.x; r < nr; r += blockDim.x) sA[r * SP + jj] = cdiv_smith(sA[r * SP + jj], d);
-    __syncthreads();
-    const int ncol = w - jj - 1;
-    if (ncol > 0) {
-      for (int t = threadIdx.x; t < (nr - r0) * ncol; t += blockDim.x) {
-        const int r = r0 + t / ncol, c = jj + 1 + t % ncol;
-        const T l = sA[r * SP + jj];
-        const T u = s_prow[c];
-        T a = sA[r * SP + c];
-        a.x -= l.x * u.x - l.y * u.y;
-        a.y -= l.x * u.y + l.y * u.x;
-        sA[r * SP + c] = a;
+    T rd;
+    rd.x = 1;
+    rd.y = 0;
+    rd = cdiv_smith(rd, d);
+    const T u = lane < w ? s_prow[lane] : T{0, 0};
+    const int jn = jj + 1;
+    R best = -1;
+    int bidx = -1;
+    // four rows per warp per iteration, independent, for latency hiding
+    constexpr int RU = 4;
+    for (int rb = max(0, j + 1 - lo) + warp; rb < nr; rb += NW * RU) {
+      T a[RU];
+#pragma unroll
+      for (int k = 0; k < RU; k++) {
+        const int r = rb + k * NW;
+        a[k] = (r < nr && lane >= jj && lane < w) ? sA[r * SP + lane] : T{0, 0};  // columns < jj are final
+      }
+#pragma unroll
+      for (int k = 0; k < RU; k++) {
+        T p, l;
+        p.x = __shfl_sync(0xffffffffu, a[k].x, jj);
+        p.y = __shfl_sync(0xffffffffu, a[k].y, jj);
+        l.x = p.x * rd.x - p.y * rd.y;
+        l.y = p.x * rd.y + p.y * rd.x;
+        if (lane == jj) {
+          a[k] = l;
+        } else {
+          a[k].x -= l.x * u.x - l.y * u.y;
+          a[k].y -= l.x * u.y + l.y * u.x;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < RU; k++) {
+        const int r = rb + k * NW;
+        if (r < nr) {
+          if (lane >= jj && lane < w) sA[r * SP + lane] = a[k];
+          if (lane == jn) {
+            const R av = fabs(a[k].x) + fabs(a[k].y);
+            if (av > best) {
+              best = av;
+              bidx = lo + r;
+            }
+          }
+        }
       }
     }
-    __syncthreads();
+    if (jn < w) publish(jn, best, bidx);
   }
-  for (int t = threadIdx.x; t < nr * w; t += blockDim.x) {
-    const int r = t / w, c = t % w;
-    A[(size_t)(lo + r) * n + c0 + c] = sA[r * SP + c];
-  }
+  __syncthreads();
+  for (int r = warp; r < nr; r += NW)
+    if (lane < w) A[(size_t)(lo + r) * n + c0 + lane] = sA[r * SP + lane];
 }
 
 // Interchanges of pivots [p0, p1) applied to columns [a0, a1) and [b0, b1).
@@ -523,9 +569,12 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
   TT_TRY(sidx.alloc(2 * (size_t)G));
   TT_TRY(srow.alloc(2 * (size_t)G * IB));
   TT_TRY(stop.alloc(2 * (size_t)IB));
+  DevBuf<unsigned long long> skey;
+  TT_TRY(skey.alloc((size_t)n));
   TT_TRY(d_info.alloc(1));
   TT_CUDA_TRY(cudaMemsetAsync(d_info.ptr, 0, sizeof(int), st));
-  PivotScratch<T> scr{sval.ptr, sidx.ptr, srow.ptr, stop.ptr};
+  TT_CUDA_TRY(cudaMemsetAsync(skey.ptr, 0, sizeof(unsigned long long) * n, st));
+  PivotScratch<T> scr{sval.ptr, sidx.ptr, srow.ptr, stop.ptr, skey.ptr};
   static bool smem_attr = false;
   if (!smem_attr) {
     TT_CUDA_TRY(cudaFuncSetAttribute(k_subpanel_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubpanelSmem));
@@ -546,8 +595,8 @@ int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, in
         const size_t smem = chunk * SP * sizeof(T);
         const double mrows = n - j0;
         ProfScope prof(TT_PROF_SUBPANEL, st, 4.0 * mrows * w * w, 2.0 * mrows * w * sizeof(T));
-        if (smem <= kSubpanelSmem) {
-          TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel_smem<T>, dim3(G), dim3(256), args, smem, st));
+        if (smem <= kSubpanelSmem && n - j0 < 0xFFFFF) {
+          TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel_smem<T>, dim3(G), dim3(SP_THREADS), args, smem, st));
         } else {
           TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
         }
