@@ -185,6 +185,30 @@ int tt_solve_faddeev_adjoint(tt_complex* U, tt_complex* dU_dtheta, int n_theta, 
                              const tt_os_indexing* os, const tt_pw_states* pw, const tt_run_params* rp,
                              tt_solve_report* report);
 
+/* P123 files in the reference's HDF5 layout, written and read by this
+ * library without libhdf5 (file format subset: superblock version 0,
+ * version-1 object headers, symbol-table root group, contiguous datasets;
+ * the reader also takes chunked tables as H5TBmake_table writes them).
+ *
+ * Replaces store_sparse_permutation_matrix_for_3N_channel_h5
+ * (CPP/disk_io_routines.cpp:1078-1164): datasets "Nalpha", "Np_WP", "Nq_WP"
+ * (int32[1]), "P123_sparse_dim" (uint64[1]), tables "p boundaries" /
+ * "q boundaries" {int32 index, float64 mesh point} and "pw channels" (10 int32
+ * fields), "row indices" / "column indices" (int32[nnz]) and "values"
+ * (float64[nnz]).  val/row/col are the COO arrays of tt_fill_P123_arrays. */
+int tt_store_P123_h5(const char* filename, const double* val, const int* row, const int* col, size_t nnz,
+                     const tt_fwp_states* fwp, const tt_pw_states* pw);
+/* Replaces read_sparse_permutation_matrix_for_3N_channel_h5
+ * (CPP/disk_io_routines.cpp:1166-1284) with its checks: Nalpha, Np_WP, Nq_WP,
+ * the boundaries (bit-equal) and the pw table must match fwp/pw, else
+ * TT_ERR_BADARG with the reference's message.  Callee allocates *val, *row,
+ * *col (free with tt_free). */
+int tt_read_P123_h5(const char* filename, double** val, int** row, int** col, size_t* nnz,
+                    const tt_fwp_states* fwp, const tt_pw_states* pw);
+/* The reference's P123 file name for a channel, folder + "/P123_sparse_JP_<2J>_<P>_Np_<Np>_Nq_<Nq>_J2max_<j>.h5"
+ * (CPP/make_permutation_matrix.cpp:1320-1323), into buf[cap]. */
+int tt_P123_h5_filename(char* buf, size_t cap, const char* folder, const tt_pw_states* pw, int Np_WP, int Nq_WP);
+
 void tt_free(void* p);
 const char* tt_last_error_string(void);
 int tt_device_count(int* count);
@@ -274,6 +298,11 @@ int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const
  * in these contacts, so the central difference is exact up to rounding). */
 int tt_run_num_lecs(const tt_run* run, int* n_lecs, double* values);
 int tt_run_lec_derivative(const tt_run* run, int k, double* dV_WP_unco, double* dV_WP_coup);
+/* Writes channel chn's resident P123 (after tt_run_build_P123) with
+ * tt_store_P123_h5 to filename, or, if NULL, to the reference's file name in
+ * the run's P123_folder (what fill_P123_arrays stores when
+ * calculate_and_store_P123 is set, CPP/make_permutation_matrix.cpp:1364-1375). */
+int tt_run_store_P123_h5(const tt_run* run, int chn, const char* filename);
 int tt_run_release_channel(tt_run* run, int chn);
 int tt_run_release_A(tt_run* run, int chn);
 

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../cuda/tt_kernels.h"
+#include "../host/tt_h5.h"
 #include "../host/tt_host.h"
 #include "../host/tt_math.h"
 #include "../host/tt_p123.h"
@@ -732,6 +733,117 @@ int tt_run_write_U_table(const tt_run* run, int chn, const tt_complex* U, const 
   }
   f << "# ################################################################################################### \n";
   f << std::endl;
+  return TT_OK;
+}
+
+
+// ---- P123 files in the reference's HDF5 layout ----
+
+static int p123_file_header(const PWChannel& c, int Np_WP, const double* p_WP, int Nq_WP, const double* q_WP,
+                            P123H5& f) {
+  if (c.Nalpha <= 0 || Np_WP <= 0 || Nq_WP <= 0 || !p_WP || !q_WP) return fail(TT_ERR_BADARG, "empty state space");
+  f.Nalpha = c.Nalpha;
+  f.Np_WP = Np_WP;
+  f.Nq_WP = Nq_WP;
+  f.p_WP.assign(p_WP, p_WP + Np_WP + 1);
+  f.q_WP.assign(q_WP, q_WP + Nq_WP + 1);
+  // write_PW_statespace_to_h5 (CPP/disk_io_routines.cpp:1474-1545): the
+  // channel's J and parity in every record
+  f.pw.resize((size_t)c.Nalpha * kPwFields);
+  for (int a = 0; a < c.Nalpha; a++) {
+    const int32_t rec[kPwFields] = {a,           c.L_2N[a],     c.S_2N[a],        c.J_2N[a],        c.T_2N[a],
+                                    c.L_1N[a],   c.two_J_1N[a], c.two_T_3N[a],    c.two_J_3N[0],    c.P_3N[0]};
+    std::memcpy(&f.pw[(size_t)a * kPwFields], rec, sizeof rec);
+  }
+  return TT_OK;
+}
+
+int tt_store_P123_h5(const char* filename, const double* val, const int* row, const int* col, size_t nnz,
+                     const tt_fwp_states* fwp, const tt_pw_states* pw) {
+  if (!filename || !fwp || !pw || (nnz && (!val || !row || !col))) return fail(TT_ERR_BADARG, "null argument");
+  P123H5 f;
+  int s = p123_file_header(view_of(pw), fwp->Np_WP, fwp->p_WP_array, fwp->Nq_WP, fwp->q_WP_array, f);
+  if (s) return s;
+  f.nnz = nnz;
+  std::string err;
+  if (!h5_write_p123(filename, f, row, col, val, &err)) return fail(TT_ERR_IO, err);
+  return TT_OK;
+}
+
+int tt_read_P123_h5(const char* filename, double** val, int** row, int** col, size_t* nnz, const tt_fwp_states* fwp,
+                    const tt_pw_states* pw) {
+  if (!filename || !val || !row || !col || !nnz || !fwp || !pw) return fail(TT_ERR_BADARG, "null argument");
+  P123H5 want, got;
+  int s = p123_file_header(view_of(pw), fwp->Np_WP, fwp->p_WP_array, fwp->Nq_WP, fwp->q_WP_array, want);
+  if (s) return s;
+  std::string err;
+  if (!h5_read_p123(filename, got, &err)) return fail(TT_ERR_IO, err);
+  // the reference's integrity checks (CPP/disk_io_routines.cpp:1209-1270)
+  if (got.Nalpha != want.Nalpha || got.Np_WP != want.Np_WP || got.Nq_WP != want.Nq_WP)
+    return fail(TT_ERR_BADARG, "File-read P123 state-space dimensions (Nalpha, Nq_WP, Np_WP) mismatch.");
+  for (int i = 0; i <= want.Np_WP; i++)
+    if (got.p_WP[i] != want.p_WP[i]) return fail(TT_ERR_BADARG, "File-read P123 p-momentum boundaries mismatch.");
+  for (int i = 0; i <= want.Nq_WP; i++)
+    if (got.q_WP[i] != want.q_WP[i]) return fail(TT_ERR_BADARG, "File-read P123 q-momentum boundaries mismatch.");
+  for (int a = 0; a < want.Nalpha; a++)
+    for (int k = 1; k < kPwFields; k++)
+      if (got.pw[(size_t)a * kPwFields + k] != want.pw[(size_t)a * kPwFields + k])
+        return fail(TT_ERR_BADARG, "File-read P123 PW state-space mismatch.");
+  const size_t m = (size_t)got.nnz;
+  *val = (double*)std::malloc(sizeof(double) * std::max<size_t>(m, 1));
+  *row = (int*)std::malloc(sizeof(int) * std::max<size_t>(m, 1));
+  *col = (int*)std::malloc(sizeof(int) * std::max<size_t>(m, 1));
+  if (!*val || !*row || !*col) {
+    std::free(*val);
+    std::free(*row);
+    std::free(*col);
+    *val = nullptr;
+    *row = *col = nullptr;
+    return fail(TT_ERR_NOMEM, "host allocation for P123 failed");
+  }
+  if (m) {
+    std::memcpy(*val, got.val.data(), sizeof(double) * m);
+    std::memcpy(*row, got.row.data(), sizeof(int) * m);
+    std::memcpy(*col, got.col.data(), sizeof(int) * m);
+  }
+  *nnz = m;
+  return TT_OK;
+}
+
+int tt_P123_h5_filename(char* buf, size_t cap, const char* folder, const tt_pw_states* pw, int Np_WP, int Nq_WP) {
+  if (!buf || !folder || !pw || !pw->two_J_3N_array || !pw->P_3N_array) return fail(TT_ERR_BADARG, "null argument");
+  const std::string name =
+      p123_h5_filename(folder, pw->two_J_3N_array[0], pw->P_3N_array[0], Np_WP, Nq_WP, pw->J_2N_max);
+  if (name.size() + 1 > cap) return fail(TT_ERR_BADARG, "file name buffer too small");
+  std::memcpy(buf, name.c_str(), name.size() + 1);
+  return TT_OK;
+}
+
+int tt_run_store_P123_h5(const tt_run* run, int chn, const char* filename) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!run->chn[chn].have_P) return fail(TT_ERR_BADARG, "P123 not built");
+  const PWChannel c = channel_view(run->pw, chn);
+  P123H5 f;
+  s = p123_file_header(c, run->fwp.Np_WP, run->fwp.p_WP.data(), run->fwp.Nq_WP, run->fwp.q_WP.data(), f);
+  if (s) return s;
+  const DeviceCSR& P = run->chn[chn].solver->P();
+  std::vector<int64_t> rowptr(P.n + 1);
+  f.nnz = (uint64_t)P.nnz;
+  f.row.resize(f.nnz);
+  f.col.resize(f.nnz);
+  f.val.resize(f.nnz);
+  if (cudaMemcpy(rowptr.data(), P.rowptr.ptr, sizeof(int64_t) * (P.n + 1), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      (f.nnz && (cudaMemcpy(f.col.data(), P.col.ptr, sizeof(int32_t) * f.nnz, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                 cudaMemcpy(f.val.data(), P.val.ptr, sizeof(double) * f.nnz, cudaMemcpyDeviceToHost) != cudaSuccess)))
+    return fail(TT_ERR_CUDA, "copy of P123 failed");
+  for (int r = 0; r < P.n; r++)
+    for (int64_t e = rowptr[r]; e < rowptr[r + 1]; e++) f.row[e] = r;
+  const std::string path = filename ? std::string(filename)
+                                    : p123_h5_filename(run->rp.P123_folder, c.two_J_3N[0], c.P_3N[0], run->fwp.Np_WP,
+                                                       run->fwp.Nq_WP, c.J_2N_max);
+  std::string err;
+  if (!h5_write_p123(path, f, nullptr, nullptr, nullptr, &err)) return fail(TT_ERR_IO, err);
   return TT_OK;
 }
 

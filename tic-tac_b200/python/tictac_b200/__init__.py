@@ -39,6 +39,7 @@ EXPORTED_SYMBOLS = (
     "tt_wigner_3j", "tt_wigner_6j", "tt_wigner_9j", "tt_clebsch_gordan", "tt_legendre_spharm_array",
     "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc", "tt_profile_begin", "tt_profile_end",
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
+    "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build")
@@ -205,6 +206,53 @@ def fill_P123_arrays(pw: PW, p_WP, q_WP, production_run=True, **rp_kw):
         lib.tt_free(ctypes.cast(row, c_void_p))
         lib.tt_free(ctypes.cast(col, c_void_p))
     return r, c, v
+
+
+def store_P123_h5(path, row, col, val, pw: PW, p_WP, q_WP) -> None:
+    """tt_store_P123_h5: one channel's COO P123 in the reference's HDF5 layout."""
+    lib = load()
+    p = np.ascontiguousarray(p_WP, dtype=np.float64)
+    q = np.ascontiguousarray(q_WP, dtype=np.float64)
+    fwp = tt_fwp_states(len(p) - 1, len(q) - 1, _dptr(p), _dptr(q))
+    r = np.ascontiguousarray(row, dtype=np.int32)
+    c = np.ascontiguousarray(col, dtype=np.int32)
+    v = np.ascontiguousarray(val, dtype=np.float64)
+    if not (len(r) == len(c) == len(v)):
+        raise ValueError("row, col and val must have the same length")
+    _check(lib.tt_store_P123_h5(os.fsencode(path), _dptr(v), _iptr(r), _iptr(c), c_size_t(len(v)), byref(fwp),
+                                byref(pw.s)))
+
+
+def read_P123_h5(path, pw: PW, p_WP, q_WP):
+    """tt_read_P123_h5: (row, col, val) of a P123 file after the reference's
+    state-space checks against pw and the boundaries."""
+    lib = load()
+    p = np.ascontiguousarray(p_WP, dtype=np.float64)
+    q = np.ascontiguousarray(q_WP, dtype=np.float64)
+    fwp = tt_fwp_states(len(p) - 1, len(q) - 1, _dptr(p), _dptr(q))
+    val = POINTER(c_double)()
+    row = POINTER(c_int)()
+    col = POINTER(c_int)()
+    nnz = c_size_t(0)
+    _check(lib.tt_read_P123_h5(os.fsencode(path), byref(val), byref(row), byref(col), byref(nnz), byref(fwp),
+                               byref(pw.s)))
+    m = nnz.value
+    try:
+        v = np.ctypeslib.as_array(val, shape=(max(m, 1),))[:m].copy()
+        r = np.ctypeslib.as_array(row, shape=(max(m, 1),))[:m].copy()
+        c = np.ctypeslib.as_array(col, shape=(max(m, 1),))[:m].copy()
+    finally:
+        lib.tt_free(ctypes.cast(val, c_void_p))
+        lib.tt_free(ctypes.cast(row, c_void_p))
+        lib.tt_free(ctypes.cast(col, c_void_p))
+    return r, c, v
+
+
+def P123_h5_filename(folder, pw: PW, Np_WP, Nq_WP) -> str:
+    lib = load()
+    buf = ctypes.create_string_buffer(4096)
+    _check(lib.tt_P123_h5_filename(buf, c_size_t(len(buf)), os.fsencode(folder), byref(pw.s), Np_WP, Nq_WP))
+    return buf.value.decode()
 
 
 class SWP:
@@ -457,6 +505,11 @@ class Run:
         ms = c_double()
         _check(self.lib.tt_run_timer_stop(self._h, byref(ms)))
         return ms.value
+
+    def store_P123_h5(self, chn, path=None):
+        """Writes the channel's resident P123 (after build_P123) in the reference's
+        HDF5 layout; path None = the reference's name in the run's P123_folder."""
+        _check(self.lib.tt_run_store_P123_h5(self._h, chn, None if path is None else os.fsencode(path)))
 
     def write_U_table(self, chn, U, path):
         U = np.ascontiguousarray(U, dtype=np.complex128)
