@@ -303,6 +303,12 @@ int tt_run_lec_derivative(const tt_run* run, int k, double* dV_WP_unco, double* 
  * the run's P123_folder (what fill_P123_arrays stores when
  * calculate_and_store_P123 is set, CPP/make_permutation_matrix.cpp:1364-1375). */
 int tt_run_store_P123_h5(const tt_run* run, int chn, const char* filename);
+/* Makes a P123 file the channel's resident P123 instead of building it, as
+ * the reference reads its file when calculate_and_store_P123 is false
+ * (CPP/make_permutation_matrix.cpp:1387-1403), with tt_read_P123_h5's checks
+ * against the run's state space; filename NULL = the reference's name in the
+ * run's P123_folder. */
+int tt_run_load_P123_h5(tt_run* run, int chn, const char* filename, int64_t* nnz);
 int tt_run_release_channel(tt_run* run, int chn);
 int tt_run_release_A(tt_run* run, int chn);
 

@@ -171,11 +171,14 @@ def test_file_name_is_the_references():
 
 
 @pytest.mark.gpu
-def test_run_handle_stores_resident_P123(tmp_path):
-    run = tt.Run(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=8, Nq_WP=8, Nphi=20, Nx=20,
-                 lab_energies="12", P123_folder=str(tmp_path))
+def test_run_handle_stores_and_loads_P123(tmp_path):
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=8, Nq_WP=8, Nphi=20, Nx=20,
+                lab_energies="12", P123_folder=str(tmp_path))
+    run = tt.Run(**opts)
+    nnzs = []
     for c in range(run.num_channels):
         nnz = run.build_P123(c)
+        nnzs.append(nnz)
         rowptr, col, val = run.P123_csr(c, nnz)
         run.store_P123_h5(c)
         pwt = run.host_array(0, c).reshape(-1, 9)
@@ -187,4 +190,18 @@ def test_run_handle_stores_resident_P123(tmp_path):
         assert np.array_equal(r, rows) and np.array_equal(cc, col) and np.array_equal(v, val)
         f = h5_spec.File(path)
         assert int(f.datasets["P123_sparse_dim"]["data"][0]) == nnz
+    # a second run reads the files instead of building P123 (calculate_and_store_P123 = false)
+    # and solves to the same U
+    run2 = tt.Run(**opts)
+    for c in range(run.num_channels):
+        assert run2.load_P123_h5(c) == nnzs[c]
+        rp2, col2, val2 = run2.P123_csr(c, nnzs[c])
+        rp1, col1, val1 = run.P123_csr(c, nnzs[c])
+        assert np.array_equal(rp1, rp2) and np.array_equal(col1, col2) and np.array_equal(val1, val2)
+        U1, _ = run.solve(c, tt.PRECISION_FP64)
+        U2, _ = run2.solve(c, tt.PRECISION_FP64)
+        assert np.array_equal(U1, U2)
+    with pytest.raises(tt.TicTacError):
+        run2.load_P123_h5(0, str(tmp_path / "missing.h5"))
+    run2.close()
     run.close()

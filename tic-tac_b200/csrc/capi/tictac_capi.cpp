@@ -847,4 +847,45 @@ int tt_run_store_P123_h5(const tt_run* run, int chn, const char* filename) {
   return TT_OK;
 }
 
+int tt_run_load_P123_h5(tt_run* run, int chn, const char* filename, int64_t* nnz) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  const PWChannel c = channel_view(run->pw, chn);
+  P123H5 want, got;
+  s = p123_file_header(c, run->fwp.Np_WP, run->fwp.p_WP.data(), run->fwp.Nq_WP, run->fwp.q_WP.data(), want);
+  if (s) return s;
+  const std::string path = filename ? std::string(filename)
+                                    : p123_h5_filename(run->rp.P123_folder, c.two_J_3N[0], c.P_3N[0], run->fwp.Np_WP,
+                                                       run->fwp.Nq_WP, c.J_2N_max);
+  std::string err;
+  if (!h5_read_p123(path, got, &err)) return fail(TT_ERR_IO, err);
+  if (got.Nalpha != want.Nalpha || got.Np_WP != want.Np_WP || got.Nq_WP != want.Nq_WP)
+    return fail(TT_ERR_BADARG, "File-read P123 state-space dimensions (Nalpha, Nq_WP, Np_WP) mismatch.");
+  if (got.p_WP != want.p_WP) return fail(TT_ERR_BADARG, "File-read P123 p-momentum boundaries mismatch.");
+  if (got.q_WP != want.q_WP) return fail(TT_ERR_BADARG, "File-read P123 q-momentum boundaries mismatch.");
+  for (size_t e = 0; e < want.pw.size(); e++)
+    if (e % kPwFields != 0 && got.pw[e] != want.pw[e])
+      return fail(TT_ERR_BADARG, "File-read P123 PW state-space mismatch.");
+  // the file holds the reference's row-major sorted COO; rebuild the row pointers
+  const int64_t n = (int64_t)want.Nalpha * want.Np_WP * want.Nq_WP;
+  const int64_t m = (int64_t)got.nnz;
+  std::vector<int64_t> rowptr(n + 1, 0);
+  for (int64_t e = 0; e < m; e++) {
+    const int32_t r = got.row[e], cc = got.col[e];
+    if (r < 0 || r >= n || cc < 0 || cc >= n) return fail(TT_ERR_BADARG, path + ": P123 index out of range");
+    if (e > 0 && (r < got.row[e - 1] || (r == got.row[e - 1] && cc <= got.col[e - 1])))
+      return fail(TT_ERR_BADARG, path + ": P123 entries are not in row-major order");
+    rowptr[r + 1]++;
+  }
+  for (int64_t r = 0; r < n; r++) rowptr[r + 1] += rowptr[r];
+  TT_TRY(ensure_solver(run, chn));
+  cudaStream_t st = run_stream(run);
+  TT_TRY(run->chn[chn].solver->set_P_host_csr(rowptr.data(), got.col.data(), got.val.data(), m, st));
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail(TT_ERR_CUDA, "upload of P123 failed");
+  run->chn[chn].have_P = true;
+  run->chn[chn].have_A = false;
+  if (nnz) *nnz = m;
+  return TT_OK;
+}
+
 }  // extern "C"

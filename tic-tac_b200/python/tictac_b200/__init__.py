@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = (
     "tt_wigner_3j", "tt_wigner_6j", "tt_wigner_9j", "tt_clebsch_gordan", "tt_legendre_spharm_array",
     "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc", "tt_profile_begin", "tt_profile_end",
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
-    "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5",
+    "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build")
@@ -510,6 +510,13 @@ class Run:
         """Writes the channel's resident P123 (after build_P123) in the reference's
         HDF5 layout; path None = the reference's name in the run's P123_folder."""
         _check(self.lib.tt_run_store_P123_h5(self._h, chn, None if path is None else os.fsencode(path)))
+
+    def load_P123_h5(self, chn, path=None):
+        """Makes a P123 file the channel's resident P123 (the reference's
+        calculate_and_store_P123 = false path); returns nnz."""
+        nnz = c_int64()
+        _check(self.lib.tt_run_load_P123_h5(self._h, chn, None if path is None else os.fsencode(path), byref(nnz)))
+        return nnz.value
 
     def write_U_table(self, chn, U, path):
         U = np.ascontiguousarray(U, dtype=np.complex128)
