@@ -278,7 +278,11 @@ int tt_run_num_energies(const tt_run* run, int* nE);
 int tt_run_energies(const tt_run* run, double* T_lab, double* E_com, int* q_com_idx);
 int tt_run_E_bound(const tt_run* run, double* E_bound);
 
-/* Device stages for one channel: P123 in HBM, A in HBM, resolvents. */
+/* Device stages for one channel: P123 in HBM, A in HBM, resolvents.
+ * tt_run_build_P123 builds P123 on the device, or, when the run has
+ * calculate_and_store_P123=false, reads the channel's P123 file from
+ * P123_folder (tt_run_load_P123_h5) as the reference does.  Storing is
+ * explicit (tt_run_store_P123_h5): the files reach GBs at Np = Nq = 30. */
 int tt_run_build_P123(tt_run* run, int chn, int64_t* nnz);
 int tt_run_build_A(tt_run* run, int chn, double* ms);
 int tt_run_build_resolvent(tt_run* run, int chn);

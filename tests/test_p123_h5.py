@@ -204,4 +204,14 @@ def test_run_handle_stores_and_loads_P123(tmp_path):
     with pytest.raises(tt.TicTacError):
         run2.load_P123_h5(0, str(tmp_path / "missing.h5"))
     run2.close()
+    # calculate_and_store_P123 = false: build_P123 reads the files, as the reference does
+    run3 = tt.Run(calculate_and_store_P123="false", **opts)
+    for c in range(run.num_channels):
+        assert run3.build_P123(c) == nnzs[c]
+        assert np.array_equal(run3.solve(c, tt.PRECISION_FP64)[0], run.solve(c, tt.PRECISION_FP64)[0])
+    run3.close()
+    run4 = tt.Run(calculate_and_store_P123="false", **dict(opts, P123_folder=str(tmp_path / "none")))
+    with pytest.raises(tt.TicTacError):
+        run4.build_P123(0)
+    run4.close()
     run.close()

@@ -464,6 +464,9 @@ static int ensure_solver(tt_run* run, int chn) {
 int tt_run_build_P123(tt_run* run, int chn, int64_t* nnz) {
   int s = check_chn(run, chn);
   if (s) return s;
+  // calculate_and_store_P123 = false: the reference reads the channel's file
+  // instead of computing P123 (CPP/make_permutation_matrix.cpp:1387-1403)
+  if (!run->rp.calculate_and_store_P123) return tt_run_load_P123_h5(run, chn, nullptr, nnz);
   TT_TRY(ensure_solver(run, chn));
   P123Tables t;
   std::string err;
