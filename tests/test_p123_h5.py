@@ -102,6 +102,29 @@ def test_round_trip_and_reference_checks(tmp_path):
         tt.read_P123_h5(tmp_path / "missing.h5", ch["pw"], ch["p"], ch["q"])
 
 
+def test_corrupt_files_are_errors(tmp_path):
+    ch = channel("lo_j1_J3_n8", 0)
+    good = tmp_path / "good.h5"
+    tt.store_P123_h5(good, ch["row"], ch["col"], ch["val"], ch["pw"], ch["p"], ch["q"])
+    raw = good.read_bytes()
+    rng = np.random.default_rng(5)
+    cases = {"truncated": raw[:len(raw) // 2], "header only": raw[:96], "not hdf5": b"x" * 200}
+    for i in range(8):  # random byte damage in the metadata (the first 2 KiB)
+        b = bytearray(raw)
+        for pos in rng.integers(8, 2048, size=4):
+            b[pos] ^= 0xFF
+        cases[f"damaged {i}"] = bytes(b)
+    for name, data in cases.items():
+        path = tmp_path / f"{name}.h5"
+        path.write_bytes(data)
+        try:
+            r, c, v = tt.read_P123_h5(path, ch["pw"], ch["p"], ch["q"])
+        except tt.TicTacError:
+            continue  # a clean error
+        # damage that misses every checked structure must still give the stored matrix
+        assert len(r) == len(c) == len(v)
+
+
 def test_empty_matrix(tmp_path):
     ch = channel("mt_swave_n16", 0)
     path = tmp_path / "empty.h5"

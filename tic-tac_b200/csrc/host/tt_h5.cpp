@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <stdexcept>
 
 namespace tt {
 
@@ -291,8 +292,8 @@ std::vector<DatasetSpec> p123_datasets(const P123H5& f, const int32_t* row, cons
 
 }  // namespace
 
-bool h5_write_p123(const std::string& path, const P123H5& f, const int32_t* row, const int32_t* col,
-                   const double* val, std::string* err) {
+static bool write_p123(const std::string& path, const P123H5& f, const int32_t* row, const int32_t* col,
+                       const double* val, std::string* err) {
   auto fail = [&](const std::string& m) {
     if (err) *err = m;
     return false;
@@ -622,8 +623,13 @@ class Reader {
   }
   // the dataset's raw elements (row-major), type size bytes each
   bool data(const Dataset& d, std::vector<uint8_t>& out) {
+    // unfiltered data never exceeds the file: bound the extent before allocating
     uint64_t n = 1;
-    for (uint64_t x : d.dims) n *= x;
+    for (uint64_t x : d.dims) {
+      if (x != 0 && n > fsize_ / x) return fail("dataset extent larger than the file");
+      n *= x;
+    }
+    if (d.type.size == 0 || (n != 0 && d.type.size > fsize_ / n)) return fail("dataset larger than the file");
     const uint64_t bytes = n * d.type.size;
     out.assign(bytes, 0);
     if (d.layout.cls == 0) {
@@ -668,6 +674,7 @@ class Reader {
     std::vector<std::pair<uint64_t, uint64_t>> chunks{{addr + 16, size}};
     unsigned seen = 0;
     for (size_t k = 0; k < chunks.size() && k < 64; k++) {
+      if (chunks[k].second > fsize_) return fail("object header block larger than the file");
       std::vector<uint8_t> b(chunks[k].second);
       if (!rd(chunks[k].first, b.data(), b.size())) return false;
       Cur m(b.data(), b.size());
@@ -697,6 +704,7 @@ class Reader {
     const uint64_t size = c.u64();
     c.u64();
     const uint64_t a = c.u64();
+    if (size > fsize_) return fail("local heap larger than the file");
     data.resize(size);
     return rd(a, data.data(), size);
   }
@@ -786,7 +794,7 @@ bool to_i64(const DType& t, const uint8_t* p, int64_t& v) {
 
 }  // namespace
 
-bool h5_read_p123(const std::string& path, P123H5& f, std::string* err) {
+static bool read_p123(const std::string& path, P123H5& f, std::string* err) {
   Reader r;
   auto fail = [&](const std::string& m) {
     if (err) *err = m;
@@ -875,6 +883,26 @@ bool h5_read_p123(const std::string& path, P123H5& f, std::string* err) {
       !sparse("values", 1, f.val.data()))
     return false;
   return true;
+}
+
+// host allocation failures become errors, never exceptions through the C ABI
+bool h5_write_p123(const std::string& path, const P123H5& f, const int32_t* row, const int32_t* col,
+                   const double* val, std::string* err) {
+  try {
+    return write_p123(path, f, row, col, val, err);
+  } catch (const std::exception& e) {
+    if (err) *err = std::string("P123 file: ") + e.what();
+    return false;
+  }
+}
+
+bool h5_read_p123(const std::string& path, P123H5& f, std::string* err) {
+  try {
+    return read_p123(path, f, err);
+  } catch (const std::exception& e) {
+    if (err) *err = path + ": " + e.what();
+    return false;
+  }
 }
 
 std::string p123_h5_filename(const std::string& folder, int two_J_3N, int P_3N, int Np_WP, int Nq_WP, int J_2N_max) {
