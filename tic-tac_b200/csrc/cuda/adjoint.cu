@@ -15,18 +15,27 @@
 namespace tt {
 namespace {
 
+// In-place transpose of a row-major n x n matrix: block (bx, by) with
+// bx >= by swaps tiles (by, bx) and (bx, by) through shared memory (a diagonal
+// tile is transposed onto itself); blocks below the diagonal exit at once.
 template <typename T>
-__global__ void k_transpose(const T* __restrict__ in, int n, T* __restrict__ out) {
-  __shared__ T tile[32][33];
+__global__ void k_transpose_inplace(T* __restrict__ a, int n) {
+  if (blockIdx.x < blockIdx.y) return;
+  __shared__ T t0[32][33], t1[32][33];
   const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  const bool diag = blockIdx.x == blockIdx.y;
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
-    const int r = by + i, c = bx + threadIdx.x;
-    if (r < n && c < n) tile[i][threadIdx.x] = in[(size_t)r * n + c];
+    const int c = threadIdx.x;
+    if (by + i < n && bx + c < n) t0[i][c] = a[(size_t)(by + i) * n + bx + c];  // tile (by, bx)
+    if (!diag && bx + i < n && by + c < n) t1[i][c] = a[(size_t)(bx + i) * n + by + c];  // tile (bx, by)
   }
   __syncthreads();
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
-    const int r = bx + i, c = by + threadIdx.x;
-    if (r < n && c < n) out[(size_t)r * n + c] = tile[threadIdx.x][i];
+    const int c = threadIdx.x;
+    // (bx + i, by + c) <- old (by + c, bx + i)
+    if (bx + i < n && by + c < n) a[(size_t)(bx + i) * n + by + c] = t0[c][i];
+    // (by + i, bx + c) <- old (bx + c, by + i)
+    if (!diag && by + i < n && bx + c < n) a[(size_t)(by + i) * n + bx + c] = t1[c][i];
   }
 }
 
@@ -244,15 +253,15 @@ int pick_device(const double* d_R, int n, const int32_t* d_row, const int32_t* d
 }
 
 template <typename T>
-int transpose_device(const T* in, int n, T* out, cudaStream_t st) {
+int transpose_inplace_device(T* a, int n, cudaStream_t st) {
   dim3 grid(ceil_div(n, 32), ceil_div(n, 32)), block(32, 8);
-  k_transpose<T><<<grid, block, 0, st>>>(in, n, out);
+  k_transpose_inplace<T><<<grid, block, 0, st>>>(a, n);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
 }
-template int transpose_device<float2>(const float2*, int, float2*, cudaStream_t);
-template int transpose_device<double2>(const double2*, int, double2*, cudaStream_t);
+template int transpose_inplace_device<float2>(float2*, int, cudaStream_t);
+template int transpose_inplace_device<double2>(double2*, int, cudaStream_t);
 
 int gemv_t_device(const double* d_A, int n, const double* d_v, int nrhs, double* d_y, cudaStream_t st) {
   if (nrhs > GT_MAXV) {

@@ -97,7 +97,7 @@ int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_
 
 // Solve (P^T L U)^T x = b, i.e. transposed systems of the same factor, for
 // nrhs complex128 columns [k][n] in place: d_LUt is the transpose of the
-// factor (transpose_device) with blkT from lu_trsv_prepare(..., true).
+// factor (transpose_inplace_device) with blkT from lu_trsv_prepare(..., true).
 template <typename T>
 int lu_solve_transposed_device(const T* d_LUt, int n, const TrsvBlocks<T>& blkT, const int32_t* d_perm, double* d_x,
                                double* d_tmp, int nrhs, cudaStream_t st);
@@ -108,8 +108,9 @@ int csc_to_csr_device(const double* h_val, const int32_t* h_row, const uint64_t*
                       DeviceCSR& out, cudaStream_t st);
 
 // Adjoint pieces (adjoint.cu); vectors are complex128 [k][n].
+// the factor transposed in place (it is not needed in row form afterwards)
 template <typename T>
-int transpose_device(const T* in, int n, T* out, cudaStream_t st);
+int transpose_inplace_device(T* a, int n, cudaStream_t st);
 // y_k = A^T v_k, k < nrhs <= 8
 int gemv_t_device(const double* d_A, int n, const double* d_v, int nrhs, double* d_y, cudaStream_t st);
 // Pade path (adjoint.cu): R[k] = A[rows[k], :] as complex; V[k] = R[k] o G[e[k]];

@@ -348,23 +348,25 @@ int ChannelSolver::solve_pade(const std::vector<int>& q_idx, const std::vector<i
 }
 
 int ChannelSolver::adjoint_energy(int j, int nE, int nd, const double* Gj, const int32_t* d_rows, const int32_t* d_perm,
-                                  double* tmp, const double* x, const SolveOptions& opt, const void* F, void* Ft,
+                                  double* tmp, const double* x, const SolveOptions& opt, void* F,
                                   TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT,
                                   double* rT, double* u, double* g, double* w, double* h, double* dots,
                                   const AdjointRequest& adj, SolveReport& r, cudaStream_t st) {
   auto t0 = std::chrono::steady_clock::now();
-  // lambda_d' = (1 - A G)^{-T} e_d' with the transposed factor
+  // lambda_d' = (1 - A G)^{-T} e_d' with the factor transposed in place: the
+  // forward solve and its refinement are done, and the next energy forms a new
+  // L, so the adjoint needs no second n x n buffer
   auto solve_t = [&](double* v) -> int {
     if (opt.mixed)
-      return lu_solve_transposed_device<float2>(static_cast<const float2*>(Ft), n, tbT32, d_perm, v, tmp, nd, st);
-    return lu_solve_transposed_device<double2>(static_cast<const double2*>(Ft), n, tbT64, d_perm, v, tmp, nd, st);
+      return lu_solve_transposed_device<float2>(static_cast<const float2*>(F), n, tbT32, d_perm, v, tmp, nd, st);
+    return lu_solve_transposed_device<double2>(static_cast<const double2*>(F), n, tbT64, d_perm, v, tmp, nd, st);
   };
   if (opt.mixed) {
-    TT_TRY(transpose_device<float2>(static_cast<const float2*>(F), n, static_cast<float2*>(Ft), st));
-    TT_TRY(lu_trsv_prepare<float2>(static_cast<const float2*>(Ft), n, tbT32, st, true));
+    TT_TRY(transpose_inplace_device<float2>(static_cast<float2*>(F), n, st));
+    TT_TRY(lu_trsv_prepare<float2>(static_cast<const float2*>(F), n, tbT32, st, true));
   } else {
-    TT_TRY(transpose_device<double2>(static_cast<const double2*>(F), n, static_cast<double2*>(Ft), st));
-    TT_TRY(lu_trsv_prepare<double2>(static_cast<const double2*>(Ft), n, tbT64, st, true));
+    TT_TRY(transpose_inplace_device<double2>(static_cast<double2*>(F), n, st));
+    TT_TRY(lu_trsv_prepare<double2>(static_cast<const double2*>(F), n, tbT64, st, true));
   }
   TT_TRY(unit_rhs_device(d_rows, n, nd, lam, st));
   TT_TRY(solve_t(lam));
@@ -461,13 +463,9 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
   DevBuf<float2> L32;
   TrsvBlocks<double2> tb64, tbT64;
   TrsvBlocks<float2> tb32, tbT32;
-  // adjoint: transposed factor and the vectors of lambda, its refinement and the products
-  DevBuf<double2> Ft64;
-  DevBuf<float2> Ft32;
+  // adjoint: the vectors of lambda, its refinement and the products
   DevBuf<double> lam, yT, rT, u, g, w, h, dots;
   if (adj && adj->n_theta > 0) {
-    if (opt.mixed) TT_TRY(Ft32.alloc((size_t)n * n));
-    else TT_TRY(Ft64.alloc((size_t)n * n));
     for (DevBuf<double>* b : {&lam, &yT, &rT, &u, &g, &w, &h}) TT_TRY(b->alloc((size_t)2 * n * nd));
     TT_TRY(dots.alloc((size_t)2 * nd * nd));
   }
@@ -551,8 +549,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       }
     }
     if (adj && adj->n_theta > 0) TT_TRY(adjoint_energy(j, nE, nd, Gj, cols.ptr, perm_d.ptr, tmp.ptr, x.ptr, opt,
-                                                      opt.mixed ? (const void*)L32.ptr : (const void*)L64.ptr,
-                                                      opt.mixed ? (void*)Ft32.ptr : (void*)Ft64.ptr, tbT32, tbT64,
+                                                      opt.mixed ? (void*)L32.ptr : (void*)L64.ptr, tbT32, tbT64,
                                                       lam.ptr, yT.ptr, rT.ptr, u.ptr, g.ptr, w.ptr, h.ptr, dots.ptr,
                                                       *adj, r, st));
     // on-shell read-out, solve_faddeev.cpp:407-431

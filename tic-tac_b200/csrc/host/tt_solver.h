@@ -85,7 +85,7 @@ class ChannelSolver {
   int solve_pade(const std::vector<int>& q_idx, const std::vector<int>& deut, std::vector<double>& U,
                  SolveReport& r, cudaStream_t st);
   int adjoint_energy(int j, int nE, int nd, const double* Gj, const int32_t* d_rows, const int32_t* d_perm,
-                     double* tmp, const double* x, const SolveOptions& opt, const void* F, void* Ft,
+                     double* tmp, const double* x, const SolveOptions& opt, void* F,
                      TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT, double* rT,
                      double* u, double* g, double* w, double* h, double* dots, const AdjointRequest& adj,
                      SolveReport& r, cudaStream_t st);
