@@ -761,6 +761,18 @@ static int p123_file_header(const PWChannel& c, int Np_WP, const double* p_WP, i
   return TT_OK;
 }
 
+// the reference's integrity checks on a read file (CPP/disk_io_routines.cpp:1209-1270)
+static int p123_file_matches(const P123H5& want, const P123H5& got) {
+  if (got.Nalpha != want.Nalpha || got.Np_WP != want.Np_WP || got.Nq_WP != want.Nq_WP)
+    return fail(TT_ERR_BADARG, "File-read P123 state-space dimensions (Nalpha, Nq_WP, Np_WP) mismatch.");
+  if (got.p_WP != want.p_WP) return fail(TT_ERR_BADARG, "File-read P123 p-momentum boundaries mismatch.");
+  if (got.q_WP != want.q_WP) return fail(TT_ERR_BADARG, "File-read P123 q-momentum boundaries mismatch.");
+  for (size_t e = 0; e < want.pw.size(); e++)  // every field but the record index
+    if (e % kPwFields != 0 && got.pw[e] != want.pw[e])
+      return fail(TT_ERR_BADARG, "File-read P123 PW state-space mismatch.");
+  return TT_OK;
+}
+
 int tt_store_P123_h5(const char* filename, const double* val, const int* row, const int* col, size_t nnz,
                      const tt_fwp_states* fwp, const tt_pw_states* pw) {
   if (!filename || !fwp || !pw || (nnz && (!val || !row || !col))) return fail(TT_ERR_BADARG, "null argument");
@@ -781,17 +793,8 @@ int tt_read_P123_h5(const char* filename, double** val, int** row, int** col, si
   if (s) return s;
   std::string err;
   if (!h5_read_p123(filename, got, &err)) return fail(TT_ERR_IO, err);
-  // the reference's integrity checks (CPP/disk_io_routines.cpp:1209-1270)
-  if (got.Nalpha != want.Nalpha || got.Np_WP != want.Np_WP || got.Nq_WP != want.Nq_WP)
-    return fail(TT_ERR_BADARG, "File-read P123 state-space dimensions (Nalpha, Nq_WP, Np_WP) mismatch.");
-  for (int i = 0; i <= want.Np_WP; i++)
-    if (got.p_WP[i] != want.p_WP[i]) return fail(TT_ERR_BADARG, "File-read P123 p-momentum boundaries mismatch.");
-  for (int i = 0; i <= want.Nq_WP; i++)
-    if (got.q_WP[i] != want.q_WP[i]) return fail(TT_ERR_BADARG, "File-read P123 q-momentum boundaries mismatch.");
-  for (int a = 0; a < want.Nalpha; a++)
-    for (int k = 1; k < kPwFields; k++)
-      if (got.pw[(size_t)a * kPwFields + k] != want.pw[(size_t)a * kPwFields + k])
-        return fail(TT_ERR_BADARG, "File-read P123 PW state-space mismatch.");
+  s = p123_file_matches(want, got);
+  if (s) return s;
   const size_t m = (size_t)got.nnz;
   *val = (double*)std::malloc(sizeof(double) * std::max<size_t>(m, 1));
   *row = (int*)std::malloc(sizeof(int) * std::max<size_t>(m, 1));
@@ -862,13 +865,8 @@ int tt_run_load_P123_h5(tt_run* run, int chn, const char* filename, int64_t* nnz
                                                        run->fwp.Nq_WP, c.J_2N_max);
   std::string err;
   if (!h5_read_p123(path, got, &err)) return fail(TT_ERR_IO, err);
-  if (got.Nalpha != want.Nalpha || got.Np_WP != want.Np_WP || got.Nq_WP != want.Nq_WP)
-    return fail(TT_ERR_BADARG, "File-read P123 state-space dimensions (Nalpha, Nq_WP, Np_WP) mismatch.");
-  if (got.p_WP != want.p_WP) return fail(TT_ERR_BADARG, "File-read P123 p-momentum boundaries mismatch.");
-  if (got.q_WP != want.q_WP) return fail(TT_ERR_BADARG, "File-read P123 q-momentum boundaries mismatch.");
-  for (size_t e = 0; e < want.pw.size(); e++)
-    if (e % kPwFields != 0 && got.pw[e] != want.pw[e])
-      return fail(TT_ERR_BADARG, "File-read P123 PW state-space mismatch.");
+  s = p123_file_matches(want, got);
+  if (s) return s;
   // the file holds the reference's row-major sorted COO; rebuild the row pointers
   const int64_t n = (int64_t)want.Nalpha * want.Np_WP * want.Nq_WP;
   const int64_t m = (int64_t)got.nnz;
