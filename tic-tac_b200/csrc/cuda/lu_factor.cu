@@ -71,6 +71,29 @@ struct PivotScratch {
   unsigned long long* key;  // [n], zero before the factorization: column j's packed pivot
 };
 
+// Matrices of equal n factored together: the sub-panel grid is split into B
+// equal groups of blocks, group b working on matrix b, all sharing each grid
+// barrier (the barrier, not the work, bounds a sub-panel column).
+constexpr int kMaxBatch = 4;
+template <typename T>
+struct SubpanelBatch {
+  T* A[kMaxBatch];
+  int32_t* ipiv[kMaxBatch];
+  unsigned long long* key[kMaxBatch];  // [n] each, zero before the factorization
+  int* info;                           // [B]
+  int B;
+};
+// a[i] by predicated selects: a runtime index into a kernel parameter array
+// would copy the whole parameter struct to local memory
+template <typename P>
+__device__ __forceinline__ P batch_pick(const P (&a)[kMaxBatch], int i) {
+  P r = a[0];
+#pragma unroll
+  for (int q = 1; q < kMaxBatch; q++)
+    if (i == q) r = a[q];
+  return r;
+}
+
 // Sub-panel rows [c0, n), columns [c0, c0+w), w <= IB.
 template <typename T>
 __global__ void __launch_bounds__(256) k_subpanel(T* __restrict__ A, int n, int c0, int w, int32_t* __restrict__ ipiv,
@@ -243,19 +266,24 @@ __device__ __forceinline__ unsigned long long pivot_key(double v, int off) {
 // so after the grid barrier each block reads one word, then the winner's
 // published row: one grid barrier, two dependent L2 reads and two block
 // barriers per column.  Row offsets below 2^20 - 1 (checked by the caller).
+// With a batch, blocks [b Gb, (b+1) Gb) factor matrix b (gridDim.x = B Gb).
 template <typename T>
-__global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(T* __restrict__ A, int n, int c0, int w,
-                                                              int32_t* __restrict__ ipiv, PivotScratch<T> scr,
-                                                              int* __restrict__ info) {
+__global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(SubpanelBatch<T> bt, int n, int c0, int w,
+                                                              PivotScratch<T> scr) {
   cg::grid_group grid = cg::this_grid();
   extern __shared__ unsigned char sp_raw[];
   T* sA = reinterpret_cast<T*>(sp_raw);  // [chunk][SP]
   using R = typename Real<T>::R;
   constexpr int NW = SP_THREADS / 32;
-  const int G = gridDim.x;
+  const int G = gridDim.x;  // scratch row slots are indexed by the global block
+  const int Gb = G / bt.B, grp = blockIdx.x / Gb, cta = blockIdx.x - grp * Gb;
+  T* __restrict__ A = batch_pick(bt.A, grp);
+  int32_t* __restrict__ ipiv = batch_pick(bt.ipiv, grp);
+  unsigned long long* __restrict__ keys = batch_pick(bt.key, grp);
+  T* __restrict__ top = scr.top + (size_t)grp * 2 * IB;  // [2][IB] per matrix
   const int m = n - c0;
-  const int chunk = (m + G - 1) / G;
-  const int lo = c0 + blockIdx.x * chunk;
+  const int chunk = (m + Gb - 1) / Gb;
+  const int lo = c0 + cta * chunk;
   const int hi = min(n, lo + chunk);
   const int nr = max(0, hi - lo);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -280,9 +308,9 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(T* __restrict__ A,
       warp_argmax<NW>(v, i);
       i = __shfl_sync(0xffffffffu, i, 0);  // lanes >= NW reduced only among themselves
       const int buf = jc & 1, j = c0 + jc;
-      if (lane == 0 && i >= 0) atomicMax(&scr.key[j], pivot_key((double)v, i - c0));
+      if (lane == 0 && i >= 0) atomicMax(&keys[j], pivot_key((double)v, i - c0));
       if (i >= 0 && lane < w) scr.row[((size_t)buf * G + blockIdx.x) * IB + lane] = sA[(i - lo) * SP + lane];
-      if (j >= lo && j < hi && lane < w) scr.top[buf * IB + lane] = sA[(j - lo) * SP + lane];
+      if (j >= lo && j < hi && lane < w) top[buf * IB + lane] = sA[(j - lo) * SP + lane];
     }
   };
   // candidate of column jc over its rows without an update (first column, or
@@ -310,21 +338,21 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(T* __restrict__ A,
     // warp 0: the column's pivot, then the winner's row and the diagonal row
     if (warp == 0) {
       unsigned long long k = 0;
-      if (lane == 0) k = __ldcg(&scr.key[j]);
+      if (lane == 0) k = __ldcg(&keys[j]);
       k = __shfl_sync(0xffffffffu, k, 0);
       const bool zero = (k >> 20) == 0;
       const int piv = zero ? j : c0 + (0xFFFFF - (int)(k & 0xFFFFF));
       if (lane == 0) {
         s_zero = zero;
-        if (blockIdx.x == 0) {
+        if (cta == 0) {
           ipiv[j] = piv;
-          if (zero && *info == 0) *info = j + 1;
+          if (zero && bt.info[grp] == 0) bt.info[grp] = j + 1;
         }
       }
       if (!zero && lane < w) {
-        const int owner = (piv - c0) / chunk;
+        const int owner = grp * Gb + (piv - c0) / chunk;
         const T pr = scr.row[((size_t)buf * G + owner) * IB + lane];
-        const T tp = scr.top[buf * IB + lane];
+        const T tp = top[buf * IB + lane];
         s_prow[lane] = pr;
         if (piv != j && piv >= lo && piv < hi) sA[(piv - lo) * SP + lane] = tp;
         if (j >= lo && j < hi) sA[(j - lo) * SP + lane] = pr;
@@ -554,89 +582,135 @@ int panel_gemm_sub(bool tc, T* C, int ldc, const T* L, int ldl, const T* U, int 
 }  // namespace
 
 template <typename T>
-int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {
+int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, cudaStream_t st, int use_tc,
+                             int* info) {
   const bool tc = use_tc != 0;
   if (tc && sizeof(T) != sizeof(float2)) {
     set_error("tensor-core trailing update is only defined for the complex64 factorisation");
     return TT_ERR_UNSUPPORTED;
+  }
+  if (B < 1 || B > kMaxBatch) {
+    set_error("LU batch of " + std::to_string(B) + " matrices (1.." + std::to_string(kMaxBatch) + ")");
+    return TT_ERR_BADARG;
   }
   const int NB = (sizeof(T) == sizeof(float2)) ? 512 : 128;
   const int G = device_sm_count();
   DevBuf<double> sval;
   DevBuf<int> sidx, d_info;
   DevBuf<T> srow, stop;
+  DevBuf<unsigned long long> skey;
   TT_TRY(sval.alloc(2 * (size_t)G));
   TT_TRY(sidx.alloc(2 * (size_t)G));
   TT_TRY(srow.alloc(2 * (size_t)G * IB));
-  TT_TRY(stop.alloc(2 * (size_t)IB));
-  DevBuf<unsigned long long> skey;
-  TT_TRY(skey.alloc((size_t)n));
-  TT_TRY(d_info.alloc(1));
-  TT_CUDA_TRY(cudaMemsetAsync(d_info.ptr, 0, sizeof(int), st));
-  TT_CUDA_TRY(cudaMemsetAsync(skey.ptr, 0, sizeof(unsigned long long) * n, st));
+  TT_TRY(stop.alloc(2 * (size_t)kMaxBatch * IB));
+  TT_TRY(skey.alloc((size_t)B * n));
+  TT_TRY(d_info.alloc(B));
+  TT_CUDA_TRY(cudaMemsetAsync(d_info.ptr, 0, sizeof(int) * B, st));
+  TT_CUDA_TRY(cudaMemsetAsync(skey.ptr, 0, sizeof(unsigned long long) * B * n, st));
   PivotScratch<T> scr{sval.ptr, sidx.ptr, srow.ptr, stop.ptr, skey.ptr};
   static bool smem_attr = false;
   if (!smem_attr) {
     TT_CUDA_TRY(cudaFuncSetAttribute(k_subpanel_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubpanelSmem));
     smem_attr = true;
   }
+  // the sub-panel of matrices [b0, b0 + nb) in one cooperative launch
+  auto subpanel = [&](int b0, int nb, int j0, int w, int grid) -> int {
+    SubpanelBatch<T> bt{};
+    for (int b = 0; b < nb; b++) {
+      bt.A[b] = As[b0 + b];
+      bt.ipiv[b] = ipivs[b0 + b];
+      bt.key[b] = skey.ptr + (size_t)(b0 + b) * n;
+    }
+    bt.info = d_info.ptr + b0;
+    bt.B = nb;
+    int nn = n, cc0 = j0, ww = w;
+    void* args[] = {&bt, &nn, &cc0, &ww, &scr};
+    const size_t chunk = (size_t)(n - j0 + grid / nb - 1) / (grid / nb);
+    TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel_smem<T>, dim3(grid), dim3(SP_THREADS), args,
+                                            chunk * SP * sizeof(T), st));
+    count_launch();
+    return TT_OK;
+  };
   for (int k = 0; k < n; k += NB) {
     const int kb = std::min(NB, n - k);
     // ---- panel [k, k+kb) in sub-panels of IB columns
     for (int j0 = k; j0 < k + kb; j0 += IB) {
       const int w = std::min(IB, k + kb - j0);
       {
-        T* Ap = A;
-        int nn = n, cc0 = j0, ww = w;
-        int32_t* ip = ipiv;
-        int* inf = d_info.ptr;
-        void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
-        const size_t chunk = (size_t)(n - j0 + G - 1) / G;
-        const size_t smem = chunk * SP * sizeof(T);
-        const double mrows = n - j0;
-        ProfScope prof(TT_PROF_SUBPANEL, st, 4.0 * mrows * w * w, 2.0 * mrows * w * sizeof(T));
-        if (smem <= kSubpanelSmem && n - j0 < 0xFFFFF) {
-          TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel_smem<T>, dim3(G), dim3(SP_THREADS), args, smem, st));
+        const size_t m = (size_t)(n - j0);
+        const int Gb = G / B;
+        const bool keyed = m < 0xFFFFF;
+        const bool together = B > 1 && keyed && ((m + Gb - 1) / Gb) * SP * sizeof(T) <= kSubpanelSmem;
+        const bool alone = keyed && ((m + G - 1) / G) * SP * sizeof(T) <= kSubpanelSmem;
+        ProfScope prof(TT_PROF_SUBPANEL, st, 4.0 * m * w * w * B, 2.0 * m * w * sizeof(T) * B);
+        if (together) {
+          TT_TRY(subpanel(0, B, j0, w, Gb * B));
         } else {
-          TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
+          for (int b = 0; b < B; b++) {
+            if (alone) {
+              TT_TRY(subpanel(b, 1, j0, w, G));
+            } else {
+              T* Ap = As[b];
+              int nn = n, cc0 = j0, ww = w;
+              int32_t* ip = ipivs[b];
+              int* inf = d_info.ptr + b;
+              void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
+              TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
+              count_launch();
+            }
+          }
         }
-        count_launch();
       }
-      TT_TRY(laswp2(A, n, ipiv, j0, j0 + w, k, j0, j0 + w, k + kb, st));
-      const int right = k + kb - (j0 + w);
-      if (right > 0) {
-        TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
-        TT_TRY(panel_gemm_sub(tc, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
-                              A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
+      for (int b = 0; b < B; b++) {
+        T* A = As[b];
+        const int32_t* ipiv = ipivs[b];
+        TT_TRY(laswp2(A, n, ipiv, j0, j0 + w, k, j0, j0 + w, k + kb, st));
+        const int right = k + kb - (j0 + w);
+        if (right > 0) {
+          TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
+          TT_TRY(panel_gemm_sub(tc, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
+                                A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
+        }
       }
     }
-    // ---- interchanges outside the panel
-    TT_TRY(laswp2(A, n, ipiv, k, k + kb, 0, k, k + kb, n, st));
-    const int rest = n - k - kb;
-    if (rest <= 0) continue;
-    // ---- U12 = L11^{-1} A12, blocked by IB
-    for (int i0 = k; i0 < k + kb; i0 += IB) {
-      const int wi = std::min(IB, k + kb - i0);
-      TT_TRY(trsm_blk(A, n, i0, wi, k + kb, n, st));
-      const int below = k + kb - (i0 + wi);
-      if (below > 0)
-        TT_TRY(panel_gemm_sub(tc, A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
-                              A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
-    }
-    // ---- trailing update
-    if (tc) {
-      TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
-    } else {
-      TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
-                      A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
+    for (int b = 0; b < B; b++) {
+      T* A = As[b];
+      const int32_t* ipiv = ipivs[b];
+      // ---- interchanges outside the panel
+      TT_TRY(laswp2(A, n, ipiv, k, k + kb, 0, k, k + kb, n, st));
+      const int rest = n - k - kb;
+      if (rest <= 0) continue;
+      // ---- U12 = L11^{-1} A12, blocked by IB
+      for (int i0 = k; i0 < k + kb; i0 += IB) {
+        const int wi = std::min(IB, k + kb - i0);
+        TT_TRY(trsm_blk(A, n, i0, wi, k + kb, n, st));
+        const int below = k + kb - (i0 + wi);
+        if (below > 0)
+          TT_TRY(panel_gemm_sub(tc, A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
+                                A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
+      }
+      // ---- trailing update
+      if (tc) {
+        TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
+      } else {
+        TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
+                        A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
+      }
     }
   }
   if (tc) TT_TRY(tc_check_error(st));
   if (info) {
-    TT_CUDA_TRY(cudaMemcpyAsync(info, d_info.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TT_CUDA_TRY(cudaMemcpyAsync(info, d_info.ptr, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
     TT_CUDA_TRY(cudaStreamSynchronize(st));
   }
   return TT_OK;
+}
+template int lu_factor_batched_device<double2>(double2* const*, int, int, int32_t* const*, cudaStream_t, int, int*);
+template int lu_factor_batched_device<float2>(float2* const*, int, int, int32_t* const*, cudaStream_t, int, int*);
+
+template <typename T>
+int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {
+  return lu_factor_batched_device<T>(&A, 1, n, &ipiv, st, use_tc, info);
 }
 template int lu_factor_device<double2>(double2*, int, int32_t*, cudaStream_t, int, int*);
 template int lu_factor_device<float2>(float2*, int, int32_t*, cudaStream_t, int, int*);

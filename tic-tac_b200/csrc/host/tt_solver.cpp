@@ -453,14 +453,24 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     return s;
   }
   const int Nq = L_.Nq, Np = L_.Np;
-  DevBuf<int32_t> ipiv, cols, rhs_e, perm_d;
-  TT_TRY(ipiv.alloc(n));
+  // complex64: up to 4 energies' matrices formed and factored together (their
+  // sub-panels share each grid barrier), as many as free HBM holds
+  int B = 1;
+  if (opt.mixed && nE > 1) {
+    size_t free_b = 0, total_b = 0;
+    TT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per = (size_t)n * n * sizeof(float2), reserve = (size_t)2 << 30;
+    const size_t fit = free_b > reserve + per ? (free_b - reserve) / per : 1;
+    B = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>((size_t)nE, 4), fit));
+  }
+  DevBuf<int32_t> ipiv_all, cols, rhs_e, perm_d;
+  TT_TRY(ipiv_all.alloc((size_t)n * B));
   DevBuf<double> b, x, y, res, d, tmp;
   TT_TRY(tmp.alloc((size_t)2 * n * nd));
   TT_TRY(b.alloc((size_t)2 * n * nd));
   TT_TRY(x.alloc((size_t)2 * n * nd));
   DevBuf<double2> L64;
-  DevBuf<float2> L32;
+  DevBuf<float2> L32all;
   TrsvBlocks<double2> tb64, tbT64;
   TrsvBlocks<float2> tb32, tbT32;
   // adjoint: the vectors of lambda, its refinement and the products
@@ -470,99 +480,114 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     TT_TRY(dots.alloc((size_t)2 * nd * nd));
   }
   if (opt.mixed) {
-    TT_TRY(L32.alloc((size_t)n * n));
+    TT_TRY(L32all.alloc((size_t)B * n * n));
     TT_TRY(y.alloc((size_t)2 * n * nd));
     TT_TRY(res.alloc((size_t)2 * n * nd));
   } else {
     TT_TRY(L64.alloc((size_t)n * n));
   }
-  for (int j = 0; j < nE; j++) {
-    std::vector<int32_t> hc(nd), he(nd, 0);
-    for (int k = 0; k < nd; k++) hc[k] = deut[k] * Nq * Np + q_idx[j] * Np + 0;
-    TT_TRY(cols.upload(hc, st));
-    TT_TRY(rhs_e.upload(he, st));
-    const double* Gj = G_.ptr + (size_t)2 * n * j;
+  for (int g0 = 0; g0 < nE; g0 += B) {
+    const int nb = std::min(B, nE - g0);
+    // ---- form and factor the group's matrices
     auto t0 = std::chrono::steady_clock::now();
-    int info = 0;
+    int info[4] = {0, 0, 0, 0};
     if (opt.mixed) {
-      TT_TRY(form_L_device<float2>(A_.ptr, Gj, n, L32.ptr, st));
+      float2* Ls[4];
+      int32_t* ps[4];
+      for (int q = 0; q < nb; q++) {
+        Ls[q] = L32all.ptr + (size_t)q * n * n;
+        ps[q] = ipiv_all.ptr + (size_t)q * n;
+        TT_TRY(form_L_device<float2>(A_.ptr, G_.ptr + (size_t)2 * n * (g0 + q), n, Ls[q], st));
+      }
       TT_CUDA_TRY(cudaStreamSynchronize(st));
       r.ms_form += ms_since(t0);
       t0 = std::chrono::steady_clock::now();
-      TT_TRY(lu_factor_device<float2>(L32.ptr, n, ipiv.ptr, st, opt.tensor_cores ? 1 : 0, &info));
+      TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, opt.tensor_cores ? 1 : 0, info));
       r.ms_factor += ms_since(t0);
     } else {
-      TT_TRY(form_L_device<double2>(A_.ptr, Gj, n, L64.ptr, st));
+      TT_TRY(form_L_device<double2>(A_.ptr, G_.ptr + (size_t)2 * n * g0, n, L64.ptr, st));
       TT_CUDA_TRY(cudaStreamSynchronize(st));
       r.ms_form += ms_since(t0);
       t0 = std::chrono::steady_clock::now();
-      TT_TRY(lu_factor_device<double2>(L64.ptr, n, ipiv.ptr, st, 0, &info));
+      TT_TRY(lu_factor_device<double2>(L64.ptr, n, ipiv_all.ptr, st, 0, &info[0]));
       r.ms_factor += ms_since(t0);
     }
-    if (info != 0) {
-      r.info = info;
-      set_error("zero pivot at column " + std::to_string(info) + " of the Faddeev kernel matrix");
-      if (rep) *rep = r;
-      return TT_ERR_SINGULAR;
-    }
-    t0 = std::chrono::steady_clock::now();
-    std::vector<int32_t> perm;
-    TT_TRY(lu_permutation(ipiv.ptr, n, perm, st));
-    TT_TRY(perm_d.upload(perm, st));
-    TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nd, b.ptr, st));
-    TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * 2 * n * nd, cudaMemcpyDeviceToDevice, st));
-    if (opt.mixed) {
-      TT_TRY(lu_trsv_prepare<float2>(L32.ptr, n, tb32, st));
-      TT_TRY(lu_solve_device<float2>(L32.ptr, n, tb32, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
-    } else {
-      TT_TRY(lu_trsv_prepare<double2>(L64.ptr, n, tb64, st));
-      TT_TRY(lu_solve_device<double2>(L64.ptr, n, tb64, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
-    }
-    TT_CUDA_TRY(cudaStreamSynchronize(st));
-    r.ms_solve += ms_since(t0);
-    if (opt.mixed) {
-      // FP64 iterative refinement: r = b - (x - A (G o x)), L d = r, x += d
+    for (int q = 0; q < nb; q++)
+      if (info[q] != 0) {
+        r.info = info[q];
+        set_error("zero pivot at column " + std::to_string(info[q]) + " of the Faddeev kernel matrix");
+        if (rep) *rep = r;
+        return TT_ERR_SINGULAR;
+      }
+    // ---- per energy: substitutions, refinement, adjoint, read-out
+    for (int q = 0; q < nb; q++) {
+      const int j = g0 + q;
+      float2* const Lq = opt.mixed ? L32all.ptr + (size_t)q * n * n : nullptr;  // this energy's factor
+      int32_t* const pivq = ipiv_all.ptr + (size_t)q * n;
+      std::vector<int32_t> hc(nd), he(nd, 0);
+      for (int k = 0; k < nd; k++) hc[k] = deut[k] * Nq * Np + q_idx[j] * Np + 0;
+      TT_TRY(cols.upload(hc, st));
+      TT_TRY(rhs_e.upload(he, st));
+      const double* Gj = G_.ptr + (size_t)2 * n * j;
       t0 = std::chrono::steady_clock::now();
-      bool converged = false;
-      int it = 0;
-      double worst = 0;
-      std::vector<double> ratio(nd), prev(nd, 0.0);
-      for (it = 1; it <= opt.refine_max_iter; it++) {
-        TT_TRY(hadamard_device(Gj, rhs_e.ptr, n, x.ptr, nd, y.ptr, st));
-        TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nd, res.ptr, st));
-        TT_TRY(lu_solve_device<float2>(L32.ptr, n, tb32, perm_d.ptr, res.ptr, tmp.ptr, nd, st));
-        TT_TRY(axpy_norms_device(x.ptr, res.ptr, n, nd, ratio.data(), st));
-        worst = refine_error_estimate(ratio, prev, it > 1);
-        if (!(worst == worst)) break;  // NaN
-        if (worst <= opt.refine_tol) {
-          converged = true;
-          break;
+      std::vector<int32_t> perm;
+      TT_TRY(lu_permutation(pivq, n, perm, st));
+      TT_TRY(perm_d.upload(perm, st));
+      TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nd, b.ptr, st));
+      TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * 2 * n * nd, cudaMemcpyDeviceToDevice, st));
+      if (opt.mixed) {
+        TT_TRY(lu_trsv_prepare<float2>(Lq, n, tb32, st));
+        TT_TRY(lu_solve_device<float2>(Lq, n, tb32, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+      } else {
+        TT_TRY(lu_trsv_prepare<double2>(L64.ptr, n, tb64, st));
+        TT_TRY(lu_solve_device<double2>(L64.ptr, n, tb64, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+      }
+      TT_CUDA_TRY(cudaStreamSynchronize(st));
+      r.ms_solve += ms_since(t0);
+      if (opt.mixed) {
+        // FP64 iterative refinement: r = b - (x - A (G o x)), L d = r, x += d
+        t0 = std::chrono::steady_clock::now();
+        bool converged = false;
+        int it = 0;
+        double worst = 0;
+        std::vector<double> ratio(nd), prev(nd, 0.0);
+        for (it = 1; it <= opt.refine_max_iter; it++) {
+          TT_TRY(hadamard_device(Gj, rhs_e.ptr, n, x.ptr, nd, y.ptr, st));
+          TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nd, res.ptr, st));
+          TT_TRY(lu_solve_device<float2>(Lq, n, tb32, perm_d.ptr, res.ptr, tmp.ptr, nd, st));
+          TT_TRY(axpy_norms_device(x.ptr, res.ptr, n, nd, ratio.data(), st));
+          worst = refine_error_estimate(ratio, prev, it > 1);
+          if (!(worst == worst)) break;  // NaN
+          if (worst <= opt.refine_tol) {
+            converged = true;
+            break;
+          }
+        }
+        r.ms_refine += ms_since(t0);
+        r.refine_iters = std::max(r.refine_iters, std::min(it, opt.refine_max_iter));
+        r.final_correction = std::max(r.final_correction, worst);
+        if (!converged) {
+          set_error("iterative refinement did not converge (last |dx|/|x| = " + std::to_string(worst) + ")");
+          if (rep) *rep = r;
+          return TT_ERR_NOCONVERGE;
         }
       }
-      r.ms_refine += ms_since(t0);
-      r.refine_iters = std::max(r.refine_iters, std::min(it, opt.refine_max_iter));
-      r.final_correction = std::max(r.final_correction, worst);
-      if (!converged) {
-        set_error("iterative refinement did not converge (last |dx|/|x| = " + std::to_string(worst) + ")");
-        if (rep) *rep = r;
-        return TT_ERR_NOCONVERGE;
-      }
+      if (adj && adj->n_theta > 0) TT_TRY(adjoint_energy(j, nE, nd, Gj, cols.ptr, perm_d.ptr, tmp.ptr, x.ptr, opt,
+                                                        opt.mixed ? (void*)Lq : (void*)L64.ptr, tbT32, tbT64,
+                                                        lam.ptr, yT.ptr, rT.ptr, u.ptr, g.ptr, w.ptr, h.ptr, dots.ptr,
+                                                        *adj, r, st));
+      // on-shell read-out, solve_faddeev.cpp:407-431
+      std::vector<double> hx((size_t)2 * n * nd);
+      TT_CUDA_TRY(cudaMemcpyAsync(hx.data(), x.ptr, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st));
+      TT_CUDA_TRY(cudaStreamSynchronize(st));
+      for (int dr = 0; dr < nd; dr++)
+        for (int dc = 0; dc < nd; dc++) {
+          const size_t row = (size_t)deut[dr] * Nq * Np + (size_t)q_idx[j] * Np + 0;
+          const size_t u = (size_t)dr * nd * nE + (size_t)dc * nE + j;
+          U[2 * u + 0] = hx[2 * ((size_t)dc * n + row) + 0];
+          U[2 * u + 1] = hx[2 * ((size_t)dc * n + row) + 1];
+        }
     }
-    if (adj && adj->n_theta > 0) TT_TRY(adjoint_energy(j, nE, nd, Gj, cols.ptr, perm_d.ptr, tmp.ptr, x.ptr, opt,
-                                                      opt.mixed ? (void*)L32.ptr : (void*)L64.ptr, tbT32, tbT64,
-                                                      lam.ptr, yT.ptr, rT.ptr, u.ptr, g.ptr, w.ptr, h.ptr, dots.ptr,
-                                                      *adj, r, st));
-    // on-shell read-out, solve_faddeev.cpp:407-431
-    std::vector<double> hx((size_t)2 * n * nd);
-    TT_CUDA_TRY(cudaMemcpyAsync(hx.data(), x.ptr, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st));
-    TT_CUDA_TRY(cudaStreamSynchronize(st));
-    for (int dr = 0; dr < nd; dr++)
-      for (int dc = 0; dc < nd; dc++) {
-        const size_t row = (size_t)deut[dr] * Nq * Np + (size_t)q_idx[j] * Np + 0;
-        const size_t u = (size_t)dr * nd * nE + (size_t)dc * nE + j;
-        U[2 * u + 0] = hx[2 * ((size_t)dc * n + row) + 0];
-        U[2 * u + 1] = hx[2 * ((size_t)dc * n + row) + 1];
-      }
   }
   if (rep) *rep = r;
   return TT_OK;
