@@ -62,3 +62,12 @@ def test_u_table_format(tmp_path):
         f = line.split()
         assert int(f[2]) == int(g["q_idx"][j])
         assert abs(complex(f[3]) - U[j]) <= 1e-15 * abs(U[j])
+
+
+def test_energy_batch_option_range():
+    opts = dict(potential_model="malfliet_tjon", J_2N_max=1, two_J_3N_max=1, Np_WP=8, Nq_WP=8, lab_energies="10")
+    for v in (1, 2, 4):
+        tt.Run(energy_batch=v, **opts).close()
+    for v in (0, 5):
+        with pytest.raises(tt.TicTacError, match="energy_batch"):
+            tt.Run(energy_batch=v, **opts)

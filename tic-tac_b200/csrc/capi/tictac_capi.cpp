@@ -109,6 +109,7 @@ SolveOptions options_of(const RunParams& rp, int precision) {
   o.pade = precision == TT_PRECISION_PADE;
   o.refine_tol = rp.refine_tol;
   o.refine_max_iter = rp.refine_max_iter;
+  o.energy_batch = rp.energy_batch;
   return o;
 }
 

@@ -56,6 +56,7 @@ struct RunParams {
   int precision_code = 1;           // TT_PRECISION_*
   double refine_tol = 1e-12;
   int refine_max_iter = 30;
+  int energy_batch = 4;  // complex64 LUs of a channel's energies factored together (1..4)
   std::vector<double> lab_energies; // set directly or read from energy_input_file
   // additive offsets to the potential's low-energy constants, in the model's
   // order (LO_internal: C_1S0, C_3S1 in MeV^-2; malfliet_tjon has none)

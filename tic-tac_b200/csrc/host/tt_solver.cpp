@@ -453,15 +453,16 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     return s;
   }
   const int Nq = L_.Nq, Np = L_.Np;
-  // complex64: up to 4 energies' matrices formed and factored together (their
-  // sub-panels share each grid barrier), as many as free HBM holds
+  // complex64: up to opt.energy_batch (<= 4) energies' matrices formed and
+  // factored together (their sub-panels share each grid barrier), as many as
+  // free HBM holds
   int B = 1;
-  if (opt.mixed && nE > 1) {
+  if (opt.mixed && nE > 1 && opt.energy_batch > 1) {
     size_t free_b = 0, total_b = 0;
     TT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     const size_t per = (size_t)n * n * sizeof(float2), reserve = (size_t)2 << 30;
     const size_t fit = free_b > reserve + per ? (free_b - reserve) / per : 1;
-    B = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>((size_t)nE, 4), fit));
+    B = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>((size_t)nE, std::min(opt.energy_batch, 4)), fit));
   }
   DevBuf<int32_t> ipiv_all, cols, rhs_e, perm_d;
   TT_TRY(ipiv_all.alloc((size_t)n * B));

@@ -33,6 +33,7 @@ struct SolveOptions {
   bool pade = false;        // Pade-resummed Neumann series on the resident A instead of an LU
   double refine_tol = 1e-12;
   int refine_max_iter = 30;
+  int energy_batch = 4;     // complex64: energies factored together at most (1..4; fewer if HBM is short)
 };
 
 struct SolveReport {

@@ -55,6 +55,10 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       rp.precision = value;
     } else if (key == "refine_tol") rp.refine_tol = std::stod(value);
     else if (key == "refine_max_iter") rp.refine_max_iter = std::stoi(value);
+    else if (key == "energy_batch") {
+      rp.energy_batch = std::stoi(value);
+      if (rp.energy_batch < 1 || rp.energy_batch > 4) return bad("energy_batch (1..4)");
+    }
     else if (key == "lab_energies") {
       rp.lab_energies.clear();
       std::stringstream ss(value);
