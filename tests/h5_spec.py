@@ -9,9 +9,9 @@ fixed string / compound (v1-v3), layout message v3 (compact, contiguous,
 chunked with a v1 B-tree index, no filters) and attribute messages v1.
 
 Writer scope: the same structures, contiguous or chunked rank-1 datasets,
-used to produce files laid out like the HDF5 library's H5TBmake_table
-(chunked tables with unlimited maximum size) that the library reader must
-also accept.
+attributes optionally in object-header continuation blocks, used to produce
+files laid out like the HDF5 library's H5TBmake_table (chunked tables with
+unlimited maximum size) that the library reader must also accept.
 """
 import struct
 
@@ -369,9 +369,10 @@ def _msg(mtype, body, flags=0):
     return _le(2, mtype) + _le(2, _pad8(len(body))) + bytes([flags, 0, 0, 0]) + body + bytes(_pad8(len(body)) - len(body))
 
 
-def _header(msgs):
+def _header(msgs, extra=0):
+    """Version-1 object header; extra = messages kept in continuation blocks."""
     body = b"".join(msgs)
-    return bytes([1, 0]) + _le(2, len(msgs)) + _le(4, 1) + _le(4, len(body)) + bytes(4) + body
+    return bytes([1, 0]) + _le(2, len(msgs) + extra) + _le(4, 1) + _le(4, len(body)) + bytes(4) + body
 
 
 def _attr(name, value):
@@ -381,8 +382,9 @@ def _attr(name, value):
 
 
 def write(path, datasets, leaf_k=4):
-    """datasets: list of dicts {name, type (bytes), n, data (bytes), chunk (int or None), attrs (list of pairs)}.
-    Rank-1 datasets only.  Links go into as many symbol-table nodes as leaf_k needs."""
+    """datasets: list of dicts {name, type (bytes), n, data (bytes), chunk (int or None), attrs (list of pairs),
+    split (bool: attributes in an object-header continuation block)}.  Rank-1 datasets only.  Links go into
+    as many symbol-table nodes as leaf_k needs."""
     ds = sorted(datasets, key=lambda d: d["name"])
     heap = bytearray(8)
     name_off = []
@@ -395,9 +397,9 @@ def write(path, datasets, leaf_k=4):
     tree_size = 24 + (2 * internal_k + 1) * 8 + 2 * internal_k * 8
     snod_size = 8 + cap * 40
 
-    def headers(addrs):
-        out = []
-        for d, a in zip(ds, addrs):
+    def headers(addrs, conts=None):
+        out, tails = [], []
+        for i, (d, a) in enumerate(zip(ds, addrs)):
             esize = len(d["data"]) // max(d["n"], 1) if d["n"] else 0
             msgs = [_msg(0x01, _space(d["n"], unlimited=d.get("chunk") is not None)), _msg(0x03, d["type"], 1),
                     _msg(0x05, bytes([2, 2, 2, 0]), 1)]
@@ -408,8 +410,15 @@ def write(path, datasets, leaf_k=4):
                 msgs.append(_msg(0x08, bytes([3, 2, 2]) + _le(8, a[1]) + _le(4, d["chunk"]) + _le(4, tsize)))
             for k, v in d.get("attrs", []):
                 msgs.append(_msg(0x0C, _attr(k, v)))
-            out.append(_header(msgs))
-        return out
+            if d.get("split") and len(msgs) > 4:
+                tail = b"".join(msgs[4:])
+                head = msgs[:4] + [_msg(0x10, _le(8, conts[i] if conts else 0) + _le(8, len(tail)))]
+                out.append(_header(head, extra=len(msgs) - 4))
+                tails.append(tail)
+            else:
+                out.append(_header(msgs))
+                tails.append(b"")
+        return out, tails
 
     a_root = 96
     root = _header([_msg(0x11, bytes(16))])
@@ -418,11 +427,15 @@ def write(path, datasets, leaf_k=4):
     a_tree = a_heapdata + len(heap)
     a_snods = [a_tree + tree_size + i * snod_size for i in range(len(groups))]
     a = a_snods[-1] + snod_size
-    probe = headers([(0, 0)] * len(ds))
+    probe, tails = headers([(0, 0)] * len(ds))
     a_oh = []
     for h in probe:
         a_oh.append(a)
         a += len(h)
+    conts = []
+    for t in tails:
+        conts.append(a if t else 0)
+        a += len(t)
     # data: contiguous blocks; chunked = one B-tree node then the chunks
     layout_addrs, blobs = [], []
     for d in ds:
@@ -450,7 +463,7 @@ def write(path, datasets, leaf_k=4):
             blobs.append((tree_at, node))
             layout_addrs.append((0, tree_at))
     eof = a
-    hdrs = headers(layout_addrs)
+    hdrs, tails = headers(layout_addrs, conts)
     img = bytearray(eof)
     sb = (SIGNATURE + bytes([0, 0, 0, 0, 0, 8, 8, 0]) + _le(2, leaf_k) + _le(2, internal_k) + _le(4, 0) +
           _le(8, 0) + _le(8, UNDEF) + _le(8, eof) + _le(8, UNDEF) +
@@ -476,6 +489,9 @@ def write(path, datasets, leaf_k=4):
         img[a_snods[gi]:a_snods[gi] + len(sn)] = sn
     for h, at in zip(hdrs, a_oh):
         img[at:at + len(h)] = h
+    for t, at in zip(tails, conts):
+        if t:
+            img[at:at + len(t)] = t
     for at, blob in blobs:
         img[at:at + len(blob)] = blob
     with open(path, "wb") as fh:

@@ -136,10 +136,11 @@ def test_empty_matrix(tmp_path):
     assert len(r) == len(c) == len(v) == 0
 
 
-def _library_style_file(path, ch, leaf_k):
+def _library_style_file(path, ch, leaf_k, split=False):
     """The same objects with the tables chunked (10 records per chunk) and of
-    unlimited maximum size, as H5TBmake_table stores them, and the links
-    spread over several symbol-table nodes."""
+    unlimited maximum size, as H5TBmake_table stores them, the links spread
+    over several symbol-table nodes, and (split) the table attributes in
+    object-header continuation blocks."""
     pwt = np.asarray(ch["pwt"]).reshape(-1, 9)
     recs = expected_pw_records(ch["pwt"])
     pw_bytes = bytearray(40 * len(recs))
@@ -163,9 +164,10 @@ def _library_style_file(path, ch, leaf_k):
         dict(name="Nq_WP", type=h5_spec.dt_int(), n=1, data=np.int32(len(ch["q"]) - 1).tobytes()),
         dict(name="P123_sparse_dim", type=h5_spec.dt_int(8, False), n=1, data=np.uint64(n).tobytes()),
         dict(name="p boundaries", type=bt, n=len(ch["p"]), data=bounds(ch["p"]), chunk=10, type_size=16,
-             attrs=[("CLASS", "TABLE"), ("VERSION", "3.0"), ("TITLE", "Info p boundaries")]),
+             attrs=[("CLASS", "TABLE"), ("VERSION", "3.0"), ("TITLE", "Info p boundaries")], split=split),
         dict(name="q boundaries", type=bt, n=len(ch["q"]), data=bounds(ch["q"]), chunk=10, type_size=16),
-        dict(name="pw channels", type=pt, n=len(pwt), data=bytes(pw_bytes), chunk=10, type_size=40),
+        dict(name="pw channels", type=pt, n=len(pwt), data=bytes(pw_bytes), chunk=10, type_size=40,
+             attrs=[("CLASS", "TABLE"), ("TITLE", "Partial wave info")], split=split),
         dict(name="row indices", type=h5_spec.dt_int(), n=n, data=np.asarray(ch["row"], "<i4").tobytes()),
         dict(name="column indices", type=h5_spec.dt_int(), n=n, data=np.asarray(ch["col"], "<i4").tobytes()),
         dict(name="values", type=h5_spec.dt_f64(), n=n, data=np.asarray(ch["val"], "<f8").tobytes()),
@@ -173,14 +175,15 @@ def _library_style_file(path, ch, leaf_k):
     h5_spec.write(path, ds, leaf_k=leaf_k)
 
 
-@pytest.mark.parametrize("leaf_k", [4, 2])
-def test_reader_accepts_library_style_tables(tmp_path, leaf_k):
+@pytest.mark.parametrize("leaf_k,split", [(4, False), (2, False), (4, True)])
+def test_reader_accepts_library_style_tables(tmp_path, leaf_k, split):
     ch = channel("lo_j1_J3_n8", 3)  # Nalpha > 10: the pw table spans several chunks
     assert len(np.asarray(ch["pwt"]).reshape(-1, 9)) > 10
     path = tmp_path / "lib.h5"
-    _library_style_file(path, ch, leaf_k)
+    _library_style_file(path, ch, leaf_k, split)
     f = h5_spec.File(path)  # the writer's own file parses
     assert f.datasets["pw channels"]["layout"]["class"] == "chunked"
+    assert f.datasets["p boundaries"]["attrs"]["TITLE"] == "Info p boundaries"
     r, c, v = tt.read_P123_h5(path, ch["pw"], ch["p"], ch["q"])
     assert np.array_equal(r, ch["row"]) and np.array_equal(c, ch["col"]) and np.array_equal(v, ch["val"])
 
