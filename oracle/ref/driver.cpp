@@ -4,7 +4,15 @@
 // as raw binary arrays so the tests can compare them with the GPU path.
 //
 //   tictac_ref dump <outdir> [--solver=reference|replica|pade] key=value ...
-//   tictac_ref time <outdir> [--channel=k] [--sample_cols=m] key=value ...
+//   tictac_ref time <outdir> [--channel=k] [--sample_cols=m] [--repeat=r] key=value ...
+//   tictac_ref info <outdir> key=value ...
+//
+// time: the dense solve of the selected channel (A columns once, then per
+// energy L = 1 - A G, R = A and zgetrf + zgetrs with nrhs = n) repeated r
+// times after one set-up, one "step" line per repetition in meta.txt; the
+// first repetition also times the fair variant (zgetrs on the on-shell
+// right-hand sides only).  info: the channels' sizes, energies and deuteron
+// states from the state-space set-up alone (no P123, no solve).
 //
 // Extra keys understood here (stripped before the reference's parser sees them):
 //   swave_only=true   apply the reference's commented-out s-wave filter
@@ -14,6 +22,7 @@
 // Parity-oracle infrastructure only.
 #include <omp.h>
 
+#include <algorithm>
 #include <chrono>
 #include <complex>
 #include <cstdio>
@@ -126,6 +135,7 @@ int main(int argc, char** argv) {
   std::string solver = "reference";
   int time_channel = -1;
   long sample_cols = -1;
+  int repeat = 1;
   bool swave = false;
   std::vector<std::string> keep_args = {"tictac_ref"};
   std::string energies;
@@ -134,6 +144,7 @@ int main(int argc, char** argv) {
     if (a.rfind("--solver=", 0) == 0) solver = a.substr(9);
     else if (a.rfind("--channel=", 0) == 0) time_channel = std::atoi(a.c_str() + 10);
     else if (a.rfind("--sample_cols=", 0) == 0) sample_cols = std::atol(a.c_str() + 14);
+    else if (a.rfind("--repeat=", 0) == 0) repeat = std::max(1, std::atoi(a.c_str() + 9));
     else if (a == "swave_only=true") swave = true;
     else if (a == "swave_only=false") swave = false;
     else if (a.rfind("lab_energies=", 0) == 0) energies = a.substr(13);
@@ -217,6 +228,14 @@ int main(int argc, char** argv) {
       pwtab.insert(pwtab.end(), v, v + 9);
     }
     const std::string tag = "_c" + std::to_string(chn);
+    if (mode == "info") {
+      channel_os_indexing os;
+      find_on_shell_bins(cfg, os, sub, fwp, swp, rp);
+      find_deuteron_channels(cfg, pw);
+      meta << "chn " << chn << " Nalpha " << sub.Nalpha << " n " << n << " nE " << cfg.num_T_lab << " nd "
+           << cfg.deuteron_num_array[chn] << "\n";
+      continue;
+    }
     dump("pw" + tag, pwtab.data(), pwtab.size());
 
     auto t0 = std::chrono::steady_clock::now();
@@ -284,6 +303,9 @@ int main(int argc, char** argv) {
       if (mode == "dump" && n <= 4096) dump("A" + tag, A.data(), A.size());
       std::vector<cdouble> L(n * n), R(n * n);
       double t_lu = 0, t_fair = 0;
+      for (int rep = 0; rep < (mode == "time" ? repeat : 1); rep++) {
+      const auto ts = std::chrono::steady_clock::now();
+      const double t_lu0 = t_lu;
       for (size_t j = 0; j < nE; j++) {
         for (size_t r = 0; r < n; r++)
           for (size_t c = 0; c < n; c++) {
@@ -296,7 +318,7 @@ int main(int argc, char** argv) {
         auto tl = std::chrono::steady_clock::now();
         solve_MM(L.data(), R.data(), (int)n);  // zgetrf + zgetrs(nrhs = n), matrix_routines.cpp:73-80
         t_lu += std::chrono::duration<double>(std::chrono::steady_clock::now() - tl).count();
-        if (mode == "time") {
+        if (mode == "time" && rep == 0) {
           // fair variant: zgetrf + zgetrs with only the on-shell right-hand sides
           std::vector<cdouble> B(n * nd);
           std::vector<long long> piv(n);
@@ -314,6 +336,14 @@ int main(int argc, char** argv) {
             const size_t cc = os.deuteron_idx_array[dc] * Nq * Np + os.q_com_idx_array[j] * Np;
             U[dr * nd * nE + dc * nE + j] = R[rr * n + cc];
           }
+      }
+      if (mode == "time") {
+        // one step: every energy's L/R formation and solve (the fair variant's time excluded)
+        const double t_step =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count() - (rep == 0 ? t_fair : 0.0);
+        meta << "step " << rep << " t " << t_step << " t_lu " << (t_lu - t_lu0) << "\n";
+        meta.flush();
+      }
       }
       meta << "timing chn " << chn << " n " << n << " t_A " << t_A << " t_getrf_getrs " << t_lu << " t_fair " << t_fair
            << " threads " << omp_get_max_threads() << "\n";

@@ -6,9 +6,10 @@ configurations and packs every stage it dumps (partial-wave tables, WP
 boundaries, V, C, SWP energies, P123 in the reference's row-major COO order,
 resolvents, on-shell U) into one .npz per case.
 
-    make -C oracle ref && python tests/golden/make_golden.py [--pade]
+    make -C oracle ref && python tests/golden/make_golden.py [--pade | --large]
 
-(--pade regenerates only the Pade fixtures <case>_pade.npz.)
+(--pade regenerates only the Pade fixtures <case>_pade.npz; --large only the
+summary fixtures of the bench-sized cases, <case>.npz with U and checksums.)
 
 Test infrastructure only; the product never reads these files.
 """
@@ -110,9 +111,74 @@ def run_pade(name, opts):
 
 PADE_CASES = ["mt_swave_n16", "lo_j1_J3_n8"]
 
+# Bench-sized cases: too large to store P123 and G, so the fixture keeps the
+# on-shell U of every channel (the reference's zgetrf + zgetrs with nrhs = n)
+# and order-independent checksums of P123 and G.
+LARGE_CASES = {
+    # the bench workload's basis (j <= 3, J <= 7/2, both parities, chiral LO) at
+    # Np = Nq = 12: eight channels, n = 3,888 .. 9,072, 8 - 18 panels of 512
+    "lo_j3_J7_n12": dict(potential_model="LO_internal", J_2N_max=3, two_J_3N_max=7, Np_WP=12, Nq_WP=12,
+                         lab_energies="10"),
+}
+
+
+def pattern_hash(row, col, n):
+    """Order-independent 64-bit hash of a sparsity pattern: the wrapping sum of
+    a 64-bit mix of each key row * n + col."""
+    k = row.astype(np.uint64) * np.uint64(n) + col.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        k = (k ^ (k >> np.uint64(31))) * np.uint64(0x9E3779B97F4A7C15)
+        k = (k ^ (k >> np.uint64(29))) * np.uint64(0xBF58476D1CE4E5B9)
+        k = k ^ (k >> np.uint64(32))
+        return int(np.sum(k, dtype=np.uint64))
+
+
+def value_checksums(row, col, val, n):
+    """Weighted sums of the values with weights fixed by the position
+    (sum v, sum v * w(row, col) with w in [1, 2), sum |v|), compared to a
+    relative tolerance."""
+    w = 1.0 + ((row.astype(np.float64) * 0.6180339887498949 + col.astype(np.float64) * 0.4142135623730951) % 1.0)
+    return np.array([np.sum(val), np.sum(val * w), np.sum(np.abs(val))])
+
+
+def vector_checksums(G):
+    """The same for a complex vector indexed by position."""
+    return np.array([np.sum(G), np.sum(G * (1.0 + (np.arange(len(G)) % 7) / 7.0)), np.sum(np.abs(G))])
+
+
+def run_large(name, opts):
+    with tempfile.TemporaryDirectory() as out:
+        args = [REF_BIN, "dump", out, "--solver=replica"] + [f"{k}={v}" for k, v in opts.items()]
+        subprocess.run(args, check=True, cwd=out, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 4)))
+        meta = read_meta(os.path.join(out, "meta.txt"))
+        data = {"opts": np.array([f"{k}={v}" for k, v in opts.items()]), "E_bound": np.array(meta["E_bound"]),
+                "T_lab": meta["T_lab"], "E_com": meta["E_com"], "q_idx": meta["q_idx"],
+                "n_chn": np.array(len(meta["channels"]))}
+        for ch in meta["channels"]:
+            c, n = ch["chn"], ch["n"]
+            t = f"_c{c}"
+            row = np.fromfile(os.path.join(out, f"p123_row{t}.bin"), dtype=np.int32)
+            col = np.fromfile(os.path.join(out, f"p123_col{t}.bin"), dtype=np.int32)
+            val = np.fromfile(os.path.join(out, f"p123_val{t}.bin"), dtype=np.float64)
+            G = np.fromfile(os.path.join(out, f"G{t}.bin"), dtype=np.complex128)
+            data["n" + t] = np.array(n)
+            data["nnz" + t] = np.array(len(val))
+            data["p123_hash" + t] = np.array(pattern_hash(row, col, n), dtype=np.uint64)
+            data["p123_sums" + t] = value_checksums(row, col, val, n)
+            data["G_sums" + t] = vector_checksums(G)
+            data["U" + t] = np.fromfile(os.path.join(out, f"U{t}.bin"), dtype=np.complex128)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+        print(name, "channels", len(meta["channels"]), "n", [ch["n"] for ch in meta["channels"]],
+              "nnz", [ch["nnz"] for ch in meta["channels"]])
+
 if __name__ == "__main__":
     if not os.path.exists(REF_BIN):
         sys.exit(f"{REF_BIN} missing: run `make -C oracle ref` first")
+    if "--large" in sys.argv:
+        for name, opts in LARGE_CASES.items():
+            run_large(name, opts)
+        sys.exit(0)
     only_pade = "--pade" in sys.argv
     for name, opts in CASES.items():
         if not only_pade:
