@@ -102,7 +102,10 @@ typedef struct tt_run_params {
   int isospin_breaking_1S0; /* default 1 */
   int production_run;       /* default 1 */
   int precision;            /* TT_PRECISION_* (replaces solve_dense/Pade selection) */
-  double refine_tol;        /* refinement stop: estimated remaining max |dx|/|x| (default 1e-12) */
+  double refine_tol;        /* refinement stop (default 1e-12): estimated remaining relative error of every
+                               on-shell entry (each U element's own |dx|/|x|; elements below 1e-6 of the
+                               largest in their column, zero by symmetry up to rounding, against that
+                               fraction) and of the whole column (max |dx| / max |x|) */
   int refine_max_iter;      /* default 30 */
 } tt_run_params;
 
@@ -115,8 +118,9 @@ typedef struct tt_solve_report {
   double ms_solve;      /* triangular solves */
   double ms_refine;     /* FP64 refinement */
   int refine_iters;     /* max over energies */
-  double final_correction; /* estimated remaining relative error at exit: the last max|dx|/max|x|, or, once two
-                              corrections contract by rho < 1/2, that times rho / (1 - rho); max over rhs/energies */
+  double final_correction; /* estimated remaining relative error at exit, the worst of the on-shell entries'
+                              and the columns' measures of refine_tol: the last relative change, or, once two
+                              corrections contract by rho < 1/2, that times rho / (1 - rho); max over energies */
   int info;             /* first zero pivot (1-based), 0 if none */
   double ms_adjoint;    /* adjoint: transposed solves, their refinement, parameter products */
   int adjoint_refine_iters;

@@ -31,7 +31,27 @@ def load_case(name):
 
 
 def rel(a, b):
+    """Normwise relative difference max|a - b| / max|b|."""
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(1e-300, float(np.max(np.abs(b)))))
+
+
+# U elements below this fraction of the largest |U| of their channel are zero by
+# symmetry up to rounding (e.g. 1e-18 between uncoupled deuteron components of a
+# central potential); their relative error is taken against the fraction.
+ZERO_FLOOR = 1e-6
+
+
+def rel_elem(a, b):
+    """Per-element relative difference max_i |a_i - b_i| / |b_i|: the metric's
+    "relative error in every on-shell U element".  Elements with |b_i| below
+    ZERO_FLOOR * max|b| are measured against ZERO_FLOOR * max|b|."""
+    a = np.asarray(a).reshape(-1)
+    b = np.asarray(b).reshape(-1)
+    if b.size == 0:
+        return 0.0
+    den = np.maximum(np.abs(b), ZERO_FLOOR * float(np.max(np.abs(b))))
+    den = np.where(den > 0, den, 1e-300)
+    return float(np.max(np.abs(a - b) / den))
 
 
 @pytest.fixture(scope="session")

@@ -10,7 +10,7 @@ import pytest
 
 import harness as oracle
 import tictac_b200 as tt
-from conftest import load_case, rel
+from conftest import load_case, rel, rel_elem
 
 # central differences with h = 1e-5 of the potential scale: truncation ~ h^2,
 # rounding ~ 1e-16 / h; the adjoint of the refined mixed solve is refined in FP64
@@ -88,7 +88,7 @@ def test_adjoint_dropin_matches_finite_differences(precision):
         tail = (swp, g["q_idx"], oracle.deuterons(pwt), tt.PW(pwt))
         U, dU, rep = tt.solve_faddeev_adjoint(*args, g["V_unco"], g["V_coup"], *tail, dVu, dVc, precision=precision,
                                               **kw)
-        assert rel(U, g[f"U_c{c}"]) <= 1e-10
+        assert rel_elem(U, g[f"U_c{c}"]) <= 1e-10
         if precision == tt.PRECISION_MIXED:
             assert rep["adjoint_refine_iters"] >= 1
         for k in range(2):
@@ -130,7 +130,7 @@ def test_adjoint_run_handle_lec_gradients():
         U64, _ = run.solve(c, tt.PRECISION_FP64)
         for prec in (tt.PRECISION_FP64, tt.PRECISION_MIXED):
             U, dU, rep = run.solve_adjoint(c, dVu, dVc, prec)
-            assert rel(U, U64) <= 1e-10
+            assert rel_elem(U, U64) <= 1e-10
             for k in range(2):
                 h = 1e-5 * abs(run.lecs()[k])
                 Up, _ = tt.solve_faddeev(G, v, r, cp, Vu + h * dVu[k], Vc + h * dVc[k], swp, q_idx, deut, tt.PW(pwt),

@@ -4,7 +4,7 @@ import pytest
 
 import harness as oracle
 import tictac_b200 as tt
-from conftest import CASES, GOLDEN, load_case, rel
+from conftest import CASES, GOLDEN, load_case, rel, rel_elem
 
 pytestmark = pytest.mark.gpu
 
@@ -58,7 +58,7 @@ def test_solve_dropin_matches_reference(case, precision):
         U, rep = tt.solve_faddeev(g[f"G_c{c}"], v, r, cp, g["V_unco"], g["V_coup"], swp, g["q_idx"],
                                   oracle.deuterons(pwt), tt.PW(pwt), precision=precision,
                                   tensor_force=int(m["tensor_force"]), isospin_breaking_1S0=int(m["iso"]))
-        assert rel(U, g[f"U_c{c}"]) <= 1e-10, (c, rep)
+        assert rel_elem(U, g[f"U_c{c}"]) <= 1e-10, (c, rep)
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -68,7 +68,7 @@ def test_run_handle_end_to_end(case):
     for c in range(run.num_channels):
         for prec in (tt.PRECISION_FP64, tt.PRECISION_MIXED):
             U, rep = run.solve(c, prec)
-            assert rel(U, g[f"U_c{c}"]) <= 1e-10
+            assert rel_elem(U, g[f"U_c{c}"]) <= 1e-10
     run.close()
 
 
@@ -110,7 +110,7 @@ def test_larger_case_against_oracle():
         U_o = oracle.dense_solve(A_o, G_o, q_idx, oracle.deuterons(pw), Nq, Np)
         for prec in PRECISIONS:
             U, rep = run.solve(c, prec)
-            assert rel(U, U_o) <= 1e-10, (prec, rep)
+            assert rel_elem(U, U_o) <= 1e-10, (prec, rep)
     run.close()
 
 
@@ -134,7 +134,7 @@ def test_ragged_block_sizes_against_oracle(Np, Nq):
         U_o = oracle.dense_solve(A_o, G_o, q_idx, oracle.deuterons(pw), Nq, Np)
         for prec in PRECISIONS:
             U, rep = run.solve(c, prec)
-            assert rel(U, U_o) <= 1e-10, (c, prec, rep)
+            assert rel_elem(U, U_o) <= 1e-10, (c, prec, rep)
     run.close()
 
 
@@ -161,7 +161,7 @@ def test_full_size_channel_mixed_agrees_with_fp64():
     U64, _ = run.solve(c, tt.PRECISION_FP64)
     Um, rep = run.solve(c, tt.PRECISION_MIXED)
     assert rep["final_correction"] <= 1e-12 and rep["refine_iters"] >= 1
-    assert rel(Um, U64) <= 1e-10
+    assert rel_elem(Um, U64) <= 1e-10
     run.close()
 
 
@@ -195,7 +195,7 @@ def test_hbm_admission_reports_nomem_without_fault():
     g, m = load_case("mt_swave_n16")
     run = tt.Run(**m["opts"])
     U, _ = run.solve(0, tt.PRECISION_FP64)
-    assert rel(U, g["U_c0"]) <= 1e-10
+    assert rel_elem(U, g["U_c0"]) <= 1e-10
 
 
 def test_no_deuteron_states_gives_empty_U():
@@ -214,3 +214,78 @@ def test_kernel_launch_counter_advances():
     run = tt.Run(**m["opts"])
     run.solve(0, tt.PRECISION_MIXED)
     assert tt.kernel_launches() > before
+
+
+def _large_fixture_tools():
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from make_golden import pattern_hash, value_checksums, vector_checksums
+    return pattern_hash, value_checksums, vector_checksums
+
+
+@pytest.mark.parametrize("product", ["bf16x3", "tf32", "bf16x3_n128"])
+def test_bench_basis_n12_against_reference(product):
+    # The bench workload's basis (j <= 3, J <= 7/2, both parities) at Np = Nq = 12: eight channels,
+    # n = 3,888 .. 9,072, so 8 - 18 panels of 512 columns with the K = 512 tensor-core trailing updates,
+    # interchanges across panels and the two on-shell energies factored together.  Against the reference's
+    # own dense solve (zgetrf + zgetrs, nrhs = n): P123 pattern (hash) and values (checksums), G
+    # (checksums) and every on-shell U element, in FP64, in mixed precision with each tensor-core product
+    # and (once) on CUDA cores.
+    pattern_hash, value_checksums, vector_checksums = _large_fixture_tools()
+    g = np.load(f"{GOLDEN}/lo_j3_J7_n12.npz")
+    opts = dict(o.split("=", 1) for o in g["opts"])
+    run = tt.Run(**opts, tc_product=product)
+    assert run.num_channels == int(g["n_chn"])
+    T, E_com, q_idx = run.energies()
+    assert np.array_equal(q_idx, g["q_idx"])
+    precisions = [tt.PRECISION_MIXED] + ([tt.PRECISION_FP64, tt.PRECISION_MIXED_SIMT] if product == "bf16x3" else [])
+    for c in range(run.num_channels):
+        n = run.channel_info(c)["n"]
+        assert n == int(g[f"n_c{c}"])
+        if product == "bf16x3":
+            nnz = run.build_P123(c)
+            assert nnz == int(g[f"nnz_c{c}"])
+            rowptr, col, val = run.P123_csr(c, nnz)
+            rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rowptr))
+            assert pattern_hash(rows, col, n) == int(g[f"p123_hash_c{c}"])
+            assert rel(value_checksums(rows, col, val, n), g[f"p123_sums_c{c}"]) <= 1e-12
+            run.build_resolvent(c)
+            assert rel(vector_checksums(run.G(c).reshape(-1)), g[f"G_sums_c{c}"]) <= 1e-11
+        for prec in precisions:
+            U, rep = run.solve(c, prec)
+            err = rel_elem(U, g[f"U_c{c}"])
+            assert err <= 1e-10, (c, n, prec, err, rep)
+        run.release(c)
+    run.close()
+
+
+@pytest.mark.parametrize("batch", [2, 3, 4])
+def test_energy_batched_factorisation_matches_one_at_a_time(batch):
+    # Five on-shell bins (T_lab = 5, 30, 100 MeV) at n = 1,100 (ragged against every block size): the
+    # complex64 matrices factored in groups of 2+2+1, 3+2 and 4+1 energies (the batched sub-panel kernel
+    # splits its grid into one group of CTAs per matrix, with a remainder group of fewer matrices) give
+    # the U of the one-at-a-time factorisation bit for bit (same arithmetic per row, same pivots), and U
+    # matches the oracle per element.
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=1, Np_WP=10, Nq_WP=10, Nphi=16, Nx=16,
+                lab_energies="5,30,100")
+    base = tt.Run(**opts, energy_batch=1)
+    run = tt.Run(**opts, energy_batch=batch)
+    T, E_com, q_idx = run.energies()
+    assert len(T) == 5
+    Np = Nq = 10
+    for c in range(run.num_channels):
+        U1, _ = base.solve(c, tt.PRECISION_MIXED)
+        Ub, rep = run.solve(c, tt.PRECISION_MIXED)
+        assert np.array_equal(U1, Ub), (c, batch, rel_elem(Ub, U1))
+        pw = run.host_array(0, c).reshape(-1, 9)
+        nnz = run.build_P123(c)
+        rowptr, col, val = run.P123_csr(c, nnz)
+        rows = np.repeat(np.arange(len(rowptr) - 1, dtype=np.int32), np.diff(rowptr))
+        lay = oracle.layout(pw, Np, run.host_array(3), run.host_array(4), run.host_array(5), run.host_array(6),
+                            run.host_array(7), run.host_array(8))
+        G_o = np.stack([oracle.resolvent(lay, pw.shape[0], Nq, Np, run.host_array(2), e + run.E_bound) for e in E_com])
+        A_o = oracle.build_A(lay, pw.shape[0], Nq, Np, rows, col, val)
+        U_o = oracle.dense_solve(A_o, G_o, q_idx, oracle.deuterons(pw), Nq, Np)
+        assert rel_elem(Ub, U_o) <= 1e-10, (c, batch, rep)
+    base.close()
+    run.close()

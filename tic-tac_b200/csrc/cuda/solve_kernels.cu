@@ -1,6 +1,7 @@
 // Kernels of the Faddeev-solve stage other than the LU factorisation:
 // resolvent diagonals, the dense kernel matrix A = C^T (2 P123) (V C),
 // L = 1 - A diag(G), right-hand sides and the FP64 refinement residual.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -308,6 +309,16 @@ __global__ void k_axpy_norm(double2* __restrict__ x, const double2* __restrict__
   }
 }
 
+// On-shell entries after the update: out[k nrows + r] = (|d_k[rows[r]]|, |x_k[rows[r]]|)
+__global__ void k_onshell_pick(const double2* __restrict__ x, const double2* __restrict__ d, int n, int nrhs,
+                               const int32_t* __restrict__ rows, int nrows, double2* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrhs * nrows) return;
+  const int k = t / nrows, r = t % nrows;
+  const size_t i = (size_t)k * n + rows[r];
+  out[t] = make_double2(hypot(d[i].x, d[i].y), hypot(x[i].x, x[i].y));
+}
+
 }  // namespace
 
 int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d_G, cudaStream_t st) {
@@ -403,23 +414,49 @@ int residual_multi_device(const double* d_A, int n, const double* d_y, const dou
   return TT_OK;
 }
 
-int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_ratio, cudaStream_t st) {
+int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_ratio, cudaStream_t st,
+                      const int32_t* d_rows, int nrows, double* h_elem) {
+  if (!d_rows || !h_elem) nrows = 0;
+  // [2 nrhs] maxima as ordered bit patterns, then nrhs x nrows (|d|, |x|) pairs
+  const size_t words = 2 * (size_t)nrhs + 2 * (size_t)nrhs * nrows;
   DevBuf<unsigned long long> mx;
-  TT_TRY(mx.alloc(2 * (size_t)nrhs));
+  TT_TRY(mx.alloc(words));
   TT_CUDA_TRY(cudaMemsetAsync(mx.ptr, 0, sizeof(unsigned long long) * 2 * nrhs, st));
   k_axpy_norm<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<double2*>(d_x),
                                                               reinterpret_cast<const double2*>(d_d), n, nrhs, mx.ptr,
                                                               mx.ptr + nrhs);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
-  std::vector<unsigned long long> h(2 * (size_t)nrhs);
-  TT_CUDA_TRY(cudaMemcpyAsync(h.data(), mx.ptr, sizeof(unsigned long long) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
+  if (nrows > 0) {
+    k_onshell_pick<<<ceil_div((size_t)nrhs * nrows, 64), 64, 0, st>>>(
+        reinterpret_cast<const double2*>(d_x), reinterpret_cast<const double2*>(d_d), n, nrhs, d_rows, nrows,
+        reinterpret_cast<double2*>(mx.ptr + 2 * nrhs));
+    count_launch();
+    TT_CUDA_TRY(cudaGetLastError());
+  }
+  std::vector<unsigned long long> h(words);
+  TT_CUDA_TRY(cudaMemcpyAsync(h.data(), mx.ptr, sizeof(unsigned long long) * words, cudaMemcpyDeviceToHost, st));
   TT_CUDA_TRY(cudaStreamSynchronize(st));
   for (int k = 0; k < nrhs; k++) {
     double dm, xm;
     memcpy(&dm, &h[k], 8);
     memcpy(&xm, &h[nrhs + k], 8);
     h_ratio[k] = xm > 0 ? dm / xm : dm;
+  }
+  if (nrows > 0) {
+    // each on-shell entry's own |dx| / |x|; entries below kOnshellZeroFloor of
+    // the largest on-shell |x| of their right-hand side are zero by symmetry
+    // up to rounding and are measured against that floor instead
+    const double* pr = reinterpret_cast<const double*>(h.data() + 2 * nrhs);
+    for (int k = 0; k < nrhs; k++) {
+      double big = 0;
+      for (int r = 0; r < nrows; r++) big = std::max(big, pr[2 * ((size_t)k * nrows + r) + 1]);
+      for (int r = 0; r < nrows; r++) {
+        const double dv = pr[2 * ((size_t)k * nrows + r)], xv = pr[2 * ((size_t)k * nrows + r) + 1];
+        const double den = std::max(xv, kOnshellZeroFloor * big);
+        h_elem[(size_t)k * nrows + r] = den > 0 ? dv / den : dv;
+      }
+    }
   }
   return TT_OK;
 }

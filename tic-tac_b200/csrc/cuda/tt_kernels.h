@@ -141,8 +141,16 @@ int spmv_t_device(const DeviceCSR& P, const double* d_u, int nrhs, double* d_g, 
 // out[a nb + b] = sum_i g_a[i] h_b[i], complex, na, nb <= 4
 int bilinear_device(int n, const double* d_g, int na, const double* d_h, int nb, double* d_out, cudaStream_t st);
 
+// On-shell U elements smaller than this fraction of the largest one of their
+// column are zero by symmetry up to rounding: their relative change is taken
+// against the fraction instead of their own magnitude.
+constexpr double kOnshellZeroFloor = 1e-6;
 // x += d ; returns max |d| / max |x| per rhs in h_ratio (host, synchronises).
-int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_dx_over_x, cudaStream_t st);
+// With d_rows (nrows entries), also each on-shell entry's relative change
+// |d_k[rows[r]]| / max(|x_k[rows[r]]|, kOnshellZeroFloor max_r |x_k[rows[r]]|)
+// in h_elem[k nrows + r].
+int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h_dx_over_x, cudaStream_t st,
+                      const int32_t* d_rows = nullptr, int nrows = 0, double* h_elem = nullptr);
 
 // Device count of SMs, cached.
 int device_sm_count();
