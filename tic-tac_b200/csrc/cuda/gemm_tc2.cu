@@ -1,0 +1,595 @@
+// Tensor-core trailing update of the complex64 LU on sm_100a, real-row form:
+//
+//   C[M x N] -= L[M x K] U[K x N]     (complex, C row-major complex64 in place)
+//
+// A complex row of L, read as 2K reals [Lr0, Li0, Lr1, Li1, ...], times the two
+// real rows that column j of U gives,
+//   re-row j: [Ur0j, -Ui0j, Ur1j, -Ui1j, ...]   im-row j: [Ui0j, Ur0j, Ui1j, Ur1j, ...]
+// is Re(LU)_ij and Im(LU)_ij.  So one real product of depth 2K with N = 256
+// B rows (128 re-rows, then the 128 im-rows of the same columns) produces a
+// 128 x 128 complex tile in one tcgen05.mma per k step, the re and im halves
+// of the accumulator landing in TMEM columns [0,128) and [128,256).  Against
+// four separate real products this reads each L tile from shared memory once
+// per k step instead of twice.
+//
+// Two operand precisions:
+//   TF32    one kind::tf32 product (K = 8 per instruction); L is read by TMA
+//           straight from the matrix (the tensor core uses the top 19 bits of
+//           each fp32), U's rows are packed rounded to tf32 (cvt.rna)
+//   BF16X3  x = hi + lo in bf16, hi.hi + hi.lo + lo.hi (kind::f16, K = 16);
+//           L and U rows packed into hi/lo planes
+// Accumulation in FP32 in TMEM, double-buffered (2 x 256 columns).
+//
+// Kernel organisation (one CTA per SM, persistent over 128 x 128 tiles):
+//   warp 0      TMA producer into a 4-stage ring (16 complex k per stage)
+//   warp 1      MMA issuer (one elected thread)
+//   warps 2..9  epilogue: C of the tile's first column chunk is loaded while
+//               the accumulator fills; per 16-column chunk the C loads are
+//               issued before the tcgen05.ld of the accumulator slice, then a
+//               coalesced C -= acc store
+// Every mbarrier wait is bounded in time; on expiry the kernel records an
+// error code, drains its own copies in flight, frees TMEM and returns.
+// No TMA load here uses cluster multicast.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "tt_kernels.h"
+#include "tt_lu_internal.h"
+
+namespace tt {
+namespace tc2 {
+
+constexpr int BM = 128;         // rows per tile (MMA M)
+constexpr int BN = 128;         // complex columns per tile (MMA N = 2 BN real rows of B)
+constexpr int KCC = 16;         // complex k per stage = 32 real k
+constexpr int STAGES = 4;
+constexpr int TMEM_COLS = 512;  // 2 accumulators x (BN re + BN im)
+constexpr int EPI_WARPS = 8;
+constexpr int NUM_THREADS = 64 + 32 * EPI_WARPS;
+constexpr int EPI_STAGE_BYTES = 32 * 16 * 8;
+constexpr uint64_t WAIT_NS = 2000000000ull;
+
+// Per-mode layout of one stage.  TF32: 32 real k in fp32 = 128 B rows,
+// SWIZZLE_128B.  BF16X3: 32 real k in bf16 = 64 B rows, SWIZZLE_64B, hi and lo
+// planes.  Every tile below is a multiple of 1 KB, so 1 KB alignment holds.
+template <int MODE>
+struct Cfg;
+template <>
+struct Cfg<TC_TF32> {
+  static constexpr int ROW_BYTES = 128;
+  static constexpr int PARTS = 1;
+  static constexpr int A_TILE = BM * ROW_BYTES;            // 16 KB
+  static constexpr int B_TILE = 2 * BN * ROW_BYTES;        // 32 KB (re-rows then im-rows)
+  static constexpr int STAGE = PARTS * (A_TILE + B_TILE);  // 48 KB
+  static constexpr int KSTEPS = 4;                         // k8 steps of 32 B per stage
+  static constexpr int TERMS = 1;
+  static constexpr uint32_t SBO = 1024;                    // 8-row swizzle atom
+  static constexpr uint64_t LAYOUT = 2;                    // SWIZZLE_128B
+};
+template <>
+struct Cfg<TC_BF16X3> {
+  static constexpr int ROW_BYTES = 64;
+  static constexpr int PARTS = 2;
+  static constexpr int A_TILE = BM * ROW_BYTES;            // 8 KB per part
+  static constexpr int B_TILE = 2 * BN * ROW_BYTES;        // 16 KB per part
+  static constexpr int STAGE = PARTS * (A_TILE + B_TILE);  // 48 KB
+  static constexpr int KSTEPS = 2;                         // k16 steps of 32 B per stage
+  static constexpr int TERMS = 3;                          // hi.hi, hi.lo, lo.hi
+  static constexpr uint32_t SBO = 512;
+  static constexpr uint64_t LAYOUT = 4;                    // SWIZZLE_64B
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false if the phase did not complete within WAIT_NS or another
+// role of this launch already reported an error.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  const uint64_t t0 = now_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*(volatile int*)err != 0) return false;
+    if (now_ns() - t0 > WAIT_NS) {
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+          "r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// K-major swizzled operand descriptor (tcgen05 shared-memory matrix descriptor).
+template <int MODE>
+__device__ __forceinline__ uint64_t op_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);    // start address
+  d |= (uint64_t)1 << 16;                      // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(Cfg<MODE>::SBO >> 4) << 32;  // stride byte offset: next 8-row atom
+  d |= (uint64_t)1 << 46;                      // descriptor version for tcgen05
+  d |= Cfg<MODE>::LAYOUT << 61;
+  return d;
+}
+
+// Instruction descriptor: D f32, A/B tf32 (2) or bf16 (1), K-major, M = 128, N = 256.
+template <int MODE>
+__host__ __device__ constexpr uint32_t idesc() {
+  constexpr uint32_t ab = (MODE == TC_TF32) ? 2u : 1u;
+  return (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)((2 * BN) >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+template <int MODE>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  constexpr uint32_t id = idesc<MODE>();
+  if constexpr (MODE == TC_TF32) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(id), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(id), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+  }
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+struct TileSched {
+  int tiles_m, tiles_n, group;
+  __device__ void coords(int t, int& tm, int& tn) const {
+    // bands of `group` row tiles swept across all column tiles (keeps a band
+    // of L rows and the current U columns resident in L2)
+    const int per_group = group * tiles_n;
+    const int g = t / per_group;
+    const int first_m = g * group;
+    const int gm = min(group, tiles_m - first_m);
+    const int r = t % per_group;
+    tm = first_m + r % gm;
+    tn = r / gm;
+  }
+};
+
+// C loads of one 16-column chunk of a 32-row slice: cv[i] = C[row0 + r][gcol0 + c], idx = i*32 + lane.
+__device__ __forceinline__ void load_c_chunk(const float2* __restrict__ C, int ldc, int M, int N, int row0, int gcol0,
+                                             int lane, float2 (&cv)[16]) {
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    const int idx = i * 32 + lane, r = idx >> 4, c = idx & 15;
+    const int grow = row0 + r, gcol = gcol0 + c;
+    cv[i] = (grow < M && gcol < N) ? __ldcs(&C[(size_t)grow * ldc + gcol]) : make_float2(0.f, 0.f);
+  }
+}
+
+// tmA: L as [rows][2K] reals (TF32: the matrix itself or a packed copy; BF16X3:
+// hi plane rows [0, M), lo plane rows [a_plane, a_plane + M)).  tmB: U as
+// [2N][2K] reals per plane (re-rows [0, N), im-rows [N, 2N); BF16X3: lo plane
+// at row offset 2N).  K complex depth, a multiple of KCC.
+template <int MODE>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    k_lu_update_tc2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    float2* __restrict__ C, int ldc, int M, int N, int K, int a_plane, int* err) {
+  using CF = Cfg<MODE>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float2* epi_stage = (float2*)(smem + STAGES * CF::STAGE);
+  uint64_t* full = (uint64_t*)(smem + STAGES * CF::STAGE + EPI_WARPS * EPI_STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;
+  uint64_t* acc_empty = acc_full + 2;
+  uint32_t* tmem_base_slot = (uint32_t*)(acc_empty + 2);
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int kchunks = K / KCC;
+  TileSched sched{(M + BM - 1) / BM, (N + BN - 1) / BN, 16};
+  const int ntiles = sched.tiles_m * sched.tiles_n;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], EPI_WARPS);  // one arrival per epilogue warp
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_base_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_base_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        int tm, tn;
+        sched.coords(t, tm, tn);
+        for (int kc = 0; kc < kchunks && ok; kc++, it++) {
+          const int s = it % STAGES;
+          const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+          if (it >= STAGES && !mbar_wait(&empty[s], ph ^ 1u, err, 1)) {
+            ok = false;
+            break;
+          }
+          unsigned char* st = smem + s * CF::STAGE;
+          mbar_expect_tx(&full[s], CF::STAGE);
+          const int x = kc * 2 * KCC;  // real k offset: 32 reals per stage
+#pragma unroll
+          for (int p = 0; p < CF::PARTS; p++) {
+            unsigned char* a = st + p * (CF::A_TILE + CF::B_TILE);
+            tma_load_2d(a, &tmA, &full[s], x, p * a_plane + tm * BM);
+            tma_load_2d(a + CF::A_TILE, &tmB, &full[s], x, p * 2 * N + tn * BN);
+            tma_load_2d(a + CF::A_TILE + CF::B_TILE / 2, &tmB, &full[s], x, p * 2 * N + N + tn * BN);
+          }
+        }
+      }
+      // drain: wait (bounded) until every issued load has landed before exit
+      for (int j = (it > STAGES ? it - STAGES : 0); j < it; j++)
+        mbar_wait(&full[j % STAGES], (uint32_t)(j / STAGES) & 1u, err, 5);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      // BF16X3 terms (A plane, B plane): hi.hi, hi.lo, lo.hi
+      const int ta[3] = {0, 0, 1};
+      const int tb[3] = {0, 1, 0};
+      int it = 0, local = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, local++) {
+        const int ab = local & 1;
+        const uint32_t aph = (uint32_t)(local >> 1) & 1u;
+        if (local >= 2 && !mbar_wait(&acc_empty[ab], aph ^ 1u, err, 2)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + ab * (2 * BN);
+        for (int kc = 0; kc < kchunks; kc++, it++) {
+          const int s = it % STAGES;
+          const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+          if (!mbar_wait(&full[s], ph, err, 3)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t s0 = smem_u32(smem + s * CF::STAGE);
+#pragma unroll
+          for (int ks = 0; ks < CF::KSTEPS; ks++) {
+#pragma unroll
+            for (int q = 0; q < CF::TERMS; q++) {
+              const uint32_t a0 = s0 + ta[q] * (CF::A_TILE + CF::B_TILE);
+              const uint32_t b0 = s0 + tb[q] * (CF::A_TILE + CF::B_TILE) + CF::A_TILE;
+              const uint64_t ad = op_desc<MODE>(a0 + ks * 32);
+              const uint64_t bd = op_desc<MODE>(b0 + ks * 32);
+              umma<MODE>(d, ad, bd, (kc == 0 && ks == 0 && q == 0) ? 0u : 1u);
+            }
+          }
+          umma_commit(&empty[s]);  // stage reusable once these MMAs completed
+        }
+        if (!ok) break;
+        umma_commit(&acc_full[ab]);
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2..9): warp w reads TMEM lane quarter
+    // w % 4 (the hardware lane-access rule) and column half (w - 2) / 4
+    const int quarter = warp & 3;
+    const int half = (warp - 2) >> 2;
+    float2* stage = epi_stage + (size_t)(warp - 2) * (32 * 16);
+    int local = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, local++) {
+      int tm, tn;
+      sched.coords(t, tm, tn);
+      const int ab = local & 1;
+      const uint32_t aph = (uint32_t)(local >> 1) & 1u;
+      const int row0 = tm * BM + quarter * 32;
+      float2 cv[16];
+      // the first chunk's C is fetched while the accumulator fills
+      load_c_chunk(C, ldc, M, N, row0, tn * BN + half * (BN / 2), lane, cv);
+      if (!mbar_wait(&acc_full[ab], aph, err, 4)) break;
+      tc_fence_after();
+      const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16) + ab * (2 * BN);
+#pragma unroll 1
+      for (int cc = 0; cc < BN / 2; cc += 16) {
+        const int col = half * (BN / 2) + cc;
+        const int gcol0 = tn * BN + col;
+        if (cc > 0) load_c_chunk(C, ldc, M, N, row0, gcol0, lane, cv);
+        float re[16], im[16];
+        tmem_ld16(lane_addr + col, re);
+        tmem_ld16(lane_addr + BN + col, im);
+        // stage this thread's row (row = lane) with an XOR swizzle on the column
+#pragma unroll
+        for (int j = 0; j < 16; j++) stage[lane * 16 + (j ^ (lane & 15))] = make_float2(re[j], im[j]);
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int idx = i * 32 + lane, r = idx >> 4, c = idx & 15;
+          const int grow = row0 + r, gcol = gcol0 + c;
+          const float2 a = stage[r * 16 + (c ^ (r & 15))];
+          if (grow < M && gcol < N) C[(size_t)grow * ldc + gcol] = make_float2(cv[i].x - a.x, cv[i].y - a.y);
+        }
+        __syncwarp();
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[ab]);
+    }
+  }
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+  }
+}
+
+// ---- operand packing
+
+__device__ __forceinline__ float round_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// L rows as [M][2K] reals.  TF32: one fp32 plane (used when the matrix itself
+// cannot be read by TMA); BF16X3: hi plane rows [0, M), lo plane [M, 2M).
+template <int MODE>
+__global__ void k_pack_A(const float2* __restrict__ L, int ldl, int M, int K, void* __restrict__ WA) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (size_t)M * K) return;
+  const int i = (int)(tid / K), kk = (int)(tid % K);
+  const float2 v = L[(size_t)i * ldl + kk];
+  if constexpr (MODE == TC_TF32) {
+    reinterpret_cast<float2*>(WA)[(size_t)i * K + kk] = v;
+  } else {
+    __nv_bfloat162* w = reinterpret_cast<__nv_bfloat162*>(WA);
+    const __nv_bfloat162 hi = __floats2bfloat162_rn(v.x, v.y);
+    const float2 hf = __bfloat1622float2(hi);
+    w[(size_t)i * K + kk] = hi;
+    w[(size_t)M * K + (size_t)i * K + kk] = __floats2bfloat162_rn(v.x - hf.x, v.y - hf.y);
+  }
+}
+
+// Column j of U as its re-row [Ur, -Ui, ...] (row j) and im-row [Ui, Ur, ...]
+// (row N + j) of a [2N][2K] real plane; BF16X3 adds the lo plane at row 2N.
+template <int MODE>
+__global__ void k_pack_B(const float2* __restrict__ U, int ldu, int K, int N, void* __restrict__ WB) {
+  __shared__ float2 tile[32][33];
+  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const int kk = k0 + r, j = j0 + tx;
+    float2 v = make_float2(0.f, 0.f);
+    if (kk < K && j < N) v = U[(size_t)kk * ldu + j];
+    tile[r][tx] = v;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int j = j0 + r, kk = k0 + tx;
+    if (j < N && kk < K) {
+      const float2 v = tile[tx][r];
+      const size_t re_at = (size_t)j * K + kk, im_at = (size_t)(N + j) * K + kk;  // in pairs of reals
+      if constexpr (MODE == TC_TF32) {
+        float2* w = reinterpret_cast<float2*>(WB);
+        const float ur = round_tf32(v.x), ui = round_tf32(v.y);
+        w[re_at] = make_float2(ur, -ui);
+        w[im_at] = make_float2(ui, ur);
+      } else {
+        __nv_bfloat162* w = reinterpret_cast<__nv_bfloat162*>(WB);
+        const size_t lo = (size_t)2 * N * K;
+        const __nv_bfloat162 hre = __floats2bfloat162_rn(v.x, -v.y);
+        const __nv_bfloat162 him = __floats2bfloat162_rn(v.y, v.x);
+        const float2 fre = __bfloat1622float2(hre), fim = __bfloat1622float2(him);
+        w[re_at] = hre;
+        w[im_at] = him;
+        w[lo + re_at] = __floats2bfloat162_rn(v.x - fre.x, -v.y - fre.y);
+        w[lo + im_at] = __floats2bfloat162_rn(v.y - fim.x, v.x - fim.y);
+      }
+    }
+  }
+}
+
+}  // namespace tc2
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn2() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// 2D real tensor [rows][cols] with row pitch `pitch_bytes`, box = one swizzle
+// row (32 reals) x box_rows.
+int make_map2(CUtensorMap* map, int mode, void* base, uint64_t rows, uint64_t cols, uint64_t pitch_bytes,
+              uint32_t box_rows) {
+  EncodeTiledFn fn = encode_fn2();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return TT_ERR_CUDA;
+  }
+  const bool tf32 = mode == TC_TF32;
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {pitch_bytes};
+  const cuuint32_t box[2] = {32, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        tf32 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return TT_ERR_CUDA;
+  }
+  return TT_OK;
+}
+
+struct TC2Workspace {
+  DevBuf<unsigned char> WA, WB;
+  DevBuf<int> err;
+  int attr_dev[2] = {-1, -1};  // device on which each mode's shared-memory attribute was set
+};
+
+TC2Workspace& workspace2() {
+  static thread_local TC2Workspace ws;
+  return ws;
+}
+
+template <int MODE>
+int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
+               cudaStream_t st) {
+  using CF = tc2::Cfg<MODE>;
+  TC2Workspace& ws = workspace2();
+  const size_t esz = (MODE == TC_TF32) ? 4 : 2;
+  // the matrix itself is the TF32 A operand when TMA can address it: 16-byte
+  // aligned base and row pitch (the panel's x offsets are multiples of 32 reals)
+  const bool direct_A = MODE == TC_TF32 && ((uintptr_t)L % 16 == 0) && ((size_t)ldl * 8 % 16 == 0);
+  const size_t needA = direct_A ? 0 : (size_t)CF::PARTS * M * 2 * K * esz;
+  const size_t needB = (size_t)CF::PARTS * 2 * N * 2 * K * esz;
+  if (needA > ws.WA.count) TT_TRY(ws.WA.alloc(needA));
+  if (needB > ws.WB.count) TT_TRY(ws.WB.alloc(needB));
+  if (!ws.err.ptr) {
+    TT_TRY(ws.err.alloc(1));
+    TT_CUDA_TRY(cudaMemsetAsync(ws.err.ptr, 0, sizeof(int), st));
+  }
+  if (!direct_A) {
+    tc2::k_pack_A<MODE><<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L, ldl, M, K, ws.WA.ptr);
+    count_launch();
+    TT_CUDA_TRY(cudaGetLastError());
+  }
+  dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
+  tc2::k_pack_B<MODE><<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  CUtensorMap mA, mB;
+  if (direct_A)
+    TT_TRY(make_map2(&mA, MODE, const_cast<float2*>(L), (uint64_t)M, (uint64_t)2 * K, (uint64_t)ldl * 8, tc2::BM));
+  else
+    TT_TRY(make_map2(&mA, MODE, ws.WA.ptr, (uint64_t)CF::PARTS * M, (uint64_t)2 * K, (uint64_t)2 * K * esz,
+                     tc2::BM));
+  TT_TRY(make_map2(&mB, MODE, ws.WB.ptr, (uint64_t)CF::PARTS * 2 * N, (uint64_t)2 * K, (uint64_t)2 * K * esz,
+                   tc2::BN));
+  const size_t smem = (size_t)tc2::STAGES * CF::STAGE + tc2::EPI_WARPS * tc2::EPI_STAGE_BYTES + 1024 + 128;
+  int dev = 0;
+  TT_CUDA_TRY(cudaGetDevice(&dev));
+  const int slot = MODE == TC_TF32 ? 0 : 1;
+  if (ws.attr_dev[slot] != dev) {
+    TT_CUDA_TRY(cudaFuncSetAttribute(tc2::k_lu_update_tc2<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    ws.attr_dev[slot] = dev;
+  }
+  const int tiles = ((M + tc2::BM - 1) / tc2::BM) * ((N + tc2::BN - 1) / tc2::BN);
+  const int grid = std::min(tiles, device_sm_count());
+  {
+    ProfScope prof(TT_PROF_TC_UPDATE, st, 8.0 * M * N * K, 16.0 * M * N + 8.0 * ((double)M + N) * K);
+    tc2::k_lu_update_tc2<MODE><<<grid, tc2::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, M, ws.err.ptr);
+  }
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+}  // namespace
+
+int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
+                 cudaStream_t st) {
+  if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
+  if (K % tc2::KCC != 0) {
+    set_error("tensor-core update needs K to be a multiple of 16");
+    return TT_ERR_BADARG;
+  }
+  if (mode == TC_TF32) return launch_tc2<TC_TF32>(C, ldc, L, ldl, U, ldu, M, N, K, st);
+  if (mode == TC_BF16X3) return launch_tc2<TC_BF16X3>(C, ldc, L, ldl, U, ldu, M, N, K, st);
+  set_error("unknown tensor-core product mode " + std::to_string(mode));
+  return TT_ERR_BADARG;
+}
+
+int tc2_check_error(cudaStream_t st) {
+  TC2Workspace& ws = workspace2();
+  if (!ws.err.ptr) return TT_OK;
+  int h = 0;
+  TT_CUDA_TRY(cudaMemcpyAsync(&h, ws.err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h != 0) {
+    TT_CUDA_TRY(cudaMemsetAsync(ws.err.ptr, 0, sizeof(int), st));
+    set_error("tensor-core update timed out waiting on a pipeline barrier (code " + std::to_string(h) + ")");
+    return TT_ERR_CUDA;
+  }
+  return TT_OK;
+}
+
+}  // namespace tt

@@ -567,15 +567,18 @@ int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st) {
   return TT_OK;
 }
 
-// C -= L U inside the panel: on the tensor cores when the factorisation uses
-// them and K is a multiple of their 32-wide k-chunk, else on the CUDA cores
+// C -= L U on the tensor cores in the factorisation's product mode when K is
+// a multiple of the mode's k-chunk, else on the CUDA cores
 template <typename T>
-int panel_gemm_sub(bool tc, T* C, int ldc, const T* L, int ldl, const T* U, int ldu, int M, int N, int K,
+int panel_gemm_sub(int mode, T* C, int ldc, const T* L, int ldl, const T* U, int ldu, int M, int N, int K,
                    cudaStream_t st) {
   if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
-  if (tc && K % 32 == 0)
+  if (mode == TC_LEGACY_BF16X3 && K % 32 == 0)
     return tc_gemm_sub(reinterpret_cast<float2*>(C), ldc, reinterpret_cast<const float2*>(L), ldl,
                        reinterpret_cast<const float2*>(U), ldu, M, N, K, st);
+  if ((mode == TC_TF32 || mode == TC_BF16X3) && K % 16 == 0)
+    return tc2_gemm_sub(mode, reinterpret_cast<float2*>(C), ldc, reinterpret_cast<const float2*>(L), ldl,
+                        reinterpret_cast<const float2*>(U), ldu, M, N, K, st);
   return gemm_sub(C, ldc, L, ldl, U, ldu, M, N, K, st);
 }
 
@@ -584,7 +587,12 @@ int panel_gemm_sub(bool tc, T* C, int ldc, const T* L, int ldl, const T* U, int 
 template <typename T>
 int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, cudaStream_t st, int use_tc,
                              int* info) {
-  const bool tc = use_tc != 0;
+  const int mode = use_tc;
+  const bool tc = mode != 0;
+  if (mode < 0 || mode > TC_BF16X3) {
+    set_error("unknown tensor-core product mode " + std::to_string(mode));
+    return TT_ERR_BADARG;
+  }
   if (tc && sizeof(T) != sizeof(float2)) {
     set_error("tensor-core trailing update is only defined for the complex64 factorisation");
     return TT_ERR_UNSUPPORTED;
@@ -668,7 +676,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
         const int right = k + kb - (j0 + w);
         if (right > 0) {
           TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
-          TT_TRY(panel_gemm_sub(tc, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
+          TT_TRY(panel_gemm_sub(mode, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
                                 A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
         }
       }
@@ -686,19 +694,25 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
         TT_TRY(trsm_blk(A, n, i0, wi, k + kb, n, st));
         const int below = k + kb - (i0 + wi);
         if (below > 0)
-          TT_TRY(panel_gemm_sub(tc, A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
+          TT_TRY(panel_gemm_sub(mode, A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
                                 A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
       }
       // ---- trailing update
-      if (tc) {
+      if (mode == TC_LEGACY_BF16X3) {
         TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
+      } else if (tc) {
+        const int r0 = k + kb;
+        TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)r0 * n + r0, n,
+                            reinterpret_cast<const float2*>(A) + (size_t)r0 * n + k, n,
+                            reinterpret_cast<const float2*>(A) + (size_t)k * n + r0, n, rest, rest, kb, st));
       } else {
         TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
                         A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
       }
     }
   }
-  if (tc) TT_TRY(tc_check_error(st));
+  if (mode == TC_LEGACY_BF16X3) TT_TRY(tc_check_error(st));
+  if (mode == TC_TF32 || mode == TC_BF16X3) TT_TRY(tc2_check_error(st));
   if (info) {
     TT_CUDA_TRY(cudaMemcpyAsync(info, d_info.ptr, sizeof(int) * B, cudaMemcpyDeviceToHost, st));
     TT_CUDA_TRY(cudaStreamSynchronize(st));

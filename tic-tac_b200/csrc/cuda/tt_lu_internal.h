@@ -12,6 +12,16 @@ int lu_update_tc(float2* A, int n, int k, int nb, cudaStream_t st);
 
 // Reports (and clears) a barrier timeout recorded by the tensor-core kernel.
 int tc_check_error(cudaStream_t st);
+
+// Product modes of the complex64 factorisation's updates (the use_tensor_cores
+// argument of lu_factor_batched_device); 0 = CUDA-core FP32 updates.
+constexpr int TC_LEGACY_BF16X3 = 1;  // gemm_tc.cu: four real products, N = 128, BF16x3 (12 MMAs per k16)
+constexpr int TC_TF32 = 2;           // gemm_tc2.cu: real-row form, N = 256, one tf32 product
+constexpr int TC_BF16X3 = 3;         // gemm_tc2.cu: real-row form, N = 256, BF16x3 (3 MMAs per k16)
+// C[M x N] -= L[M x K] U[K x N] in the real-row form (gemm_tc2.cu), K % 16 == 0.
+int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
+                 cudaStream_t st);
+int tc2_check_error(cudaStream_t st);
 // C[M x N] -= L[M x K] U[K x N], complex64 row-major operands, K % 64 == 0.
 int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
                 cudaStream_t st);

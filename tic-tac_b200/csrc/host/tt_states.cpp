@@ -55,7 +55,12 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       rp.precision = value;
     } else if (key == "refine_tol") rp.refine_tol = std::stod(value);
     else if (key == "refine_max_iter") rp.refine_max_iter = std::stoi(value);
-    else if (key == "energy_batch") {
+    else if (key == "tc_product") {
+      if (value == "bf16x3_n128") rp.tc_product = 1;
+      else if (value == "tf32") rp.tc_product = 2;
+      else if (value == "bf16x3") rp.tc_product = 3;
+      else return bad("tc_product (tf32, bf16x3 or bf16x3_n128)");
+    } else if (key == "energy_batch") {
       rp.energy_batch = std::stoi(value);
       if (rp.energy_batch < 1 || rp.energy_batch > 4) return bad("energy_batch (1..4)");
     }
