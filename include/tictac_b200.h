@@ -292,8 +292,14 @@ int tt_run_build_A(tt_run* run, int chn, double* ms);
 int tt_run_build_resolvent(tt_run* run, int chn);
 /* Solve all on-shell energies of the channel; U as in tt_solve_faddeev_equations. */
 int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_report* report);
-/* Release the channel's device data (all of it, or only A and the resolvents,
- * keeping P123 resident for the next parameter set or energy scan). */
+/* tt_run_solve for a subset of the run's on-shell energies: energy_idx[n_sel]
+ * indexes tt_run_energies (distinct); U[d'*nd*n_sel + d*n_sel + s] for energy
+ * energy_idx[s].  The unit of work a scan is sharded by across GPUs, one
+ * (channel, energy) item or a group of them (the reference shards whole
+ * channels across processes, CPP/main.cpp:168-170).  The channel's resident
+ * resolvents afterwards hold the selected energies; tt_run_solve rebuilds them. */
+int tt_run_solve_energies(tt_run* run, int chn, int precision, int n_sel, const int* energy_idx, tt_complex* U,
+                          tt_solve_report* report);
 /* tt_run_solve plus dU/dtheta (see tt_solve_faddeev_adjoint), for dV/dtheta
  * arrays over all 2N channels of the run (sizes as tt_run_get_host_array
  * which = 3 and 4). */
@@ -317,6 +323,8 @@ int tt_run_store_P123_h5(const tt_run* run, int chn, const char* filename);
  * against the run's state space; filename NULL = the reference's name in the
  * run's P123_folder. */
 int tt_run_load_P123_h5(tt_run* run, int chn, const char* filename, int64_t* nnz);
+/* Release the channel's device data (all of it, or only A and the resolvents,
+ * keeping P123 resident for the next parameter set or energy scan). */
 int tt_run_release_channel(tt_run* run, int chn);
 int tt_run_release_A(tt_run* run, int chn);
 

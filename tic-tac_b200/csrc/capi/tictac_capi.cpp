@@ -520,6 +520,38 @@ int tt_run_solve(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_re
   return TT_OK;
 }
 
+int tt_run_solve_energies(tt_run* run, int chn, int precision, int n_sel, const int* energy_idx, tt_complex* U,
+                          tt_solve_report* report) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!U || n_sel < 0 || (n_sel > 0 && !energy_idx)) return fail(TT_ERR_BADARG, "null or negative argument");
+  if (precision < TT_PRECISION_FP64 || precision > TT_PRECISION_PADE) return fail(TT_ERR_BADARG, "unknown precision");
+  const int nE = (int)run->os.E_com.size();
+  std::vector<double> E;
+  std::vector<int> q;
+  for (int k = 0; k < n_sel; k++) {
+    const int j = energy_idx[k];
+    if (j < 0 || j >= nE) return fail(TT_ERR_BADARG, "energy index " + std::to_string(j) + " outside the run's bins");
+    for (int k2 = 0; k2 < k; k2++)
+      if (energy_idx[k2] == j) return fail(TT_ERR_BADARG, "energy index listed twice");
+    E.push_back(run->os.E_com[j] + run->swp.E_bound);  // CPP/main.cpp:391
+    q.push_back(run->os.q_com_idx[j]);
+  }
+  double msA = 0;
+  if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
+  // the channel's resolvents now hold the selected energies only
+  run->chn[chn].have_G = false;
+  TT_TRY(run->chn[chn].solver->resolvent(E, run_stream(run)));
+  const std::vector<int> deut = deuteron_indices(channel_view(run->pw, chn));
+  std::vector<double> Uh;
+  SolveReport rep;
+  s = run->chn[chn].solver->solve(q, deut, options_of(run->rp, precision), Uh, &rep, run_stream(run));
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  return TT_OK;
+}
+
 int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const double* dVu, const double* dVc,
                          tt_complex* U, tt_complex* dU, tt_solve_report* report) {
   int s = check_chn(run, chn);

@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = (
     "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc", "tt_profile_begin", "tt_profile_end",
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
+    "tt_run_solve_energies",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build")
@@ -457,6 +458,16 @@ class Run:
         U = np.zeros(nE * nd * nd, dtype=np.complex128)
         rep = tt_solve_report()
         _check(self.lib.tt_run_solve(self._h, chn, precision, U.ctypes.data_as(c_void_p), byref(rep)))
+        return U, rep.as_dict()
+
+    def solve_energies(self, chn, energy_idx, precision=PRECISION_MIXED):
+        """tt_run_solve_energies: U of the selected on-shell energies, [d'][d][s] flattened."""
+        idx = np.ascontiguousarray(energy_idx, dtype=np.int32)
+        nd = self.channel_info(chn)["n_deuteron"]
+        U = np.zeros(len(idx) * nd * nd, dtype=np.complex128)
+        rep = tt_solve_report()
+        _check(self.lib.tt_run_solve_energies(self._h, chn, precision, len(idx), _iptr(idx) if len(idx) else None,
+                                              U.ctypes.data_as(c_void_p), byref(rep)))
         return U, rep.as_dict()
 
     def solve_adjoint(self, chn, dV_unco, dV_coup, precision=PRECISION_MIXED):
