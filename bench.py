@@ -12,9 +12,16 @@ LU-factorised per energy, on-shell columns solved and refined to 1e-12.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU: one process per GPU (torchrun); rank r solves its own pair of
-on-shell energies (T_lab = 10 + 6 r MeV) for all channels -- independent
-replicas over the energy scan, no collective on the data path (weak scaling).
+Multi-GPU: one process per GPU (torchrun).  On N GPUs the workload is a scan
+of N lab energies with 2N distinct on-shell bins; its (channel, energies)
+items (each channel's bins in pairs, weighted by n^3) are assigned to the
+ranks longest-processing-time first, each rank builds P123 and A only for the
+channels it owns, and the U arrays are gathered on rank 0 in the reference's
+layout.  No collective on the data path (weak scaling: the items grow with N).
+
+--impl reference times the reference's own dense LAPACK path (the compiled
+reference, oracle/_ref/tictac_ref) on the host cores; it loads nothing of this
+repository's library.
 """
 import argparse
 import json
@@ -138,13 +145,23 @@ def step_flops(ns, nE):
 # DRAM traffic of the tensor-core update per algorithmic byte (C read + written
 # as complex64, L and U panels read once): dram__bytes_read.sum +
 # dram__bytes_write.sum over 16 M N + 8 (M + N) K for two launches (M = N = 7536
-# and 7280, K = 256) of the n = 9072 capture in profiles/k_lu_update_tc_n9072.md
+# and 7280, K = 256) of an ncu capture of the n = 9072 channel
 # (926.4 / 939.5 MB and 861.2 / 877.8 MB); traffic grows with the tile count, so
 # the ratio scales the bench's mean launch to a per-launch traffic figure.
 TC_TRAFFIC_PER_ALGO_BYTE = 0.984
 
 
-def roofline_of(kern, timed_ms, ms_step, ns, nE):
+# Tensor work per algorithmic complex flop of each product and the kernel
+# that runs it: BF16x3 takes 3 bf16 products; TF32 one product at half the
+# bf16 rate
+PRODUCTS = {
+    "bf16x3": (3.0, "k_lu_update_tc2<BF16X3> (complex64 C -= L U, real-row form, BF16x3 on tcgen05)"),
+    "tf32": (2.0, "k_lu_update_tc2<TF32> (complex64 C -= L U, real-row form, TF32 on tcgen05)"),
+    "bf16x3_n128": (3.0, "k_lu_update_tc (complex64 C -= L U, four real products, BF16x3 on tcgen05)"),
+}
+
+
+def roofline_of(kern, timed_ms, ms_step, ns, nE, product="bf16x3"):
     """Roofline of the dominant kernel class over the timed region: algorithmic
     flops (or bytes) per launch over the CUDA-event time per launch."""
     hbm, tf_burst, tf_sust, peak_kind = load_peaks()
@@ -161,19 +178,20 @@ def roofline_of(kern, timed_ms, ms_step, ns, nE):
         return None, kernels
     per_launch_s = k["ms"] * 1e-3 / k["launches"]
     if dom == "tc_update":
-        # complex64 product in BF16x3: 3 bf16 tensor products per fp32-accurate
-        # product, so the tensor roofline for algorithmic flops is peak / 3;
-        # the kernel runs inside a seconds-long step -> sustained figure
+        # the tensor roofline for algorithmic flops is the bf16 peak over the
+        # product's cost factor; the kernel runs inside a seconds-long step,
+        # so the sustained figure
+        factor, kname = PRODUCTS[product]
         achieved = k["flops"] / k["launches"] / per_launch_s / 1e12
-        peak = tf_sust / 3.0
+        peak = tf_sust / factor
         traffic = None
         if TC_TRAFFIC_PER_ALGO_BYTE:
             traffic = TC_TRAFFIC_PER_ALGO_BYTE * k["bytes"] / k["launches"]
         roof = {"bound": "tensor", "achieved": round(achieved, 2), "peak": round(peak, 1), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
-                "kernel": "k_lu_update_tc (complex64 trailing update C -= L U, BF16x3 on tcgen05)",
+                "kernel": kname,
                 "flops_per_launch": k["flops"] / k["launches"], "ms_per_launch": round(per_launch_s * 1e3, 3),
-                "peak_source": f"{peak_kind} bf16_tflops_sustained {tf_sust} / 3 (BF16x3 split factor)"}
+                "peak_source": f"{peak_kind} bf16_tflops_sustained {tf_sust} / {factor:g} ({product} product)"}
     else:
         achieved = k["bytes"] / k["launches"] / per_launch_s / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
@@ -183,29 +201,62 @@ def roofline_of(kern, timed_ms, ms_step, ns, nE):
     return roof, kernels
 
 
+def scan_lab_energies(cfg, world):
+    """Lab energies of the workload at `world` GPUs: T_lab = 10 MeV (two
+    on-shell bins) on one GPU; on N GPUs the scan continues with N - 1 further
+    lab energies placed between the next pairs of bin mid-points, so every lab
+    energy brings two new on-shell bins (2N bins in all) and the (channel,
+    energy) items grow with N."""
+    if world == 1:
+        return [10.0]
+    import tictac_b200 as tt
+    probe = tt.Run(**dict(cfg, lab_energies=",".join(str(x) for x in np.arange(1.0, 400.0, 0.5))))
+    T, _, _ = probe.energies()
+    probe.close()
+    T = list(T)
+    k0 = next(i for i in range(len(T) - 1) if T[i] <= 10.0 <= T[i + 1])
+    if k0 + 2 * world > len(T):
+        raise SystemExit(f"the q grid has no {2 * world} on-shell bins above 10 MeV")
+    return [10.0] + [0.5 * (T[k0 + 2 * r] + T[k0 + 2 * r + 1]) for r in range(1, world)]
+
+
+def elem_rel(a, b, floor=1e-6):
+    """Relative error of every element of a against b (elements below `floor`
+    of max|b| are zero by symmetry up to rounding and measured against it)."""
+    a, b = np.asarray(a).reshape(-1), np.asarray(b).reshape(-1)
+    if b.size == 0:
+        return 0.0
+    den = np.maximum(np.abs(b), floor * float(np.max(np.abs(b))))
+    return float(np.max(np.abs(a - b) / np.where(den > 0, den, 1e-300)))
+
+
 def run_ours(args, world, rank, local, pg):
     import tictac_b200 as tt
-    os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
+    from tictac_b200 import shard
     cfg = dict(CONFIGS[args.config])
-    cfg["lab_energies"] = str(10.0 + 6.0 * rank)
+    lab = scan_lab_energies(cfg, world)
+    cfg["lab_energies"] = ",".join(f"{x:.12g}" for x in lab)
+    cfg["tc_product"] = args.tc_product
     prec = tt.PRECISION_MIXED if args.precision == "mixed" else tt.PRECISION_FP64
     t_setup = time.perf_counter()
     run = tt.Run(**cfg)
-    chans = [int(c) for c in args.channels.split(",")] if args.channels else list(range(run.num_channels))
-    nch = len(chans)
-    infos = [run.channel_info(c) for c in chans]
+    all_chans = [int(c) for c in args.channels.split(",")] if args.channels else list(range(run.num_channels))
+    infos_all = [run.channel_info(c) for c in range(run.num_channels)]
     T_lab, E_com, q_idx = run.energies()
     nE = len(T_lab)
-    nnz = [run.build_P123(c) for c in chans]  # resident for the whole run
+    # (channel, energies) items over the ranks, longest processing time first
+    plans = shard.plan([infos_all[c]["n"] for c in all_chans], nE, world, group=2)
+    mine = {all_chans[i]: js for i, js in plans[rank].items()}
+    infos = [infos_all[c] for c in all_chans]
+    nnz = {c: run.build_P123(c) for c in mine}  # resident for the whole run
     t_setup = time.perf_counter() - t_setup
 
     def one_step():
-        Us = []
-        for c in chans:
+        Us = {}
+        for c, js in mine.items():
             run.build_A(c)
-            run.build_resolvent(c)
-            U, rep = run.solve(c, prec)
-            Us.append(U)
+            U, rep = run.solve_energies(c, js, prec)
+            Us[c] = (js, U)
             run.release_A(c)
         return Us
 
@@ -218,17 +269,24 @@ def run_ours(args, world, rank, local, pg):
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             run.timer_start()
-            one_step()
+            Us = one_step()
             times.append(run.timer_stop())
     kern = tt.profile_end()
     launches = tt.kernel_launches() - launches0
     barrier(pg)
     ms_step = allreduce_max(pg, float(np.mean(times)))
-    energies_per_step = nE * world
+    energies_per_step = nE  # every channel at every on-shell energy of the scan, over all ranks
     value = energies_per_step / (ms_step * 1e-3)
-    roofline, kernels = roofline_of(kern, float(np.sum(times)), ms_step, [i["n"] for i in infos], nE)
+    roofline, kernels = roofline_of(kern, float(np.sum(times)), float(np.mean(times)),
+                                    [infos_all[c]["n"] for c, js in mine.items() for _ in js], 1, args.tc_product)
+    # U of every (channel, energy) gathered on rank 0 in the reference's layout
+    gathered = shard.gather_to_rank0(pg, Us)
+    U_all = None
+    if rank == 0:
+        U_all = shard.assemble_U(gathered, [infos_all[c]["n_deuteron"] if c in all_chans else 0
+                                            for c in range(run.num_channels)], nE)
 
-    # end to end through the drop-in C-ABI call with host buffers
+    # end to end through the drop-in C-ABI call with host buffers, this rank's items
     e2e = None
     if args.e2e_steps > 0:
         host = []
@@ -243,19 +301,20 @@ def run_ours(args, world, rank, local, pg):
         n_unco = len(e_unco) // (Np + 1)
         n_coup = len(e_coup) // (2 * (Np + 1))
         swp = tt.SWP(Np, Nq, n_unco, n_coup, run.E_bound, e_unco, e_coup, C_unco, C_coup, q_WP)
-        for i, c in enumerate(chans):
-            rowptr, col, val = run.P123_csr(c, nnz[i])
-            n = infos[i]["n"]
+        for c, js in mine.items():
+            rowptr, col, val = run.P123_csr(c, nnz[c])
+            n = infos_all[c]["n"]
             rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rowptr))
             order = np.lexsort((rows, col))
             colptr = np.zeros(n + 1, dtype=np.uint64)
             np.add.at(colptr, col + 1, 1)
             colptr = np.cumsum(colptr).astype(np.uint64)
             run.build_resolvent(c)
-            G = run.G(c).reshape(-1)
+            G = run.G(c).reshape(nE, n)[js].reshape(-1)
             pwt = run.host_array(0, c).reshape(-1, 9)
             deut = [a for a in range(len(pwt)) if tuple(pwt[a, :4]) == (0, 1, 1, 0)]
-            host.append((G, val[order].copy(), rows[order].copy(), colptr, tt.PW(pwt, cfg["J_2N_max"]), deut))
+            host.append((G, val[order].copy(), rows[order].copy(), colptr, tt.PW(pwt, cfg["J_2N_max"]), deut,
+                         q_idx[js]))
             run.release(c)
         # inputs live in pinned host memory, as a caller streaming channels would keep them
         import torch
@@ -273,12 +332,13 @@ def run_ours(args, world, rank, local, pg):
         host = [tuple(pin(x) if isinstance(x, np.ndarray) else x for x in h) for h in host]
         V_unco, V_coup = pin(V_unco), pin(V_coup)
         h2d = sum(h[0].nbytes + h[1].nbytes + h[2].nbytes + h[3].nbytes for h in host) + \
-            nch * (V_unco.nbytes + V_coup.nbytes + C_unco.nbytes + C_coup.nbytes + e_unco.nbytes + e_coup.nbytes)
-        d2h = sum(16 * nE * len(h[5]) ** 2 for h in host)
+            len(host) * (V_unco.nbytes + V_coup.nbytes + C_unco.nbytes + C_coup.nbytes + e_unco.nbytes +
+                         e_coup.nbytes)
+        d2h = sum(16 * len(h[6]) * len(h[5]) ** 2 for h in host)
 
         def e2e_step():
-            for (G, v, r, cp, pw, deut) in host:
-                tt.solve_faddeev(G, v, r, cp, V_unco, V_coup, swp, q_idx, deut, pw, precision=prec)
+            for (G, v, r, cp, pw, deut, qs) in host:
+                tt.solve_faddeev(G, v, r, cp, V_unco, V_coup, swp, qs, deut, pw, precision=prec)
 
         e2e_step()
         barrier(pg)
@@ -289,94 +349,141 @@ def run_ours(args, world, rank, local, pg):
             te.append(time.perf_counter() - t0)
         t_e2e = allreduce_max(pg, float(np.mean(te)))
         e2e = {"value": round(energies_per_step / t_e2e, 6), "unit": "energies/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "timer": "host perf_counter around the synchronous C-ABI call"}
-    # the metric's comparison: mixed+refined against the plain FP64 solve on the
-    # smallest channel (same inputs, same energies), outside the timed region
+               "d2h_bytes_per_step": int(d2h), "timer": "host perf_counter around the synchronous C-ABI calls"}
+    # the metric's comparison: the same step in FP64 against the mixed+refined
+    # solve, every channel (or the smallest with --fp64-check 1), with the
+    # relative error of every on-shell U element
     fp64 = None
-    if args.fp64_check and prec == tt.PRECISION_MIXED:
-        i = min(range(nch), key=lambda k: infos[k]["n"])
-        c = chans[i]
-        run.build_A(c)
-        run.build_resolvent(c)
-        Um, rm = run.solve(c, tt.PRECISION_MIXED)
-        U64, r64 = run.solve(c, tt.PRECISION_FP64)
-        t_m = rm["ms_form"] + rm["ms_factor"] + rm["ms_solve"] + rm["ms_refine"]
-        t_64 = r64["ms_form"] + r64["ms_factor"] + r64["ms_solve"] + r64["ms_refine"]
-        fp64 = {"channel": c, "n": infos[i]["n"], "mixed_ms": round(t_m, 1), "fp64_ms": round(t_64, 1),
-                "speedup": round(t_64 / t_m, 2), "refine_iters": rm["refine_iters"],
-                "max_rel_diff_U": float(np.max(np.abs(Um - U64)) / np.max(np.abs(U64)))}
-        # adjoint: dU/dLEC for the potential's contact constants on the same channel
+    if args.fp64_check and prec == tt.PRECISION_MIXED and world == 1:
+        cmp_chans = all_chans if args.fp64_check >= 2 else [min(all_chans, key=lambda c: infos_all[c]["n"])]
+        rows, t_mix, t_64, worst = [], 0.0, 0.0, 0.0
+        for c in cmp_chans:
+            run.timer_start()
+            run.build_A(c)
+            run.build_resolvent(c)
+            Um, rm = run.solve(c, tt.PRECISION_MIXED)
+            tm = run.timer_stop()
+            run.timer_start()
+            run.build_A(c)
+            run.build_resolvent(c)
+            U64, r64 = run.solve(c, tt.PRECISION_FP64)
+            t64 = run.timer_stop()
+            err = elem_rel(Um, U64)
+            worst = max(worst, err)
+            t_mix += tm
+            t_64 += t64
+            rows.append({"channel": c, "n": infos_all[c]["n"], "mixed_ms": round(tm, 1), "fp64_ms": round(t64, 1),
+                         "speedup": round(t64 / tm, 2), "refine_iters": rm["refine_iters"],
+                         "final_correction": rm["final_correction"], "max_elem_rel_err_U": err,
+                         "fp64_lu_tflops": round(8.0 / 3.0 * infos_all[c]["n"] ** 3 * nE / (r64["ms_factor"] * 1e-3)
+                                                 / 1e12, 2)})
+            if c != cmp_chans[0]:
+                run.release_A(c)
+        fp64 = {"channels": len(cmp_chans), "mixed_ms": round(t_mix, 1), "fp64_ms": round(t_64, 1),
+                "fp64_value": nE / (t_64 * 1e-3) if len(cmp_chans) == len(all_chans) else None,
+                "speedup": round(t_64 / t_mix, 2), "max_elem_rel_err_U": worst, "per_channel": rows}
+        c = cmp_chans[0]
+        # adjoint: dU/dLEC for the potential's contact constants on the first channel
         nl = len(run.lecs())
         if nl:
             dV = [run.lec_derivative(k) for k in range(nl)]
             Ua, dU, ra = run.solve_adjoint(c, np.stack([d[0] for d in dV]), np.stack([d[1] for d in dV]),
                                            tt.PRECISION_MIXED)
             t_f = ra["ms_form"] + ra["ms_factor"] + ra["ms_solve"] + ra["ms_refine"]
-            fp64["adjoint"] = {"n_theta": nl, "forward_ms": round(t_f, 1), "adjoint_ms": round(ra["ms_adjoint"], 1),
+            fp64["adjoint"] = {"channel": c, "n_theta": nl, "forward_ms": round(t_f, 1),
+                               "adjoint_ms": round(ra["ms_adjoint"], 1),
                                "adjoint_over_forward": round(ra["ms_adjoint"] / t_f, 3),
                                "adjoint_refine_iters": ra["adjoint_refine_iters"],
                                "max_abs_dU_dLEC": float(np.max(np.abs(dU)))}
         # the reference's production path: Pade-resummed Neumann series (about 1e-6)
         Up, rpd = run.solve(c, tt.PRECISION_PADE)
-        fp64["pade"] = {"ms": round(rpd["ms_solve"], 1), "order": rpd["refine_iters"],
+        U64, _ = run.solve(c, tt.PRECISION_FP64)
+        fp64["pade"] = {"channel": c, "ms": round(rpd["ms_solve"], 1), "order": rpd["refine_iters"],
                         "max_rel_diff_U_vs_fp64": float(np.max(np.abs(Up - U64)) / np.max(np.abs(U64)))}
         run.release_A(c)
     return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, kernels=kernels, e2e=e2e,
-                infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times, launches=launches, fp64=fp64)
+                infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times, launches=launches, fp64=fp64,
+                lab=lab, plan=plans, U_all=U_all)
 
 
-REF_SAMPLE_N = 12
+# Np = Nq of the reference's timed sample: channel 0 of the workload's basis at
+# this grid (n = 6,075 for j <= 3, J <= 7/2), about 10 s per step of both
+# on-shell energies on 16 host threads, so 25 steps stay within minutes
+REF_SAMPLE_N = 15
+REF_BIN = os.path.join(HERE, "oracle", "_ref", "tictac_ref")
 
 
-def reference_sample(args, sample_N=REF_SAMPLE_N, channel=None):
-    """Time the reference's own dense LAPACK solve (oracle/_ref/tictac_ref,
-    OpenMP + OpenBLAS on all host cores) on one channel of the same physics at
-    Np_WP = Nq_WP = sample_N and scale to the workload by n^3."""
-    binp = os.path.join(HERE, "oracle", "_ref", "tictac_ref")
-    if not os.path.exists(binp):
+def _ref_opts(cfg, N, energies="10"):
+    opts = [f"{k}={v}" for k, v in cfg.items() if k not in ("Np_WP", "Nq_WP")]
+    return opts + [f"Np_WP={N}", f"Nq_WP={N}", f"lab_energies={energies}"]
+
+
+def _read_meta(path):
+    chans, steps, timing = [], [], {}
+    with open(path) as f:
+        for line in f:
+            tok = line.split()
+            if not tok:
+                continue
+            if tok[0] == "chn":
+                chans.append({k: float(v) if "." in v or "e" in v else int(v) for k, v in zip(tok[::2], tok[1::2])})
+            elif tok[0] == "step":
+                steps.append(dict(zip(tok[::2], [float(x) for x in tok[1::2]])))
+            elif tok[0] == "timing":
+                timing = dict(zip(tok[1::2], tok[2::2]))
+    return chans, steps, timing
+
+
+def reference_info(cfg):
+    """Channel sizes, on-shell energies and deuteron states of the workload from
+    the reference build's own state-space set-up (tictac_ref info)."""
+    if not os.path.exists(REF_BIN):
         return None, "oracle/_ref/tictac_ref not built"
-    cfg = dict(CONFIGS[args.config])
+    with tempfile.TemporaryDirectory() as out:
+        subprocess.run([REF_BIN, "info", out] + _ref_opts(cfg, cfg["Np_WP"]), check=True, cwd=out,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=600)
+        chans, _, _ = _read_meta(os.path.join(out, "meta.txt"))
+    return [{"n": c["n"], "nE": c["nE"], "nd": c["nd"]} for c in chans], None
+
+
+def reference_sample(cfg, steps, sample_N=REF_SAMPLE_N, channel=0):
+    """The reference's own dense LAPACK solve (oracle/_ref/tictac_ref: A columns,
+    then per energy L = 1 - A G, R = A, zgetrf + zgetrs with nrhs = n; OpenMP +
+    OpenBLAS on all host cores) of one channel of the workload's basis at
+    Np = Nq = sample_N, set up once and timed for `steps` repetitions."""
+    if not os.path.exists(REF_BIN):
+        return None, "oracle/_ref/tictac_ref not built"
     cores = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as out:
-        opts = [f"{k}={v}" for k, v in cfg.items() if k not in ("Np_WP", "Nq_WP")]
-        opts += [f"Np_WP={sample_N}", f"Nq_WP={sample_N}", "lab_energies=10"]
-        ch = channel if channel is not None else 0
-        cmd = [binp, "time", out, f"--channel={ch}"] + opts
+        cmd = [REF_BIN, "time", out, f"--channel={channel}", f"--repeat={steps}"] + _ref_opts(cfg, sample_N)
         t0 = time.perf_counter()
         subprocess.run(cmd, check=True, cwd=out, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
-                       env=dict(os.environ, OMP_NUM_THREADS=str(cores)), timeout=900)
+                       env=dict(os.environ, OMP_NUM_THREADS=str(cores)), timeout=3000)
         wall = time.perf_counter() - t0
-        t = {}
-        with open(os.path.join(out, "meta.txt")) as f:
-            for line in f:
-                tok = line.split()
-                if tok and tok[0] == "timing":
-                    t = dict(zip(tok[1::2], tok[2::2]))
-                if tok and tok[0] == "chn":
-                    meta = dict(zip(tok[::2], tok[1::2]))
-    n_s = int(t["n"])
+        chans, st, t = _read_meta(os.path.join(out, "meta.txt"))
+    meta = chans[0]
     nE = int(meta["nE"])
-    per_energy = (float(t["t_A"]) + float(t["t_getrf_getrs"])) / nE
-    return dict(n_sample=n_s, per_energy_s=per_energy, t_A=float(t["t_A"]) / nE,
-                t_lu=float(t["t_getrf_getrs"]) / nE, t_fair=float(t["t_fair"]) / nE,
-                t_p123=float(meta["t_p123"]), cores=cores, wall=wall), None
+    return dict(n_sample=int(t["n"]), nE=nE, step_s=[x["t"] for x in st], t_A=float(t["t_A"]),
+                t_fair=float(t["t_fair"]) / nE, t_p123=float(meta["t_p123"]), cores=cores, wall=wall,
+                sample_N=sample_N), None
 
 
-def cpu_phases(ref, infos):
-    """Per-phase seconds of the reference sample (per energy, P123 once per
-    channel) and the energies/s a fairer CPU path would reach: the same A
-    columns, then zgetrf + zgetrs with only the nd on-shell right-hand sides
-    instead of nrhs = n, extrapolated by n^3 like the value."""
-    fair = 1.0 / sum((ref["t_A"] + ref["t_fair"]) * (i["n"] / ref["n_sample"]) ** 3 for i in infos)
-    return {"sample_n": ref["n_sample"], "p123_s": round(ref["t_p123"], 4), "A_columns_s": round(ref["t_A"], 4),
-            "zgetrf_zgetrs_nrhs_n_s": round(ref["t_lu"], 4), "zgetrf_zgetrs_nrhs_nd_s": round(ref["t_fair"], 4),
-            "fair_value": fair}
-
-
-def cpu_value_for(infos, ref):
-    # seconds per energy for all channels of the workload, scaled by n^3
-    s = sum(ref["per_energy_s"] * (i["n"] / ref["n_sample"]) ** 3 for i in infos)
-    return 1.0 / s
+def reference_value(ref, infos, timed):
+    """Energies/s of the reference path over the workload from the sample's
+    timed steps: per energy, the A columns (rebuilt for every energy, as the
+    reference's faddeev_dense_solver does, scaled by n^2 Np) and the L/R
+    formation and LAPACK solve (scaled by n^3) for every channel."""
+    n_s, N_s = ref["n_sample"], ref["sample_N"]
+    lu = float(np.mean(timed)) / ref["nE"]
+    factor = sum((i["n"] / n_s) ** 3 for i in infos)
+    a_factor = sum((i["n"] / n_s) ** 2 * (i["N"] / N_s) for i in infos)
+    per_energy = lu * factor + ref["t_A"] * a_factor
+    fair = ref["t_fair"] * factor + ref["t_A"] * a_factor
+    return 1.0 / per_energy, {"sample_n": n_s, "sample_Np_Nq": N_s, "extrapolation_factor_n3": round(factor, 1),
+                              "p123_s": round(ref["t_p123"], 4), "A_columns_s": round(ref["t_A"], 4),
+                              "form_zgetrf_zgetrs_nrhs_n_s_per_energy": round(lu, 4),
+                              "zgetrf_zgetrs_nrhs_nd_s_per_energy": round(ref["t_fair"], 4),
+                              "fair_value": 1.0 / fair}
 
 
 def main():
@@ -387,80 +494,98 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=list(CONFIGS), default="j3_J7_n30")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--tc-product", choices=list(PRODUCTS), default="bf16x3",
+                    help="tensor-core product of the complex64 LU")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--fp64-check", type=int, default=1, help="time FP64 vs mixed on the smallest channel")
+    ap.add_argument("--fp64-check", type=int, default=2,
+                    help="FP64 step against mixed: 0 off, 1 smallest channel, 2 every channel")
     ap.add_argument("--channels", default="", help="comma list of channel indices to step (default: all)")
     args = ap.parse_args()
-    world, rank, local, pg = dist_setup()
     cfg = CONFIGS[args.config]
-    config = {"workload": f"{args.config}: LO-OPEP (stands in for N3LO-Idaho), j<=3, J<=7/2 both parities, "
-                          f"Np=Nq={cfg['Np_WP']}, T_lab=10 MeV (rank r: 10+6r MeV)",
-              "channels_per_step": None, "energies_per_rank": None, "parallelism": f"replicas x{world}",
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    config = {"workload": f"{args.config}: LO-OPEP (stands in for N3LO-Idaho), j<={cfg['J_2N_max']}, "
+                          f"J<={cfg['two_J_3N_max']}/2 both parities, Np=Nq={cfg['Np_WP']}, T_lab=10 MeV on one GPU "
+                          f"(two on-shell bins); on N GPUs a scan of N lab energies with 2N distinct on-shell bins",
+              "channels_per_step": None, "energies_per_step": None,
+              "parallelism": f"(channel, energy) items over {world} GPU(s), longest processing time first",
               "l2": "inputs larger than L2 (A is 25.7 GB for the largest channel)"}
 
     if args.impl == "reference":
-        if rank != 0:
+        # the reference's own CPU path; nothing of this repository's library is loaded
+        if int(os.environ.get("RANK", "0")) != 0:
             return
-        import tictac_b200 as tt
-        run = tt.Run(**dict(cfg, lab_energies="10"))
-        infos = [run.channel_info(c) for c in range(run.num_channels)]
-        nE = len(run.energies()[0])
-        run.close()
+        infos, why = reference_info(cfg)
+        if infos is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        for i in infos:
+            i["N"] = cfg["Np_WP"]
+        nE = infos[0]["nE"]
+        ref, why = reference_sample(cfg, args.warmup + max(1, args.steps))
+        if ref is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        timed = ref["step_s"][args.warmup:]
+        v, phases = reference_value(ref, infos, timed)
         config["channels_per_step"] = len(infos)
-        config["energies_per_rank"] = nE
+        config["energies_per_step"] = nE
         config["n_per_channel"] = [i["n"] for i in infos]
-        samples = []
-        for _ in range(args.warmup + max(1, args.steps)):
-            r2, why = reference_sample(args)
-            if r2 is None:
-                print(json.dumps({"impl": "reference", "unavailable": why}))
-                return
-            samples.append(r2)
-        ref = dict(samples[-1])
-        for k in ("per_energy_s", "t_A", "t_lu", "t_fair"):
-            ref[k] = float(np.mean([x[k] for x in samples[args.warmup:]]))
-        v = cpu_value_for(infos, ref)
-        sample = (f"reference dense LAPACK solve (A columns + zgetrf + zgetrs nrhs=n) of channel 0 at "
-                  f"Np=Nq={REF_SAMPLE_N} (n={ref['n_sample']}), T_lab=10 MeV, {ref['cores']} threads, "
-                  f"extrapolated by n^3 to every channel of the workload")
+        sample = (f"reference dense LAPACK solve (A columns, then per energy L/R formation + zgetrf + zgetrs "
+                  f"nrhs=n) of channel 0 at Np=Nq={ref['sample_N']} (n={ref['n_sample']}), both on-shell "
+                  f"energies of T_lab=10 MeV per step, {ref['cores']} threads; extrapolated to the workload by "
+                  f"sum over channels of (n/{ref['n_sample']})^3 = {phases['extrapolation_factor_n3']}")
         print(json.dumps({"metric": METRIC, "value": v, "unit": "energies/s", "impl": "reference", "n_gpus": world,
-                          "steps": args.steps, "warmup": args.warmup, "ms_step": nE / v * 1e3,
+                          "steps": args.steps, "warmup": args.warmup,
+                          "ms_step": round(float(np.mean(timed)) * 1e3, 3),
+                          "ms_step_note": "measured time of one sample step (n above); value is extrapolated",
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
                           "data": "synthetic (seeded LO potential)", "config": config,
                           "cpu_baseline": {"value": v, "unit": "energies/s", "cores": ref["cores"],
-                                           "kind": "reference", "sample": sample,
-                                           "phases": cpu_phases(ref, infos)},
-                          "e2e": {"value": v, "unit": "energies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+                                           "kind": "reference", "sample": sample, "phases": phases},
+                          "e2e": {"value": v, "unit": "energies/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
         return
 
+    world, rank, local, pg = dist_setup()
     r = run_ours(args, world, rank, local, pg)
     if rank == 0:
         config["channels_per_step"] = len(r["infos"])
-        config["energies_per_rank"] = r["nE"]
+        config["energies_per_step"] = r["nE"]
+        config["lab_energies_mev"] = [round(x, 6) for x in r["lab"]]
         config["n_per_channel"] = [i["n"] for i in r["infos"]]
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            ref, why = reference_sample(args)
+            infos = [dict(i, N=cfg["Np_WP"]) for i in r["infos"]]
+            ref, why = reference_sample(cfg, 1)
             if ref is not None:
-                v = cpu_value_for(r["infos"], ref)
+                v, phases = reference_value(ref, infos, ref["step_s"])
                 cpu = {"value": v, "unit": "energies/s", "cores": ref["cores"], "kind": "reference",
-                       "sample": f"reference dense LAPACK solve of channel 0 at Np=Nq={REF_SAMPLE_N} (n={ref['n_sample']}), "
-                                 f"scaled by n^3 to all {len(r['infos'])} channels",
-                       "phases": cpu_phases(ref, r["infos"])}
+                       "sample": f"reference dense LAPACK solve of channel 0 at Np=Nq={ref['sample_N']} "
+                                 f"(n={ref['n_sample']}), one step of both energies, extrapolated by "
+                                 f"{phases['extrapolation_factor_n3']} (sum of (n/n_sample)^3) to all "
+                                 f"{len(infos)} channels",
+                       "phases": phases}
+        fp = r["fp64"]
+        prod = args.tc_product
         out = {"metric": METRIC, "value": round(r["value"], 6), "unit": "energies/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_step": round(r["ms_step"], 3),
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-               "dtype": "complex64 LU (BF16x3 tcgen05) + FP64 refinement" if args.precision == "mixed" else "complex128",
+               "dtype": (f"complex64 LU (tcgen05 {prod} products) + FP64 refinement" if args.precision == "mixed"
+                         else "complex128"),
                "data": "synthetic (chiral LO potential on the reference's default Chebyshev WP grid)",
                "config": config, "clocks": r["clocks"], "roofline": r["roofline"], "cpu_baseline": cpu,
                "e2e": r["e2e"], "gpu_launches": int(r["launches"]),
-               "channel_solves_per_s": round(len(r["infos"]) * r["nE"] * world / (r["ms_step"] * 1e-3), 4),
-               "kernels": r["kernels"], "fp64_comparison": r["fp64"], "setup_s": round(r["t_setup"], 3)}
+               "mixed_over_fp64": (round(r["value"] / fp["fp64_value"], 3)
+                                   if fp and fp.get("fp64_value") else None),
+               "max_elem_rel_err_U_vs_fp64": fp["max_elem_rel_err_U"] if fp else None,
+               "channel_solves_per_s": round(len(r["infos"]) * r["nE"] / (r["ms_step"] * 1e-3), 4),
+               "kernels": r["kernels"], "fp64_comparison": fp, "setup_s": round(r["t_setup"], 3),
+               "U_gathered": {"channels": len(r["U_all"]), "energies": r["nE"],
+                              "layout": "U[d' nd nE + d nE + j] per channel on rank 0"}}
         print(json.dumps(out))
     if pg is not None:
         pg.destroy_process_group()
-
 
 if __name__ == "__main__":
     main()
