@@ -172,6 +172,8 @@ def roofline_of(kern, timed_ms, ms_step, ns, nE, product="bf16x3"):
                              "share_of_timed": round(k["ms"] / timed_ms, 4),
                              "tflops": round(k["flops"] / (k["ms"] * 1e-3) / 1e12, 2) if k["ms"] else None,
                              "gbs": round(k["bytes"] / (k["ms"] * 1e-3) / 1e9, 1) if k["ms"] else None}
+    # launch gaps and kernels outside the classes: the rest of the timed region
+    kernels["unattributed"] = {"share_of_timed": round(1.0 - sum(k["ms"] for k in kern.values()) / timed_ms, 4)}
     dom = max(kern, key=lambda nm: kern[nm]["ms"])
     k = kern[dom]
     if k["launches"] == 0:

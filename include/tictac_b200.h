@@ -235,7 +235,19 @@ unsigned long long tt_kernel_launches(void);
 #define TT_PROF_TRSV 2
 #define TT_PROF_RESIDUAL 3
 #define TT_PROF_A_BUILD 4
-#define TT_PROF_COUNT 5
+/*   PANEL_TRSM  U = L^-1 X for the 32-wide unit-lower blocks of the panels: 4 w^2 cols flops
+ *   OPERANDS    packing the tensor-core operands (splits, real-row planes): bytes read + written
+ *   LASWP       row interchanges: 4 swaps cols sizeof(elem) bytes
+ *   FORM_L      L = 1 - A G: 8 n^2 bytes read + n^2 sizeof(elem) written
+ *   SUBST_PREP  inverted diagonal blocks of the substitutions and their neighbour products
+ *   SIMT_UPDATE C -= L U on the CUDA cores (complex128 factorisation, small K): 8 M N K flops */
+#define TT_PROF_PANEL_TRSM 5
+#define TT_PROF_OPERANDS 6
+#define TT_PROF_LASWP 7
+#define TT_PROF_FORM_L 8
+#define TT_PROF_SUBST_PREP 9
+#define TT_PROF_SIMT_UPDATE 10
+#define TT_PROF_COUNT 11
 typedef struct tt_kernel_profile {
   unsigned long long launches;
   double ms;

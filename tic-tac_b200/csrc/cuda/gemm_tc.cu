@@ -453,13 +453,16 @@ int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, i
     TT_TRY(ws.err.alloc(1));
     TT_CUDA_TRY(cudaMemsetAsync(ws.err.ptr, 0, sizeof(int), st));
   }
-  tc::k_split_L<<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L, ldl, M, K, ws.WA.ptr);
-  count_launch();
-  TT_CUDA_TRY(cudaGetLastError());
-  dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
-  tc::k_split_U<<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
-  count_launch();
-  TT_CUDA_TRY(cudaGetLastError());
+  {
+    ProfScope prof(TT_PROF_OPERANDS, st, 0.0, 16.0 * ((double)M + N) * K);
+    tc::k_split_L<<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L, ldl, M, K, ws.WA.ptr);
+    count_launch();
+    TT_CUDA_TRY(cudaGetLastError());
+    dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
+    tc::k_split_U<<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
+    count_launch();
+    TT_CUDA_TRY(cudaGetLastError());
+  }
   CUtensorMap mA, mB;
   TT_TRY(make_map(&mA, ws.WA.ptr, (uint64_t)M, (uint64_t)4 * K, tc::BM));
   TT_TRY(make_map(&mB, ws.WB.ptr, (uint64_t)N, (uint64_t)4 * K, tc::BN));

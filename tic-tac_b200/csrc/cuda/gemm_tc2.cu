@@ -526,15 +526,19 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
     TT_TRY(ws.err.alloc(1));
     TT_CUDA_TRY(cudaMemsetAsync(ws.err.ptr, 0, sizeof(int), st));
   }
-  if (!direct_A) {
-    tc2::k_pack_A<MODE><<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L, ldl, M, K, ws.WA.ptr);
+  {
+    ProfScope prof(TT_PROF_OPERANDS, st, 0.0,
+                   8.0 * (direct_A ? 0.0 : (double)M) * K + (double)needA + 8.0 * N * K + (double)needB);
+    if (!direct_A) {
+      tc2::k_pack_A<MODE><<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L, ldl, M, K, ws.WA.ptr);
+      count_launch();
+      TT_CUDA_TRY(cudaGetLastError());
+    }
+    dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
+    tc2::k_pack_B<MODE><<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
     count_launch();
     TT_CUDA_TRY(cudaGetLastError());
   }
-  dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
-  tc2::k_pack_B<MODE><<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
-  count_launch();
-  TT_CUDA_TRY(cudaGetLastError());
   CUtensorMap mA, mB;
   if (direct_A)
     TT_TRY(make_map2(&mA, MODE, const_cast<float2*>(L), (uint64_t)M, (uint64_t)2 * K, (uint64_t)ldl * 8, tc2::BM));

@@ -469,6 +469,7 @@ int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st, b
     TT_TRY(blk.mU.alloc(need));
   }
   blk.n = n;
+  ProfScope prof(TT_PROF_SUBST_PREP, st, 0.0, 2.0 * (double)n * TSB * sizeof(T));
   const size_t smem = (size_t)TSB * TLD * sizeof(T);
   static bool attr = false;
   if (!attr) {

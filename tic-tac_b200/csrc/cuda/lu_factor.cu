@@ -542,6 +542,7 @@ template <typename T>
 int gemm_sub(T* C, int ldc, const T* L, int ldl, const T* U, int ldu, int M, int N, int K, cudaStream_t st) {
   if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
   dim3 grid(ceil_div(N, 64), ceil_div(M, 64));
+  ProfScope prof(TT_PROF_SIMT_UPDATE, st, 8.0 * M * N * K, 2.0 * M * N * sizeof(T) + ((double)M + N) * K * sizeof(T));
   k_gemm_sub<T><<<grid, 256, 0, st>>>(C, ldc, L, ldl, U, ldu, M, N, K);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
@@ -552,6 +553,7 @@ template <typename T>
 int laswp2(T* A, int n, const int32_t* ipiv, int p0, int p1, int a0, int a1, int b0, int b1, cudaStream_t st) {
   const int cols = std::max(0, a1 - a0) + std::max(0, b1 - b0);
   if (cols <= 0 || p1 <= p0) return TT_OK;
+  ProfScope prof(TT_PROF_LASWP, st, 0.0, 4.0 * (p1 - p0) * cols * sizeof(T));
   k_laswp2<T><<<ceil_div(cols, 256), 256, 0, st>>>(A, n, ipiv, p0, p1, a0, std::max(a0, a1), b0, std::max(b0, b1));
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
@@ -561,6 +563,7 @@ int laswp2(T* A, int n, const int32_t* ipiv, int p0, int p1, int a0, int a1, int
 template <typename T>
 int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st) {
   if (ce <= cb) return TT_OK;
+  ProfScope prof(TT_PROF_PANEL_TRSM, st, 4.0 * w * w * (double)(ce - cb), 2.0 * w * (double)(ce - cb) * sizeof(T));
   k_trsm_blk<T><<<ceil_div(ce - cb, 32), 256, 0, st>>>(A, n, r0, w, cb, ce);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());

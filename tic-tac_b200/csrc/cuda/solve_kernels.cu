@@ -377,6 +377,7 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, doubl
 template <typename T>
 int form_L_device(const double* d_A, const double* d_G, int n, T* d_L, cudaStream_t st) {
   const size_t total = (size_t)n * n;
+  ProfScope prof(TT_PROF_FORM_L, st, 2.0 * (double)total, (8.0 + sizeof(T)) * (double)total);
   k_form_L<T><<<ceil_div(total, 256), 256, 0, st>>>(d_A, reinterpret_cast<const double2*>(d_G), n, d_L);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());

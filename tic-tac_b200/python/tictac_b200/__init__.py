@@ -43,7 +43,8 @@ EXPORTED_SYMBOLS = (
     "tt_run_solve_energies",
 )
 
-PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build")
+PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
+                   "subst_prep", "simt_update")
 
 
 class TicTacError(RuntimeError):
