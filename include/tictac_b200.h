@@ -157,7 +157,9 @@ int tt_calculate_resolvent_array_in_SWP_basis(tt_complex* G, double E, const tt_
  * make it before any stream capture.  Nothing has to be zeroed beforehand;
  * every call rewrites the tables it reads.  Calls that overlap in time on one
  * device (other streams or host threads) share the scratch and race:
- * serialise them.  Returns when the work is queued on `stream`. */
+ * serialise them.  Returns when the work is queued on `stream`; a call first
+ * waits until the previous call's copy of its tables to the device has read
+ * the library's host staging buffer. */
 #define TT_RESOLVENT_NOALLOC_SCRATCH_BYTES (256u * 1024u)
 int tt_calculate_resolvent_array_in_SWP_basis_noalloc(tt_complex* G_dev, const double* E, int nE,
                                                       const tt_swp_states* swp, const tt_pw_states* pw,

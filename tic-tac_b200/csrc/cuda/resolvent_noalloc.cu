@@ -9,6 +9,11 @@
 // it reads, on the caller's stream, before the kernel that reads it.  Calls
 // that overlap in time on one device (different streams or host threads)
 // share the one array and race; calls on one stream are ordered by it.
+//
+// The tables are assembled on the host in one static staging buffer and
+// copied with one cudaMemcpyAsync.  A copy from pageable memory may still be
+// reading its source after the call returns, so each copy records an event
+// and the next call waits for it before it rewrites the staging buffer.
 #include <mutex>
 
 #include "../host/tt_solver.h"
@@ -24,9 +29,11 @@ static __device__ __align__(256) unsigned char g_resolvent_scratch[kScratchBytes
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_scratch_addr[kMaxDevices];
-// host image of the tables; a pageable-to-device cudaMemcpyAsync has consumed
-// its source when it returns, so the next call may overwrite it
+// host image of the tables, shared by all calls (under g_mu)
 alignas(256) unsigned char g_stage[kScratchBytes];
+// the last copy out of g_stage, and its device; waited for before g_stage is rewritten
+cudaEvent_t g_stage_copied[kMaxDevices];
+int g_stage_dev = -1;
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -37,6 +44,15 @@ int scratch_address(void** out) {
     set_error("device ordinal " + std::to_string(dev) + " is beyond the " + std::to_string(kMaxDevices) +
               " devices the static resolvent scratch is tracked for");
     return TT_ERR_UNSUPPORTED;
+  }
+  if (!g_stage_copied[dev]) {
+    const cudaError_t e = cudaEventCreateWithFlags(&g_stage_copied[dev], cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      g_stage_copied[dev] = nullptr;
+      set_error(std::string("creating the staging event on device ") + std::to_string(dev) + " failed: " +
+                cudaGetErrorString(e));
+      return TT_ERR_CUDA;
+    }
   }
   if (!g_scratch_addr[dev]) {
     void* p = nullptr;
@@ -72,6 +88,16 @@ int resolvent_noalloc(const RunParams& rp, const PWChannel& ch, int Np, int Nq, 
   std::lock_guard<std::mutex> lock(g_mu);
   void* base = nullptr;
   TT_TRY(scratch_address(&base));
+  int dev = 0;
+  TT_CUDA_TRY(cudaGetDevice(&dev));
+  // the previous call's copy must have read the staging buffer before it is rewritten
+  if (g_stage_dev >= 0) {
+    int cur = dev;
+    if (g_stage_dev != cur) TT_CUDA_TRY(cudaSetDevice(g_stage_dev));
+    const cudaError_t e = cudaEventSynchronize(g_stage_copied[g_stage_dev]);
+    if (g_stage_dev != cur) TT_CUDA_TRY(cudaSetDevice(cur));
+    TT_CUDA_TRY(e);
+  }
   std::string err;
   if (!channel_energy_offsets(rp, ch, Np, n_unco, n_coup, reinterpret_cast<int32_t*>(g_stage + off_e_off), &err)) {
     set_error(err);
@@ -85,6 +111,8 @@ int resolvent_noalloc(const RunParams& rp, const PWChannel& ch, int Np, int Nq, 
   double* e = reinterpret_cast<double*>(g_stage + off_E);
   for (int i = 0; i < nE; i++) e[i] = E[i];
   TT_CUDA_TRY(cudaMemcpyAsync(base, g_stage, bytes, cudaMemcpyHostToDevice, st));
+  TT_CUDA_TRY(cudaEventRecord(g_stage_copied[dev], st));
+  g_stage_dev = dev;
   unsigned char* d = static_cast<unsigned char*>(base);
   return resolvent_device_tables(ch.Nalpha, Nq, Np, reinterpret_cast<const int32_t*>(d + off_e_off),
                                  reinterpret_cast<const double*>(d + off_swp),
