@@ -467,11 +467,7 @@ int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, i
   TT_TRY(make_map(&mA, ws.WA.ptr, (uint64_t)M, (uint64_t)4 * K, tc::BM));
   TT_TRY(make_map(&mB, ws.WB.ptr, (uint64_t)N, (uint64_t)4 * K, tc::BN));
   const size_t smem = (size_t)tc::STAGES * tc::STAGE_BYTES + tc::EPI_WARPS * tc::EPI_STAGE_BYTES + 1024 + 128;
-  static bool attr = false;
-  if (!attr) {
-    TT_CUDA_TRY(cudaFuncSetAttribute(tc::k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
+  TT_TRY(smem_limit_once((const void*)tc::k_lu_update_tc, (int)smem));
   const int tiles = ((M + tc::BM - 1) / tc::BM) * ((N + tc::BN - 1) / tc::BN);
   const int grid = std::min(tiles, device_sm_count());
   {

@@ -501,7 +501,6 @@ int make_map2(CUtensorMap* map, int mode, void* base, uint64_t rows, uint64_t co
 struct TC2Workspace {
   DevBuf<unsigned char> WA, WB;
   DevBuf<int> err;
-  int attr_dev[2] = {-1, -1};  // device on which each mode's shared-memory attribute was set
 };
 
 TC2Workspace& workspace2() {
@@ -548,14 +547,7 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
   TT_TRY(make_map2(&mB, MODE, ws.WB.ptr, (uint64_t)CF::PARTS * 2 * N, (uint64_t)2 * K, (uint64_t)2 * K * esz,
                    tc2::BN));
   const size_t smem = (size_t)tc2::STAGES * CF::STAGE + tc2::EPI_WARPS * tc2::EPI_STAGE_BYTES + 1024 + 128;
-  int dev = 0;
-  TT_CUDA_TRY(cudaGetDevice(&dev));
-  const int slot = MODE == TC_TF32 ? 0 : 1;
-  if (ws.attr_dev[slot] != dev) {
-    TT_CUDA_TRY(cudaFuncSetAttribute(tc2::k_lu_update_tc2<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-    ws.attr_dev[slot] = dev;
-  }
+  TT_TRY(smem_limit_once((const void*)tc2::k_lu_update_tc2<MODE>, (int)smem));
   const int tiles = ((M + tc2::BM - 1) / tc2::BM) * ((N + tc2::BN - 1) / tc2::BN);
   const int grid = std::min(tiles, device_sm_count());
   {

@@ -471,22 +471,12 @@ int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st, b
   blk.n = n;
   ProfScope prof(TT_PROF_SUBST_PREP, st, 0.0, 2.0 * (double)n * TSB * sizeof(T));
   const size_t smem = (size_t)TSB * TLD * sizeof(T);
-  static bool attr = false;
-  if (!attr) {
-    TT_CUDA_TRY(
-        cudaFuncSetAttribute(k_inv_diag<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TT_CUDA_TRY(
-        cudaFuncSetAttribute(k_inv_diag<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TT_CUDA_TRY(
-        cudaFuncSetAttribute(k_inv_diag<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TT_CUDA_TRY(
-        cudaFuncSetAttribute(k_inv_diag<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TT_CUDA_TRY(
-        cudaFuncSetAttribute(k_prev_mul<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem)));
-    TT_CUDA_TRY(
-        cudaFuncSetAttribute(k_prev_mul<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * smem)));
-    attr = true;
-  }
+  TT_TRY(smem_limit_once((const void*)k_inv_diag<T, false, true>, (int)(smem)));
+  TT_TRY(smem_limit_once((const void*)k_inv_diag<T, true, false>, (int)(smem)));
+  TT_TRY(smem_limit_once((const void*)k_inv_diag<T, false, false>, (int)(smem)));
+  TT_TRY(smem_limit_once((const void*)k_inv_diag<T, true, true>, (int)(smem)));
+  TT_TRY(smem_limit_once((const void*)k_prev_mul<T, false>, (int)(2 * smem)));
+  TT_TRY(smem_limit_once((const void*)k_prev_mul<T, true>, (int)(2 * smem)));
   if (!transposed) {
     k_inv_diag<T, false, true><<<nb, 512, smem, st>>>(d_LU, n, blk.invL.ptr);
     count_launch();
@@ -525,12 +515,8 @@ int trsv_sweeps(const T* d_LU, int n, const TrsvBlocks<T>& blk, double2* x, int 
               " bytes of shared memory per CTA (limit " + std::to_string(kMaxSmem) + ")");
     return TT_ERR_UNSUPPORTED;
   }
-  static bool attr = false;
-  if (!attr) {
-    TT_CUDA_TRY(cudaFuncSetAttribute(k_trsv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-    TT_CUDA_TRY(cudaFuncSetAttribute(k_trsv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-    attr = true;
-  }
+  TT_TRY(smem_limit_once((const void*)k_trsv<T, false>, (int)kMaxSmem));
+  TT_TRY(smem_limit_once((const void*)k_trsv<T, true>, (int)kMaxSmem));
   for (int k0 = 0; k0 < nrhs; k0 += RHS) {
     int kn = std::min(RHS, nrhs - k0);
     double2* xk = x + (size_t)k0 * n;

@@ -619,11 +619,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   TT_CUDA_TRY(cudaMemsetAsync(d_info.ptr, 0, sizeof(int) * B, st));
   TT_CUDA_TRY(cudaMemsetAsync(skey.ptr, 0, sizeof(unsigned long long) * B * n, st));
   PivotScratch<T> scr{sval.ptr, sidx.ptr, srow.ptr, stop.ptr, skey.ptr};
-  static bool smem_attr = false;
-  if (!smem_attr) {
-    TT_CUDA_TRY(cudaFuncSetAttribute(k_subpanel_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubpanelSmem));
-    smem_attr = true;
-  }
+  TT_TRY(smem_limit_once((const void*)k_subpanel_smem<T>, (int)kSubpanelSmem));
   // the sub-panel of matrices [b0, b0 + nb) in one cooperative launch
   auto subpanel = [&](int b0, int nb, int j0, int w, int grid) -> int {
     SubpanelBatch<T> bt{};

@@ -4,6 +4,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <tuple>
 
 #include "tt_kernels.h"
 
@@ -366,7 +369,7 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, doubl
   // shared memory is sized for 2 Np x Np blocks
   const size_t smem = (size_t)2 * L.Np * L.Np * sizeof(double);
   dim3 grid(ceil_div(n, 128), L.Nalpha * L.Nq);
-  if (smem > 48 * 1024) TT_CUDA_TRY(cudaFuncSetAttribute(k_ct<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > 48 * 1024) TT_TRY(smem_limit_once((const void*)k_ct<32>, (int)smem));
   k_ct<32><<<grid, 256, smem, st>>>(L.Nalpha, L.Nq, L.Np, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
                                     L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, d_B, d_A);
   count_launch();
@@ -459,6 +462,19 @@ int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h
       }
     }
   }
+  return TT_OK;
+}
+
+int smem_limit_once(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::set<std::tuple<const void*, int, int>> done;
+  int dev = 0;
+  TT_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_tuple(kernel, dev, bytes);
+  if (done.count(key)) return TT_OK;
+  TT_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.insert(key);
   return TT_OK;
 }
 

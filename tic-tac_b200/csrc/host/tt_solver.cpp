@@ -481,7 +481,14 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     TT_TRY(dots.alloc((size_t)2 * nd * nd));
   }
   if (opt.mixed) {
-    TT_TRY(L32all.alloc((size_t)B * n * n));
+    // the batch was sized from free HBM before the per-solve buffers: fewer
+    // matrices when their allocation still does not fit
+    for (;;) {
+      const int s = L32all.alloc((size_t)B * n * n);
+      if (s == TT_OK) break;
+      if (s != TT_ERR_NOMEM || B == 1) return s;
+      B--;
+    }
     TT_TRY(y.alloc((size_t)2 * n * nd));
     TT_TRY(res.alloc((size_t)2 * n * nd));
   } else {
