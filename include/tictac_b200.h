@@ -249,7 +249,10 @@ unsigned long long tt_kernel_launches(void);
 #define TT_PROF_FORM_L 8
 #define TT_PROF_SUBST_PREP 9
 #define TT_PROF_SIMT_UPDATE 10
-#define TT_PROF_COUNT 11
+/*   TC_PANEL    the tensor-core updates inside a panel and of its U block row (K below 256),
+ *               booked apart from TC_UPDATE (the trailing updates, K >= 256): 8 M N K flops */
+#define TT_PROF_TC_PANEL 11
+#define TT_PROF_COUNT 12
 typedef struct tt_kernel_profile {
   unsigned long long launches;
   double ms;

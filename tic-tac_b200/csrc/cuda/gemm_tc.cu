@@ -471,7 +471,8 @@ int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, i
   const int tiles = ((M + tc::BM - 1) / tc::BM) * ((N + tc::BN - 1) / tc::BN);
   const int grid = std::min(tiles, device_sm_count());
   {
-    ProfScope prof(TT_PROF_TC_UPDATE, st, 8.0 * M * N * K, 16.0 * M * N + 8.0 * ((double)M + N) * K);
+    ProfScope prof(K >= 256 ? TT_PROF_TC_UPDATE : TT_PROF_TC_PANEL, st, 8.0 * M * N * K,
+                   16.0 * M * N + 8.0 * ((double)M + N) * K);
     tc::k_lu_update_tc<<<grid, tc::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, ws.err.ptr);
   }
   count_launch();

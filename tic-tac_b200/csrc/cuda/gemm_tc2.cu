@@ -551,7 +551,8 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
   const int tiles = ((M + tc2::BM - 1) / tc2::BM) * ((N + tc2::BN - 1) / tc2::BN);
   const int grid = std::min(tiles, device_sm_count());
   {
-    ProfScope prof(TT_PROF_TC_UPDATE, st, 8.0 * M * N * K, 16.0 * M * N + 8.0 * ((double)M + N) * K);
+    ProfScope prof(K >= 256 ? TT_PROF_TC_UPDATE : TT_PROF_TC_PANEL, st, 8.0 * M * N * K,
+                   16.0 * M * N + 8.0 * ((double)M + N) * K);
     tc2::k_lu_update_tc2<MODE><<<grid, tc2::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, M, ws.err.ptr);
   }
   count_launch();
