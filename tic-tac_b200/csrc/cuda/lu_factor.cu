@@ -21,6 +21,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <functional>
 
 #include "tt_kernels.h"
 #include "tt_lu_internal.h"
@@ -638,36 +639,86 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     count_launch();
     return TT_OK;
   };
+  // pivoted factorisation of columns [j0, j0 + w), w <= IB, rows [j0, n), of all B matrices
+  auto leaf = [&](int j0, int w) -> int {
+    const size_t m = (size_t)(n - j0);
+    const int Gb = G / B;
+    const bool keyed = m < 0xFFFFF;
+    const bool together = B > 1 && keyed && ((m + Gb - 1) / Gb) * SP * sizeof(T) <= kSubpanelSmem;
+    const bool alone = keyed && ((m + G - 1) / G) * SP * sizeof(T) <= kSubpanelSmem;
+    ProfScope prof(TT_PROF_SUBPANEL, st, 4.0 * m * w * w * B, 2.0 * m * w * sizeof(T) * B);
+    if (together) return subpanel(0, B, j0, w, Gb * B);
+    for (int b = 0; b < B; b++) {
+      if (alone) {
+        TT_TRY(subpanel(b, 1, j0, w, G));
+      } else {
+        T* Ap = As[b];
+        int nn = n, cc0 = j0, ww = w;
+        int32_t* ip = ipivs[b];
+        int* inf = d_info.ptr + b;
+        void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
+        TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
+        count_launch();
+      }
+    }
+    return TT_OK;
+  };
+  // split of a block of h rows or columns: the largest multiple of IB not above h / 2, at least IB
+  auto half = [](int h) { return std::max(IB, (h / 2) / IB * IB); };
+  // rows [r0, r0 + h) of columns [cb, ce) <- L^{-1} of them, L the unit-lower h x h block at (r0, r0):
+  // halves recursively, so that most of the work is one update of depth h / 2
+  std::function<int(T*, int, int, int, int)> trsm_rec = [&](T* A, int r0, int h, int cb, int ce) -> int {
+    if (h <= IB) return trsm_blk(A, n, r0, h, cb, ce, st);
+    const int h1 = half(h);
+    TT_TRY(trsm_rec(A, r0, h1, cb, ce));
+    TT_TRY(panel_gemm_sub(mode, A + (size_t)(r0 + h1) * n + cb, n, A + (size_t)(r0 + h1) * n + r0, n,
+                          A + (size_t)r0 * n + cb, n, h - h1, ce - cb, h1, st));
+    return trsm_rec(A, r0 + h1, h - h1, cb, ce);
+  };
+  // columns [c0, c0 + w) of the panel [k, k + kb) factored by recursive halving:
+  // left half, its U block and the update of the right half (depth w / 2), right half
+  std::function<int(int, int, int, int)> factor_cols = [&](int k, int kb, int c0, int w) -> int {
+    if (w <= IB) {
+      TT_TRY(leaf(c0, w));
+      for (int b = 0; b < B; b++) TT_TRY(laswp2(As[b], n, ipivs[b], c0, c0 + w, k, c0, c0 + w, k + kb, st));
+      return TT_OK;
+    }
+    const int h = half(w);
+    TT_TRY(factor_cols(k, kb, c0, h));
+    for (int b = 0; b < B; b++) {
+      T* A = As[b];
+      TT_TRY(trsm_rec(A, c0, h, c0 + h, c0 + w));
+      TT_TRY(panel_gemm_sub(mode, A + (size_t)(c0 + h) * n + (c0 + h), n, A + (size_t)(c0 + h) * n + c0, n,
+                            A + (size_t)c0 * n + (c0 + h), n, n - c0 - h, w - h, h, st));
+    }
+    return factor_cols(k, kb, c0 + h, w - h);
+  };
+  const bool blocked = mode == TC_LEGACY_BF16X3;  // the sub-panel-by-sub-panel order of the first kernel
   for (int k = 0; k < n; k += NB) {
     const int kb = std::min(NB, n - k);
+    const int rest = n - k - kb;
+    if (!blocked) {
+      TT_TRY(factor_cols(k, kb, k, kb));
+      for (int b = 0; b < B; b++) {
+        T* A = As[b];
+        // ---- interchanges outside the panel, U12 = L11^{-1} A12, trailing update
+        TT_TRY(laswp2(A, n, ipivs[b], k, k + kb, 0, k, k + kb, n, st));
+        if (rest <= 0) continue;
+        TT_TRY(trsm_rec(A, k, kb, k + kb, n));
+        if (tc)
+          TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)(k + kb) * n + (k + kb), n,
+                              reinterpret_cast<const float2*>(A) + (size_t)(k + kb) * n + k, n,
+                              reinterpret_cast<const float2*>(A) + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
+        else
+          TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
+                          A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
+      }
+      continue;
+    }
     // ---- panel [k, k+kb) in sub-panels of IB columns
     for (int j0 = k; j0 < k + kb; j0 += IB) {
       const int w = std::min(IB, k + kb - j0);
-      {
-        const size_t m = (size_t)(n - j0);
-        const int Gb = G / B;
-        const bool keyed = m < 0xFFFFF;
-        const bool together = B > 1 && keyed && ((m + Gb - 1) / Gb) * SP * sizeof(T) <= kSubpanelSmem;
-        const bool alone = keyed && ((m + G - 1) / G) * SP * sizeof(T) <= kSubpanelSmem;
-        ProfScope prof(TT_PROF_SUBPANEL, st, 4.0 * m * w * w * B, 2.0 * m * w * sizeof(T) * B);
-        if (together) {
-          TT_TRY(subpanel(0, B, j0, w, Gb * B));
-        } else {
-          for (int b = 0; b < B; b++) {
-            if (alone) {
-              TT_TRY(subpanel(b, 1, j0, w, G));
-            } else {
-              T* Ap = As[b];
-              int nn = n, cc0 = j0, ww = w;
-              int32_t* ip = ipivs[b];
-              int* inf = d_info.ptr + b;
-              void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
-              TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
-              count_launch();
-            }
-          }
-        }
-      }
+      TT_TRY(leaf(j0, w));
       for (int b = 0; b < B; b++) {
         T* A = As[b];
         const int32_t* ipiv = ipivs[b];
@@ -685,7 +736,6 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
       const int32_t* ipiv = ipivs[b];
       // ---- interchanges outside the panel
       TT_TRY(laswp2(A, n, ipiv, k, k + kb, 0, k, k + kb, n, st));
-      const int rest = n - k - kb;
       if (rest <= 0) continue;
       // ---- U12 = L11^{-1} A12, blocked by IB
       for (int i0 = k; i0 < k + kb; i0 += IB) {
@@ -697,17 +747,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
                                 A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
       }
       // ---- trailing update
-      if (mode == TC_LEGACY_BF16X3) {
-        TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
-      } else if (tc) {
-        const int r0 = k + kb;
-        TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)r0 * n + r0, n,
-                            reinterpret_cast<const float2*>(A) + (size_t)r0 * n + k, n,
-                            reinterpret_cast<const float2*>(A) + (size_t)k * n + r0, n, rest, rest, kb, st));
-      } else {
-        TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
-                        A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
-      }
+      TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
     }
   }
   if (mode == TC_LEGACY_BF16X3) TT_TRY(tc_check_error(st));
