@@ -280,6 +280,78 @@ __global__ void __launch_bounds__(256) k_residual(const double* __restrict__ A, 
   }
 }
 
+// r_v = b_v - x_v + A y_v for NV <= 4 vectors in one pass over A (even n):
+// a CTA owns 32 rows (4 per warp); per 256-column tile the NV slices of y are
+// staged once in shared memory, and each lane keeps 4 rows x 4 double2 of A in
+// flight (8 columns per row), so y is read from L2 once per 32 rows of A.
+constexpr int R2_ROWS = 32, R2_TILE = 256;
+template <int NV>
+__global__ void __launch_bounds__(256, 1) k_residual2(const double* __restrict__ A, int n,
+                                                       const double2* __restrict__ y, const double2* __restrict__ b,
+                                                       const double2* __restrict__ x, double2* __restrict__ r) {
+  __shared__ double2 sy[NV][R2_TILE];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row0 = (int64_t)blockIdx.x * R2_ROWS + warp * 4;
+  const double* Ar[4];
+#pragma unroll
+  for (int h = 0; h < 4; h++) Ar[h] = A + (size_t)min(row0 + h, (int64_t)n - 1) * n;
+  double sr[4][NV], si[4][NV];
+#pragma unroll
+  for (int h = 0; h < 4; h++)
+#pragma unroll
+    for (int v = 0; v < NV; v++) sr[h][v] = si[h][v] = 0.0;
+  for (int c0 = 0; c0 < n; c0 += R2_TILE) {
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < NV; v++) {
+      const int c = c0 + threadIdx.x;
+      sy[v][threadIdx.x] = c < n ? y[(size_t)v * n + c] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2 a[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int c = c0 + 2 * lane + 64 * u;  // c and c + 1 (n even, c even)
+#pragma unroll
+      for (int h = 0; h < 4; h++)
+        a[h][u] = c < n ? __ldcs(reinterpret_cast<const double2*>(Ar[h] + c)) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int cl = 2 * lane + 64 * u;
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        const double2 y0 = sy[v][cl], y1 = sy[v][cl + 1];
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+          sr[h][v] += a[h][u].x * y0.x + a[h][u].y * y1.x;
+          si[h][v] += a[h][u].x * y0.y + a[h][u].y * y1.y;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 4; h++)
+#pragma unroll
+    for (int v = 0; v < NV; v++)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sr[h][v] += __shfl_xor_sync(0xffffffffu, sr[h][v], o);
+        si[h][v] += __shfl_xor_sync(0xffffffffu, si[h][v], o);
+      }
+  if (lane == 0) {
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      if (row0 + h >= n) break;
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        const size_t o = (size_t)v * n + row0 + h;
+        r[o] = make_double2(b[o].x - x[o].x + sr[h][v], b[o].y - x[o].y + si[h][v]);
+      }
+    }
+  }
+}
+
 __global__ void k_hadamard(const double2* __restrict__ G, const int32_t* __restrict__ rhs_e, int n,
                            const double2* __restrict__ x, int nrhs, double2* __restrict__ y) {
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -408,6 +480,28 @@ int hadamard_device(const double* d_G, const int32_t* d_rhs_e, int n, const doub
 
 int residual_multi_device(const double* d_A, int n, const double* d_y, const double* d_b, const double* d_x, int nrhs,
                           double* d_r, cudaStream_t st) {
+  if (n % 2 == 0) {
+    // one pass over A per group of up to 4 vectors
+    ProfScope prof(TT_PROF_RESIDUAL, st, 4.0 * n * (double)n * nrhs, 8.0 * n * (double)n * ((nrhs + 3) / 4));
+    const unsigned grid = ceil_div((size_t)n, R2_ROWS);
+    for (int v0 = 0; v0 < nrhs; v0 += 4) {
+      const int nv = std::min(4, nrhs - v0);
+      const size_t o = (size_t)v0 * n;
+      const double2* y = reinterpret_cast<const double2*>(d_y) + o;
+      const double2* b = reinterpret_cast<const double2*>(d_b) + o;
+      const double2* x = reinterpret_cast<const double2*>(d_x) + o;
+      double2* r = reinterpret_cast<double2*>(d_r) + o;
+      switch (nv) {
+        case 1: k_residual2<1><<<grid, 256, 0, st>>>(d_A, n, y, b, x, r); break;
+        case 2: k_residual2<2><<<grid, 256, 0, st>>>(d_A, n, y, b, x, r); break;
+        case 3: k_residual2<3><<<grid, 256, 0, st>>>(d_A, n, y, b, x, r); break;
+        default: k_residual2<4><<<grid, 256, 0, st>>>(d_A, n, y, b, x, r); break;
+      }
+      count_launch();
+      TT_CUDA_TRY(cudaGetLastError());
+    }
+    return TT_OK;
+  }
   ProfScope prof(TT_PROF_RESIDUAL, st, 4.0 * n * (double)n * nrhs,
                  8.0 * n * (double)n * ((nrhs + RES_MAXR - 1) / RES_MAXR));
   k_residual<<<ceil_div(ceil_div((size_t)n, RES_ROWS) * 32, 256), 256, 0, st>>>(

@@ -464,22 +464,10 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     const size_t fit = free_b > reserve + per ? (free_b - reserve) / per : 1;
     B = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>((size_t)nE, std::min(opt.energy_batch, 4)), fit));
   }
-  DevBuf<int32_t> ipiv_all, cols, rhs_e, perm_d;
+  DevBuf<int32_t> ipiv_all, cols, rhs_e;
   TT_TRY(ipiv_all.alloc((size_t)n * B));
-  DevBuf<double> b, x, y, res, d, tmp;
-  TT_TRY(tmp.alloc((size_t)2 * n * nd));
-  TT_TRY(b.alloc((size_t)2 * n * nd));
-  TT_TRY(x.alloc((size_t)2 * n * nd));
   DevBuf<double2> L64;
   DevBuf<float2> L32all;
-  TrsvBlocks<double2> tb64, tbT64;
-  TrsvBlocks<float2> tb32, tbT32;
-  // adjoint: the vectors of lambda, its refinement and the products
-  DevBuf<double> lam, yT, rT, u, g, w, h, dots;
-  if (adj && adj->n_theta > 0) {
-    for (DevBuf<double>* b : {&lam, &yT, &rT, &u, &g, &w, &h}) TT_TRY(b->alloc((size_t)2 * n * nd));
-    TT_TRY(dots.alloc((size_t)2 * nd * nd));
-  }
   if (opt.mixed) {
     // the batch was sized from free HBM before the per-solve buffers: fewer
     // matrices when their allocation still does not fit
@@ -489,10 +477,29 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       if (s != TT_ERR_NOMEM || B == 1) return s;
       B--;
     }
-    TT_TRY(y.alloc((size_t)2 * n * nd));
-    TT_TRY(res.alloc((size_t)2 * n * nd));
   } else {
     TT_TRY(L64.alloc((size_t)n * n));
+  }
+  // right-hand sides, solutions and refinement vectors of a group's energies:
+  // [q][d][n] complex128, energy q of the group, deuteron column d
+  const size_t vec = (size_t)2 * n * nd;
+  DevBuf<double> b, x, y, res, tmp;
+  TT_TRY(tmp.alloc(vec));
+  TT_TRY(b.alloc(vec * B));
+  TT_TRY(x.alloc(vec * B));
+  if (opt.mixed) {
+    TT_TRY(y.alloc(vec * B));
+    TT_TRY(res.alloc(vec * B));
+  }
+  std::vector<DevBuf<int32_t>> perm_d(B);
+  std::vector<TrsvBlocks<float2>> tb32(B);
+  TrsvBlocks<double2> tb64, tbT64;
+  TrsvBlocks<float2> tbT32;
+  // adjoint: the vectors of lambda, its refinement and the products
+  DevBuf<double> lam, yT, rT, u, g, w, h, dots;
+  if (adj && adj->n_theta > 0) {
+    for (DevBuf<double>* v : {&lam, &yT, &rT, &u, &g, &w, &h}) TT_TRY(v->alloc(vec));
+    TT_TRY(dots.alloc((size_t)2 * nd * nd));
   }
   for (int g0 = 0; g0 < nE; g0 += B) {
     const int nb = std::min(B, nE - g0);
@@ -527,77 +534,103 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
         if (rep) *rep = r;
         return TT_ERR_SINGULAR;
       }
-    // ---- per energy: substitutions, refinement, adjoint, read-out
+    // on-shell rows (= the columns of A taken as right-hand sides) of every
+    // (energy, deuteron) of the group, and each vector's energy in the group
+    std::vector<int32_t> hc((size_t)nb * nd), he((size_t)nb * nd);
+    for (int q = 0; q < nb; q++)
+      for (int k = 0; k < nd; k++) {
+        hc[(size_t)q * nd + k] = deut[k] * Nq * Np + q_idx[g0 + q] * Np + 0;
+        he[(size_t)q * nd + k] = q;
+      }
+    TT_TRY(cols.upload(hc, st));
+    TT_TRY(rhs_e.upload(he, st));
+    const double* Gg = G_.ptr + (size_t)2 * n * g0;  // the group's resolvents [q][n]
+    auto factor_of = [&](int q) -> float2* { return L32all.ptr + (size_t)q * n * n; };
+    // ---- per energy: right-hand sides and the first solve with its factor
+    t0 = std::chrono::steady_clock::now();
+    TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nb * nd, b.ptr, st));
+    TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * vec * nb, cudaMemcpyDeviceToDevice, st));
     for (int q = 0; q < nb; q++) {
-      const int j = g0 + q;
-      float2* const Lq = opt.mixed ? L32all.ptr + (size_t)q * n * n : nullptr;  // this energy's factor
-      int32_t* const pivq = ipiv_all.ptr + (size_t)q * n;
-      std::vector<int32_t> hc(nd), he(nd, 0);
-      for (int k = 0; k < nd; k++) hc[k] = deut[k] * Nq * Np + q_idx[j] * Np + 0;
-      TT_TRY(cols.upload(hc, st));
-      TT_TRY(rhs_e.upload(he, st));
-      const double* Gj = G_.ptr + (size_t)2 * n * j;
-      t0 = std::chrono::steady_clock::now();
       std::vector<int32_t> perm;
-      TT_TRY(lu_permutation(pivq, n, perm, st));
-      TT_TRY(perm_d.upload(perm, st));
-      TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nd, b.ptr, st));
-      TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * 2 * n * nd, cudaMemcpyDeviceToDevice, st));
+      TT_TRY(lu_permutation(ipiv_all.ptr + (size_t)q * n, n, perm, st));
+      TT_TRY(perm_d[q].upload(perm, st));
       if (opt.mixed) {
-        TT_TRY(lu_trsv_prepare<float2>(Lq, n, tb32, st));
-        TT_TRY(lu_solve_device<float2>(Lq, n, tb32, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+        TT_TRY(lu_trsv_prepare<float2>(factor_of(q), n, tb32[q], st));
+        TT_TRY(lu_solve_device<float2>(factor_of(q), n, tb32[q], perm_d[q].ptr, x.ptr + vec * q, tmp.ptr, nd, st));
       } else {
         TT_TRY(lu_trsv_prepare<double2>(L64.ptr, n, tb64, st));
-        TT_TRY(lu_solve_device<double2>(L64.ptr, n, tb64, perm_d.ptr, x.ptr, tmp.ptr, nd, st));
+        TT_TRY(lu_solve_device<double2>(L64.ptr, n, tb64, perm_d[q].ptr, x.ptr + vec * q, tmp.ptr, nd, st));
       }
-      TT_CUDA_TRY(cudaStreamSynchronize(st));
-      r.ms_solve += ms_since(t0);
-      if (opt.mixed) {
-        // FP64 iterative refinement: r = b - (x - A (G o x)), L d = r, x += d.
-        // Stop when the estimated remaining relative error of every on-shell
-        // entry (the U elements: rows cols[] of each column) is below the
-        // tolerance, with the whole column's max|dx|/max|x| as a floor (the
-        // adjoint reads all of x).
-        t0 = std::chrono::steady_clock::now();
-        bool converged = false;
-        int it = 0;
-        double worst = 0;
-        std::vector<double> ratio((size_t)nd + (size_t)nd * nd), prev(ratio.size(), 0.0);
-        for (it = 1; it <= opt.refine_max_iter; it++) {
-          TT_TRY(hadamard_device(Gj, rhs_e.ptr, n, x.ptr, nd, y.ptr, st));
-          TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nd, res.ptr, st));
-          TT_TRY(lu_solve_device<float2>(Lq, n, tb32, perm_d.ptr, res.ptr, tmp.ptr, nd, st));
-          TT_TRY(axpy_norms_device(x.ptr, res.ptr, n, nd, ratio.data(), st, cols.ptr, nd, ratio.data() + nd));
-          worst = refine_error_estimate(ratio, prev, it > 1);
-          if (!(worst == worst)) break;  // NaN
-          if (worst <= opt.refine_tol) {
-            converged = true;
+    }
+    TT_CUDA_TRY(cudaStreamSynchronize(st));
+    r.ms_solve += ms_since(t0);
+    if (opt.mixed) {
+      // FP64 iterative refinement of the group's energies together: one
+      // residual pass over A for all their columns, r = b - (x - A (G o x)),
+      // then each energy's correction L d = r with its own factor, x += d.
+      // An energy stops when the estimated remaining relative error of every
+      // on-shell entry (the U elements: rows cols[] of each column) is below
+      // the tolerance, with the whole column's max|dx|/max|x| as a floor (the
+      // adjoint reads all of x).
+      t0 = std::chrono::steady_clock::now();
+      std::vector<char> done(nb, 0);
+      std::vector<int> iters(nb, 0);
+      std::vector<double> worst(nb, 0.0);
+      std::vector<std::vector<double>> prev(nb, std::vector<double>((size_t)nd + (size_t)nd * nd, 0.0));
+      std::vector<double> ratio((size_t)nd + (size_t)nd * nd);
+      int left = nb;
+      for (int it = 1; it <= opt.refine_max_iter && left > 0; it++) {
+        TT_TRY(hadamard_device(Gg, rhs_e.ptr, n, x.ptr, nb * nd, y.ptr, st));
+        TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nb * nd, res.ptr, st));
+        for (int q = 0; q < nb; q++) {
+          if (done[q]) continue;
+          TT_TRY(lu_solve_device<float2>(factor_of(q), n, tb32[q], perm_d[q].ptr, res.ptr + vec * q, tmp.ptr, nd,
+                                         st));
+          TT_TRY(axpy_norms_device(x.ptr + vec * q, res.ptr + vec * q, n, nd, ratio.data(), st,
+                                   cols.ptr + (size_t)q * nd, nd, ratio.data() + nd));
+          worst[q] = refine_error_estimate(ratio, prev[q], it > 1);
+          iters[q] = it;
+          if (!(worst[q] == worst[q])) {  // NaN: no convergence
+            left = 0;
             break;
           }
+          if (worst[q] <= opt.refine_tol) {
+            done[q] = 1;
+            left--;
+          }
         }
-        r.ms_refine += ms_since(t0);
-        r.refine_iters = std::max(r.refine_iters, std::min(it, opt.refine_max_iter));
-        r.final_correction = std::max(r.final_correction, worst);
-        if (!converged) {
-          set_error("iterative refinement did not converge (last |dx|/|x| = " + std::to_string(worst) + ")");
+      }
+      r.ms_refine += ms_since(t0);
+      for (int q = 0; q < nb; q++) {
+        r.refine_iters = std::max(r.refine_iters, iters[q]);
+        r.final_correction = std::max(r.final_correction, worst[q]);
+        if (!(worst[q] == worst[q])) r.final_correction = worst[q];
+      }
+      for (int q = 0; q < nb; q++)
+        if (!done[q]) {
+          set_error("iterative refinement did not converge (last |dx|/|x| = " + std::to_string(worst[q]) + ")");
           if (rep) *rep = r;
           return TT_ERR_NOCONVERGE;
         }
-      }
-      if (adj && adj->n_theta > 0) TT_TRY(adjoint_energy(j, nE, nd, Gj, cols.ptr, perm_d.ptr, tmp.ptr, x.ptr, opt,
-                                                        opt.mixed ? (void*)Lq : (void*)L64.ptr, tbT32, tbT64,
-                                                        lam.ptr, yT.ptr, rT.ptr, u.ptr, g.ptr, w.ptr, h.ptr, dots.ptr,
-                                                        *adj, r, st));
-      // on-shell read-out, solve_faddeev.cpp:407-431
-      std::vector<double> hx((size_t)2 * n * nd);
-      TT_CUDA_TRY(cudaMemcpyAsync(hx.data(), x.ptr, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st));
+    }
+    // ---- per energy: adjoint, on-shell read-out (solve_faddeev.cpp:407-431)
+    for (int q = 0; q < nb; q++) {
+      const int j = g0 + q;
+      const double* Gj = G_.ptr + (size_t)2 * n * j;
+      double* xq = x.ptr + vec * q;
+      if (adj && adj->n_theta > 0)
+        TT_TRY(adjoint_energy(j, nE, nd, Gj, cols.ptr + (size_t)q * nd, perm_d[q].ptr, tmp.ptr, xq, opt,
+                              opt.mixed ? (void*)factor_of(q) : (void*)L64.ptr, tbT32, tbT64, lam.ptr, yT.ptr, rT.ptr,
+                              u.ptr, g.ptr, w.ptr, h.ptr, dots.ptr, *adj, r, st));
+      std::vector<double> hx(vec);
+      TT_CUDA_TRY(cudaMemcpyAsync(hx.data(), xq, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, st));
       TT_CUDA_TRY(cudaStreamSynchronize(st));
       for (int dr = 0; dr < nd; dr++)
         for (int dc = 0; dc < nd; dc++) {
           const size_t row = (size_t)deut[dr] * Nq * Np + (size_t)q_idx[j] * Np + 0;
-          const size_t u = (size_t)dr * nd * nE + (size_t)dc * nE + j;
-          U[2 * u + 0] = hx[2 * ((size_t)dc * n + row) + 0];
-          U[2 * u + 1] = hx[2 * ((size_t)dc * n + row) + 1];
+          const size_t uu = (size_t)dr * nd * nE + (size_t)dc * nE + j;
+          U[2 * uu + 0] = hx[2 * ((size_t)dc * n + row) + 0];
+          U[2 * uu + 1] = hx[2 * ((size_t)dc * n + row) + 1];
         }
     }
   }
