@@ -242,7 +242,7 @@ unsigned long long tt_kernel_launches(void);
  *   LASWP       row interchanges: 4 swaps cols sizeof(elem) bytes
  *   FORM_L      L = 1 - A G: 8 n^2 bytes read + n^2 sizeof(elem) written
  *   SUBST_PREP  inverted diagonal blocks of the substitutions and their neighbour products
- *   SIMT_UPDATE C -= L U on the CUDA cores (complex128 factorisation, small K): 8 M N K flops */
+ *   SIMT_UPDATE C -= L U on the CUDA cores (complex64 without tensor cores): 8 M N K flops */
 #define TT_PROF_PANEL_TRSM 5
 #define TT_PROF_OPERANDS 6
 #define TT_PROF_LASWP 7
@@ -252,7 +252,9 @@ unsigned long long tt_kernel_launches(void);
 /*   TC_PANEL    the tensor-core updates inside a panel and of its U block row (K below 256),
  *               booked apart from TC_UPDATE (the trailing updates, K >= 256): 8 M N K flops */
 #define TT_PROF_TC_PANEL 11
-#define TT_PROF_COUNT 12
+/*   FP64_UPDATE C -= L U of the complex128 factorisation on the FP64 tensor cores (DMMA): 8 M N K flops */
+#define TT_PROF_FP64_UPDATE 12
+#define TT_PROF_COUNT 13
 typedef struct tt_kernel_profile {
   unsigned long long launches;
   double ms;

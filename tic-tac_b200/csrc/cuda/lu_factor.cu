@@ -542,6 +542,9 @@ __global__ void __launch_bounds__(256) k_gemm_sub(T* __restrict__ C, int ldc, co
 template <typename T>
 int gemm_sub(T* C, int ldc, const T* L, int ldl, const T* U, int ldu, int M, int N, int K, cudaStream_t st) {
   if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
+  if constexpr (sizeof(T) == sizeof(double2))
+    return zgemm_sub_dmma(reinterpret_cast<double2*>(C), ldc, reinterpret_cast<const double2*>(L), ldl,
+                          reinterpret_cast<const double2*>(U), ldu, M, N, K, st);
   dim3 grid(ceil_div(N, 64), ceil_div(M, 64));
   ProfScope prof(TT_PROF_SIMT_UPDATE, st, 8.0 * M * N * K, 2.0 * M * N * sizeof(T) + ((double)M + N) * K * sizeof(T));
   k_gemm_sub<T><<<grid, 256, 0, st>>>(C, ldc, L, ldl, U, ldu, M, N, K);

@@ -22,6 +22,9 @@ constexpr int TC_BF16X3 = 3;         // gemm_tc2.cu: real-row form, N = 256, BF1
 int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
                  cudaStream_t st);
 int tc2_check_error(cudaStream_t st);
+// C[M x N] -= L[M x K] U[K x N], complex128, on the FP64 tensor cores (zgemm_dmma.cu).
+int zgemm_sub_dmma(double2* C, int ldc, const double2* L, int ldl, const double2* U, int ldu, int M, int N, int K,
+                   cudaStream_t st);
 // C[M x N] -= L[M x K] U[K x N], complex64 row-major operands, K % 64 == 0.
 int tc_gemm_sub(float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
                 cudaStream_t st);

@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
-                   "subst_prep", "simt_update", "tc_panel")
+                   "subst_prep", "simt_update", "tc_panel", "fp64_update")
 
 
 class TicTacError(RuntimeError):
