@@ -239,6 +239,7 @@ def run_ours(args, world, rank, local, pg):
     lab = scan_lab_energies(cfg, world)
     cfg["lab_energies"] = ",".join(f"{x:.12g}" for x in lab)
     cfg["tc_product"] = args.tc_product
+    cfg["panel_order"] = args.panel_order
     prec = tt.PRECISION_MIXED if args.precision == "mixed" else tt.PRECISION_FP64
     t_setup = time.perf_counter()
     run = tt.Run(**cfg)
@@ -267,7 +268,8 @@ def run_ours(args, world, rank, local, pg):
     barrier(pg)
     times = []
     launches0 = tt.kernel_launches()
-    tt.profile_begin()
+    # the timed steps record events only around the roofline kernel's launches
+    tt.profile_begin(["tc_update"])
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             run.timer_start()
@@ -279,8 +281,17 @@ def run_ours(args, world, rank, local, pg):
     ms_step = allreduce_max(pg, float(np.mean(times)))
     energies_per_step = nE  # every channel at every on-shell energy of the scan, over all ranks
     value = energies_per_step / (ms_step * 1e-3)
-    roofline, kernels = roofline_of(kern, float(np.sum(times)), float(np.mean(times)),
-                                    [infos_all[c]["n"] for c, js in mine.items() for _ in js], 1, args.tc_product)
+    items = [infos_all[c]["n"] for c, js in mine.items() for _ in js]
+    roofline, _ = roofline_of(kern, float(np.sum(times)), float(np.mean(times)), items, 1, args.tc_product)
+    # breakdown: one more step with every kernel class timed (not part of the value)
+    kernels = None
+    if args.breakdown:
+        tt.profile_begin()
+        run.timer_start()
+        one_step()
+        t_bd = run.timer_stop()
+        _, kernels = roofline_of(tt.profile_end(), t_bd, t_bd, items, 1, args.tc_product)
+        kernels["step_ms"] = round(t_bd, 1)
     # U of every (channel, energy) gathered on rank 0 in the reference's layout
     gathered = shard.gather_to_rank0(pg, Us)
     U_all = None
@@ -498,6 +509,10 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--tc-product", choices=list(PRODUCTS), default="bf16x3",
                     help="tensor-core product of the complex64 LU")
+    ap.add_argument("--panel-order", choices=["recursive", "blocked"], default="recursive",
+                    help="LU panels by recursive halving or in 32-column steps")
+    ap.add_argument("--breakdown", type=int, default=1,
+                    help="one extra step with every kernel class timed, for the per-class breakdown")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp64-check", type=int, default=2,

@@ -262,6 +262,10 @@ typedef struct tt_kernel_profile {
   double bytes;
 } tt_kernel_profile;
 int tt_profile_begin(void);
+/* Classes recorded by the next regions, bit k = class k (default all): a
+ * region that times only the classes it reports keeps the event records of the
+ * other launches off the host path. */
+int tt_profile_select(unsigned long long class_mask);
 int tt_profile_end(void);
 int tt_profile_read(int kernel_class, tt_kernel_profile* out);
 

@@ -111,6 +111,7 @@ SolveOptions options_of(const RunParams& rp, int precision) {
   o.refine_max_iter = rp.refine_max_iter;
   o.energy_batch = rp.energy_batch;
   o.tc_product = rp.tc_product;
+  o.panel_blocked = rp.panel_blocked;
   return o;
 }
 

@@ -16,6 +16,7 @@ struct Record {
 struct ProfState {
   std::mutex mu;
   bool on = false;
+  unsigned long long mask = ~0ull;  // classes recorded while on
   std::vector<cudaEvent_t> pool;  // reused across regions
   size_t used = 0;
   std::vector<Record> recs;
@@ -31,7 +32,7 @@ ProfState& state() {
 long take_event(ProfState& s) {
   if (s.used == s.pool.size()) {
     cudaEvent_t e;
-    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    if (cudaEventCreateWithFlags(&e, cudaEventDefault) != cudaSuccess) return -1;
     s.pool.push_back(e);
   }
   return (long)s.used++;
@@ -41,7 +42,7 @@ long take_event(ProfState& s) {
 
 ProfScope::ProfScope(int kernel_class, cudaStream_t st, double flops, double bytes) {
   ProfState& s = state();
-  if (!s.on) return;
+  if (!s.on || !((s.mask >> kernel_class) & 1ull)) return;
   std::lock_guard<std::mutex> lock(s.mu);
   if (!s.on) return;
   const long e = take_event(s);
@@ -68,6 +69,13 @@ ProfScope::~ProfScope() {
 using namespace tt;
 
 extern "C" {
+
+int tt_profile_select(unsigned long long class_mask) {
+  ProfState& s = state();
+  std::lock_guard<std::mutex> lock(s.mu);
+  s.mask = class_mask;
+  return TT_OK;
+}
 
 int tt_profile_begin(void) {
   ProfState& s = state();

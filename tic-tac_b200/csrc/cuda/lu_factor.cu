@@ -593,7 +593,7 @@ int panel_gemm_sub(int mode, T* C, int ldc, const T* L, int ldl, const T* U, int
 
 template <typename T>
 int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, cudaStream_t st, int use_tc,
-                             int* info) {
+                             int* info, bool blocked_order) {
   const int mode = use_tc;
   const bool tc = mode != 0;
   if (mode < 0 || mode > TC_BF16X3) {
@@ -696,7 +696,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     }
     return factor_cols(k, kb, c0 + h, w - h);
   };
-  const bool blocked = mode == TC_LEGACY_BF16X3;  // the sub-panel-by-sub-panel order of the first kernel
+  const bool blocked = blocked_order || mode == TC_LEGACY_BF16X3;
   for (int k = 0; k < n; k += NB) {
     const int kb = std::min(NB, n - k);
     const int rest = n - k - kb;
@@ -750,7 +750,15 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
                                 A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
       }
       // ---- trailing update
-      TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
+      if (mode == TC_LEGACY_BF16X3)
+        TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
+      else if (tc)
+        TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)(k + kb) * n + (k + kb), n,
+                            reinterpret_cast<const float2*>(A) + (size_t)(k + kb) * n + k, n,
+                            reinterpret_cast<const float2*>(A) + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
+      else
+        TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
+                        A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
     }
   }
   if (mode == TC_LEGACY_BF16X3) TT_TRY(tc_check_error(st));
@@ -761,8 +769,10 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   }
   return TT_OK;
 }
-template int lu_factor_batched_device<double2>(double2* const*, int, int, int32_t* const*, cudaStream_t, int, int*);
-template int lu_factor_batched_device<float2>(float2* const*, int, int, int32_t* const*, cudaStream_t, int, int*);
+template int lu_factor_batched_device<double2>(double2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
+                                               bool);
+template int lu_factor_batched_device<float2>(float2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
+                                              bool);
 
 template <typename T>
 int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {

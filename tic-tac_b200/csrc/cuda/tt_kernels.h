@@ -77,9 +77,11 @@ int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_te
 // B <= 4 matrices of equal n factored together (each sub-panel of all of them
 // in one cooperative launch, one grid barrier per column for the batch);
 // info[B] receives each matrix's first zero pivot (1-based) or 0.
+// blocked: the panel in 32-column steps, each followed by its rank-32 update
+// (otherwise recursive halving of the panel and of the U12 solve).
 template <typename T>
 int lu_factor_batched_device(T* const* d_L, int B, int n, int32_t* const* d_ipiv, cudaStream_t st,
-                             int use_tensor_cores, int* info);
+                             int use_tensor_cores, int* info, bool blocked = false);
 // Row permutation of the interchange sequence ipiv (host, once per factorisation).
 int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cudaStream_t st);
 // Inverted diagonal blocks of one LU factor (unit lower and upper) and their

@@ -517,14 +517,17 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       TT_CUDA_TRY(cudaStreamSynchronize(st));
       r.ms_form += ms_since(t0);
       t0 = std::chrono::steady_clock::now();
-      TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, opt.tensor_cores ? opt.tc_product : 0, info));
+      TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, opt.tensor_cores ? opt.tc_product : 0, info,
+                                              opt.panel_blocked));
       r.ms_factor += ms_since(t0);
     } else {
       TT_TRY(form_L_device<double2>(A_.ptr, G_.ptr + (size_t)2 * n * g0, n, L64.ptr, st));
       TT_CUDA_TRY(cudaStreamSynchronize(st));
       r.ms_form += ms_since(t0);
       t0 = std::chrono::steady_clock::now();
-      TT_TRY(lu_factor_device<double2>(L64.ptr, n, ipiv_all.ptr, st, 0, &info[0]));
+      double2* L64p = L64.ptr;
+      int32_t* piv0 = ipiv_all.ptr;
+      TT_TRY(lu_factor_batched_device<double2>(&L64p, 1, n, &piv0, st, 0, &info[0], opt.panel_blocked));
       r.ms_factor += ms_since(t0);
     }
     for (int q = 0; q < nb; q++)

@@ -30,6 +30,7 @@ int resolvent_noalloc(const RunParams& rp, const PWChannel& ch, int Np, int Nq, 
 struct SolveOptions {
   bool mixed = true;        // complex64 LU on tensor cores + FP64 refinement; false: complex128 LU
   bool tensor_cores = true; // trailing update on tcgen05 (mixed only)
+  bool panel_blocked = false;  // LU panels in 32-column steps instead of recursive halving
   int tc_product = 3;       // product mode of the tensor-core updates: 1 BF16x3 with N = 128 tiles,
                             // 2 TF32, 3 BF16x3 (real-row form, N = 256)
   bool pade = false;        // Pade-resummed Neumann series on the resident A instead of an LU

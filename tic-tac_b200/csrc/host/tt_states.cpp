@@ -55,7 +55,11 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       rp.precision = value;
     } else if (key == "refine_tol") rp.refine_tol = std::stod(value);
     else if (key == "refine_max_iter") rp.refine_max_iter = std::stoi(value);
-    else if (key == "tc_product") {
+    else if (key == "panel_order") {
+      if (value == "blocked") rp.panel_blocked = true;
+      else if (value == "recursive") rp.panel_blocked = false;
+      else return bad("panel_order (recursive or blocked)");
+    } else if (key == "tc_product") {
       if (value == "bf16x3_n128") rp.tc_product = 1;
       else if (value == "tf32") rp.tc_product = 2;
       else if (value == "bf16x3") rp.tc_product = 3;

@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc", "tt_profile_begin", "tt_profile_end",
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
-    "tt_run_solve_energies",
+    "tt_run_solve_energies", "tt_profile_select",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
@@ -278,9 +278,15 @@ class tt_kernel_profile(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_ulonglong), ("ms", c_double), ("flops", c_double), ("bytes", c_double)]
 
 
-def profile_begin() -> None:
-    """Start event timing of the kernel classes in PROFILE_CLASSES."""
-    _check(load().tt_profile_begin())
+def profile_begin(classes=None) -> None:
+    """Start event timing of the kernel classes in PROFILE_CLASSES (or only of
+    the named ones)."""
+    lib = load()
+    mask = (1 << len(PROFILE_CLASSES)) - 1 if classes is None else \
+        sum(1 << PROFILE_CLASSES.index(c) for c in classes)
+    lib.tt_profile_select.argtypes = [ctypes.c_ulonglong]
+    _check(lib.tt_profile_select(mask))
+    _check(lib.tt_profile_begin())
 
 
 def profile_end() -> dict:
