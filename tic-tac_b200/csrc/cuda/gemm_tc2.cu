@@ -222,7 +222,7 @@ __device__ __forceinline__ void load_c_chunk(const float2* __restrict__ C, int l
 template <int MODE>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     k_lu_update_tc2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                    float2* __restrict__ C, int ldc, int M, int N, int K, int a_plane, int* err) {
+                    float2* __restrict__ C, int ldc, int M, int N, int K, int a_plane, int store, int* err) {
   using CF = Cfg<MODE>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -347,8 +347,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       const uint32_t aph = (uint32_t)(local >> 1) & 1u;
       const int row0 = tm * BM + quarter * 32;
       float2 cv[16];
-      // the first chunk's C is fetched while the accumulator fills
-      load_c_chunk(C, ldc, M, N, row0, tn * BN + half * (BN / 2), lane, cv);
+      // the first chunk's C is fetched while the accumulator fills (store: C = acc, nothing to fetch)
+      if (!store) load_c_chunk(C, ldc, M, N, row0, tn * BN + half * (BN / 2), lane, cv);
       if (!mbar_wait(&acc_full[ab], aph, err, 4)) break;
       tc_fence_after();
       const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16) + ab * (2 * BN);
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       for (int cc = 0; cc < BN / 2; cc += 16) {
         const int col = half * (BN / 2) + cc;
         const int gcol0 = tn * BN + col;
-        if (cc > 0) load_c_chunk(C, ldc, M, N, row0, gcol0, lane, cv);
+        if (cc > 0 && !store) load_c_chunk(C, ldc, M, N, row0, gcol0, lane, cv);
         float re[16], im[16];
         tmem_ld16(lane_addr + col, re);
         tmem_ld16(lane_addr + BN + col, im);
@@ -369,7 +369,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
           const int idx = i * 32 + lane, r = idx >> 4, c = idx & 15;
           const int grow = row0 + r, gcol = gcol0 + c;
           const float2 a = stage[r * 16 + (c ^ (r & 15))];
-          if (grow < M && gcol < N) C[(size_t)grow * ldc + gcol] = make_float2(cv[i].x - a.x, cv[i].y - a.y);
+          if (grow < M && gcol < N)
+            C[(size_t)grow * ldc + gcol] = store ? a : make_float2(cv[i].x - a.x, cv[i].y - a.y);
         }
         __syncwarp();
       }
@@ -510,7 +511,7 @@ TC2Workspace& workspace2() {
 
 template <int MODE>
 int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
-               cudaStream_t st) {
+               cudaStream_t st, int store) {
   using CF = tc2::Cfg<MODE>;
   TC2Workspace& ws = workspace2();
   const size_t esz = (MODE == TC_TF32) ? 4 : 2;
@@ -553,7 +554,8 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
   {
     ProfScope prof(K >= 256 ? TT_PROF_TC_UPDATE : TT_PROF_TC_PANEL, st, 8.0 * M * N * K,
                    16.0 * M * N + 8.0 * ((double)M + N) * K);
-    tc2::k_lu_update_tc2<MODE><<<grid, tc2::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, M, ws.err.ptr);
+    tc2::k_lu_update_tc2<MODE><<<grid, tc2::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, M, store,
+                                                                     ws.err.ptr);
   }
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
@@ -563,14 +565,14 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
 }  // namespace
 
 int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
-                 cudaStream_t st) {
+                 cudaStream_t st, int store) {
   if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
   if (K % tc2::KCC != 0) {
     set_error("tensor-core update needs K to be a multiple of 16");
     return TT_ERR_BADARG;
   }
-  if (mode == TC_TF32) return launch_tc2<TC_TF32>(C, ldc, L, ldl, U, ldu, M, N, K, st);
-  if (mode == TC_BF16X3) return launch_tc2<TC_BF16X3>(C, ldc, L, ldl, U, ldu, M, N, K, st);
+  if (mode == TC_TF32) return launch_tc2<TC_TF32>(C, ldc, L, ldl, U, ldu, M, N, K, st, store);
+  if (mode == TC_BF16X3) return launch_tc2<TC_BF16X3>(C, ldc, L, ldl, U, ldu, M, N, K, st, store);
   set_error("unknown tensor-core product mode " + std::to_string(mode));
   return TT_ERR_BADARG;
 }

@@ -268,9 +268,11 @@ __device__ __forceinline__ unsigned long long pivot_key(double v, int off) {
 // published row: one grid barrier, two dependent L2 reads and two block
 // barriers per column.  Row offsets below 2^20 - 1 (checked by the caller).
 // With a batch, blocks [b Gb, (b+1) Gb) factor matrix b (gridDim.x = B Gb).
+// With pk0 < pk1, the sub-panel's interchanges are also applied to the other
+// columns [pk0, c0) and [c0 + w, pk1) of its panel after one more grid barrier.
 template <typename T>
-__global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(SubpanelBatch<T> bt, int n, int c0, int w,
-                                                              PivotScratch<T> scr) {
+__global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(SubpanelBatch<T> bt, int n, int c0, int w, int pk0,
+                                                              int pk1, PivotScratch<T> scr) {
   cg::grid_group grid = cg::this_grid();
   extern __shared__ unsigned char sp_raw[];
   T* sA = reinterpret_cast<T*>(sp_raw);  // [chunk][SP]
@@ -417,6 +419,95 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(SubpanelBatch<T> b
   __syncthreads();
   for (int r = warp; r < nr; r += NW)
     if (lane < w) A[(size_t)(lo + r) * n + c0 + lane] = sA[r * SP + lane];
+  if (pk1 - pk0 > w) {
+    // every column's pivot is in ipiv once all blocks passed this barrier
+    grid.sync();
+    const int nl = c0 - pk0, nc = nl + (pk1 - (c0 + w));
+    for (int t = cta * SP_THREADS + threadIdx.x; t < nc; t += Gb * SP_THREADS) {
+      const int c = t < nl ? pk0 + t : c0 + w + (t - nl);
+      for (int jj = 0; jj < w; jj++) {
+        const int j = c0 + jj, p = __ldcg(&ipiv[j]);
+        if (p != j) {
+          const T a = A[(size_t)j * n + c];
+          A[(size_t)j * n + c] = A[(size_t)p * n + c];
+          A[(size_t)p * n + c] = a;
+        }
+      }
+    }
+  }
+}
+
+// X = L^{-1} for the w x w unit-lower block L at (r0, r0) of A (ld n),
+// w <= INV_MAX, into X[w][w] (row-major, ld w).  CTA cb computes the column
+// block [32 cb, 32 cb + 32) of X by block forward substitution, the block
+// column held in shared memory: per 32-row block, T = E - sum L[ib][jb] X[jb]
+// over the blocks already solved (256 threads, 4 entries each), then the unit
+// diagonal block solved row by row by one warp (lanes = columns).
+constexpr int INV_MAX = 512;
+constexpr int INV_LD = 33;
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv_unit_lower(const T* __restrict__ A, int n, int r0, int w,
+                                                        T* __restrict__ X) {
+  extern __shared__ unsigned char inv_raw[];
+  T* sX = reinterpret_cast<T*>(inv_raw);  // [w][INV_LD]
+  __shared__ T sT[32][INV_LD];
+  __shared__ T sD[32][INV_LD];
+  const int c0 = blockIdx.x * 32;
+  const int nb = (w + 31) / 32;
+  const int tid = threadIdx.x, row = tid >> 3, cq = (tid & 7) * 4;
+  for (int ib = blockIdx.x; ib < nb; ib++) {
+    const int i0 = ib * 32, hi = min(32, w - i0);
+    T acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      acc[q].x = (i0 + row == c0 + cq + q) ? 1 : 0;
+      acc[q].y = 0;
+    }
+    if (row < hi) {
+      const T* Lr = A + (size_t)(r0 + i0 + row) * n + r0;
+      for (int kk = c0; kk < i0; kk++) {  // rows of X above c0 are zero
+        const T l = Lr[kk];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const T x = sX[kk * INV_LD + cq + q];
+          acc[q].x -= l.x * x.x - l.y * x.y;
+          acc[q].y -= l.x * x.y + l.y * x.x;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) sT[row][cq + q] = acc[q];
+    for (int t = tid; t < 32 * 32; t += 256) {
+      const int i = t >> 5, j = t & 31;
+      T d;
+      d.x = 0;
+      d.y = 0;
+      if (i < hi && j < hi) d = A[(size_t)(r0 + i0 + i) * n + r0 + i0 + j];
+      sD[i][j] = d;
+    }
+    __syncthreads();
+    if (tid < 32) {
+      for (int i = 0; i < hi; i++) {
+        T v = sT[i][tid];
+        for (int j = 0; j < i; j++) {
+          const T d = sD[i][j], x = sX[(i0 + j) * INV_LD + tid];
+          v.x -= d.x * x.x - d.y * x.y;
+          v.y -= d.x * x.y + d.y * x.x;
+        }
+        sX[(i0 + i) * INV_LD + tid] = v;
+      }
+    }
+    __syncthreads();
+  }
+  for (int t = tid; t < w * 32; t += 256) {
+    const int r = t >> 5, c = t & 31;
+    if (c0 + c >= w) continue;
+    T v;
+    v.x = 0;
+    v.y = 0;
+    if (r >= c0) v = sX[r * INV_LD + c];
+    X[(size_t)r * w + c0 + c] = v;
+  }
 }
 
 // Interchanges of pivots [p0, p1) applied to columns [a0, a1) and [b0, b1).
@@ -565,6 +656,22 @@ int laswp2(T* A, int n, const int32_t* ipiv, int p0, int p1, int a0, int a1, int
 }
 
 template <typename T>
+int inv_unit_lower(const T* A, int n, int r0, int w, T* X, cudaStream_t st) {
+  if (w <= 0) return TT_OK;
+  if (w > INV_MAX) {
+    set_error("unit-lower inverse of a block wider than " + std::to_string(INV_MAX));
+    return TT_ERR_BADARG;
+  }
+  const int smem = w * INV_LD * (int)sizeof(T);
+  TT_TRY(smem_limit_once((const void*)k_inv_unit_lower<T>, smem));
+  ProfScope prof(TT_PROF_PANEL_TRSM, st, 8.0 / 6.0 * w * (double)w * w, 2.0 * w * (double)w * sizeof(T));
+  k_inv_unit_lower<T><<<ceil_div(w, 32), 256, smem, st>>>(A, n, r0, w, X);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+template <typename T>
 int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st) {
   if (ce <= cb) return TT_OK;
   ProfScope prof(TT_PROF_PANEL_TRSM, st, 4.0 * w * w * (double)(ce - cb), 2.0 * w * (double)(ce - cb) * sizeof(T));
@@ -625,7 +732,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   PivotScratch<T> scr{sval.ptr, sidx.ptr, srow.ptr, stop.ptr, skey.ptr};
   TT_TRY(smem_limit_once((const void*)k_subpanel_smem<T>, (int)kSubpanelSmem));
   // the sub-panel of matrices [b0, b0 + nb) in one cooperative launch
-  auto subpanel = [&](int b0, int nb, int j0, int w, int grid) -> int {
+  auto subpanel = [&](int b0, int nb, int j0, int w, int pk0, int pk1, int grid) -> int {
     SubpanelBatch<T> bt{};
     for (int b = 0; b < nb; b++) {
       bt.A[b] = As[b0 + b];
@@ -634,26 +741,27 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     }
     bt.info = d_info.ptr + b0;
     bt.B = nb;
-    int nn = n, cc0 = j0, ww = w;
-    void* args[] = {&bt, &nn, &cc0, &ww, &scr};
+    int nn = n, cc0 = j0, ww = w, p0 = pk0, p1 = pk1;
+    void* args[] = {&bt, &nn, &cc0, &ww, &p0, &p1, &scr};
     const size_t chunk = (size_t)(n - j0 + grid / nb - 1) / (grid / nb);
     TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel_smem<T>, dim3(grid), dim3(SP_THREADS), args,
                                             chunk * SP * sizeof(T), st));
     count_launch();
     return TT_OK;
   };
-  // pivoted factorisation of columns [j0, j0 + w), w <= IB, rows [j0, n), of all B matrices
-  auto leaf = [&](int j0, int w) -> int {
+  // pivoted factorisation of columns [j0, j0 + w), w <= IB, rows [j0, n), of all B matrices,
+  // with its interchanges applied to the panel's other columns [pk0, j0) and [j0 + w, pk1)
+  auto leaf = [&](int j0, int w, int pk0, int pk1) -> int {
     const size_t m = (size_t)(n - j0);
     const int Gb = G / B;
     const bool keyed = m < 0xFFFFF;
     const bool together = B > 1 && keyed && ((m + Gb - 1) / Gb) * SP * sizeof(T) <= kSubpanelSmem;
     const bool alone = keyed && ((m + G - 1) / G) * SP * sizeof(T) <= kSubpanelSmem;
     ProfScope prof(TT_PROF_SUBPANEL, st, 4.0 * m * w * w * B, 2.0 * m * w * sizeof(T) * B);
-    if (together) return subpanel(0, B, j0, w, Gb * B);
+    if (together) return subpanel(0, B, j0, w, pk0, pk1, Gb * B);
     for (int b = 0; b < B; b++) {
       if (alone) {
-        TT_TRY(subpanel(b, 1, j0, w, G));
+        TT_TRY(subpanel(b, 1, j0, w, pk0, pk1, G));
       } else {
         T* Ap = As[b];
         int nn = n, cc0 = j0, ww = w;
@@ -662,16 +770,28 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
         void* args[] = {&Ap, &nn, &cc0, &ww, &ip, &scr, &inf};
         TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_subpanel<T>, dim3(G), dim3(256), args, 0, st));
         count_launch();
+        TT_TRY(laswp2(As[b], n, ipivs[b], j0, j0 + w, pk0, j0, j0 + w, pk1, st));
       }
     }
     return TT_OK;
   };
   // split of a block of h rows or columns: the largest multiple of IB not above h / 2, at least IB
   auto half = [](int h) { return std::max(IB, (h / 2) / IB * IB); };
+  // the tensor-core modes solve a block row with the explicit inverse of its
+  // unit-lower block: X = L^{-1} once, then U = X A in one product
+  const bool inv_solve = (mode == TC_TF32 || mode == TC_BF16X3);
+  DevBuf<T> Xinv;
+  if (inv_solve) TT_TRY(Xinv.alloc((size_t)std::min(NB, INV_MAX) * std::min(NB, INV_MAX)));
   // rows [r0, r0 + h) of columns [cb, ce) <- L^{-1} of them, L the unit-lower h x h block at (r0, r0):
   // halves recursively, so that most of the work is one update of depth h / 2
   std::function<int(T*, int, int, int, int)> trsm_rec = [&](T* A, int r0, int h, int cb, int ce) -> int {
     if (h <= IB) return trsm_blk(A, n, r0, h, cb, ce, st);
+    if (inv_solve && h % 16 == 0 && h <= INV_MAX) {
+      TT_TRY(inv_unit_lower(A, n, r0, h, Xinv.ptr, st));
+      return tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)r0 * n + cb, n,
+                          reinterpret_cast<const float2*>(Xinv.ptr), h,
+                          reinterpret_cast<const float2*>(A) + (size_t)r0 * n + cb, n, h, ce - cb, h, st, 1);
+    }
     const int h1 = half(h);
     TT_TRY(trsm_rec(A, r0, h1, cb, ce));
     TT_TRY(panel_gemm_sub(mode, A + (size_t)(r0 + h1) * n + cb, n, A + (size_t)(r0 + h1) * n + r0, n,
@@ -682,9 +802,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   // left half, its U block and the update of the right half (depth w / 2), right half
   std::function<int(int, int, int, int)> factor_cols = [&](int k, int kb, int c0, int w) -> int {
     if (w <= IB) {
-      TT_TRY(leaf(c0, w));
-      for (int b = 0; b < B; b++) TT_TRY(laswp2(As[b], n, ipivs[b], c0, c0 + w, k, c0, c0 + w, k + kb, st));
-      return TT_OK;
+      return leaf(c0, w, k, k + kb);
     }
     const int h = half(w);
     TT_TRY(factor_cols(k, kb, c0, h));
@@ -721,11 +839,9 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     // ---- panel [k, k+kb) in sub-panels of IB columns
     for (int j0 = k; j0 < k + kb; j0 += IB) {
       const int w = std::min(IB, k + kb - j0);
-      TT_TRY(leaf(j0, w));
+      TT_TRY(leaf(j0, w, k, k + kb));
       for (int b = 0; b < B; b++) {
         T* A = As[b];
-        const int32_t* ipiv = ipivs[b];
-        TT_TRY(laswp2(A, n, ipiv, j0, j0 + w, k, j0, j0 + w, k + kb, st));
         const int right = k + kb - (j0 + w);
         if (right > 0) {
           TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
@@ -740,8 +856,11 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
       // ---- interchanges outside the panel
       TT_TRY(laswp2(A, n, ipiv, k, k + kb, 0, k, k + kb, n, st));
       if (rest <= 0) continue;
-      // ---- U12 = L11^{-1} A12, blocked by IB
-      for (int i0 = k; i0 < k + kb; i0 += IB) {
+      // ---- U12 = L11^{-1} A12: with the explicit inverse in the tensor-core
+      // modes, else blocked by IB
+      if (inv_solve) {
+        TT_TRY(trsm_rec(A, k, kb, k + kb, n));
+      } else for (int i0 = k; i0 < k + kb; i0 += IB) {
         const int wi = std::min(IB, k + kb - i0);
         TT_TRY(trsm_blk(A, n, i0, wi, k + kb, n, st));
         const int below = k + kb - (i0 + wi);

@@ -18,9 +18,11 @@ int tc_check_error(cudaStream_t st);
 constexpr int TC_LEGACY_BF16X3 = 1;  // gemm_tc.cu: four real products, N = 128, BF16x3 (12 MMAs per k16)
 constexpr int TC_TF32 = 2;           // gemm_tc2.cu: real-row form, N = 256, one tf32 product
 constexpr int TC_BF16X3 = 3;         // gemm_tc2.cu: real-row form, N = 256, BF16x3 (3 MMAs per k16)
-// C[M x N] -= L[M x K] U[K x N] in the real-row form (gemm_tc2.cu), K % 16 == 0.
+// C[M x N] -= L[M x K] U[K x N] in the real-row form (gemm_tc2.cu), K % 16 == 0;
+// store != 0: C = L U (C is not read; it may be U's own storage, which is
+// packed before the product, but must not overlap L).
 int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
-                 cudaStream_t st);
+                 cudaStream_t st, int store = 0);
 int tc2_check_error(cudaStream_t st);
 // C[M x N] -= L[M x K] U[K x N], complex128, on the FP64 tensor cores (zgemm_dmma.cu).
 int zgemm_sub_dmma(double2* C, int ldc, const double2* L, int ldl, const double2* U, int ldu, int M, int N, int K,
