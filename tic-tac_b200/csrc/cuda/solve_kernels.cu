@@ -160,16 +160,23 @@ __global__ void __launch_bounds__(256) k_ct(int Na, int Nq, int Np, const int32_
   double acc[MAXH];
 #pragma unroll
   for (int h = 0; h < MAXH; h++) acc[h] = 0.0;
+  constexpr int PU = 8;  // B rows loaded ahead of their products (independent loads in flight)
   for (int t = 0; t < ncpl; t++) {
     const int ai = cpl[t0 + t];
     const double* Bcol = B + ((size_t)ai * Nq * Np + (size_t)q * Np) * n + c;
     const double* Ct = sCt + t * Np * Np;
-    for (int pi = 0; pi < Np; pi++) {
-      const double bv = Bcol[(size_t)pi * n];
+    for (int p0 = 0; p0 < Np; p0 += PU) {
+      double bv[PU];
 #pragma unroll
-      for (int h = 0; h < MAXH; h++) {
-        const int pr = 2 * h + half;
-        if (pr < Np) acc[h] += Ct[pr * Np + pi] * bv;
+      for (int u = 0; u < PU; u++) bv[u] = (p0 + u < Np) ? __ldcs(Bcol + (size_t)(p0 + u) * n) : 0.0;
+#pragma unroll
+      for (int u = 0; u < PU; u++) {
+        if (p0 + u >= Np) break;
+#pragma unroll
+        for (int h = 0; h < MAXH; h++) {
+          const int pr = 2 * h + half;
+          if (pr < Np) acc[h] += Ct[pr * Np + p0 + u] * bv[u];
+        }
       }
     }
   }
@@ -177,7 +184,7 @@ __global__ void __launch_bounds__(256) k_ct(int Na, int Nq, int Np, const int32_
 #pragma unroll
   for (int h = 0; h < MAXH; h++) {
     const int pr = 2 * h + half;
-    if (pr < Np) Acol[(size_t)pr * n] = acc[h];
+    if (pr < Np) __stcs(Acol + (size_t)pr * n, acc[h]);
   }
 }
 
