@@ -44,7 +44,13 @@ CONFIGS = {
     "j3_J7_n12": dict(potential_model="LO_internal", J_2N_max=3, two_J_3N_max=7, Np_WP=12, Nq_WP=12),
     # small case for quick checks of this script
     "j1_J3_n12": dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=12, Nq_WP=12),
+    # the batched energy scan: j <= 2, J <= 5/2 (six channels, n = 10,944 .. 20,160), Np = Nq = 24,
+    # 64 lab energies drawn uniformly in 1-200 MeV (seed 2024) collapsing to their distinct on-shell
+    # bins; each channel's bins factored four at a time; LO-OPEP stands in for Nijmegen-I
+    "j2_J5_n24_scan64": dict(potential_model="LO_internal", J_2N_max=2, two_J_3N_max=5, Np_WP=24, Nq_WP=24),
 }
+# lab energies of the scan configurations: (count, low MeV, high MeV, seed)
+SCANS = {"j2_J5_n24_scan64": (64, 1.0, 200.0, 2024)}
 METRIC = "energies/sec, mixed+refined vs FP64 on B200 at <=1e-10 rel err in on-shell U"
 
 
@@ -203,12 +209,15 @@ def roofline_of(kern, timed_ms, ms_step, ns, nE, product="bf16x3"):
     return roof, kernels
 
 
-def scan_lab_energies(cfg, world):
+def scan_lab_energies(cfg, world, name=""):
     """Lab energies of the workload at `world` GPUs: T_lab = 10 MeV (two
     on-shell bins) on one GPU; on N GPUs the scan continues with N - 1 further
     lab energies placed between the next pairs of bin mid-points, so every lab
     energy brings two new on-shell bins (2N bins in all) and the (channel,
     energy) items grow with N."""
+    if name in SCANS:
+        count, lo, hi, seed = SCANS[name]
+        return sorted(float(x) for x in np.random.default_rng(seed).uniform(lo, hi, count))
     if world == 1:
         return [10.0]
     import tictac_b200 as tt
@@ -236,7 +245,7 @@ def run_ours(args, world, rank, local, pg):
     import tictac_b200 as tt
     from tictac_b200 import shard
     cfg = dict(CONFIGS[args.config])
-    lab = scan_lab_energies(cfg, world)
+    lab = scan_lab_energies(cfg, world, args.config)
     cfg["lab_energies"] = ",".join(f"{x:.12g}" for x in lab)
     cfg["tc_product"] = args.tc_product
     cfg["panel_order"] = args.panel_order
@@ -248,7 +257,8 @@ def run_ours(args, world, rank, local, pg):
     T_lab, E_com, q_idx = run.energies()
     nE = len(T_lab)
     # (channel, energies) items over the ranks, longest processing time first
-    plans = shard.plan([infos_all[c]["n"] for c in all_chans], nE, world, group=2)
+    group = 4 if args.config in SCANS else 2  # energies factored together per channel
+    plans = shard.plan([infos_all[c]["n"] for c in all_chans], nE, world, group=group)
     mine = {all_chans[i]: js for i, js in plans[rank].items()}
     infos = [infos_all[c] for c in all_chans]
     nnz = {c: run.build_P123(c) for c in mine}  # resident for the whole run
@@ -447,13 +457,14 @@ def _read_meta(path):
     return chans, steps, timing
 
 
-def reference_info(cfg):
+def reference_info(cfg, lab):
     """Channel sizes, on-shell energies and deuteron states of the workload from
     the reference build's own state-space set-up (tictac_ref info)."""
     if not os.path.exists(REF_BIN):
         return None, "oracle/_ref/tictac_ref not built"
+    energies = ",".join(f"{x:.12g}" for x in lab)
     with tempfile.TemporaryDirectory() as out:
-        subprocess.run([REF_BIN, "info", out] + _ref_opts(cfg, cfg["Np_WP"]), check=True, cwd=out,
+        subprocess.run([REF_BIN, "info", out] + _ref_opts(cfg, cfg["Np_WP"], energies), check=True, cwd=out,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=600)
         chans, _, _ = _read_meta(os.path.join(out, "meta.txt"))
     return [{"n": c["n"], "nE": c["nE"], "nd": c["nd"]} for c in chans], None
@@ -532,7 +543,8 @@ def main():
         # the reference's own CPU path; nothing of this repository's library is loaded
         if int(os.environ.get("RANK", "0")) != 0:
             return
-        infos, why = reference_info(cfg)
+        lab = scan_lab_energies(cfg, 1, args.config) if args.config in SCANS else [10.0]
+        infos, why = reference_info(cfg, lab)
         if infos is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return
