@@ -5,8 +5,8 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
-#include <set>
-#include <tuple>
+#include <map>
+#include <utility>
 
 #include "tt_kernels.h"
 
@@ -568,14 +568,14 @@ int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h
 
 int smem_limit_once(const void* kernel, int bytes) {
   static std::mutex mu;
-  static std::set<std::tuple<const void*, int, int>> done;
+  static std::map<std::pair<const void*, int>, int> limit;  // (kernel, device) -> limit set so far
   int dev = 0;
   TT_CUDA_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lock(mu);
-  const auto key = std::make_tuple(kernel, dev, bytes);
-  if (done.count(key)) return TT_OK;
+  int& cur = limit[std::make_pair(kernel, dev)];
+  if (bytes <= cur) return TT_OK;  // only ever raised: a launch needing less still fits
   TT_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  done.insert(key);
+  cur = bytes;
   return TT_OK;
 }
 

@@ -101,8 +101,8 @@ struct DeviceCSR {
 
 inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 
-// Raises a kernel's dynamic shared-memory limit to `bytes` on the current
-// device, once per (kernel, device, bytes): function attributes are per device.
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` (never lowers it): function attributes are per device.
 int smem_limit_once(const void* kernel, int bytes);
 
 }  // namespace tt
