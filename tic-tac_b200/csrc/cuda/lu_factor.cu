@@ -463,18 +463,31 @@ __global__ void __launch_bounds__(256) k_inv_unit_lower(const T* __restrict__ A,
       acc[q].x = (i0 + row == c0 + cq + q) ? 1 : 0;
       acc[q].y = 0;
     }
-    if (row < hi) {
-      const T* Lr = A + (size_t)(r0 + i0 + row) * n + r0;
-      for (int kk = c0; kk < i0; kk++) {  // rows of X above c0 are zero
-        const T l = Lr[kk];
+    // rows of X above c0 are zero: sum over the 32-column tiles [c0, i0) of the
+    // block row, each staged in shared memory with coalesced loads
+    for (int k0 = c0; k0 < i0; k0 += 32) {
+      __syncthreads();
+      for (int t = tid; t < 32 * 32; t += 256) {
+        const int i = t >> 5, j = t & 31;
+        T l;
+        l.x = 0;
+        l.y = 0;
+        if (i < hi) l = A[(size_t)(r0 + i0 + i) * n + r0 + k0 + j];
+        sD[i][j] = l;
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int kk = 0; kk < 32; kk++) {
+        const T l = sD[row][kk];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          const T x = sX[kk * INV_LD + cq + q];
+          const T x = sX[(k0 + kk) * INV_LD + cq + q];
           acc[q].x -= l.x * x.x - l.y * x.y;
           acc[q].y -= l.x * x.y + l.y * x.x;
         }
       }
     }
+    __syncthreads();
 #pragma unroll
     for (int q = 0; q < 4; q++) sT[row][cq + q] = acc[q];
     for (int t = tid; t < 32 * 32; t += 256) {
