@@ -325,7 +325,14 @@ int tt_run_solve_energies(tt_run* run, int chn, int precision, int n_sel, const 
                           tt_solve_report* report);
 /* tt_run_solve plus dU/dtheta (see tt_solve_faddeev_adjoint), for dV/dtheta
  * arrays over all 2N channels of the run (sizes as tt_run_get_host_array
- * which = 3 and 4). */
+ * which = 3 and 4).  With the run option adjoint_basis=total (default) this is
+ * the total derivative: the SWP eigenvectors C, bin energies e_SWP and the
+ * deuteron energy move with the potential (first-order perturbation of each
+ * 2N block's eigenproblem, CPP/make_swp_states.cpp:114-183), and with them the
+ * resolvent (CPP/make_resolvent.cpp:14-80, energies E_com + E_bound):
+ *   dU = lambda^T dA (e + G o x) + (A^T lambda)^T (dG o x),
+ *   dA = OP(dC)^T (2P) OP(V C) + OP(C)^T (2P) OP(dV C + V dC).
+ * adjoint_basis=fixed keeps the basis and G, as tt_solve_faddeev_adjoint. */
 int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const double* dV_WP_unco_dtheta,
                          const double* dV_WP_coup_dtheta, tt_complex* U, tt_complex* dU_dtheta,
                          tt_solve_report* report);

@@ -1,10 +1,14 @@
 """Adjoint dU/dtheta (tt_solve_faddeev_adjoint, tt_run_solve_adjoint) against
-central finite differences of the FP64 solve, and the potential's LEC
-derivatives.
+central finite differences, and the potential's LEC derivatives.
 
-The derivative is that of the solve with respect to its potential arguments:
-the scattering wave-packet basis (C, e_SWP) and the resolvent G are inputs of
-solve_faddeev_equations and stay fixed, as in the finite differences here."""
+Two derivatives are checked.  The drop-in adjoint differentiates
+solve_faddeev_equations with respect to its potential arguments: the
+scattering wave-packet basis (C, e_SWP) and the resolvent G are inputs of that
+function and stay fixed, as in the finite differences of the drop-in solve.
+The run handle's adjoint (adjoint_basis=total, the default) is the physical
+derivative: the SWP eigenstates, bin energies and deuteron energy move with the
+potential, and with them the resolvent; it is checked against differences of
+whole runs with shifted low-energy constants."""
 import numpy as np
 import pytest
 
@@ -107,7 +111,7 @@ def test_adjoint_run_handle_lec_gradients():
     # differences of the drop-in FP64 solve with V +- h dV/dC
     opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=8, Nq_WP=8, Nphi=20, Nx=20,
                 lab_energies="12")
-    run = tt.Run(**opts)
+    run = tt.Run(**opts, adjoint_basis="fixed")
     Np = Nq = 8
     T, E_com, q_idx = run.energies()
     dV = [run.lec_derivative(k) for k in range(2)]
@@ -177,3 +181,46 @@ def test_torch_autograd_wrapper():
         e[k] = h
         fd = ((u_of_theta(e, problem).abs() ** 2).sum() - (u_of_theta(-e, problem).abs() ** 2).sum()) / (2 * h)
         assert abs(fd.item() - theta.grad[k].item()) <= 1e-6 * abs(theta.grad[k].item())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [tt.PRECISION_FP64, tt.PRECISION_MIXED])
+def test_adjoint_total_derivative_matches_full_runs(precision):
+    # dU/dC_1S0 and dU/dC_3S1 with the chain rule through the SWP eigenstates,
+    # bin energies, deuteron energy and resolvent, against central differences
+    # of whole FP64 runs with the constants shifted by +- 1e-4 of their value
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=8, Nq_WP=8, Nphi=20, Nx=20,
+                lab_energies="12")
+    run = tt.Run(**opts)
+    lecs = run.lecs()
+    dV = [run.lec_derivative(k) for k in range(2)]
+    dVu = np.stack([d[0] for d in dV])
+    dVc = np.stack([d[1] for d in dV])
+    shifted = []
+    for k in range(2):
+        h = 1e-4 * abs(lecs[k])
+        pair = []
+        for sgn in (1.0, -1.0):
+            off = [0.0, 0.0]
+            off[k] = sgn * h
+            pair.append(tt.Run(lec_offsets=",".join(repr(o) for o in off), **opts))
+        shifted.append((h, pair))
+    fixed = tt.Run(**opts, adjoint_basis="fixed")
+    miss = []
+    for c in range(run.num_channels):
+        U, dU, rep = run.solve_adjoint(c, dVu, dVc, precision)
+        _, dU_fixed, _ = fixed.solve_adjoint(c, dVu, dVc, tt.PRECISION_FP64)
+        for k, (h, (rp, rm)) in enumerate(shifted):
+            Up, _ = rp.solve(c, tt.PRECISION_FP64)
+            Um, _ = rm.solve(c, tt.PRECISION_FP64)
+            fd = (Up - Um) / (2 * h)
+            assert np.max(np.abs(fd)) > 0
+            assert rel(dU[k], fd) <= FD_TOL, (c, k, rel(dU[k], fd))
+            miss.append(rel(dU_fixed[k], fd))
+    # the basis held fixed misses the chain rule by far more than the tolerance
+    assert max(miss) > 100 * FD_TOL, miss
+    for _, pair in shifted:
+        for r in pair:
+            r.close()
+    fixed.close()
+    run.close()

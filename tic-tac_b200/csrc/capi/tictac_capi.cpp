@@ -567,15 +567,41 @@ int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const
   const std::vector<int> deut = deuteron_indices(ch);
   std::vector<double> Uh, dUh, dvc;
   AdjointRequest adj;
-  DevBuf<double> d_dvc;
+  DevBuf<double> d_dvc, d_dc, d_de;
   if (n_theta > 0) {
     size_t per = 0;
     TT_TRY(dvc_blocks(run->rp, ch, run->swp, n_theta, dVu, dVc, dvc, per));
-    TT_TRY(d_dvc.upload(dvc, run_stream(run)));
     adj.n_theta = n_theta;
-    adj.d_dVC = d_dvc.ptr;
     adj.vc_count = per;
     adj.dU = &dUh;
+    if (run->rp.adjoint_total) {
+      // the SWP basis moves with the potential: dC, de_SWP, dE_bound per
+      // parameter, and d(V C) = dV C + V dC
+      const size_t Np = run->swp.Np_WP, nu = Np * Np * run->swp.n_unco, nc = 4 * Np * Np * run->swp.n_coup;
+      std::vector<double> dcb, deb;
+      for (int k = 0; k < n_theta; k++) {
+        SWPStates dswp;
+        swp_derivative(run->fwp, run->V_unco, run->V_coup, run->swp, dVu + k * nu, nc ? dVc + k * nc : nullptr,
+                       dswp);
+        ChannelLayout Ld;
+        std::string err;
+        if (!build_channel_layout(run->rp, ch, dswp, run->V_unco, run->V_coup, Ld, &err)) return fail(TT_ERR_BADARG, err);
+        if (Ld.VC.size() != per) return fail(TT_ERR_BADARG, "derivative blocks do not match the channel layout");
+        for (size_t i = 0; i < per; i++) dvc[(size_t)k * per + i] += Ld.VC[i];  // + V dC
+        adj.c_count = Ld.C.size();
+        adj.e_count = Ld.e_swp.size();
+        dcb.insert(dcb.end(), Ld.C.begin(), Ld.C.end());
+        deb.insert(deb.end(), Ld.e_swp.begin(), Ld.e_swp.end());
+        adj.dEb.push_back(dswp.E_bound);
+      }
+      TT_TRY(d_dc.upload(dcb, run_stream(run)));
+      TT_TRY(d_de.upload(deb, run_stream(run)));
+      adj.total = true;
+      adj.d_dC = d_dc.ptr;
+      adj.d_de = d_de.ptr;
+    }
+    TT_TRY(d_dvc.upload(dvc, run_stream(run)));
+    adj.d_dVC = d_dvc.ptr;
   }
   SolveReport rep;
   s = run->chn[chn].solver->solve(run->os.q_com_idx, deut, options_of(run->rp, precision), Uh, &rep,

@@ -134,6 +134,29 @@ __global__ void k_block_apply(int Na, int Nq, int Np, const int32_t* __restrict_
 }
 
 // g_k += 2 P^T u_k over the CSR rows, warp per row
+// out_k = 2 P u_k (CSR rows, one warp per row)
+__global__ void k_spmv(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                       const double* __restrict__ val, int n, const double2* __restrict__ u, int nrhs,
+                       double2* __restrict__ out) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int r = (int)warp;
+  for (int k = 0; k < nrhs; k++) {
+    double sr = 0, si = 0;
+    for (int64_t e = rowptr[r] + lane; e < rowptr[r + 1]; e += 32) {
+      const double2 uu = u[(size_t)k * n + col[e]];
+      sr += val[e] * uu.x;
+      si += val[e] * uu.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) out[(size_t)k * n + r] = make_double2(2.0 * sr, 2.0 * si);
+  }
+}
+
 __global__ void k_spmv_t(const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                          const double* __restrict__ val, int n, const double2* __restrict__ u, int nrhs,
                          double2* __restrict__ g) {
@@ -311,6 +334,21 @@ int block_apply_device(const DeviceLayout& L, const double* d_X, const double* d
   k_block_apply<<<ceil_div(total, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, L.blk.ptr, L.part.ptr, L.cpl_off.ptr,
                                                       L.cpl.ptr, L.blk_off.ptr, L.blk_dim.ptr, d_X,
                                                       reinterpret_cast<const double2*>(d_in), nrhs,
+                                                      reinterpret_cast<double2*>(d_out));
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int spmv_device(const DeviceCSR& P, const double* d_u, int nrhs, double* d_out, cudaStream_t st) {
+  const int n = P.n;
+  if (n == 0) return TT_OK;
+  if (P.nnz == 0) {
+    TT_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(double2) * (size_t)n * nrhs, st));
+    return TT_OK;
+  }
+  k_spmv<<<ceil_div((size_t)n * 32, 256), 256, 0, st>>>(P.rowptr.ptr, P.col.ptr, P.val.ptr, n,
+                                                      reinterpret_cast<const double2*>(d_u), nrhs,
                                                       reinterpret_cast<double2*>(d_out));
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());

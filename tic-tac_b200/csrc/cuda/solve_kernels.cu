@@ -76,6 +76,62 @@ __global__ void k_resolvent(int Na, int Nq, int Np, const int32_t* __restrict__ 
   G[tid] = make_double2(re, im);
 }
 
+// First-order change dG of the resolvents of k_resolvent for a change de of
+// the SWP energy boundaries (layout of e_swp) and dEb of the deuteron energy,
+// the energies being E_j = E_com,j + E_bound (make_resolvent.cpp:14-80
+// differentiated; d(x ln|x|) = (ln|x| + 1) dx, d(x theta(x)) = theta(x) dx).
+__global__ void k_dresolvent(int Na, int Nq, int Np, const int32_t* __restrict__ e_off,
+                             const double* __restrict__ e_swp, const double* __restrict__ de_swp,
+                             const double* __restrict__ qwp, const double* __restrict__ E, int nE, double dEb,
+                             double2* __restrict__ dG) {
+  const int n = Na * Nq * Np;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (size_t)n * nE) return;
+  const int j = (int)(tid / n), idx = (int)(tid % n);
+  const int a = idx / (Nq * Np), q = (idx / Np) % Nq, p = idx % Np;
+  const double e_lo = e_swp[e_off[a] + p], e_hi = e_swp[e_off[a] + p + 1];
+  const double de_lo = de_swp[e_off[a] + p], de_hi = de_swp[e_off[a] + p + 1];
+  const double q_lo = qwp[q], q_hi = qwp[q + 1];
+  const double En = E[j], dE = dEb;
+  double dre, dim;
+  if (e_lo < 0) {
+    const double Eb = e_lo, dEbl = de_lo;
+    const double den = kMn_d + kMn_d + kMp_d + Eb;
+    const double mu1 = kMn_d * (kMn_d + kMp_d + Eb) / den;
+    const double dmu1 = kMn_d * kMn_d / (den * den) * dEbl;
+    const double Eq_lo = q_lo * q_lo / (2 * mu1), Eq_hi = q_hi * q_hi / (2 * mu1);
+    const double dEq_lo = -Eq_lo * dmu1 / mu1, dEq_hi = -Eq_hi * dmu1 / mu1;
+    const double Dq = Eq_hi - Eq_lo, dDq = dEq_hi - dEq_lo;
+    const double x = Eq_lo + Eb - En, y = Eq_hi + Eb - En;
+    const double dx = dEq_lo + dEbl - dE, dy = dEq_hi + dEbl - dE;
+    const double re = log(fabs(x / y)) / Dq;
+    const double im = (heaviside(y) - heaviside(x)) * (-M_PI) / Dq;
+    dre = (dx / x - dy / y) / Dq - re * dDq / Dq;
+    dim = -im * dDq / Dq;
+  } else {
+    const double mu1 = kMn_d * (kMn_d + kMp_d) / (kMn_d + kMn_d + kMp_d);
+    const double Eq_lo = q_lo * q_lo / (2 * mu1), Eq_hi = q_hi * q_hi / (2 * mu1);
+    const double Ep = 0.5 * (e_lo + e_hi), Eq = 0.5 * (Eq_lo + Eq_hi);
+    const double Dq = Eq_hi - Eq_lo, Dp = e_hi - e_lo;
+    const double DM = 0.5 * (Dp - Dq), DP = 0.5 * (Dp + Dq), D = Ep + Eq - En;
+    const double dDp = de_hi - de_lo, dD = 0.5 * (de_lo + de_hi) - dE;
+    const double xs[4] = {D + DM, D - DM, D + DP, D - DP};
+    const double dxs[4] = {dD + 0.5 * dDp, dD - 0.5 * dDp, dD + 0.5 * dDp, dD - 0.5 * dDp};
+    const double sg[4] = {1.0, 1.0, -1.0, -1.0};
+    double nre = 0, nim = 0, dnre = 0, dnim = 0;
+    for (int t = 0; t < 4; t++) {
+      nre += sg[t] * xs[t] * log(fabs(xs[t]));
+      nim += sg[t] * xs[t] * heaviside(xs[t]);
+      dnre += sg[t] * (log(fabs(xs[t])) + 1.0) * dxs[t];
+      dnim += sg[t] * heaviside(xs[t]) * dxs[t];
+    }
+    const double re = nre / (Dp * Dq), im = nim * M_PI / (Dp * Dq);
+    dre = dnre / (Dp * Dq) - re * dDp / Dp;
+    dim = dnim * M_PI / (Dp * Dq) - im * dDp / Dp;
+  }
+  dG[tid] = make_double2(dre, dim);
+}
+
 __device__ __forceinline__ int64_t lower_bound_col(const int32_t* __restrict__ col, int64_t lo, int64_t hi,
                                                    int32_t key) {
   while (lo < hi) {
@@ -408,6 +464,17 @@ int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d
   if (total == 0) return TT_OK;
   k_resolvent<<<ceil_div(total, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, L.e_off.ptr, L.e_swp.ptr, L.q_WP.ptr, d_E,
                                                     nE, reinterpret_cast<double2*>(d_G));
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int dresolvent_device(const DeviceLayout& L, const double* d_de, double dEb, const double* d_E, int nE, double* d_dG,
+                      cudaStream_t st) {
+  const size_t total = (size_t)L.n * nE;
+  if (total == 0) return TT_OK;
+  k_dresolvent<<<ceil_div(total, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, L.e_off.ptr, L.e_swp.ptr, d_de, L.q_WP.ptr,
+                                                     d_E, nE, dEb, reinterpret_cast<double2*>(d_dG));
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;

@@ -138,6 +138,13 @@ int make_w_device(const double* d_x, const double* d_G, const int32_t* d_rows, i
 // out_k = OP(X) in_k with X in the layout of C / VC (one block per 2N channel)
 int block_apply_device(const DeviceLayout& L, const double* d_X, const double* d_in, int nrhs, double* d_out,
                        cudaStream_t st);
+// out_k = 2 P u_k
+int spmv_device(const DeviceCSR& P, const double* d_u, int nrhs, double* d_out, cudaStream_t st);
+// dG[j*n + i]: first-order change of the resolvents for a change de of the SWP
+// energy boundaries (layout of the layout's e_swp) and dEb of the deuteron
+// energy, energies E[j] = E_com,j + E_bound
+int dresolvent_device(const DeviceLayout& L, const double* d_de, double dEb, const double* d_E, int nE, double* d_dG,
+                      cudaStream_t st);
 // g_k = 2 P^T u_k
 int spmv_t_device(const DeviceCSR& P, const double* d_u, int nrhs, double* d_g, cudaStream_t st);
 // out[a nb + b] = sum_i g_a[i] h_b[i], complex, na, nb <= 4

@@ -58,7 +58,8 @@ struct RunParams {
   int refine_max_iter = 30;
   int energy_batch = 4;  // complex64 LUs of a channel's energies factored together (1..4)
   int tc_product = 3;
-  bool panel_blocked = false;  // LU panels in 32-column steps (else recursive halving)    // tensor-core product of the complex64 LU: 1 bf16x3_n128, 2 tf32, 3 bf16x3
+  bool panel_blocked = false;  // LU panels in 32-column steps (else recursive halving)
+  bool adjoint_total = true;   // run-handle adjoint: total derivative (basis and resolvent move with V)    // tensor-core product of the complex64 LU: 1 bf16x3_n128, 2 tf32, 3 bf16x3
   std::vector<double> lab_energies; // set directly or read from energy_input_file
   // additive offsets to the potential's low-energy constants, in the model's
   // order (LO_internal: C_1S0, C_3S1 in MeV^-2; malfliet_tjon has none)
@@ -127,6 +128,16 @@ bool make_swp_states(const RunParams& rp, const FWPStates& fwp, const PWStates& 
                      SWPStates& swp, std::string* err);
 // Symmetric eigenproblem, eigenvalues ascending, eigenvectors as columns of z (row-major n x n).
 void symmetric_eigen(const double* A, int n, double* w, double* z);
+// First-order change d of the SWP states (C, e_SWP boundaries, E_bound) of
+// make_swp_states for a change (dV_unco, dV_coup) of the WP potential
+// matrices, by perturbation theory of each 2N block's eigenproblem
+// (H0 + V) C = C diag(eps): d eps_m = c_m^T dV c_m and
+// d c_m = sum_{l != m} c_l (c_l^T dV c_m) / (eps_m - eps_l), carried through
+// the bin-boundary rule of CPP/make_swp_states.cpp:146-183.  d has swp's
+// sizes; d.C_* = dC, d.e_* = de, d.E_bound = dE_bound.  Pairs of eigenvalues
+// closer than 1e-12 of their scale (degenerate) contribute nothing.
+void swp_derivative(const FWPStates& fwp, const std::vector<double>& V_unco, const std::vector<double>& V_coup,
+                    const SWPStates& swp, const double* dV_unco, const double* dV_coup, SWPStates& d);
 
 // On-shell indexing (find_on_shell_bins / find_deuteron_channels,
 // CPP/run_organizer.cpp:4-131, 342-378).

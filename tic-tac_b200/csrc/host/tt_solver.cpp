@@ -191,10 +191,9 @@ int ChannelSolver::build_A(cudaStream_t st, double* ms) {
 
 int ChannelSolver::resolvent(const std::vector<double>& E, cudaStream_t st) {
   nE_ = (int)E.size();
-  DevBuf<double> dE;
-  TT_TRY(dE.upload(E, st));
+  TT_TRY(E_.upload(E, st));
   TT_TRY(G_.alloc((size_t)2 * n * std::max(1, nE_)));
-  TT_TRY(resolvent_device(L_, dE.ptr, nE_, G_.ptr, st));
+  TT_TRY(resolvent_device(L_, E_.ptr, nE_, G_.ptr, st));
   TT_CUDA_TRY(cudaStreamSynchronize(st));
   return TT_OK;
 }
@@ -398,17 +397,50 @@ int ChannelSolver::adjoint_energy(int j, int nE, int nd, const double* Gj, const
   TT_TRY(block_apply_device(L_, L_.C.ptr, lam, nd, u, st));
   TT_TRY(spmv_t_device(P_, u, nd, g, st));
   TT_TRY(make_w_device(x, Gj, d_rows, n, nd, w, st));
-  std::vector<double> hd((size_t)2 * nd * nd);
-  for (int k = 0; k < adj.n_theta; k++) {
-    TT_TRY(block_apply_device(L_, adj.d_dVC + (size_t)k * adj.vc_count, w, nd, h, st));
-    TT_TRY(bilinear_device(n, g, nd, h, nd, dots, st));
+  // total derivative: with dA = OP(dC)^T (2P) OP(VC) + OP(C)^T (2P) OP(d(VC)) and
+  // dU = lambda^T dA w + lambda^T A (dG o x), the extra pieces are
+  // u2 = 2 P OP(VC) w and A^T lambda, once per energy
+  DevBuf<double> u2, t2, dG;
+  DevBuf<int32_t> zero_e;
+  if (adj.total) {
+    const size_t vec = (size_t)2 * n * nd;
+    TT_TRY(u2.alloc(vec));
+    TT_TRY(t2.alloc(vec));
+    TT_TRY(dG.alloc((size_t)2 * n));
+    TT_TRY(zero_e.upload(std::vector<int32_t>(nd, 0), st));
+    TT_TRY(block_apply_device(L_, L_.VC.ptr, w, nd, t2.ptr, st));
+    TT_TRY(spmv_device(P_, t2.ptr, nd, u2.ptr, st));
+    TT_TRY(gemv_t_device(A_.ptr, n, lam, nd, yT, st));
+  }
+  std::vector<double> hd((size_t)2 * nd * nd), acc((size_t)2 * nd * nd);
+  auto add_dots = [&]() -> int {
     TT_CUDA_TRY(cudaMemcpyAsync(hd.data(), dots, sizeof(double) * hd.size(), cudaMemcpyDeviceToHost, st));
     TT_CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < acc.size(); i++) acc[i] += hd[i];
+    return TT_OK;
+  };
+  for (int k = 0; k < adj.n_theta; k++) {
+    std::fill(acc.begin(), acc.end(), 0.0);
+    // lambda^T OP(C)^T (2P) OP(d(VC)) w = g^T h
+    TT_TRY(block_apply_device(L_, adj.d_dVC + (size_t)k * adj.vc_count, w, nd, h, st));
+    TT_TRY(bilinear_device(n, g, nd, h, nd, dots, st));
+    TT_TRY(add_dots());
+    if (adj.total) {
+      // (OP(dC) lambda)^T u2
+      TT_TRY(block_apply_device(L_, adj.d_dC + (size_t)k * adj.c_count, lam, nd, u, st));
+      TT_TRY(bilinear_device(n, u, nd, u2.ptr, nd, dots, st));
+      TT_TRY(add_dots());
+      // (A^T lambda)^T (dG o x)
+      TT_TRY(dresolvent_device(L_, adj.d_de + (size_t)k * adj.e_count, adj.dEb[k], E_.ptr + j, 1, dG.ptr, st));
+      TT_TRY(hadamard_device(dG.ptr, zero_e.ptr, n, x, nd, t2.ptr, st));
+      TT_TRY(bilinear_device(n, yT, nd, t2.ptr, nd, dots, st));
+      TT_TRY(add_dots());
+    }
     for (int dr = 0; dr < nd; dr++)
       for (int dc = 0; dc < nd; dc++) {
         const size_t o = (size_t)k * nd * nd * nE + (size_t)dr * nd * nE + (size_t)dc * nE + j;
-        (*adj.dU)[2 * o + 0] = hd[2 * (dr * nd + dc) + 0];
-        (*adj.dU)[2 * o + 1] = hd[2 * (dr * nd + dc) + 1];
+        (*adj.dU)[2 * o + 0] = acc[2 * (dr * nd + dc) + 0];
+        (*adj.dU)[2 * o + 1] = acc[2 * (dr * nd + dc) + 1];
       }
   }
   r.ms_adjoint += ms_since(t0);

@@ -53,9 +53,16 @@ struct SolveReport {
 // device.  dU receives [n_theta][nd][nd][nE] interleaved complex.
 struct AdjointRequest {
   int n_theta = 0;
-  const double* d_dVC = nullptr;  // n_theta * vc_count doubles
+  const double* d_dVC = nullptr;  // n_theta * vc_count doubles: d(V C) blocks (dV C, plus V dC when total)
   size_t vc_count = 0;
   std::vector<double>* dU = nullptr;
+  // total derivative: the SWP basis and the resolvent move with the potential
+  bool total = false;
+  const double* d_dC = nullptr;   // n_theta * c_count doubles: dC blocks (layout of C)
+  size_t c_count = 0;
+  const double* d_de = nullptr;   // n_theta * e_count doubles: d e_SWP (layout of the channel's e_swp)
+  size_t e_count = 0;
+  std::vector<double> dEb;        // n_theta: d E_bound
 };
 
 class ChannelSolver {
@@ -95,7 +102,7 @@ class ChannelSolver {
                      SolveReport& r, cudaStream_t st);
   DeviceLayout L_;
   DeviceCSR P_;
-  DevBuf<double> A_, G_;
+  DevBuf<double> A_, G_, E_;  // E_: the energies of the resolvents in G_
   int nE_ = 0;
 };
 

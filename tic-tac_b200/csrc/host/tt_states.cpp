@@ -55,7 +55,11 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       rp.precision = value;
     } else if (key == "refine_tol") rp.refine_tol = std::stod(value);
     else if (key == "refine_max_iter") rp.refine_max_iter = std::stoi(value);
-    else if (key == "panel_order") {
+    else if (key == "adjoint_basis") {
+      if (value == "total") rp.adjoint_total = true;
+      else if (value == "fixed") rp.adjoint_total = false;
+      else return bad("adjoint_basis (total or fixed)");
+    } else if (key == "panel_order") {
       if (value == "blocked") rp.panel_blocked = true;
       else if (value == "recursive") rp.panel_blocked = false;
       else return bad("panel_order (recursive or blocked)");

@@ -486,4 +486,83 @@ bool make_swp_states(const RunParams& rp, const FWPStates& fwp, const PWStates& 
   return true;
 }
 
+void swp_derivative(const FWPStates& fwp, const std::vector<double>& V_unco, const std::vector<double>& V_coup,
+                    const SWPStates& swp, const double* dV_unco, const double* dV_coup, SWPStates& d) {
+  const int Np = swp.Np_WP;
+  d = swp;
+  d.E_bound = 0;
+  std::fill(d.e_unco.begin(), d.e_unco.end(), 0.0);
+  std::fill(d.e_coup.begin(), d.e_coup.end(), 0.0);
+  std::vector<double> H0(Np);
+  for (int i = 0; i < Np; i++) {
+    const double p1 = fwp.p_WP[i], p2 = fwp.p_WP[i + 1];
+    H0[i] = (p2 * p2 + p2 * p1 + p1 * p1) / (6 * kMu23);
+  }
+  auto block = [&](int dim, bool coupled, const double* V, const double* dV, const double* C, double* dC, double* de) {
+    // H and dH symmetric from their upper triangles, as make_swp_states builds H
+    std::vector<double> H((size_t)dim * dim), dH((size_t)dim * dim);
+    for (int i = 0; i < dim; i++)
+      for (int j = i; j < dim; j++) {
+        double h = V[(size_t)i * dim + j];
+        if (i == j) h += H0[i % Np];
+        H[(size_t)i * dim + j] = H[(size_t)j * dim + i] = h;
+        dH[(size_t)i * dim + j] = dH[(size_t)j * dim + i] = dV[(size_t)i * dim + j];
+      }
+    // eps_m (Rayleigh quotients of the stored eigenvectors) and M = C^T dH C
+    std::vector<double> HC((size_t)dim * dim, 0.0), dHC((size_t)dim * dim, 0.0), eps(dim), M((size_t)dim * dim);
+    for (int i = 0; i < dim; i++)
+      for (int k = 0; k < dim; k++) {
+        const double h = H[(size_t)i * dim + k], dh = dH[(size_t)i * dim + k];
+        for (int m = 0; m < dim; m++) {
+          HC[(size_t)i * dim + m] += h * C[(size_t)k * dim + m];
+          dHC[(size_t)i * dim + m] += dh * C[(size_t)k * dim + m];
+        }
+      }
+    for (int l = 0; l < dim; l++)
+      for (int m = 0; m < dim; m++) {
+        double s = 0, sh = 0;
+        for (int i = 0; i < dim; i++) {
+          s += C[(size_t)i * dim + l] * dHC[(size_t)i * dim + m];
+          if (l == m) sh += C[(size_t)i * dim + l] * HC[(size_t)i * dim + m];
+        }
+        M[(size_t)l * dim + m] = s;
+        if (l == m) eps[m] = sh;
+      }
+    for (int m = 0; m < dim; m++)
+      for (int i = 0; i < dim; i++) {
+        double v = 0;
+        for (int l = 0; l < dim; l++) {
+          if (l == m) continue;
+          const double gap = eps[m] - eps[l];
+          if (std::fabs(gap) <= 1e-12 * (std::fabs(eps[m]) + std::fabs(eps[l]) + 1.0)) continue;
+          v += C[(size_t)i * dim + l] * M[(size_t)l * dim + m] / gap;
+        }
+        dC[(size_t)i * dim + m] = v;
+      }
+    // bin boundaries (make_swp_bin_boundaries): mid-points of consecutive
+    // eigenvalues per half, the last bin as wide again as half the one before,
+    // the bound state's bin [E_bound, 0]
+    for (int h = 0; h < (coupled ? 2 : 1); h++) {
+      double* e = de + h * (Np + 1);
+      const int off = h * Np;
+      e[0] = 0;
+      for (int i = 0; i < Np - 1; i++) e[i + 1] = 0.5 * (M[(size_t)(off + i + 1) * dim + off + i + 1] +
+                                                      M[(size_t)(off + i) * dim + off + i]);
+      e[Np] = M[(size_t)(off + Np - 1) * dim + off + Np - 1] + 0.5 * (e[Np - 1] - e[Np - 2]);
+    }
+    if (eps[0] < 0) {
+      de[0] = M[0];
+      de[1] = 0;
+      d.E_bound = M[0];
+    }
+  };
+  const size_t nu = (size_t)Np * Np, nc = (size_t)4 * Np * Np;
+  for (int b = 0; b < swp.n_unco; b++)
+    block(Np, false, &V_unco[b * nu], dV_unco + b * nu, &swp.C_unco[b * nu], &d.C_unco[b * nu],
+          &d.e_unco[(size_t)b * (Np + 1)]);
+  for (int b = 0; b < swp.n_coup; b++)
+    block(2 * Np, true, &V_coup[b * nc], dV_coup + b * nc, &swp.C_coup[b * nc], &d.C_coup[b * nc],
+          &d.e_coup[(size_t)b * 2 * (Np + 1)]);
+}
+
 }  // namespace tt
