@@ -336,6 +336,20 @@ int tt_run_solve_energies(tt_run* run, int chn, int precision, int n_sel, const 
 int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const double* dV_WP_unco_dtheta,
                          const double* dV_WP_coup_dtheta, tt_complex* U, tt_complex* dU_dtheta,
                          tt_solve_report* report);
+/* The same derivative as a forward/backward pair, the contract of an
+ * autograd function (no counterpart in the reference):
+ * tt_run_adjoint_forward solves (as tt_run_solve) and keeps every energy's LU
+ * factor, row interchanges and refined solution in the run handle when they
+ * fit in HBM together (one energy group); tt_run_adjoint_backward takes a
+ * cotangent U_bar (layout of U) and returns
+ *   theta_bar[k] = Re sum_e conj(U_bar[e]) dU[e]/dtheta_k
+ * for n_theta derivatives dV/dtheta (as tt_run_solve_adjoint), with the kept
+ * factors (transposed solves only), or, when they were not kept, by factoring
+ * again.  One backward per forward; the kept factors are released by it. */
+int tt_run_adjoint_forward(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_report* report);
+int tt_run_adjoint_backward(tt_run* run, int chn, int n_theta, const double* dV_WP_unco_dtheta,
+                            const double* dV_WP_coup_dtheta, const tt_complex* U_bar, double* theta_bar,
+                            tt_solve_report* report);
 /* Low-energy constants of the run's potential that the option lec_offsets
  * moves (LO_internal: C_1S0, C_3S1; none for malfliet_tjon), their values,
  * and dV/dLEC_k in the WP basis for all 2N channels (the potential is linear

@@ -224,3 +224,52 @@ def test_adjoint_total_derivative_matches_full_runs(precision):
             r.close()
     fixed.close()
     run.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [tt.PRECISION_FP64, tt.PRECISION_MIXED])
+def test_forward_backward_pair_autograd(precision):
+    # the run handle's forward (factors kept) and backward (cotangent) through
+    # torch.autograd, against central differences of the loss over whole runs
+    import torch
+
+    from tictac_b200.autograd import u_of_lecs
+
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=8, Nq_WP=8, Nphi=20, Nx=20,
+                lab_energies="12")
+    c = 2
+    theta = torch.zeros(2, dtype=torch.float64, requires_grad=True)
+    loss = (u_of_lecs(theta, opts, c, precision).abs() ** 2).sum()
+    loss.backward()
+    run = tt.Run(**opts)
+    lecs = run.lecs()
+    run.close()
+    for k in range(2):
+        h = 1e-4 * abs(lecs[k])
+        e = torch.zeros(2, dtype=torch.float64)
+        e[k] = h
+        lp = (u_of_lecs(e, opts, c, tt.PRECISION_FP64).abs() ** 2).sum().item()
+        lm = (u_of_lecs(-e, opts, c, tt.PRECISION_FP64).abs() ** 2).sum().item()
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - theta.grad[k].item()) <= FD_TOL * max(abs(fd), 1e-300), (k, fd, theta.grad[k].item())
+
+
+@pytest.mark.gpu
+def test_backward_without_kept_factors_factors_again():
+    # five on-shell energies with energy_batch=2: the forward solve cannot keep
+    # every energy's factor, so backward factors again; same result as the
+    # one-call adjoint
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=1, Np_WP=8, Nq_WP=8, Nphi=16, Nx=16,
+                lab_energies="5,30,100", energy_batch=2)
+    run = tt.Run(**opts)
+    dV = [run.lec_derivative(k) for k in range(2)]
+    dVu = np.stack([d[0] for d in dV])
+    dVc = np.stack([d[1] for d in dV])
+    U, dU, _ = run.solve_adjoint(0, dVu, dVc, tt.PRECISION_MIXED)
+    Uf, _ = run.adjoint_forward(0, tt.PRECISION_MIXED)
+    assert rel_elem(Uf, U) <= 1e-10
+    Ubar = np.conj(Uf)
+    g, _ = run.adjoint_backward(0, dVu, dVc, Ubar)
+    ref = np.real(np.conj(Ubar)[None, :] * dU).sum(axis=1)
+    assert np.allclose(g, ref, rtol=1e-8, atol=0)
+    run.close()

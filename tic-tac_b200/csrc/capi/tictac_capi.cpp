@@ -45,6 +45,7 @@ int fail(int code, const std::string& msg) {
 struct ChannelState {
   std::unique_ptr<ChannelSolver> solver;
   bool have_P = false, have_A = false, have_G = false;
+  int fwd_precision = -1;  // precision of the last tt_run_adjoint_forward
 };
 
 // Per-thread stream for the drop-in entry points.
@@ -413,6 +414,51 @@ static cudaStream_t run_stream(tt_run* run) {
   return run->stream;
 }
 
+// Device blocks of an adjoint request for n_theta potential derivatives of a
+// run: d(V C) (and, for the total derivative, dC, de_SWP and dE_bound from the
+// SWP eigenproblem's first-order perturbation).
+struct AdjointBuffers {
+  DevBuf<double> dvc, dc, de;
+};
+
+static int adjoint_request(tt_run* run, const PWChannel& ch, int n_theta, const double* dVu, const double* dVc,
+                    AdjointRequest& adj, AdjointBuffers& ab) {
+  std::vector<double> dvc;
+  size_t per = 0;
+  TT_TRY(dvc_blocks(run->rp, ch, run->swp, n_theta, dVu, dVc, dvc, per));
+  adj.n_theta = n_theta;
+  adj.vc_count = per;
+  if (run->rp.adjoint_total) {
+    // the SWP basis moves with the potential: dC, de_SWP, dE_bound per
+    // parameter, and d(V C) = dV C + V dC
+    const size_t Np = run->swp.Np_WP, nu = Np * Np * run->swp.n_unco, nc = 4 * Np * Np * run->swp.n_coup;
+    std::vector<double> dcb, deb;
+    for (int k = 0; k < n_theta; k++) {
+      SWPStates dswp;
+      swp_derivative(run->fwp, run->V_unco, run->V_coup, run->swp, dVu + k * nu, nc ? dVc + k * nc : nullptr, dswp);
+      ChannelLayout Ld;
+      std::string err;
+      if (!build_channel_layout(run->rp, ch, dswp, run->V_unco, run->V_coup, Ld, &err)) return fail(TT_ERR_BADARG, err);
+      if (Ld.VC.size() != per) return fail(TT_ERR_BADARG, "derivative blocks do not match the channel layout");
+      for (size_t i = 0; i < per; i++) dvc[(size_t)k * per + i] += Ld.VC[i];  // + V dC
+      adj.c_count = Ld.C.size();
+      adj.e_count = Ld.e_swp.size();
+      dcb.insert(dcb.end(), Ld.C.begin(), Ld.C.end());
+      deb.insert(deb.end(), Ld.e_swp.begin(), Ld.e_swp.end());
+      adj.dEb.push_back(dswp.E_bound);
+    }
+    TT_TRY(ab.dc.upload(dcb, run_stream(run)));
+    TT_TRY(ab.de.upload(deb, run_stream(run)));
+    adj.total = true;
+    adj.d_dC = ab.dc.ptr;
+    adj.d_de = ab.de.ptr;
+  }
+  TT_TRY(ab.dvc.upload(dvc, run_stream(run)));
+  adj.d_dVC = ab.dvc.ptr;
+  return TT_OK;
+}
+
+
 int tt_run_num_channels(const tt_run* run, int* n) {
   if (!run || !n) return fail(TT_ERR_BADARG, "null argument");
   *n = run->pw.N_chn_3N;
@@ -565,43 +611,12 @@ int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const
   if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));
   const PWChannel ch = channel_view(run->pw, chn);
   const std::vector<int> deut = deuteron_indices(ch);
-  std::vector<double> Uh, dUh, dvc;
+  std::vector<double> Uh, dUh;
   AdjointRequest adj;
-  DevBuf<double> d_dvc, d_dc, d_de;
+  AdjointBuffers ab;
   if (n_theta > 0) {
-    size_t per = 0;
-    TT_TRY(dvc_blocks(run->rp, ch, run->swp, n_theta, dVu, dVc, dvc, per));
-    adj.n_theta = n_theta;
-    adj.vc_count = per;
+    TT_TRY(adjoint_request(run, ch, n_theta, dVu, dVc, adj, ab));
     adj.dU = &dUh;
-    if (run->rp.adjoint_total) {
-      // the SWP basis moves with the potential: dC, de_SWP, dE_bound per
-      // parameter, and d(V C) = dV C + V dC
-      const size_t Np = run->swp.Np_WP, nu = Np * Np * run->swp.n_unco, nc = 4 * Np * Np * run->swp.n_coup;
-      std::vector<double> dcb, deb;
-      for (int k = 0; k < n_theta; k++) {
-        SWPStates dswp;
-        swp_derivative(run->fwp, run->V_unco, run->V_coup, run->swp, dVu + k * nu, nc ? dVc + k * nc : nullptr,
-                       dswp);
-        ChannelLayout Ld;
-        std::string err;
-        if (!build_channel_layout(run->rp, ch, dswp, run->V_unco, run->V_coup, Ld, &err)) return fail(TT_ERR_BADARG, err);
-        if (Ld.VC.size() != per) return fail(TT_ERR_BADARG, "derivative blocks do not match the channel layout");
-        for (size_t i = 0; i < per; i++) dvc[(size_t)k * per + i] += Ld.VC[i];  // + V dC
-        adj.c_count = Ld.C.size();
-        adj.e_count = Ld.e_swp.size();
-        dcb.insert(dcb.end(), Ld.C.begin(), Ld.C.end());
-        deb.insert(deb.end(), Ld.e_swp.begin(), Ld.e_swp.end());
-        adj.dEb.push_back(dswp.E_bound);
-      }
-      TT_TRY(d_dc.upload(dcb, run_stream(run)));
-      TT_TRY(d_de.upload(deb, run_stream(run)));
-      adj.total = true;
-      adj.d_dC = d_dc.ptr;
-      adj.d_de = d_de.ptr;
-    }
-    TT_TRY(d_dvc.upload(dvc, run_stream(run)));
-    adj.d_dVC = d_dvc.ptr;
   }
   SolveReport rep;
   s = run->chn[chn].solver->solve(run->os.q_com_idx, deut, options_of(run->rp, precision), Uh, &rep,
@@ -610,6 +625,71 @@ int tt_run_solve_adjoint(tt_run* run, int chn, int precision, int n_theta, const
   if (s != TT_OK) return s;
   std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
   if (n_theta > 0) std::memcpy(dU, dUh.data(), sizeof(double) * dUh.size());
+  return TT_OK;
+}
+
+int tt_run_adjoint_forward(tt_run* run, int chn, int precision, tt_complex* U, tt_solve_report* report) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!U) return fail(TT_ERR_BADARG, "null U");
+  if (precision != TT_PRECISION_FP64 && precision != TT_PRECISION_MIXED && precision != TT_PRECISION_MIXED_SIMT)
+    return fail(TT_ERR_UNSUPPORTED, "the adjoint needs an LU precision");
+  double msA = 0;
+  if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
+  if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));
+  const std::vector<int> deut = deuteron_indices(channel_view(run->pw, chn));
+  SolveOptions o = options_of(run->rp, precision);
+  o.keep_factors = true;
+  std::vector<double> Uh;
+  SolveReport rep;
+  s = run->chn[chn].solver->solve(run->os.q_com_idx, deut, o, Uh, &rep, run_stream(run));
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  run->chn[chn].fwd_precision = precision;
+  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  return TT_OK;
+}
+
+int tt_run_adjoint_backward(tt_run* run, int chn, int n_theta, const double* dVu, const double* dVc,
+                            const tt_complex* U_bar, double* theta_bar, tt_solve_report* report) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (n_theta < 0 || (n_theta > 0 && (!U_bar || !theta_bar || !dVu || (run->swp.n_coup && !dVc))))
+    return fail(TT_ERR_BADARG, "null or negative argument");
+  const int precision = run->chn[chn].fwd_precision;
+  if (precision < 0) return fail(TT_ERR_BADARG, "no forward solve of this channel (tt_run_adjoint_forward)");
+  if (n_theta == 0) return TT_OK;
+  const PWChannel ch = channel_view(run->pw, chn);
+  const std::vector<int> deut = deuteron_indices(ch);
+  AdjointRequest adj;
+  AdjointBuffers ab;
+  TT_TRY(adjoint_request(run, ch, n_theta, dVu, dVc, adj, ab));
+  std::vector<double> dUh, Uh;
+  SolveReport rep;
+  double msA = 0;
+  if (run->chn[chn].solver->kept()) {
+    s = run->chn[chn].solver->backward(adj, dUh, &rep, run_stream(run));
+  } else {
+    // the forward factors were not kept (HBM): factor again with the request
+    if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
+    if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));
+    adj.dU = &dUh;
+    s = run->chn[chn].solver->solve(run->os.q_com_idx, deut, options_of(run->rp, precision), Uh, &rep,
+                                    run_stream(run), &adj);
+  }
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  run->chn[chn].fwd_precision = -1;
+  // theta_bar_k = Re sum_e conj(U_bar_e) dU_e / dtheta_k
+  const size_t ne = dUh.size() / 2 / (size_t)n_theta;
+  for (int k = 0; k < n_theta; k++) {
+    double acc = 0;
+    for (size_t e = 0; e < ne; e++) {
+      const double dr = dUh[2 * ((size_t)k * ne + e)], di = dUh[2 * ((size_t)k * ne + e) + 1];
+      acc += U_bar[e].re * dr + U_bar[e].im * di;
+    }
+    theta_bar[k] = acc;
+  }
   return TT_OK;
 }
 

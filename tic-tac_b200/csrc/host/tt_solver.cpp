@@ -459,6 +459,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     return TT_ERR_BADARG;
   }
   U.assign((size_t)2 * nd * nd * nE, 0.0);
+  drop_kept();
   if (adj) {
     if (!adj->dU || (adj->n_theta > 0 && !adj->d_dVC)) {
       set_error("adjoint request without output or derivative blocks");
@@ -668,7 +669,57 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
           U[2 * uu + 1] = hx[2 * ((size_t)dc * n + row) + 1];
         }
     }
+    if (opt.keep_factors && !adj && nb == nE) {
+      // one group held every energy: its factors stay for backward()
+      kept_.valid = true;
+      kept_.opt = opt;
+      kept_.nE = nE;
+      kept_.nd = nd;
+      kept_.L32 = std::move(L32all);
+      kept_.L64 = std::move(L64);
+      kept_.perm.clear();
+      for (int q = 0; q < nb; q++) kept_.perm.push_back(std::move(perm_d[q]));
+      kept_.x = std::move(x);
+      kept_.cols = std::move(cols);
+      TT_CUDA_TRY(cudaStreamSynchronize(st));
+    }
   }
+  if (rep) *rep = r;
+  return TT_OK;
+}
+
+int ChannelSolver::backward(const AdjointRequest& adj, std::vector<double>& dU, SolveReport* rep, cudaStream_t st) {
+  if (!kept_.valid) {
+    set_error("no factors kept from a forward solve");
+    return TT_ERR_UNSUPPORTED;
+  }
+  const int nE = kept_.nE, nd = kept_.nd;
+  if (nE != nE_) {
+    set_error("the resolvents changed since the forward solve");
+    return TT_ERR_BADARG;
+  }
+  if (nd > 4) {
+    set_error("the adjoint handles at most 4 deuteron states per channel");
+    return TT_ERR_UNSUPPORTED;
+  }
+  dU.assign((size_t)adj.n_theta * 2 * nd * nd * nE, 0.0);
+  SolveReport r;
+  const size_t vec = (size_t)2 * n * nd;
+  DevBuf<double> tmp, lam, yT, rT, u, g, w, h, dots;
+  for (DevBuf<double>* v : {&tmp, &lam, &yT, &rT, &u, &g, &w, &h}) TT_TRY(v->alloc(vec));
+  TT_TRY(dots.alloc((size_t)2 * nd * nd));
+  TrsvBlocks<float2> tbT32;
+  TrsvBlocks<double2> tbT64;
+  AdjointRequest a = adj;
+  a.dU = &dU;
+  for (int j = 0; j < nE; j++) {
+    void* F = kept_.opt.mixed ? (void*)(kept_.L32.ptr + (size_t)j * n * n) : (void*)kept_.L64.ptr;
+    TT_TRY(adjoint_energy(j, nE, nd, G_.ptr + (size_t)2 * n * j, kept_.cols.ptr + (size_t)j * nd, kept_.perm[j].ptr,
+                          tmp.ptr, kept_.x.ptr + vec * j, kept_.opt, F, tbT32, tbT64, lam.ptr, yT.ptr, rT.ptr, u.ptr,
+                          g.ptr, w.ptr, h.ptr, dots.ptr, a, r, st));
+  }
+  // the factors were transposed in place by the adjoint solves
+  drop_kept();
   if (rep) *rep = r;
   return TT_OK;
 }

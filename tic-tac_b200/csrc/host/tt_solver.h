@@ -37,6 +37,7 @@ struct SolveOptions {
   double refine_tol = 1e-12;
   int refine_max_iter = 30;
   int energy_batch = 4;     // complex64: energies factored together at most (1..4; fewer if HBM is short)
+  bool keep_factors = false;  // keep every energy's factor and solution for backward() (when they fit)
 };
 
 struct SolveReport {
@@ -81,10 +82,18 @@ class ChannelSolver {
   int solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
             std::vector<double>& U_interleaved, SolveReport* rep, cudaStream_t st,
             const AdjointRequest* adj = nullptr);
+  // Adjoint of the last solve(keep_factors) from the factors it kept:
+  // dU/dtheta of adj for its energies.  TT_ERR_UNSUPPORTED when nothing was
+  // kept (the energies' factors did not fit at once): the caller then runs
+  // solve() with the request, which factors again.
+  int backward(const AdjointRequest& adj, std::vector<double>& dU, SolveReport* rep, cudaStream_t st);
+  bool kept() const { return kept_.valid; }
+  void drop_kept() { kept_ = Kept(); }
   void release_A() {
     A_.release();
     G_.release();
     nE_ = 0;
+    drop_kept();
   }
   const DeviceCSR& P() const { return P_; }
   const double* A() const { return A_.ptr; }
@@ -100,6 +109,19 @@ class ChannelSolver {
                      TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT, double* rT,
                      double* u, double* g, double* w, double* h, double* dots, const AdjointRequest& adj,
                      SolveReport& r, cudaStream_t st);
+  // state a solve(keep_factors) leaves for backward(): each energy's factor,
+  // row permutation and refined solution
+  struct Kept {
+    bool valid = false;
+    SolveOptions opt;
+    int nE = 0, nd = 0;
+    DevBuf<float2> L32;
+    DevBuf<double2> L64;
+    std::vector<DevBuf<int32_t>> perm;
+    DevBuf<double> x;
+    DevBuf<int32_t> cols;
+  };
+  Kept kept_;
   DeviceLayout L_;
   DeviceCSR P_;
   DevBuf<double> A_, G_, E_;  // E_: the energies of the resolvents in G_

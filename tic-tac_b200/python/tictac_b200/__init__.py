@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "tt_gauss_legendre", "tt_calculate_resolvent_array_in_SWP_basis_noalloc", "tt_profile_begin", "tt_profile_end",
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
-    "tt_run_solve_energies", "tt_profile_select",
+    "tt_run_solve_energies", "tt_profile_select", "tt_run_adjoint_forward", "tt_run_adjoint_backward",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
@@ -479,8 +479,10 @@ class Run:
 
     def solve_adjoint(self, chn, dV_unco, dV_coup, precision=PRECISION_MIXED):
         """U and dU/dtheta_k for potential derivatives over all 2N channels of the
-        run ([n_theta][...] in the layout of host_array(3) / host_array(4)), the
-        wave-packet basis and the resolvent held fixed."""
+        run ([n_theta][...] in the layout of host_array(3) / host_array(4)): the
+        total derivative (the SWP basis, deuteron energy and resolvent move with
+        the potential), or with them held fixed when the run has
+        adjoint_basis=fixed."""
         info = self.channel_info(chn)
         nE = len(self.energies()[0])
         nd = info["n_deuteron"]
@@ -494,6 +496,29 @@ class Run:
         _check(self.lib.tt_run_solve_adjoint(self._h, chn, precision, ctypes.c_int(n_theta), _dptr(dVu), _dptr(dVc),
                                              U.ctypes.data_as(c_void_p), dU.ctypes.data_as(c_void_p), byref(rep)))
         return U, dU, rep.as_dict()
+
+    def adjoint_forward(self, chn, precision=PRECISION_MIXED):
+        """tt_run_adjoint_forward: U, keeping the factors for adjoint_backward."""
+        info = self.channel_info(chn)
+        nE = len(self.energies()[0])
+        nd = info["n_deuteron"]
+        U = np.zeros(nE * nd * nd, dtype=np.complex128)
+        rep = tt_solve_report()
+        _check(self.lib.tt_run_adjoint_forward(self._h, chn, precision, U.ctypes.data_as(c_void_p), byref(rep)))
+        return U, rep.as_dict()
+
+    def adjoint_backward(self, chn, dV_unco, dV_coup, U_bar):
+        """tt_run_adjoint_backward: theta_bar_k = Re sum conj(U_bar) dU/dtheta_k."""
+        dVu = np.ascontiguousarray(dV_unco, dtype=np.float64)
+        n_theta = dVu.shape[0]
+        dVc = np.ascontiguousarray(dV_coup if dV_coup is not None and np.size(dV_coup) else np.zeros((n_theta, 1)),
+                                   dtype=np.float64)
+        Ub = np.ascontiguousarray(U_bar, dtype=np.complex128)
+        out = np.zeros(n_theta, dtype=np.float64)
+        rep = tt_solve_report()
+        _check(self.lib.tt_run_adjoint_backward(self._h, chn, ctypes.c_int(n_theta), _dptr(dVu), _dptr(dVc),
+                                                Ub.ctypes.data_as(c_void_p), _dptr(out), byref(rep)))
+        return out, rep.as_dict()
 
     def lecs(self):
         """Values of the potential's adjustable low-energy constants."""
