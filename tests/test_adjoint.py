@@ -259,9 +259,10 @@ def test_backward_without_kept_factors_factors_again():
     # five on-shell energies with energy_batch=2: the forward solve cannot keep
     # every energy's factor, so backward factors again; same result as the
     # one-call adjoint
-    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=1, Np_WP=8, Nq_WP=8, Nphi=16, Nx=16,
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=1, Np_WP=10, Nq_WP=10, Nphi=16, Nx=16,
                 lab_energies="5,30,100", energy_batch=2)
     run = tt.Run(**opts)
+    assert len(run.energies()[0]) == 5
     dV = [run.lec_derivative(k) for k in range(2)]
     dVu = np.stack([d[0] for d in dV])
     dVc = np.stack([d[1] for d in dV])
