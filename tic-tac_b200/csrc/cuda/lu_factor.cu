@@ -438,88 +438,133 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(SubpanelBatch<T> b
 }
 
 // X = L^{-1} for the w x w unit-lower block L at (r0, r0) of A (ld n),
-// w <= INV_MAX, into X[w][w] (row-major, ld w).  CTA cb computes the column
-// block [32 cb, 32 cb + 32) of X by block forward substitution, the block
-// column held in shared memory: per 32-row block, T = E - sum L[ib][jb] X[jb]
-// over the blocks already solved (256 threads, 4 entries each), then the unit
-// diagonal block solved row by row by one warp (lanes = columns).
+// w <= INV_MAX, into X[w][w] (row-major, ld w), by recursive doubling:
+// k_inv_diag32 inverts the 32 x 32 diagonal blocks (one CTA each), then per
+// level s = 64, 128, .. every pair of inverted s/2 blocks is joined,
+//   [X11 0; X21 X22] with X21 = -X22 (L21 X11),
+// one CTA per 32 x 32 tile of X21 (k_inv_join), all pairs of a level in one
+// launch.  Entries above the diagonal are written as zero.
 constexpr int INV_MAX = 512;
-constexpr int INV_LD = 33;
 template <typename T>
-__global__ void __launch_bounds__(256) k_inv_unit_lower(const T* __restrict__ A, int n, int r0, int w,
-                                                        T* __restrict__ X) {
-  extern __shared__ unsigned char inv_raw[];
-  T* sX = reinterpret_cast<T*>(inv_raw);  // [w][INV_LD]
-  __shared__ T sT[32][INV_LD];
-  __shared__ T sD[32][INV_LD];
-  const int c0 = blockIdx.x * 32;
-  const int nb = (w + 31) / 32;
+__device__ __forceinline__ void cfma_sub(T& acc, T a, T b) {
+  acc.x -= a.x * b.x - a.y * b.y;
+  acc.y -= a.x * b.y + a.y * b.x;
+}
+template <typename T>
+__device__ __forceinline__ void cfma_add(T& acc, T a, T b) {
+  acc.x += a.x * b.x - a.y * b.y;
+  acc.y += a.x * b.y + a.y * b.x;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv_diag32(const T* __restrict__ A, int n, int r0, int w, T* __restrict__ X) {
+  __shared__ T sL[32][33];
+  __shared__ T sX[32][33];
+  const int i0 = blockIdx.x * 32, hi = min(32, w - i0);
+  for (int t = threadIdx.x; t < 32 * 32; t += 256) {
+    const int i = t >> 5, j = t & 31;
+    T l;
+    l.x = 0;
+    l.y = 0;
+    if (i < hi && j < hi) l = A[(size_t)(r0 + i0 + i) * n + r0 + i0 + j];
+    sL[i][j] = l;
+  }
+  __syncthreads();
+  // one warp, lane = column c of the inverse: row i = e_i - sum_{j<i} L[i][j] X[j]
+  if (threadIdx.x < 32) {
+    const int c = threadIdx.x;
+    for (int i = 0; i < hi; i++) {
+      T v;
+      v.x = (i == c) ? 1 : 0;
+      v.y = 0;
+      for (int j = c; j < i; j++) cfma_sub(v, sL[i][j], sX[j][c]);
+      sX[i][c] = v;
+    }
+  }
+  __syncthreads();
+  // the whole 32-row band of X: the diagonal block, zeros elsewhere in the band
+  for (int t = threadIdx.x; t < hi * w; t += 256) {
+    const int i = t / w, c = t % w;
+    T v;
+    v.x = 0;
+    v.y = 0;
+    if (c >= i0 && c - i0 < hi && c - i0 <= i) v = sX[i][c - i0];
+    X[(size_t)(i0 + i) * w + c] = v;
+  }
+}
+
+// Level s: pair p joins the blocks [p s, p s + s/2) and [p s + s/2, p s + s)
+// (the second may be shorter at the end of w).  CTA (tile ty, tx, pair p)
+// computes X21[ty][tx] = -sum_m X22[ty][m] (L21 X11)[m][tx] over the 32-row
+// tiles m of the second block.
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv_join(const T* __restrict__ A, int n, int r0, int w, int s,
+                                                  T* __restrict__ X) {
+  extern __shared__ unsigned char join_raw[];
+  T(*sT)[33] = reinterpret_cast<T(*)[33]>(join_raw);  // (L21 X11) column tile, up to s/2 rows
+  __shared__ T sa[32][33];
+  __shared__ T sb[32][33];
+  const int h = s / 2;
+  const int p = blockIdx.z, base = p * s;
+  const int h2 = min(h, w - base - h);  // rows of the second block
+  if (h2 <= 0) return;
+  const int ty = blockIdx.y, tx = blockIdx.x;  // tile row within block 2, tile column within block 1
+  if (ty * 32 >= h2) return;
   const int tid = threadIdx.x, row = tid >> 3, cq = (tid & 7) * 4;
-  for (int ib = blockIdx.x; ib < nb; ib++) {
-    const int i0 = ib * 32, hi = min(32, w - i0);
+  const int c0 = base + tx * 32;  // columns of X11 (block 1)
+  // sT[m][c] = sum_k L21[m][k] X11[k][c] for all rows m of block 2 (k over block 1; X11 lower: k >= c)
+  for (int m0 = 0; m0 < h2; m0 += 32) {
     T acc[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      acc[q].x = (i0 + row == c0 + cq + q) ? 1 : 0;
-      acc[q].y = 0;
-    }
-    // rows of X above c0 are zero: sum over the 32-column tiles [c0, i0) of the
-    // block row, each staged in shared memory with coalesced loads
-    for (int k0 = c0; k0 < i0; k0 += 32) {
+    for (int q = 0; q < 4; q++) acc[q].x = acc[q].y = 0;
+    for (int k0 = tx * 32; k0 < h; k0 += 32) {
       __syncthreads();
-      for (int t = tid; t < 32 * 32; t += 256) {
+      for (int t = tid; t < 1024; t += 256) {
         const int i = t >> 5, j = t & 31;
-        T l;
-        l.x = 0;
-        l.y = 0;
-        if (i < hi) l = A[(size_t)(r0 + i0 + i) * n + r0 + k0 + j];
-        sD[i][j] = l;
+        T a, b;
+        a.x = a.y = b.x = b.y = 0;
+        if (m0 + i < h2) a = A[(size_t)(r0 + base + h + m0 + i) * n + r0 + base + k0 + j];
+        b = X[(size_t)(base + k0 + i) * w + c0 + j];
+        sa[i][j] = a;
+        sb[i][j] = b;
       }
       __syncthreads();
 #pragma unroll 8
       for (int kk = 0; kk < 32; kk++) {
-        const T l = sD[row][kk];
+        const T a = sa[row][kk];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const T x = sX[(k0 + kk) * INV_LD + cq + q];
-          acc[q].x -= l.x * x.x - l.y * x.y;
-          acc[q].y -= l.x * x.y + l.y * x.x;
-        }
+        for (int q = 0; q < 4; q++) cfma_add(acc[q], a, sb[kk][cq + q]);
       }
     }
-    __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; q++) sT[row][cq + q] = acc[q];
-    for (int t = tid; t < 32 * 32; t += 256) {
-      const int i = t >> 5, j = t & 31;
-      T d;
-      d.x = 0;
-      d.y = 0;
-      if (i < hi && j < hi) d = A[(size_t)(r0 + i0 + i) * n + r0 + i0 + j];
-      sD[i][j] = d;
-    }
-    __syncthreads();
-    if (tid < 32) {
-      for (int i = 0; i < hi; i++) {
-        T v = sT[i][tid];
-        for (int j = 0; j < i; j++) {
-          const T d = sD[i][j], x = sX[(i0 + j) * INV_LD + tid];
-          v.x -= d.x * x.x - d.y * x.y;
-          v.y -= d.x * x.y + d.y * x.x;
-        }
-        sX[(i0 + i) * INV_LD + tid] = v;
-      }
-    }
-    __syncthreads();
+    for (int q = 0; q < 4; q++) sT[m0 + row][cq + q] = acc[q];
   }
-  for (int t = tid; t < w * 32; t += 256) {
-    const int r = t >> 5, c = t & 31;
-    if (c0 + c >= w) continue;
-    T v;
-    v.x = 0;
-    v.y = 0;
-    if (r >= c0) v = sX[r * INV_LD + c];
-    X[(size_t)r * w + c0 + c] = v;
+  __syncthreads();
+  // X21[ty][tx] = -sum_m X22[ty rows][m] sT[m][.]  (X22 lower: m <= row)
+  T acc[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) acc[q].x = acc[q].y = 0;
+  for (int m0 = 0; m0 <= ty * 32; m0 += 32) {
+    __syncthreads();
+    for (int t = tid; t < 1024; t += 256) {
+      const int i = t >> 5, j = t & 31;
+      T a;
+      a.x = a.y = 0;
+      if (ty * 32 + i < h2 && m0 + j < h2) a = X[(size_t)(base + h + ty * 32 + i) * w + base + h + m0 + j];
+      sa[i][j] = a;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < 32; kk++) {
+      const T a = sa[row][kk];
+#pragma unroll
+      for (int q = 0; q < 4; q++) cfma_sub(acc[q], a, sT[m0 + kk][cq + q]);
+    }
+  }
+  const int gr = base + h + ty * 32 + row;
+  if (ty * 32 + row < h2) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) X[(size_t)gr * w + c0 + cq + q] = acc[q];
   }
 }
 
@@ -671,16 +716,24 @@ int laswp2(T* A, int n, const int32_t* ipiv, int p0, int p1, int a0, int a1, int
 template <typename T>
 int inv_unit_lower(const T* A, int n, int r0, int w, T* X, cudaStream_t st) {
   if (w <= 0) return TT_OK;
-  if (w > INV_MAX) {
-    set_error("unit-lower inverse of a block wider than " + std::to_string(INV_MAX));
+  if (w > INV_MAX || w % 32 != 0) {
+    set_error("unit-lower inverse of a block of " + std::to_string(w) + " rows (multiples of 32 up to " +
+              std::to_string(INV_MAX) + ")");
     return TT_ERR_BADARG;
   }
-  const int smem = w * INV_LD * (int)sizeof(T);
-  TT_TRY(smem_limit_once((const void*)k_inv_unit_lower<T>, smem));
   ProfScope prof(TT_PROF_PANEL_TRSM, st, 8.0 / 6.0 * w * (double)w * w, 2.0 * w * (double)w * sizeof(T));
-  k_inv_unit_lower<T><<<ceil_div(w, 32), 256, smem, st>>>(A, n, r0, w, X);
+  k_inv_diag32<T><<<w / 32, 256, 0, st>>>(A, n, r0, w, X);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
+  for (int s = 64; s / 2 < w; s *= 2) {
+    const int h = s / 2;
+    dim3 grid(h / 32, h / 32, (w + s - 1) / s);
+    const int smem = h * 33 * (int)sizeof(T);
+    TT_TRY(smem_limit_once((const void*)k_inv_join<T>, smem));
+    k_inv_join<T><<<grid, 256, smem, st>>>(A, n, r0, w, s, X);
+    count_launch();
+    TT_CUDA_TRY(cudaGetLastError());
+  }
   return TT_OK;
 }
 
@@ -799,7 +852,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   // halves recursively, so that most of the work is one update of depth h / 2
   std::function<int(T*, int, int, int, int)> trsm_rec = [&](T* A, int r0, int h, int cb, int ce) -> int {
     if (h <= IB) return trsm_blk(A, n, r0, h, cb, ce, st);
-    if (inv_solve && h % 16 == 0 && h <= INV_MAX) {
+    if (inv_solve && h % 32 == 0 && h <= INV_MAX) {
       TT_TRY(inv_unit_lower(A, n, r0, h, Xinv.ptr, st));
       return tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)r0 * n + cb, n,
                           reinterpret_cast<const float2*>(Xinv.ptr), h,
