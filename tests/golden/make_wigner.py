@@ -29,6 +29,39 @@ def valid9(a):
             and tri(a[1], a[4], a[7]) and tri(a[2], a[5], a[8]))
 
 
+def tri_pick(a, b):
+    """A doubled j3 coupling a and b (triangle and parity), or None."""
+    lo, hi = abs(a - b), a + b
+    if hi < lo:
+        return None
+    return int(lo + 2 * rng.integers(0, (hi - lo) // 2 + 1))
+
+
+def large_9j(count, top):
+    """Valid 9j symbols with doubled arguments up to `top`: the recoupling
+    coefficients of two-body j <= 4 and three-body J <= 9/2 reach about 18."""
+    t, v = [], []
+    while len(t) < count:
+        a = [0] * 9
+        a[0], a[1] = (int(x) for x in rng.integers(0, top + 1, 2))
+        a[3], a[4] = (int(x) for x in rng.integers(0, top + 1, 2))
+        a[2], a[5] = tri_pick(a[0], a[1]), tri_pick(a[3], a[4])
+        a[6], a[7] = tri_pick(a[0], a[3]), tri_pick(a[1], a[4])
+        if None in a[:8] or max(a[:8]) > top:
+            continue
+        lo = max(abs(a[6] - a[7]), abs(a[2] - a[5]))
+        hi = min(a[6] + a[7], a[2] + a[5], top)
+        cands = [x for x in range(lo, hi + 1) if (a[6] + a[7] + x) % 2 == 0 and (a[2] + a[5] + x) % 2 == 0]
+        if not cands:
+            continue
+        a[8] = int(cands[rng.integers(0, len(cands))])
+        if not valid9(a):
+            continue
+        t.append(tuple(a))
+        v.append(float(wigner_9j(*[h(x) for x in a])))
+    return t, v
+
+
 def main():
     t3, v3 = [], []
     while len(t3) < 400:
@@ -74,7 +107,9 @@ def main():
         except ValueError:
             val = 0
         v9.append(float(val))
-    np.savez_compressed(os.path.join(HERE, "wigner.npz"), t3=np.array(t3), v3=np.array(v3), t6=np.array(t6),
+    t9b, v9b = large_9j(120, 18)
+    np.savez_compressed(os.path.join(HERE, "wigner.npz"), t9b=np.array(t9b), v9b=np.array(v9b), t3=np.array(t3),
+                        v3=np.array(v3), t6=np.array(t6),
                         v6=np.array(v6), t9=np.array(t9), v9=np.array(v9))
 
 

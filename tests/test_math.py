@@ -17,6 +17,12 @@ def test_wigner_symbols_against_sympy():
             assert tt.wigner6j(*t) == 0.0 or abs(tt.wigner6j(*t)) < 1e-16
     for t, v in zip(d["t9"], d["v9"]):
         assert abs(tt.wigner9j(*t) - v) <= 1e-13 * max(1.0, abs(v))
+    # valid 9j symbols with doubled arguments up to 18, the range the recoupling
+    # coefficients of two-body j <= 4 and J <= 9/2 reach; the same code is the
+    # 9j of the shim the reference build links, so this check is its
+    # independent pin
+    for t, v in zip(d["t9b"], d["v9b"]):
+        assert abs(tt.wigner9j(*t) - v) <= 1e-12 * max(1e-3, abs(v)), (t, v, tt.wigner9j(*t))
 
 
 def test_clebsch_gordan_orthonormality():
