@@ -518,9 +518,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=list(CONFIGS), default="j3_J7_n30")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--tc-product", choices=list(PRODUCTS), default="bf16x3",
+    ap.add_argument("--tc-product", choices=list(PRODUCTS), default="tf32",
                     help="tensor-core product of the complex64 LU")
-    ap.add_argument("--panel-order", choices=["recursive", "blocked"], default="recursive",
+    ap.add_argument("--panel-order", choices=["recursive", "blocked"], default="blocked",
                     help="LU panels by recursive halving or in 32-column steps")
     ap.add_argument("--breakdown", type=int, default=1,
                     help="one extra step with every kernel class timed, for the per-class breakdown")

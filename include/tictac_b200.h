@@ -124,6 +124,7 @@ typedef struct tt_solve_report {
   int info;             /* first zero pivot (1-based), 0 if none */
   double ms_adjoint;    /* adjoint: transposed solves, their refinement, parameter products */
   int adjoint_refine_iters;
+  int product_fallbacks; /* energy groups factored again with BF16x3 because their TF32 factors did not refine */
 } tt_solve_report;
 
 /* ---- layer 1: drop-in entry points ---------------------------------- */

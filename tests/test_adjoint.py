@@ -203,7 +203,7 @@ def test_adjoint_total_derivative_matches_full_runs(precision):
         for sgn in (1.0, -1.0):
             off = [0.0, 0.0]
             off[k] = sgn * h
-            pair.append(tt.Run(lec_offsets=",".join(repr(o) for o in off), **opts))
+            pair.append(tt.Run(lec_offsets=",".join(repr(float(o)) for o in off), **opts))
         shifted.append((h, pair))
     fixed = tt.Run(**opts, adjoint_basis="fixed")
     miss = []

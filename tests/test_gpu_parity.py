@@ -289,3 +289,19 @@ def test_energy_batched_factorisation_matches_one_at_a_time(batch):
         assert rel_elem(Ub, U_o) <= 1e-10, (c, batch, rep)
     base.close()
     run.close()
+
+
+def test_tf32_refinement_falls_back_to_bf16x3():
+    # with at most three refinement steps the TF32 factors (about 2^-11 per
+    # product, four steps to 1e-12) do not refine in time; each such energy
+    # group is factored again with BF16x3 (two steps), and U still matches the
+    # reference in every element
+    g, m = load_case("lo_j1_J3_n8")
+    run = tt.Run(**m["opts"], tc_product="tf32", refine_max_iter=3)
+    fallbacks = 0
+    for c in range(run.num_channels):
+        U, rep = run.solve(c, tt.PRECISION_MIXED)
+        assert rel_elem(U, g[f"U_c{c}"]) <= 1e-10, (c, rep)
+        fallbacks += rep["product_fallbacks"]
+    assert fallbacks >= 1
+    run.close()

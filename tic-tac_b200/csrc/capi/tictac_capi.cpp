@@ -128,6 +128,7 @@ void fill_report(const SolveReport& r, double ms_A, tt_solve_report* out) {
   out->info = r.info;
   out->ms_adjoint = r.ms_adjoint;
   out->adjoint_refine_iters = r.adjoint_refine_iters;
+  out->product_fallbacks = r.product_fallbacks;
 }
 
 // dV_k C blocks (layout of ChannelLayout::VC) of n_theta potential derivatives

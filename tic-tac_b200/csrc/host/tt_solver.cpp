@@ -5,7 +5,10 @@
 #include <complex>
 #include <cmath>
 #include <cstdlib>
+#include <algorithm>
 #include <map>
+
+#include "../cuda/tt_lu_internal.h"
 
 namespace tt {
 
@@ -534,7 +537,10 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     for (DevBuf<double>* v : {&lam, &yT, &rT, &u, &g, &w, &h}) TT_TRY(v->alloc(vec));
     TT_TRY(dots.alloc((size_t)2 * nd * nd));
   }
-  for (int g0 = 0; g0 < nE; g0 += B) {
+  // a TF32 factor whose refinement does not converge is made again with BF16x3
+  const int product0 = opt.tensor_cores ? opt.tc_product : 0;
+  int product = product0;
+  for (int g0 = 0; g0 < nE;) {
     const int nb = std::min(B, nE - g0);
     // ---- form and factor the group's matrices
     auto t0 = std::chrono::steady_clock::now();
@@ -550,8 +556,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       TT_CUDA_TRY(cudaStreamSynchronize(st));
       r.ms_form += ms_since(t0);
       t0 = std::chrono::steady_clock::now();
-      TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, opt.tensor_cores ? opt.tc_product : 0, info,
-                                              opt.panel_blocked));
+      TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, product, info, opt.panel_blocked));
       r.ms_factor += ms_since(t0);
     } else {
       TT_TRY(form_L_device<double2>(A_.ptr, G_.ptr + (size_t)2 * n * g0, n, L64.ptr, st));
@@ -615,7 +620,10 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       std::vector<std::vector<double>> prev(nb, std::vector<double>((size_t)nd + (size_t)nd * nd, 0.0));
       std::vector<double> ratio((size_t)nd + (size_t)nd * nd);
       int left = nb;
-      for (int it = 1; it <= opt.refine_max_iter && left > 0; it++) {
+      // TF32 factors refine in about 4 steps here; one that needs more than 12
+      // is made again with BF16x3 rather than iterated to the limit
+      const int max_it = product == TC_TF32 ? std::min(opt.refine_max_iter, 12) : opt.refine_max_iter;
+      for (int it = 1; it <= max_it && left > 0; it++) {
         TT_TRY(hadamard_device(Gg, rhs_e.ptr, n, x.ptr, nb * nd, y.ptr, st));
         TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nb * nd, res.ptr, st));
         for (int q = 0; q < nb; q++) {
@@ -642,12 +650,19 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
         r.final_correction = std::max(r.final_correction, worst[q]);
         if (!(worst[q] == worst[q])) r.final_correction = worst[q];
       }
-      for (int q = 0; q < nb; q++)
-        if (!done[q]) {
-          set_error("iterative refinement did not converge (last |dx|/|x| = " + std::to_string(worst[q]) + ")");
-          if (rep) *rep = r;
-          return TT_ERR_NOCONVERGE;
+      if (std::find(done.begin(), done.end(), 0) != done.end()) {
+        if (product == TC_TF32) {
+          // the same group again with the BF16x3 product
+          product = TC_BF16X3;
+          r.product_fallbacks++;
+          continue;
         }
+        int q = 0;
+        while (done[q]) q++;
+        set_error("iterative refinement did not converge (last |dx|/|x| = " + std::to_string(worst[q]) + ")");
+        if (rep) *rep = r;
+        return TT_ERR_NOCONVERGE;
+      }
     }
     // ---- per energy: adjoint, on-shell read-out (solve_faddeev.cpp:407-431)
     for (int q = 0; q < nb; q++) {
@@ -683,6 +698,8 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       kept_.cols = std::move(cols);
       TT_CUDA_TRY(cudaStreamSynchronize(st));
     }
+    g0 += nb;
+    product = product0;
   }
   if (rep) *rep = r;
   return TT_OK;

@@ -30,9 +30,10 @@ int resolvent_noalloc(const RunParams& rp, const PWChannel& ch, int Np, int Nq, 
 struct SolveOptions {
   bool mixed = true;        // complex64 LU on tensor cores + FP64 refinement; false: complex128 LU
   bool tensor_cores = true; // trailing update on tcgen05 (mixed only)
-  bool panel_blocked = false;  // LU panels in 32-column steps instead of recursive halving
-  int tc_product = 3;       // product mode of the tensor-core updates: 1 BF16x3 with N = 128 tiles,
-                            // 2 TF32, 3 BF16x3 (real-row form, N = 256)
+  bool panel_blocked = true;  // LU panels in 32-column steps instead of recursive halving
+  int tc_product = 2;        // product mode of the tensor-core updates: 1 BF16x3 with N = 128 tiles,
+                             // 2 TF32 (a group whose refinement does not converge is factored
+                             // again with 3), 3 BF16x3 (real-row form, N = 256)
   bool pade = false;        // Pade-resummed Neumann series on the resident A instead of an LU
   double refine_tol = 1e-12;
   int refine_max_iter = 30;
@@ -47,6 +48,7 @@ struct SolveReport {
   int info = 0;                  // first zero pivot (1-based) if any
   double ms_adjoint = 0;         // transposed solves, their refinement and the parameter products
   int adjoint_refine_iters = 0;  // max over energies
+  int product_fallbacks = 0;     // energy groups factored again with BF16x3 after TF32 did not refine
 };
 
 // Parameter derivatives wanted from a solve: dV/dtheta_k C for k < n_theta,

@@ -85,7 +85,7 @@ class tt_run_params(ctypes.Structure):
 class tt_solve_report(ctypes.Structure):
     _fields_ = [("ms_A", c_double), ("ms_form", c_double), ("ms_factor", c_double), ("ms_solve", c_double),
                 ("ms_refine", c_double), ("refine_iters", c_int), ("final_correction", c_double), ("info", c_int),
-                ("ms_adjoint", c_double), ("adjoint_refine_iters", c_int)]
+                ("ms_adjoint", c_double), ("adjoint_refine_iters", c_int), ("product_fallbacks", c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
