@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "tc2_pack.cuh"
 #include "tt_kernels.h"
 #include "tt_lu_internal.h"
 
@@ -390,12 +391,6 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 
 // ---- operand packing
 
-__device__ __forceinline__ float round_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-
 // L rows as [M][2K] reals.  TF32: one fp32 plane (used when the matrix itself
 // cannot be read by TMA); BF16X3: hi plane rows [0, M), lo plane [M, 2M).
 template <int MODE>
@@ -433,23 +428,7 @@ __global__ void k_pack_B(const float2* __restrict__ U, int ldu, int K, int N, vo
     const int j = j0 + r, kk = k0 + tx;
     if (j < N && kk < K) {
       const float2 v = tile[tx][r];
-      const size_t re_at = (size_t)j * K + kk, im_at = (size_t)(N + j) * K + kk;  // in pairs of reals
-      if constexpr (MODE == TC_TF32) {
-        float2* w = reinterpret_cast<float2*>(WB);
-        const float ur = round_tf32(v.x), ui = round_tf32(v.y);
-        w[re_at] = make_float2(ur, -ui);
-        w[im_at] = make_float2(ui, ur);
-      } else {
-        __nv_bfloat162* w = reinterpret_cast<__nv_bfloat162*>(WB);
-        const size_t lo = (size_t)2 * N * K;
-        const __nv_bfloat162 hre = __floats2bfloat162_rn(v.x, -v.y);
-        const __nv_bfloat162 him = __floats2bfloat162_rn(v.y, v.x);
-        const float2 fre = __bfloat1622float2(hre), fim = __bfloat1622float2(him);
-        w[re_at] = hre;
-        w[im_at] = him;
-        w[lo + re_at] = __floats2bfloat162_rn(v.x - fre.x, -v.y - fre.y);
-        w[lo + im_at] = __floats2bfloat162_rn(v.y - fim.x, v.x - fim.y);
-      }
+      tc2_pack_b(MODE, WB, N, K, j, kk, v);
     }
   }
 }
@@ -511,7 +490,7 @@ TC2Workspace& workspace2() {
 
 template <int MODE>
 int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
-               cudaStream_t st, int store) {
+               cudaStream_t st, int store, bool prepacked) {
   using CF = tc2::Cfg<MODE>;
   TC2Workspace& ws = workspace2();
   const size_t esz = (MODE == TC_TF32) ? 4 : 2;
@@ -534,10 +513,12 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
       count_launch();
       TT_CUDA_TRY(cudaGetLastError());
     }
-    dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
-    tc2::k_pack_B<MODE><<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
-    count_launch();
-    TT_CUDA_TRY(cudaGetLastError());
+    if (!prepacked) {
+      dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
+      tc2::k_pack_B<MODE><<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
+      count_launch();
+      TT_CUDA_TRY(cudaGetLastError());
+    }
   }
   CUtensorMap mA, mB;
   if (direct_A)
@@ -564,15 +545,24 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
 
 }  // namespace
 
+void* tc2_b_workspace(int mode, int N, int K, int* status) {
+  TC2Workspace& ws = workspace2();
+  const size_t esz = (mode == TC_TF32) ? 4 : 2, parts = (mode == TC_TF32) ? 1 : 2;
+  const size_t need = parts * 2 * (size_t)N * 2 * K * esz;
+  *status = TT_OK;
+  if (need > ws.WB.count) *status = ws.WB.alloc(need);
+  return *status == TT_OK ? ws.WB.ptr : nullptr;
+}
+
 int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
-                 cudaStream_t st, int store) {
+                 cudaStream_t st, int store, bool prepacked) {
   if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
   if (K % tc2::KCC != 0) {
     set_error("tensor-core update needs K to be a multiple of 16");
     return TT_ERR_BADARG;
   }
-  if (mode == TC_TF32) return launch_tc2<TC_TF32>(C, ldc, L, ldl, U, ldu, M, N, K, st, store);
-  if (mode == TC_BF16X3) return launch_tc2<TC_BF16X3>(C, ldc, L, ldl, U, ldu, M, N, K, st, store);
+  if (mode == TC_TF32) return launch_tc2<TC_TF32>(C, ldc, L, ldl, U, ldu, M, N, K, st, store, prepacked);
+  if (mode == TC_BF16X3) return launch_tc2<TC_BF16X3>(C, ldc, L, ldl, U, ldu, M, N, K, st, store, prepacked);
   set_error("unknown tensor-core product mode " + std::to_string(mode));
   return TT_ERR_BADARG;
 }

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <functional>
 
+#include "tc2_pack.cuh"
 #include "tt_kernels.h"
 #include "tt_lu_internal.h"
 
@@ -589,8 +590,11 @@ __global__ void k_laswp2(T* __restrict__ A, int n, const int32_t* __restrict__ i
 }
 
 // X <- L^{-1} X, L the w x w unit-lower block at (r0, r0), X = rows [r0, r0+w) of columns [cb, ce).
+// With pack_mode (complex64 only), X is also written as the packed B operand
+// of the real-row tensor-core update that follows (w deep, ce - cb columns).
 template <typename T>
-__global__ void __launch_bounds__(256) k_trsm_blk(T* __restrict__ A, int n, int r0, int w, int cb, int ce) {
+__global__ void __launch_bounds__(256) k_trsm_blk(T* __restrict__ A, int n, int r0, int w, int cb, int ce,
+                                                  int pack_mode, void* __restrict__ WB) {
   __shared__ T sL[IB][IB + 1];
   __shared__ T sX[IB][33];
   const int c0 = cb + blockIdx.x * 32;
@@ -618,7 +622,15 @@ __global__ void __launch_bounds__(256) k_trsm_blk(T* __restrict__ A, int n, int 
   }
   for (int t = threadIdx.x; t < w * 32; t += blockDim.x) {
     const int i = t / 32, c = c0 + t % 32;
-    if (c < ce) A[(size_t)(r0 + i) * n + c] = sX[i][t % 32];
+    if (c < ce) {
+      A[(size_t)(r0 + i) * n + c] = sX[i][t % 32];
+      if constexpr (sizeof(T) == sizeof(float2)) {
+        if (pack_mode) {
+          const T v = sX[i][t % 32];
+          tc2_pack_b(pack_mode, WB, ce - cb, w, c - cb, i, make_float2(v.x, v.y));
+        }
+      }
+    }
   }
 }
 
@@ -738,10 +750,10 @@ int inv_unit_lower(const T* A, int n, int r0, int w, T* X, cudaStream_t st) {
 }
 
 template <typename T>
-int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st) {
+int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st, int pack_mode = 0, void* WB = nullptr) {
   if (ce <= cb) return TT_OK;
   ProfScope prof(TT_PROF_PANEL_TRSM, st, 4.0 * w * w * (double)(ce - cb), 2.0 * w * (double)(ce - cb) * sizeof(T));
-  k_trsm_blk<T><<<ceil_div(ce - cb, 32), 256, 0, st>>>(A, n, r0, w, cb, ce);
+  k_trsm_blk<T><<<ceil_div(ce - cb, 32), 256, 0, st>>>(A, n, r0, w, cb, ce, pack_mode, WB);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
@@ -909,7 +921,17 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
       for (int b = 0; b < B; b++) {
         T* A = As[b];
         const int right = k + kb - (j0 + w);
-        if (right > 0) {
+        if (right > 0 && inv_solve && w % 16 == 0) {
+          // the solved block row is written straight into the update's operand planes
+          int ws = TT_OK;
+          void* WB = tc2_b_workspace(mode, right, w, &ws);
+          TT_TRY(ws);
+          TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st, mode, WB));
+          TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)(j0 + w) * n + (j0 + w), n,
+                              reinterpret_cast<const float2*>(A) + (size_t)(j0 + w) * n + j0, n,
+                              reinterpret_cast<const float2*>(A) + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right,
+                              w, st, 0, true));
+        } else if (right > 0) {
           TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
           TT_TRY(panel_gemm_sub(mode, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
                                 A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));

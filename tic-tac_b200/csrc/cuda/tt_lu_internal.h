@@ -21,8 +21,11 @@ constexpr int TC_BF16X3 = 3;         // gemm_tc2.cu: real-row form, N = 256, BF1
 // C[M x N] -= L[M x K] U[K x N] in the real-row form (gemm_tc2.cu), K % 16 == 0;
 // store != 0: C = L U (C is not read; it may be U's own storage, which is
 // packed before the product, but must not overlap L).
+// prepacked: U's operand planes are already in the workspace (tc2_b_workspace).
 int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
-                 cudaStream_t st, int store = 0);
+                 cudaStream_t st, int store = 0, bool prepacked = false);
+// The B-operand workspace of tc2_gemm_sub, grown to an N-column, K-deep operand.
+void* tc2_b_workspace(int mode, int N, int K, int* status);
 int tc2_check_error(cudaStream_t st);
 // C[M x N] -= L[M x K] U[K x N], complex128, on the FP64 tensor cores (zgemm_dmma.cu).
 int zgemm_sub_dmma(double2* C, int ldc, const double2* L, int ldl, const double2* U, int ldu, int M, int N, int K,
