@@ -351,6 +351,13 @@ int tt_run_adjoint_forward(tt_run* run, int chn, int precision, tt_complex* U, t
 int tt_run_adjoint_backward(tt_run* run, int chn, int n_theta, const double* dV_WP_unco_dtheta,
                             const double* dV_WP_coup_dtheta, const tt_complex* U_bar, double* theta_bar,
                             tt_solve_report* report);
+/* First-order change of the run's SWP states for a change dV (layout of
+ * tt_run_get_host_array which = 3, 4) of the WP potential matrices: dC (which =
+ * 5, 6), the bin boundaries de_SWP (which = 7, 8) and dE_bound, from the
+ * perturbation of each 2N block's eigenproblem (host FP64; the adjoint's
+ * basis derivative).  Any output may be NULL. */
+int tt_run_swp_derivative(const tt_run* run, const double* dV_WP_unco, const double* dV_WP_coup, double* dC_unco,
+                          double* dC_coup, double* de_unco, double* de_coup, double* dE_bound);
 /* Low-energy constants of the run's potential that the option lec_offsets
  * moves (LO_internal: C_1S0, C_3S1; none for malfliet_tjon), their values,
  * and dV/dLEC_k in the WP basis for all 2N channels (the potential is linear

@@ -198,7 +198,7 @@ def test_adjoint_total_derivative_matches_full_runs(precision):
     dVc = np.stack([d[1] for d in dV])
     shifted = []
     for k in range(2):
-        h = 1e-4 * abs(lecs[k])
+        h = 1e-5 * abs(lecs[k])
         pair = []
         for sgn in (1.0, -1.0):
             off = [0.0, 0.0]
@@ -245,7 +245,7 @@ def test_forward_backward_pair_autograd(precision):
     lecs = run.lecs()
     run.close()
     for k in range(2):
-        h = 1e-4 * abs(lecs[k])
+        h = 1e-5 * abs(lecs[k])
         e = torch.zeros(2, dtype=torch.float64)
         e[k] = h
         lp = (u_of_lecs(e, opts, c, tt.PRECISION_FP64).abs() ** 2).sum().item()
@@ -273,4 +273,34 @@ def test_backward_without_kept_factors_factors_again():
     g, _ = run.adjoint_backward(0, dVu, dVc, Ubar)
     ref = np.real(np.conj(Ubar)[None, :] * dU).sum(axis=1)
     assert np.allclose(g, ref, rtol=1e-8, atol=0)
+    run.close()
+
+
+def test_swp_derivative_matches_run_differences():
+    # the SWP basis derivative (eigenvectors, bin boundaries, deuteron energy)
+    # against central differences of runs with a shifted contact constant;
+    # host only
+    opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=3, Np_WP=8, Nq_WP=8, Nphi=20, Nx=20,
+                lab_energies="12")
+    run = tt.Run(**opts)
+    lecs = run.lecs()
+    for k in range(2):
+        dVu, dVc = run.lec_derivative(k)
+        dCu, dCc, deu, dec, dEb = run.swp_derivative(dVu, dVc)
+        h = 1e-5 * abs(lecs[k])
+        rs = []
+        for sgn in (1.0, -1.0):
+            off = [0.0, 0.0]
+            off[k] = sgn * h
+            rs.append(tt.Run(lec_offsets=",".join(repr(float(o)) for o in off), **opts))
+        for which, d in ((5, dCu), (6, dCc), (7, deu), (8, dec)):
+            fd = (rs[0].host_array(which) - rs[1].host_array(which)) / (2 * h)
+            if np.max(np.abs(fd)) > 0:
+                assert rel(d, fd) <= 1e-6, (k, which, rel(d, fd))
+            else:
+                assert np.max(np.abs(d)) == 0.0
+        fdEb = (rs[0].E_bound - rs[1].E_bound) / (2 * h)
+        assert abs(dEb - fdEb) <= 1e-6 * max(abs(fdEb), 1e-300) or fdEb == dEb == 0.0
+        for r in rs:
+            r.close()
     run.close()

@@ -694,6 +694,19 @@ int tt_run_adjoint_backward(tt_run* run, int chn, int n_theta, const double* dVu
   return TT_OK;
 }
 
+int tt_run_swp_derivative(const tt_run* run, const double* dVu, const double* dVc, double* dC_unco, double* dC_coup,
+                          double* de_unco, double* de_coup, double* dE_bound) {
+  if (!run || !dVu || (run->swp.n_coup && !dVc)) return fail(TT_ERR_BADARG, "null argument");
+  SWPStates d;
+  swp_derivative(run->fwp, run->V_unco, run->V_coup, run->swp, dVu, dVc, d);
+  if (dC_unco) std::memcpy(dC_unco, d.C_unco.data(), sizeof(double) * d.C_unco.size());
+  if (dC_coup) std::memcpy(dC_coup, d.C_coup.data(), sizeof(double) * d.C_coup.size());
+  if (de_unco) std::memcpy(de_unco, d.e_unco.data(), sizeof(double) * d.e_unco.size());
+  if (de_coup) std::memcpy(de_coup, d.e_coup.data(), sizeof(double) * d.e_coup.size());
+  if (dE_bound) *dE_bound = d.E_bound;
+  return TT_OK;
+}
+
 int tt_run_num_lecs(const tt_run* run, int* n_lecs, double* values) {
   if (!run || !n_lecs) return fail(TT_ERR_BADARG, "null argument");
   *n_lecs = num_lecs(run->rp.potential_model);

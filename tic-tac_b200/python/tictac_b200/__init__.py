@@ -41,6 +41,7 @@ EXPORTED_SYMBOLS = (
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
     "tt_run_solve_energies", "tt_profile_select", "tt_run_adjoint_forward", "tt_run_adjoint_backward",
+    "tt_run_swp_derivative",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
@@ -519,6 +520,17 @@ class Run:
         _check(self.lib.tt_run_adjoint_backward(self._h, chn, ctypes.c_int(n_theta), _dptr(dVu), _dptr(dVc),
                                                 Ub.ctypes.data_as(c_void_p), _dptr(out), byref(rep)))
         return out, rep.as_dict()
+
+    def swp_derivative(self, dV_unco, dV_coup):
+        """tt_run_swp_derivative: (dC_unco, dC_coup, de_unco, de_coup, dE_bound)."""
+        dVu = np.ascontiguousarray(dV_unco, dtype=np.float64)
+        dVc = np.ascontiguousarray(dV_coup if dV_coup is not None and np.size(dV_coup) else np.zeros(1),
+                                   dtype=np.float64)
+        out = [np.zeros_like(self.host_array(w)) for w in (5, 6, 7, 8)]
+        dEb = c_double(0)
+        _check(self.lib.tt_run_swp_derivative(self._h, _dptr(dVu), _dptr(dVc), *[_dptr(o) if o.size else None
+                                                                                  for o in out], byref(dEb)))
+        return tuple(out) + (dEb.value,)
 
     def lecs(self):
         """Values of the potential's adjustable low-energy constants."""
