@@ -51,6 +51,8 @@ CONFIGS = {
 }
 # lab energies of the scan configurations: (count, low MeV, high MeV, seed)
 SCANS = {"j2_J5_n24_scan64": (64, 1.0, 200.0, 2024)}
+# phase times of a solve report (build A, form 1 - A G, factor, substitute, refine)
+PHASES = ("ms_A", "ms_form", "ms_factor", "ms_solve", "ms_refine")
 METRIC = "energies/sec, mixed+refined vs FP64 on B200 at <=1e-10 rel err in on-shell U"
 
 
@@ -264,12 +266,15 @@ def run_ours(args, world, rank, local, pg):
     nnz = {c: run.build_P123(c) for c in mine}  # resident for the whole run
     t_setup = time.perf_counter() - t_setup
 
+    phases = {}  # per channel: the solve report's phase times of the latest step
+
     def one_step():
         Us = {}
         for c, js in mine.items():
             run.build_A(c)
             U, rep = run.solve_energies(c, js, prec)
             Us[c] = (js, U)
+            phases[c] = {k: round(rep[k], 1) for k in PHASES}
             run.release_A(c)
         return Us
 
@@ -302,6 +307,7 @@ def run_ours(args, world, rank, local, pg):
         t_bd = run.timer_stop()
         _, kernels = roofline_of(tt.profile_end(), t_bd, t_bd, items, 1, args.tc_product)
         kernels["step_ms"] = round(t_bd, 1)
+        kernels["per_channel_phases_ms"] = {str(c): phases[c] for c in mine}
     # U of every (channel, energy) gathered on rank 0 in the reference's layout
     gathered = shard.gather_to_rank0(pg, Us)
     U_all = None
@@ -398,6 +404,7 @@ def run_ours(args, world, rank, local, pg):
             rows.append({"channel": c, "n": infos_all[c]["n"], "mixed_ms": round(tm, 1), "fp64_ms": round(t64, 1),
                          "speedup": round(t64 / tm, 2), "refine_iters": rm["refine_iters"],
                          "final_correction": rm["final_correction"], "max_elem_rel_err_U": err,
+                         "mixed_phases_ms": {k: round(rm[k], 1) for k in PHASES},
                          "fp64_lu_tflops": round(8.0 / 3.0 * infos_all[c]["n"] ** 3 * nE / (r64["ms_factor"] * 1e-3)
                                                  / 1e12, 2)})
             if c != cmp_chans[0]:

@@ -297,6 +297,10 @@ typedef struct tt_run tt_run;
  * bins on the host (CPP/main.cpp:98-378). */
 int tt_run_create(tt_run** run, int nopt, const char* const* opts);
 void tt_run_destroy(tt_run* run);
+/* Change one option of the linear solve (tc_product, panel_width, panel_order,
+ * energy_batch, refine_tol, refine_max_iter) for the run's next solves; the
+ * states, grids and built operators stay.  Other keys: TT_ERR_BADARG. */
+int tt_run_set_solve_option(tt_run* run, const char* key, const char* value);
 
 /* Counts and per-channel facts. */
 int tt_run_num_channels(const tt_run* run, int* n_chn);

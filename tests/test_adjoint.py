@@ -301,6 +301,16 @@ def test_swp_derivative_matches_run_differences():
                 assert np.max(np.abs(d)) == 0.0
         fdEb = (rs[0].E_bound - rs[1].E_bound) / (2 * h)
         assert abs(dEb - fdEb) <= 1e-6 * max(abs(fdEb), 1e-300) or fdEb == dEb == 0.0
+        # the on-shell energies E_j = E_com,j + E_bound: E_com,j is the bin's
+        # mid-point energy with the n-d reduced mass mu1(E_bound), so
+        # dE_j = dEb (1 - E_com,j dln mu1/dEb), Md = Mn + Mp + E_bound
+        Mn, Mp = 939.565, 938.272
+        Md = Mn + Mp + run.E_bound
+        dlnmu1 = 1.0 / Md - 1.0 / (Mn + Md)
+        E_com = run.energies()[1]
+        dE = dEb * (1.0 - E_com * dlnmu1)
+        fdE = ((rs[0].energies()[1] + rs[0].E_bound) - (rs[1].energies()[1] + rs[1].E_bound)) / (2 * h)
+        assert np.max(np.abs(dE - fdE)) <= 1e-6 * max(np.max(np.abs(fdE)), 1e-300) or np.all(fdE == 0.0), (k, dE, fdE)
         for r in rs:
             r.close()
     run.close()

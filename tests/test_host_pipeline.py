@@ -71,3 +71,35 @@ def test_energy_batch_option_range():
     for v in (0, 5):
         with pytest.raises(tt.TicTacError, match="energy_batch"):
             tt.Run(energy_batch=v, **opts)
+
+
+def test_solve_options_on_a_run():
+    opts = dict(potential_model="malfliet_tjon", J_2N_max=1, two_J_3N_max=1, Np_WP=8, Nq_WP=8, lab_energies="10")
+    for v in (0, 32, 256, 384, 512):
+        tt.Run(panel_width=v, **opts).close()
+    for v in (16, 600, -32):
+        with pytest.raises(tt.TicTacError, match="panel_width"):
+            tt.Run(panel_width=v, **opts)
+    run = tt.Run(**opts)
+    for k, v in (("panel_width", 384), ("tc_product", "bf16x3"), ("panel_order", "recursive"), ("energy_batch", 2),
+                 ("refine_tol", 1e-11), ("refine_max_iter", 30)):
+        run.set_solve_option(k, v)
+    with pytest.raises(tt.TicTacError, match="panel_width"):
+        run.set_solve_option("panel_width", 48)
+    # state-space options are fixed once the run is built
+    with pytest.raises(tt.TicTacError, match="not a solve option"):
+        run.set_solve_option("Np_WP", 10)
+    run.close()
+
+
+def test_panel_table_rows_and_header():
+    from tictac_b200 import autotune
+    timings = {"tf32": {9072: {256: 3.0, 512: 2.0}, 20000: {256: 9.0, 512: 8.0}, 56700: {256: 50.0, 512: 51.0}},
+               "bf16x3": {9072: {256: 4.0, 512: 5.0}}}
+    rows = autotune.table_rows(timings)
+    assert rows == [(2, (20000 + 56700) // 2, 512), (2, 1 << 30, 256), (3, 1 << 30, 256)]
+    h = autotune.render_header(rows, "test")
+    assert "{2, 38350, 512}," in h and "{2, 1 << 30, 256}," in h and "{1, 1 << 30, 512}," in h
+    # the committed header has the same shape as the rendered one
+    src = open(autotune.HEADER).read()
+    assert "kPanelWidthTable" in src and "struct PanelWidthRow" in src

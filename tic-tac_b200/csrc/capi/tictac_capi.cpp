@@ -113,6 +113,7 @@ SolveOptions options_of(const RunParams& rp, int precision) {
   o.energy_batch = rp.energy_batch;
   o.tc_product = rp.tc_product;
   o.panel_blocked = rp.panel_blocked;
+  o.panel_width = rp.panel_width;
   return o;
 }
 
@@ -395,6 +396,20 @@ int tt_run_create(tt_run** out, int nopt, const char* const* opts) {
   return TT_OK;
 }
 
+int tt_run_set_solve_option(tt_run* run, const char* key, const char* value) {
+  if (!run || !key || !value) return fail(TT_ERR_BADARG, "null run, key or value");
+  static const char* const kSolveKeys[] = {"tc_product", "panel_width", "panel_order", "energy_batch",
+                                           "refine_tol", "refine_max_iter"};
+  bool ok = false;
+  for (const char* k : kSolveKeys) ok = ok || std::strcmp(k, key) == 0;
+  if (!ok) return fail(TT_ERR_BADARG, std::string("not a solve option: ") + key);
+  std::string err;
+  RunParams rp = run->rp;
+  if (!set_run_parameter(rp, key, value, &err)) return fail(TT_ERR_BADARG, err);
+  run->rp = rp;
+  return TT_OK;
+}
+
 void tt_run_destroy(tt_run* run) {
   if (!run) return;
   run->chn.clear();
@@ -451,6 +466,10 @@ static int adjoint_request(tt_run* run, const PWChannel& ch, int n_theta, const 
     TT_TRY(ab.dc.upload(dcb, run_stream(run)));
     TT_TRY(ab.de.upload(deb, run_stream(run)));
     adj.total = true;
+    // mu1 = Mn Md / (Mn + Md), Md = Mn + Mp + E_bound (CPP/General_functions/kinetic_conversion.cpp:10-13)
+    const double Md = kMn + kMp + run->swp.E_bound;
+    adj.E_bound = run->swp.E_bound;
+    adj.dlnmu1_dEb = 1.0 / Md - 1.0 / (kMn + Md);
     adj.d_dC = ab.dc.ptr;
     adj.d_de = ab.de.ptr;
   }

@@ -778,7 +778,7 @@ int panel_gemm_sub(int mode, T* C, int ldc, const T* L, int ldl, const T* U, int
 
 template <typename T>
 int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, cudaStream_t st, int use_tc,
-                             int* info, bool blocked_order) {
+                             int* info, bool blocked_order, int panel) {
   const int mode = use_tc;
   const bool tc = mode != 0;
   if (mode < 0 || mode > TC_BF16X3) {
@@ -793,7 +793,11 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     set_error("LU batch of " + std::to_string(B) + " matrices (1.." + std::to_string(kMaxBatch) + ")");
     return TT_ERR_BADARG;
   }
-  const int NB = (sizeof(T) == sizeof(float2)) ? 512 : 128;
+  if (panel < 0 || panel > INV_MAX || panel % IB != 0) {
+    set_error("panel width " + std::to_string(panel) + " (a multiple of 32 up to 512)");
+    return TT_ERR_BADARG;
+  }
+  const int NB = panel ? panel : (sizeof(T) == sizeof(float2)) ? 512 : 128;
   const int G = device_sm_count();
   DevBuf<double> sval;
   DevBuf<int> sidx, d_info;
@@ -977,9 +981,9 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   return TT_OK;
 }
 template int lu_factor_batched_device<double2>(double2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                               bool);
+                                               bool, int);
 template int lu_factor_batched_device<float2>(float2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                              bool);
+                                              bool, int);
 
 template <typename T>
 int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {

@@ -77,12 +77,13 @@ __global__ void k_resolvent(int Na, int Nq, int Np, const int32_t* __restrict__ 
 }
 
 // First-order change dG of the resolvents of k_resolvent for a change de of
-// the SWP energy boundaries (layout of e_swp) and dEb of the deuteron energy,
-// the energies being E_j = E_com,j + E_bound (make_resolvent.cpp:14-80
-// differentiated; d(x ln|x|) = (ln|x| + 1) dx, d(x theta(x)) = theta(x) dx).
+// the SWP energy boundaries (layout of e_swp; a bound state's lower boundary
+// is E_bound, which also sets the n-d reduced mass of its bins) and dEn of the
+// energies E_j = E_com,j + E_bound (make_resolvent.cpp:14-80 differentiated;
+// d(x ln|x|) = (ln|x| + 1) dx, d(x theta(x)) = theta(x) dx).
 __global__ void k_dresolvent(int Na, int Nq, int Np, const int32_t* __restrict__ e_off,
                              const double* __restrict__ e_swp, const double* __restrict__ de_swp,
-                             const double* __restrict__ qwp, const double* __restrict__ E, int nE, double dEb,
+                             const double* __restrict__ qwp, const double* __restrict__ E, int nE, double dEn,
                              double2* __restrict__ dG) {
   const int n = Na * Nq * Np;
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -92,7 +93,7 @@ __global__ void k_dresolvent(int Na, int Nq, int Np, const int32_t* __restrict__
   const double e_lo = e_swp[e_off[a] + p], e_hi = e_swp[e_off[a] + p + 1];
   const double de_lo = de_swp[e_off[a] + p], de_hi = de_swp[e_off[a] + p + 1];
   const double q_lo = qwp[q], q_hi = qwp[q + 1];
-  const double En = E[j], dE = dEb;
+  const double En = E[j], dE = dEn;
   double dre, dim;
   if (e_lo < 0) {
     const double Eb = e_lo, dEbl = de_lo;
@@ -469,12 +470,12 @@ int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d
   return TT_OK;
 }
 
-int dresolvent_device(const DeviceLayout& L, const double* d_de, double dEb, const double* d_E, int nE, double* d_dG,
+int dresolvent_device(const DeviceLayout& L, const double* d_de, double dE, const double* d_E, int nE, double* d_dG,
                       cudaStream_t st) {
   const size_t total = (size_t)L.n * nE;
   if (total == 0) return TT_OK;
   k_dresolvent<<<ceil_div(total, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, L.e_off.ptr, L.e_swp.ptr, d_de, L.q_WP.ptr,
-                                                     d_E, nE, dEb, reinterpret_cast<double2*>(d_dG));
+                                                     d_E, nE, dE, reinterpret_cast<double2*>(d_dG));
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;

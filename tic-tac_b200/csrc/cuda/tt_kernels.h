@@ -79,9 +79,11 @@ int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_te
 // info[B] receives each matrix's first zero pivot (1-based) or 0.
 // blocked: the panel in 32-column steps, each followed by its rank-32 update
 // (otherwise recursive halving of the panel and of the U12 solve).
+// panel: the outer panel width (a multiple of 32 up to 512; 0 = 512 for
+// complex64, 128 for complex128).
 template <typename T>
 int lu_factor_batched_device(T* const* d_L, int B, int n, int32_t* const* d_ipiv, cudaStream_t st,
-                             int use_tensor_cores, int* info, bool blocked = false);
+                             int use_tensor_cores, int* info, bool blocked = false, int panel = 0);
 // Row permutation of the interchange sequence ipiv (host, once per factorisation).
 int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cudaStream_t st);
 // Inverted diagonal blocks of one LU factor (unit lower and upper) and their
@@ -141,9 +143,11 @@ int block_apply_device(const DeviceLayout& L, const double* d_X, const double* d
 // out_k = 2 P u_k
 int spmv_device(const DeviceCSR& P, const double* d_u, int nrhs, double* d_out, cudaStream_t st);
 // dG[j*n + i]: first-order change of the resolvents for a change de of the SWP
-// energy boundaries (layout of the layout's e_swp) and dEb of the deuteron
-// energy, energies E[j] = E_com,j + E_bound
-int dresolvent_device(const DeviceLayout& L, const double* d_de, double dEb, const double* d_E, int nE, double* d_dG,
+// energy boundaries (layout of the layout's e_swp; the bound state's lower
+// boundary is E_bound, which also moves the n-d reduced mass of its
+// bound-continuum bins) and dE of the energies E[j] = E_com,j + E_bound (the
+// same dE for the nE energies given)
+int dresolvent_device(const DeviceLayout& L, const double* d_de, double dE, const double* d_E, int nE, double* d_dG,
                       cudaStream_t st);
 // g_k = 2 P^T u_k
 int spmv_t_device(const DeviceCSR& P, const double* d_u, int nrhs, double* d_g, cudaStream_t st);

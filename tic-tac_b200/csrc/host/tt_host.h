@@ -59,6 +59,7 @@ struct RunParams {
   int energy_batch = 4;  // complex64 LUs of a channel's energies factored together (1..4)
   int tc_product = 2;          // tensor-core product of the complex64 LU: 1 bf16x3_n128, 2 tf32, 3 bf16x3
   bool panel_blocked = true;   // LU panels in 32-column steps (else recursive halving)
+  int panel_width = 0;         // complex64 LU panel width, 0 = the tuning table's choice
   bool adjoint_total = true;   // run-handle adjoint: total derivative (basis and resolvent move with V)
   std::vector<double> lab_energies; // set directly or read from energy_input_file
   // additive offsets to the potential's low-energy constants, in the model's

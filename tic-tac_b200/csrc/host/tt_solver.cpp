@@ -9,6 +9,7 @@
 #include <map>
 
 #include "../cuda/tt_lu_internal.h"
+#include "tt_panel_table.h"
 
 namespace tt {
 
@@ -194,6 +195,7 @@ int ChannelSolver::build_A(cudaStream_t st, double* ms) {
 
 int ChannelSolver::resolvent(const std::vector<double>& E, cudaStream_t st) {
   nE_ = (int)E.size();
+  Eh_ = E;
   TT_TRY(E_.upload(E, st));
   TT_TRY(G_.alloc((size_t)2 * n * std::max(1, nE_)));
   TT_TRY(resolvent_device(L_, E_.ptr, nE_, G_.ptr, st));
@@ -204,6 +206,13 @@ int ChannelSolver::resolvent(const std::vector<double>& E, cudaStream_t st) {
 namespace {
 
 using cd = std::complex<double>;
+
+// Panel width of the complex64 LU for order n and tensor-core product.
+int tuned_panel_width(int n, int product) {
+  for (const PanelWidthRow& r : kPanelWidthTable)
+    if (r.product == product && n <= r.n_max) return r.width;
+  return 512;
+}
 
 // Determinant by LU with partial pivoting, pivots chosen by |re| + |im| as
 // LAPACK's zgetrf does (determinant, CPP/General_functions/matrix_routines.cpp:82-101).
@@ -434,7 +443,8 @@ int ChannelSolver::adjoint_energy(int j, int nE, int nd, const double* Gj, const
       TT_TRY(bilinear_device(n, u, nd, u2.ptr, nd, dots, st));
       TT_TRY(add_dots());
       // (A^T lambda)^T (dG o x)
-      TT_TRY(dresolvent_device(L_, adj.d_de + (size_t)k * adj.e_count, adj.dEb[k], E_.ptr + j, 1, dG.ptr, st));
+      const double dEj = adj.dEb[k] * (1.0 - (Eh_[j] - adj.E_bound) * adj.dlnmu1_dEb);
+      TT_TRY(dresolvent_device(L_, adj.d_de + (size_t)k * adj.e_count, dEj, E_.ptr + j, 1, dG.ptr, st));
       TT_TRY(hadamard_device(dG.ptr, zero_e.ptr, n, x, nd, t2.ptr, st));
       TT_TRY(bilinear_device(n, yT, nd, t2.ptr, nd, dots, st));
       TT_TRY(add_dots());
@@ -556,7 +566,8 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       TT_CUDA_TRY(cudaStreamSynchronize(st));
       r.ms_form += ms_since(t0);
       t0 = std::chrono::steady_clock::now();
-      TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, product, info, opt.panel_blocked));
+      TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, product, info, opt.panel_blocked,
+                                              opt.panel_width ? opt.panel_width : tuned_panel_width(n, product)));
       r.ms_factor += ms_since(t0);
     } else {
       TT_TRY(form_L_device<double2>(A_.ptr, G_.ptr + (size_t)2 * n * g0, n, L64.ptr, st));

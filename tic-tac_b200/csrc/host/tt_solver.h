@@ -31,6 +31,7 @@ struct SolveOptions {
   bool mixed = true;        // complex64 LU on tensor cores + FP64 refinement; false: complex128 LU
   bool tensor_cores = true; // trailing update on tcgen05 (mixed only)
   bool panel_blocked = true;  // LU panels in 32-column steps instead of recursive halving
+  int panel_width = 0;        // complex64 LU panel width (0: the tuning table's choice for n, else 512)
   int tc_product = 2;        // product mode of the tensor-core updates: 1 BF16x3 with N = 128 tiles,
                              // 2 TF32 (a group whose refinement does not converge is factored
                              // again with 3), 3 BF16x3 (real-row form, N = 256)
@@ -66,6 +67,11 @@ struct AdjointRequest {
   const double* d_de = nullptr;   // n_theta * e_count doubles: d e_SWP (layout of the channel's e_swp)
   size_t e_count = 0;
   std::vector<double> dEb;        // n_theta: d E_bound
+  // the on-shell energies E_j = E_com,j + E_bound move with E_bound also
+  // through E_com,j = (q_j^2 + q_{j+1}^2) / (4 mu1(E_bound)) (the bin mid-point
+  // energy of CPP/run_organizer.cpp:92-110): dE_j = dEb (1 - E_com,j dln mu1/dEb)
+  double E_bound = 0;
+  double dlnmu1_dEb = 0;
 };
 
 class ChannelSolver {
@@ -126,7 +132,8 @@ class ChannelSolver {
   Kept kept_;
   DeviceLayout L_;
   DeviceCSR P_;
-  DevBuf<double> A_, G_, E_;  // E_: the energies of the resolvents in G_
+  DevBuf<double> A_, G_, E_;
+  std::vector<double> Eh_;  // host copy of E_  // E_: the energies of the resolvents in G_
   int nE_ = 0;
 };
 

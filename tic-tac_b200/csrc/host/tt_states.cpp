@@ -59,6 +59,9 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       if (value == "total") rp.adjoint_total = true;
       else if (value == "fixed") rp.adjoint_total = false;
       else return bad("adjoint_basis (total or fixed)");
+    } else if (key == "panel_width") {
+      rp.panel_width = std::stoi(value);
+      if (rp.panel_width < 0 || rp.panel_width > 512 || rp.panel_width % 32) return bad("panel_width (0 or 32..512)");
     } else if (key == "panel_order") {
       if (value == "blocked") rp.panel_blocked = true;
       else if (value == "recursive") rp.panel_blocked = false;

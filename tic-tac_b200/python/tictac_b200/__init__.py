@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = (
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
     "tt_run_solve_energies", "tt_profile_select", "tt_run_adjoint_forward", "tt_run_adjoint_backward",
-    "tt_run_swp_derivative",
+    "tt_run_swp_derivative", "tt_run_set_solve_option",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
@@ -546,6 +546,11 @@ class Run:
         dVc = np.zeros(max(1, self.host_array(4).size))
         _check(self.lib.tt_run_lec_derivative(self._h, k, _dptr(dVu), _dptr(dVc)))
         return dVu, dVc[:self.host_array(4).size]
+
+    def set_solve_option(self, key, value):
+        """Change a solve option (tc_product, panel_width, panel_order, energy_batch, refine_tol,
+        refine_max_iter) for the next solves."""
+        _check(self.lib.tt_run_set_solve_option(self._h, str(key).encode(), str(value).encode()))
 
     def release(self, chn):
         _check(self.lib.tt_run_release_channel(self._h, chn))
