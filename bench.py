@@ -251,6 +251,8 @@ def run_ours(args, world, rank, local, pg):
     cfg["lab_energies"] = ",".join(f"{x:.12g}" for x in lab)
     cfg["tc_product"] = args.tc_product
     cfg["panel_order"] = args.panel_order
+    cfg["panel_width"] = args.panel_width
+    cfg["inverse_block"] = args.inverse_block
     prec = tt.PRECISION_MIXED if args.precision == "mixed" else tt.PRECISION_FP64
     t_setup = time.perf_counter()
     run = tt.Run(**cfg)
@@ -271,10 +273,11 @@ def run_ours(args, world, rank, local, pg):
     def one_step():
         Us = {}
         for c, js in mine.items():
-            run.build_A(c)
+            ms_A = run.build_A(c)
             U, rep = run.solve_energies(c, js, prec)
             Us[c] = (js, U)
             phases[c] = {k: round(rep[k], 1) for k in PHASES}
+            phases[c]["ms_A"] = round(ms_A, 1)  # host clock around the A build, allocation included
             run.release_A(c)
         return Us
 
@@ -290,6 +293,7 @@ def run_ours(args, world, rank, local, pg):
             run.timer_start()
             Us = one_step()
             times.append(run.timer_stop())
+    step_phases = {str(c): dict(v) for c, v in phases.items()}
     kern = tt.profile_end()
     launches = tt.kernel_launches() - launches0
     barrier(pg)
@@ -433,7 +437,7 @@ def run_ours(args, world, rank, local, pg):
         run.release_A(c)
     return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, kernels=kernels, e2e=e2e,
                 infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times, launches=launches, fp64=fp64,
-                lab=lab, plan=plans, U_all=U_all)
+                lab=lab, plan=plans, U_all=U_all, step_phases=step_phases)
 
 
 # Np = Nq of the reference's timed sample: channel 0 of the workload's basis at
@@ -529,6 +533,9 @@ def main():
                     help="tensor-core product of the complex64 LU")
     ap.add_argument("--panel-order", choices=["recursive", "blocked"], default="blocked",
                     help="LU panels by recursive halving or in 32-column steps")
+    ap.add_argument("--panel-width", type=int, default=0, help="LU panel width (0: the library's table)")
+    ap.add_argument("--inverse-block", type=int, default=0,
+                    help="largest unit-lower block solved through its explicit inverse (0: the library's default)")
     ap.add_argument("--breakdown", type=int, default=1,
                     help="one extra step with every kernel class timed, for the per-class breakdown")
     ap.add_argument("--e2e-steps", type=int, default=1)
@@ -539,12 +546,19 @@ def main():
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.config in SCANS:
+        count, lo, hi, seed = SCANS[args.config]
+        energies_text = (f"{count} lab energies drawn uniformly in {lo:g}-{hi:g} MeV (seed {seed}), their distinct "
+                         f"on-shell bins factored four per channel at a time, split over the N GPUs")
+    else:
+        energies_text = ("T_lab=10 MeV on one GPU (two on-shell bins); on N GPUs a scan of N lab energies with 2N "
+                         "distinct on-shell bins")
     config = {"workload": f"{args.config}: LO-OPEP (stands in for N3LO-Idaho), j<={cfg['J_2N_max']}, "
-                          f"J<={cfg['two_J_3N_max']}/2 both parities, Np=Nq={cfg['Np_WP']}, T_lab=10 MeV on one GPU "
-                          f"(two on-shell bins); on N GPUs a scan of N lab energies with 2N distinct on-shell bins",
+                          f"J<={cfg['two_J_3N_max']}/2 both parities, Np=Nq={cfg['Np_WP']}, {energies_text}",
               "channels_per_step": None, "energies_per_step": None,
               "parallelism": f"(channel, energy) items over {world} GPU(s), longest processing time first",
-              "l2": "inputs larger than L2 (A is 25.7 GB for the largest channel)"}
+              "l2": "inputs larger than L2 (a channel's FP64 A is n x n doubles: 0.66 GB at n = 9,072, 25.7 GB at "
+                    "n = 56,700; the L2 holds 126 MB)"}
 
     if args.impl == "reference":
         # the reference's own CPU path; nothing of this repository's library is loaded
@@ -617,6 +631,8 @@ def main():
                "max_elem_rel_err_U_vs_fp64": fp["max_elem_rel_err_U"] if fp else None,
                "channel_solves_per_s": round(len(r["infos"]) * r["nE"] / (r["ms_step"] * 1e-3), 4),
                "kernels": r["kernels"], "fp64_comparison": fp, "setup_s": round(r["t_setup"], 3),
+               "timed_steps_ms": [round(t, 1) for t in r["times"]],
+               "last_timed_step_phases_ms": r["step_phases"],
                "U_gathered": {"channels": len(r["U_all"]), "energies": r["nE"],
                               "layout": "U[d' nd nE + d nE + j] per channel on rank 0"}}
         print(json.dumps(out))

@@ -219,6 +219,11 @@ int tt_P123_h5_filename(char* buf, size_t cap, const char* folder, const tt_pw_s
 void tt_free(void* p);
 const char* tt_last_error_string(void);
 int tt_device_count(int* count);
+/* Large device blocks (256 MB and up) that the library releases are kept for
+ * its next allocations of about the same size (cudaMalloc / cudaFree of tens
+ * of GB cost milliseconds each); this returns the current device's cached
+ * blocks to the driver.  tt_run_destroy does the same. */
+int tt_release_cached_device_memory(void);
 /* Kernels launched by this library since load (diagnostic). */
 unsigned long long tt_kernel_launches(void);
 
@@ -298,7 +303,7 @@ typedef struct tt_run tt_run;
 int tt_run_create(tt_run** run, int nopt, const char* const* opts);
 void tt_run_destroy(tt_run* run);
 /* Change one option of the linear solve (tc_product, panel_width, panel_order,
- * energy_batch, refine_tol, refine_max_iter) for the run's next solves; the
+ * inverse_block, energy_batch, refine_tol, refine_max_iter) for the run's next solves; the
  * states, grids and built operators stay.  Other keys: TT_ERR_BADARG. */
 int tt_run_set_solve_option(tt_run* run, const char* key, const char* value);
 

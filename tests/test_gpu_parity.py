@@ -310,16 +310,19 @@ def test_tf32_refinement_falls_back_to_bf16x3():
 @pytest.mark.parametrize("product", ["tf32", "bf16x3"])
 def test_panel_widths_agree(product):
     # n = 1,100 factored with outer panels of 32, 96, 256 and 512 columns
-    # (ragged last panel for each): the refined U agrees per element with the
-    # FP64 solve whatever the panel width
+    # (ragged last panel for each) and unit-lower inverses of 32 to 512 rows:
+    # the refined U agrees per element with the FP64 solve whatever the choice
     opts = dict(potential_model="LO_internal", J_2N_max=1, two_J_3N_max=1, Np_WP=10, Nq_WP=10, Nphi=16, Nx=16,
                 lab_energies="5,30")
     run = tt.Run(**opts, tc_product=product)
     for c in range(run.num_channels):
         U64, _ = run.solve(c, tt.PRECISION_FP64)
-        for w in (32, 96, 256, 512):
+        # panel widths, and the largest unit-lower block solved by its explicit inverse
+        for w, ib in ((32, 0), (96, 0), (256, 0), (512, 0), (512, 32), (512, 256), (512, 512)):
             run.set_solve_option("panel_width", w)
+            run.set_solve_option("inverse_block", ib)
             U, rep = run.solve(c, tt.PRECISION_MIXED)
-            assert rel_elem(U, U64) <= 1e-10, (c, w, rep)
+            assert rel_elem(U, U64) <= 1e-10, (c, w, ib, rep)
         run.set_solve_option("panel_width", 0)
+        run.set_solve_option("inverse_block", 0)
     run.close()

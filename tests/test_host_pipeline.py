@@ -82,10 +82,12 @@ def test_solve_options_on_a_run():
             tt.Run(panel_width=v, **opts)
     run = tt.Run(**opts)
     for k, v in (("panel_width", 384), ("tc_product", "bf16x3"), ("panel_order", "recursive"), ("energy_batch", 2),
-                 ("refine_tol", 1e-11), ("refine_max_iter", 30)):
+                 ("refine_tol", 1e-11), ("refine_max_iter", 30), ("inverse_block", 256)):
         run.set_solve_option(k, v)
     with pytest.raises(tt.TicTacError, match="panel_width"):
         run.set_solve_option("panel_width", 48)
+    with pytest.raises(tt.TicTacError, match="inverse_block"):
+        run.set_solve_option("inverse_block", 1024)
     # state-space options are fixed once the run is built
     with pytest.raises(tt.TicTacError, match="not a solve option"):
         run.set_solve_option("Np_WP", 10)

@@ -114,6 +114,7 @@ SolveOptions options_of(const RunParams& rp, int precision) {
   o.tc_product = rp.tc_product;
   o.panel_blocked = rp.panel_blocked;
   o.panel_width = rp.panel_width;
+  o.inverse_block = rp.inverse_block;
   return o;
 }
 
@@ -396,10 +397,15 @@ int tt_run_create(tt_run** out, int nopt, const char* const* opts) {
   return TT_OK;
 }
 
+int tt_release_cached_device_memory(void) {
+  device_cache_trim();
+  return TT_OK;
+}
+
 int tt_run_set_solve_option(tt_run* run, const char* key, const char* value) {
   if (!run || !key || !value) return fail(TT_ERR_BADARG, "null run, key or value");
   static const char* const kSolveKeys[] = {"tc_product", "panel_width", "panel_order", "energy_batch",
-                                           "refine_tol", "refine_max_iter"};
+                                           "refine_tol", "refine_max_iter", "inverse_block"};
   bool ok = false;
   for (const char* k : kSolveKeys) ok = ok || std::strcmp(k, key) == 0;
   if (!ok) return fail(TT_ERR_BADARG, std::string("not a solve option: ") + key);
@@ -413,6 +419,7 @@ int tt_run_set_solve_option(tt_run* run, const char* key, const char* value) {
 void tt_run_destroy(tt_run* run) {
   if (!run) return;
   run->chn.clear();
+  device_cache_trim();
   if (run->ev0) cudaEventDestroy(run->ev0);
   if (run->ev1) cudaEventDestroy(run->ev1);
   if (run->stream) cudaStreamDestroy(run->stream);

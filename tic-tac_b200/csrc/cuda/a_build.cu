@@ -1,0 +1,216 @@
+// The dense kernel matrix of one 3N channel,
+//   A = C^T (2 P123) (V C)                      (solve_faddeev.cpp:4-181),
+// in one pass over P123 that writes each element of A once.
+//
+// Index of a state: (alpha, q, p) -> (alpha Nq + q) Np + p.  C and V C are
+// block diagonal over the 2N blocks: alpha couples only with the partners of
+// its coupling list (itself and at most one other partial wave of the same 2N
+// block), and
+//   A[(ar,q,pr), (ac,q',pc)] = sum_{ai in cpl(ar)} sum_pi Ct(ar,ai)[pr][pi] T_ai[(q,pi), (q',pc)],
+//   T_ai[(q,pi), (q',pc)]     = 2 sum_{aj in cpl(ac)} sum_pj P[(ai,q,pi), (aj,q',pj)] VC[(aj,pj), (ac,pc)].
+// The reference forms the product column by column (calculate_PVC_col,
+// calculate_CPVC_col); here one CTA owns a row block (ar, q) and a column
+// partial wave ac, walks the P123 rows (ai, q, pi) of the coupled ai once over
+// the q' range of the coupled aj (sorted columns; each row's start of every
+// alpha range is tabulated once per channel), accumulates T for a chunk of q'
+// in shared memory, contracts it with Ct and streams the chunk of A out.
+// No n x n intermediate: HBM traffic is the A written once plus P123 read
+// (twice per coupled pair).
+#include <algorithm>
+#include <climits>
+
+#include "tt_kernels.h"
+
+namespace tt {
+namespace {
+
+constexpr int AB_THREADS = 256;
+constexpr int AB_COLS = 128;  // columns of A per chunk: QW = AB_COLS / Np values of q'
+
+__device__ __forceinline__ int64_t first_col_at_least(const int32_t* __restrict__ col, int64_t lo, int64_t hi,
+                                                      int32_t key) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (col[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// aoff[r * (Na + 1) + a] = first nonzero of row r with column >= a Nq Np,
+// relative to rowptr[r], for a = 0 .. Na
+__global__ void k_alpha_offsets(int n, int Na, int NqNp, const int64_t* __restrict__ rowptr,
+                                const int32_t* __restrict__ col, int32_t* __restrict__ aoff) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (size_t)n * (Na + 1)) return;
+  const int r = (int)(tid / (Na + 1)), a = (int)(tid % (Na + 1));
+  const int64_t lo = rowptr[r], hi = rowptr[r + 1];
+  aoff[tid] = (int32_t)(first_col_at_least(col, lo, hi, a * NqNp) - lo);
+}
+
+// One CTA per (row block R = ar Nq + q, column partial wave ac); MAXH >= Np / 2.
+// Dynamic shared memory: Ct [2][Np][Np], T [2 Np][QW Np] (doubles), cursors [2 Np][2] (int64).
+template <int MAXH>
+__global__ void __launch_bounds__(AB_THREADS) k_abuild(int Na, int Nq, int Np, const int64_t* __restrict__ rowptr,
+                                                       const int32_t* __restrict__ col,
+                                                       const double* __restrict__ val,
+                                                       const int32_t* __restrict__ aoff,
+                                                       const int32_t* __restrict__ blk,
+                                                       const int32_t* __restrict__ part,
+                                                       const int32_t* __restrict__ cpl_off,
+                                                       const int32_t* __restrict__ cpl,
+                                                       const int64_t* __restrict__ blk_off,
+                                                       const int32_t* __restrict__ blk_dim,
+                                                       const double* __restrict__ Cm,
+                                                       const double* __restrict__ VC, double* __restrict__ A) {
+  extern __shared__ double ab_smem[];
+  const int n = Na * Nq * Np, NqNp = Nq * Np;
+  const int QW = max(1, AB_COLS / Np), CW = QW * Np;
+  double* sCt = ab_smem;                      // [t][pr][pi]
+  double* sT = sCt + 2 * Np * Np;             // [t Np + pi][c]
+  int64_t* sCur = reinterpret_cast<int64_t*>(sT + 2 * Np * CW);  // [t Np + pi][t2]
+  const int R = blockIdx.x, ac = blockIdx.y;
+  const int ar = R / Nq, q = R % Nq;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cr0 = cpl_off[ar], ncr = cpl_off[ar + 1] - cr0;
+  const int cc0 = cpl_off[ac], ncc = cpl_off[ac + 1] - cc0;
+  const int RT = ncr * Np;  // rows of T
+  // Ct(ar, ai)[pr][pi] = C[(part_i, pi), (part_r, pr)] of ar's 2N block
+  {
+    const int b = blk[ar], dimb = blk_dim[b], part_r = part[ar];
+    const double* Cb = Cm + blk_off[b];
+    for (int i = tid; i < ncr * Np * Np; i += AB_THREADS) {
+      const int t = i / (Np * Np), pr = (i / Np) % Np, pi = i % Np;
+      const int ai = cpl[cr0 + t];
+      sCt[i] = Cb[(size_t)(part[ai] * Np + pi) * dimb + part_r * Np + pr];
+    }
+  }
+  // cursors: each T row's position in the P123 row, per coupled column partial wave aj
+  for (int i = tid; i < RT * 2; i += AB_THREADS) {
+    const int rr = i >> 1, t2 = i & 1;
+    int64_t e = 0;
+    if (t2 < ncc) {
+      const int ai = cpl[cr0 + rr / Np], pi = rr % Np, aj = cpl[cc0 + t2];
+      const int r = (ai * Nq + q) * Np + pi;
+      e = rowptr[r] + aoff[(size_t)r * (Na + 1) + aj];
+    }
+    sCur[i] = e;
+  }
+  const int bc = blk[ac], dimc = blk_dim[bc], part_c = part[ac];
+  const double* VCb = VC + blk_off[bc];
+  const int half = tid >> 7, c = tid & 127;
+  for (int q0 = 0; q0 < Nq; q0 += QW) {
+    const int cw = min(QW, Nq - q0) * Np;  // columns of this chunk
+    __syncthreads();
+    for (int i = tid; i < RT * CW; i += AB_THREADS) sT[i] = 0.0;
+    __syncthreads();
+    // ---- T chunk: one warp per T row (warp-private rows: no atomics)
+    for (int rr = warp; rr < RT; rr += AB_THREADS / 32) {
+      const int ai = cpl[cr0 + rr / Np], pi = rr % Np;
+      const int r = (ai * Nq + q) * Np + pi;
+      double* Trow = sT + (size_t)rr * CW;
+      for (int t2 = 0; t2 < ncc; t2++) {
+        const int aj = cpl[cc0 + t2], part_j = part[aj];
+        const int64_t e_end = rowptr[r] + aoff[(size_t)r * (Na + 1) + aj + 1];
+        const int32_t lim = aj * NqNp + min(q0 + QW, Nq) * Np;  // first column past the chunk
+        const int32_t base = aj * NqNp + q0 * Np;
+        int64_t e = sCur[rr * 2 + t2];
+        bool done = e >= e_end;
+        while (!done) {
+          // 32 nonzeros per coalesced load, then applied one by one from registers
+          const int64_t el = e + lane;
+          const int32_t cl = el < e_end ? col[el] : INT_MAX;
+          const double vl = el < e_end ? val[el] : 0.0;
+          int used = 0;
+          for (int i = 0; i < 32; i++) {
+            const int32_t cj = __shfl_sync(0xffffffffu, cl, i);
+            if (cj >= lim) {  // past the chunk (or the end of the aj range): uniform over the warp
+              done = true;
+              break;
+            }
+            const double v = 2.0 * __shfl_sync(0xffffffffu, vl, i);
+            const int rel = cj - base, qq = rel / Np, pj = rel % Np;
+            const double* vrow = VCb + (size_t)(part_j * Np + pj) * dimc + part_c * Np;
+            for (int pc = lane; pc < Np; pc += 32) Trow[qq * Np + pc] += v * vrow[pc];
+            used++;
+          }
+          e += used;
+          if (e >= e_end) done = true;
+        }
+        if (lane == 0) sCur[rr * 2 + t2] = e;
+      }
+    }
+    __syncthreads();
+    // ---- A chunk: thread (half, c) computes rows pr = half + 2h of column c
+    if (c < cw) {
+      double acc[MAXH];
+#pragma unroll
+      for (int h = 0; h < MAXH; h++) acc[h] = 0.0;
+      for (int t = 0; t < ncr; t++) {
+        const double* Ct = sCt + t * Np * Np;
+        for (int pi = 0; pi < Np; pi++) {
+          const double tv = sT[(size_t)(t * Np + pi) * CW + c];
+#pragma unroll
+          for (int h = 0; h < MAXH; h++) {
+            const int pr = 2 * h + half;
+            if (2 * h < Np) acc[h] += Ct[min(pr, Np - 1) * Np + pi] * tv;
+          }
+        }
+      }
+      double* Acol = A + (size_t)R * Np * n + (size_t)(ac * Nq + q0) * Np + c;
+#pragma unroll
+      for (int h = 0; h < MAXH; h++) {
+        const int pr = 2 * h + half;
+        if (pr < Np) __stcs(Acol + (size_t)pr * n, acc[h]);
+      }
+    }
+  }
+}
+
+size_t abuild_smem(int Np) {
+  const int CW = std::max(1, AB_COLS / Np) * Np;
+  return (size_t)(2 * Np * Np + 2 * Np * CW) * sizeof(double) + (size_t)2 * Np * 2 * sizeof(int64_t);
+}
+
+}  // namespace
+
+int alpha_offsets_device(const DeviceLayout& L, const DeviceCSR& P, int32_t* d_aoff, cudaStream_t st) {
+  const size_t total = (size_t)L.n * (L.Nalpha + 1);
+  if (total == 0) return TT_OK;
+  k_alpha_offsets<<<ceil_div(total, 256), 256, 0, st>>>(L.n, L.Nalpha, L.Nq * L.Np, P.rowptr.ptr, P.col.ptr, d_aoff);
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+int build_A_device(const DeviceLayout& L, const DeviceCSR& P, const int32_t* d_aoff, double* d_A, cudaStream_t st) {
+  const int n = L.n;
+  if (n == 0) return TT_OK;
+  if (L.Np > 64) {
+    set_error("Np_WP > 64 is not supported by the A-build kernel");
+    return TT_ERR_UNSUPPORTED;
+  }
+  // dense contraction 2 k Np n^2 and sparse product 2 k Np nnz flops (k = mean
+  // coupled partners); A written once, P123 read once per coupled column wave
+  const double kcpl = L.Nalpha ? (double)L.cpl.count / L.Nalpha : 0.0;
+  ProfScope prof(TT_PROF_A_BUILD, st, 2.0 * kcpl * L.Np * ((double)P.nnz + (double)n * n),
+                 12.0 * kcpl * (double)P.nnz + 8.0 * (double)n * n);
+  const size_t smem = abuild_smem(L.Np);
+  dim3 grid(L.Nalpha * L.Nq, L.Nalpha);
+  if (L.Np <= 32) {
+    TT_TRY(smem_limit_once((const void*)k_abuild<16>, (int)smem));
+    k_abuild<16><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr, d_aoff,
+                                                 L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr, L.blk_off.ptr,
+                                                 L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
+  } else {
+    TT_TRY(smem_limit_once((const void*)k_abuild<32>, (int)smem));
+    k_abuild<32><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr, d_aoff,
+                                                 L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr, L.blk_off.ptr,
+                                                 L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
+  }
+  count_launch();
+  TT_CUDA_TRY(cudaGetLastError());
+  return TT_OK;
+}
+
+}  // namespace tt

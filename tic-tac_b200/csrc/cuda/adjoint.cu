@@ -2,7 +2,7 @@
 // perturbations dV/dtheta of the two-body potential.
 //
 // With A = OP(C)^T (2 P123) OP(V C) (the block operators of the 2N structure,
-// A built by k_pvc/k_ct) and x_d = (1 - A G)^{-1} A e_d the on-shell columns,
+// A built by k_abuild) and x_d = (1 - A G)^{-1} A e_d the on-shell columns,
 //   dU[d'][d] = lambda_d'^T dA w_d,  lambda_d' = (1 - A G)^{-T} e_d',
 //   w_d = e_d + G o x_d,  dA = OP(C)^T (2 P123) OP(dV C),
 // so that per parameter only g_d'^T OP(dV C) w_d is needed, with

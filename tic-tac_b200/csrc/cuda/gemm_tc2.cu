@@ -100,20 +100,25 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// try_wait with a suspend-time hint: the waiting thread sleeps until the phase
+// completes or about SUSPEND_NS pass, instead of spinning on issue slots that
+// the MMA-issuing warp shares
+constexpr uint32_t SUSPEND_NS = 20000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(SUSPEND_NS)
       : "memory");
   return ok != 0;
 }
 // Bounded wait: false if the phase did not complete within WAIT_NS or another
 // role of this launch already reported an error.
 __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = now_ns();
   while (!mbar_try_wait(bar, parity)) {
     if (*(volatile int*)err != 0) return false;

@@ -778,7 +778,7 @@ int panel_gemm_sub(int mode, T* C, int ldc, const T* L, int ldl, const T* U, int
 
 template <typename T>
 int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, cudaStream_t st, int use_tc,
-                             int* info, bool blocked_order, int panel) {
+                             int* info, bool blocked_order, int panel, int inv_block) {
   const int mode = use_tc;
   const bool tc = mode != 0;
   if (mode < 0 || mode > TC_BF16X3) {
@@ -797,6 +797,11 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     set_error("panel width " + std::to_string(panel) + " (a multiple of 32 up to 512)");
     return TT_ERR_BADARG;
   }
+  if (inv_block < 0 || inv_block > INV_MAX || inv_block % IB != 0) {
+    set_error("inverse block " + std::to_string(inv_block) + " (a multiple of 32 up to 512)");
+    return TT_ERR_BADARG;
+  }
+  const int IVB = inv_block ? inv_block : 128;
   const int NB = panel ? panel : (sizeof(T) == sizeof(float2)) ? 512 : 128;
   const int G = device_sm_count();
   DevBuf<double> sval;
@@ -863,12 +868,12 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   // unit-lower block: X = L^{-1} once, then U = X A in one product
   const bool inv_solve = (mode == TC_TF32 || mode == TC_BF16X3);
   DevBuf<T> Xinv;
-  if (inv_solve) TT_TRY(Xinv.alloc((size_t)std::min(NB, INV_MAX) * std::min(NB, INV_MAX)));
+  if (inv_solve) TT_TRY(Xinv.alloc((size_t)std::min(NB, IVB) * std::min(NB, IVB)));
   // rows [r0, r0 + h) of columns [cb, ce) <- L^{-1} of them, L the unit-lower h x h block at (r0, r0):
   // halves recursively, so that most of the work is one update of depth h / 2
   std::function<int(T*, int, int, int, int)> trsm_rec = [&](T* A, int r0, int h, int cb, int ce) -> int {
     if (h <= IB) return trsm_blk(A, n, r0, h, cb, ce, st);
-    if (inv_solve && h % 32 == 0 && h <= INV_MAX) {
+    if (inv_solve && h % 32 == 0 && h <= IVB) {
       TT_TRY(inv_unit_lower(A, n, r0, h, Xinv.ptr, st));
       return tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)r0 * n + cb, n,
                           reinterpret_cast<const float2*>(Xinv.ptr), h,
@@ -981,9 +986,9 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   return TT_OK;
 }
 template int lu_factor_batched_device<double2>(double2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                               bool, int);
+                                               bool, int, int);
 template int lu_factor_batched_device<float2>(float2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                              bool, int);
+                                              bool, int, int);
 
 template <typename T>
 int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {

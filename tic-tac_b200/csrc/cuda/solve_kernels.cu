@@ -1,6 +1,6 @@
-// Kernels of the Faddeev-solve stage other than the LU factorisation:
-// resolvent diagonals, the dense kernel matrix A = C^T (2 P123) (V C),
-// L = 1 - A diag(G), right-hand sides and the FP64 refinement residual.
+// Kernels of the Faddeev-solve stage other than the LU factorisation and the
+// A build (a_build.cu): resolvent diagonals, L = 1 - A diag(G), right-hand
+// sides and the FP64 refinement residual.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -131,118 +131,6 @@ __global__ void k_dresolvent(int Na, int Nq, int Np, const int32_t* __restrict__
     dim = dnim * M_PI / (Dp * Dq) - im * dDp / Dp;
   }
   dG[tid] = make_double2(dre, dim);
-}
-
-__device__ __forceinline__ int64_t lower_bound_col(const int32_t* __restrict__ col, int64_t lo, int64_t hi,
-                                                   int32_t key) {
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (col[mid] < key) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
-// B = 2 P123 (V C)_big, one warp per (row r, alpha_c); calculate_PVC_col
-// (solve_faddeev.cpp:4-48) restated row-wise.  B must be zeroed.
-__global__ void k_pvc(int Na, int Nq, int Np, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
-                      const double* __restrict__ val, const int32_t* __restrict__ blk,
-                      const int32_t* __restrict__ part, const int32_t* __restrict__ cpl_off,
-                      const int32_t* __restrict__ cpl, const int64_t* __restrict__ blk_off,
-                      const int32_t* __restrict__ blk_dim, const double* __restrict__ VC, double* __restrict__ B) {
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const int n = Na * Nq * Np;
-  if (warp >= (int64_t)n * Na) return;
-  const int r = (int)(warp / Na), ac = (int)(warp % Na);
-  const int NqNp = Nq * Np;
-  const int64_t r_lo = rowptr[r], r_hi = rowptr[r + 1];
-  if (r_lo == r_hi) return;
-  const int b = blk[ac];
-  const int dimb = blk_dim[b];
-  const double* VCb = VC + blk_off[b];
-  const int part_c = part[ac];
-  double* Brow = B + (size_t)r * n + (size_t)ac * NqNp;
-  for (int t = cpl_off[ac]; t < cpl_off[ac + 1]; t++) {
-    const int aj = cpl[t];
-    const int part_j = part[aj];
-    const int64_t lo = lower_bound_col(col, r_lo, r_hi, aj * NqNp);
-    const int64_t hi = lower_bound_col(col, lo, r_hi, (aj + 1) * NqNp);
-    for (int pc0 = 0; pc0 < Np; pc0 += 32) {
-      const int pc = pc0 + lane;
-      double acc = 0.0;
-      int cur_q = -1;
-      for (int64_t e = lo; e < hi; e++) {
-        const int cj = col[e] - aj * NqNp;
-        const int q = cj / Np, pj = cj % Np;
-        if (q != cur_q) {
-          if (cur_q >= 0 && pc < Np) Brow[cur_q * Np + pc] += acc;
-          acc = 0.0;
-          cur_q = q;
-        }
-        if (pc < Np) acc += (2 * val[e]) * VCb[(size_t)(part_j * Np + pj) * dimb + part_c * Np + pc];
-      }
-      if (cur_q >= 0 && pc < Np) Brow[cur_q * Np + pc] += acc;
-    }
-  }
-}
-
-// A = C^T_big B: block (alpha_r, q) x 128 columns; calculate_CPVC_col
-// (solve_faddeev.cpp:50-181) restated as small dense products.
-template <int MAXH>
-__global__ void __launch_bounds__(256) k_ct(int Na, int Nq, int Np, const int32_t* __restrict__ blk,
-                                            const int32_t* __restrict__ part, const int32_t* __restrict__ cpl_off,
-                                            const int32_t* __restrict__ cpl, const int64_t* __restrict__ blk_off,
-                                            const int32_t* __restrict__ blk_dim, const double* __restrict__ Cm,
-                                            const double* __restrict__ B, double* __restrict__ A) {
-  extern __shared__ double sCt[];  // [ncpl][Np][Np]: Ct[pr][pi]
-  const int n = Na * Nq * Np;
-  const int ar = blockIdx.y / Nq, q = blockIdx.y % Nq;
-  const int c = blockIdx.x * 128 + (threadIdx.x & 127);
-  const int half = threadIdx.x >> 7;
-  const int b = blk[ar];
-  const int dimb = blk_dim[b];
-  const double* Cb = Cm + blk_off[b];
-  const int part_r = part[ar];
-  const int t0 = cpl_off[ar], t1 = cpl_off[ar + 1];
-  const int ncpl = t1 - t0;
-  for (int i = threadIdx.x; i < ncpl * Np * Np; i += blockDim.x) {
-    const int t = i / (Np * Np), pr = (i / Np) % Np, pi = i % Np;
-    const int ai = cpl[t0 + t];
-    // Ct(alpha_r, alpha_i)(pr, pi) = C[(part_i, pi), (part_r, pr)]
-    sCt[i] = Cb[(size_t)(part[ai] * Np + pi) * dimb + part_r * Np + pr];
-  }
-  __syncthreads();
-  if (c >= n) return;
-  double acc[MAXH];
-#pragma unroll
-  for (int h = 0; h < MAXH; h++) acc[h] = 0.0;
-  constexpr int PU = 8;  // B rows loaded ahead of their products (independent loads in flight)
-  for (int t = 0; t < ncpl; t++) {
-    const int ai = cpl[t0 + t];
-    const double* Bcol = B + ((size_t)ai * Nq * Np + (size_t)q * Np) * n + c;
-    const double* Ct = sCt + t * Np * Np;
-    for (int p0 = 0; p0 < Np; p0 += PU) {
-      double bv[PU];
-#pragma unroll
-      for (int u = 0; u < PU; u++) bv[u] = (p0 + u < Np) ? __ldcs(Bcol + (size_t)(p0 + u) * n) : 0.0;
-#pragma unroll
-      for (int u = 0; u < PU; u++) {
-        if (p0 + u >= Np) break;
-#pragma unroll
-        for (int h = 0; h < MAXH; h++) {
-          const int pr = 2 * h + half;
-          if (pr < Np) acc[h] += Ct[pr * Np + p0 + u] * bv[u];
-        }
-      }
-    }
-  }
-  double* Acol = A + ((size_t)ar * Nq * Np + (size_t)q * Np) * n + c;
-#pragma unroll
-  for (int h = 0; h < MAXH; h++) {
-    const int pr = 2 * h + half;
-    if (pr < Np) __stcs(Acol + (size_t)pr * n, acc[h]);
-  }
 }
 
 template <typename T>
@@ -487,38 +375,6 @@ int resolvent_device_tables(int Na, int Nq, int Np, const int32_t* e_off, const 
   if (total == 0) return TT_OK;
   k_resolvent<<<ceil_div(total, 256), 256, 0, st>>>(Na, Nq, Np, e_off, e_swp, q_WP, d_E, nE,
                                                     reinterpret_cast<double2*>(d_G));
-  count_launch();
-  TT_CUDA_TRY(cudaGetLastError());
-  return TT_OK;
-}
-
-int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, double* d_A, cudaStream_t st) {
-  const int n = L.n;
-  if (L.Np > 64) {
-    set_error("Np_WP > 64 is not supported by the A-build kernel");
-    return TT_ERR_UNSUPPORTED;
-  }
-  // SpMM 2 k Np nnz + block product 2 k Np n^2 flops (k = mean coupled partners);
-  // CSR read once, B written, read, A written
-  const double kcpl = L.Nalpha ? (double)L.cpl.count / L.Nalpha : 0.0;
-  ProfScope prof(TT_PROF_A_BUILD, st, 2.0 * kcpl * L.Np * ((double)P.nnz + (double)n * n),
-                 12.0 * (double)P.nnz + 24.0 * (double)n * n);
-  TT_CUDA_TRY(cudaMemsetAsync(d_B, 0, sizeof(double) * (size_t)n * n, st));
-  if (P.nnz > 0) {
-    const size_t warps = (size_t)n * L.Nalpha;
-    k_pvc<<<ceil_div(warps * 32, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
-                                                     L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr, L.blk_off.ptr,
-                                                     L.blk_dim.ptr, L.VC.ptr, d_B);
-    count_launch();
-    TT_CUDA_TRY(cudaGetLastError());
-  }
-  // the coupling lists hold at most 2 partners per alpha for the 2N structure;
-  // shared memory is sized for 2 Np x Np blocks
-  const size_t smem = (size_t)2 * L.Np * L.Np * sizeof(double);
-  dim3 grid(ceil_div(n, 128), L.Nalpha * L.Nq);
-  if (smem > 48 * 1024) TT_TRY(smem_limit_once((const void*)k_ct<32>, (int)smem));
-  k_ct<32><<<grid, 256, smem, st>>>(L.Nalpha, L.Nq, L.Np, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
-                                    L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, d_B, d_A);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;

@@ -48,38 +48,83 @@ struct ProfScope {
     if (_s != TT_OK) return _s; \
   } while (0)
 
+// Large device blocks (at least kCacheMinBytes) that a DevBuf releases are
+// kept for reuse instead of going back to the driver, where cudaMalloc and
+// cudaFree of tens of GB take 5-35 ms each.  A cached block serves a request
+// of at most its size and at least two thirds of it.  Releasing a block waits
+// for the device, as cudaFree does, so a block is idle when it is handed out
+// again.  Cached blocks are freed when an allocation would otherwise fail, by
+// device_cache_trim(), and by tt_run_destroy / tt_release_cached_device_memory.
+constexpr size_t kCacheMinBytes = size_t(256) << 20;
+void* device_cache_take(size_t bytes, size_t* capacity);
+void device_cache_give(void* p, size_t capacity);
+size_t device_cache_bytes();  // cached on the current device
+void device_cache_trim();     // frees the current device's cached blocks
+
 // Owning device buffer.  alloc() reports NOMEM through the status path instead
 // of faulting.
 template <typename T>
 struct DevBuf {
   T* ptr = nullptr;
   size_t count = 0;
+  size_t cap = 0;  // bytes of the underlying block
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count) { o.ptr = nullptr; o.count = 0; }
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), cap(o.cap) {
+    o.ptr = nullptr;
+    o.count = 0;
+    o.cap = 0;
+  }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); ptr = o.ptr; count = o.count; o.ptr = nullptr; o.count = 0; }
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      count = o.count;
+      cap = o.cap;
+      o.ptr = nullptr;
+      o.count = 0;
+      o.cap = 0;
+    }
     return *this;
   }
   ~DevBuf() { release(); }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+      if (cap >= kCacheMinBytes) device_cache_give(ptr, cap);
+      else cudaFree(ptr);
+    }
     ptr = nullptr;
     count = 0;
+    cap = 0;
   }
   int alloc(size_t n) {
     release();
     if (n == 0) return TT_OK;
-    cudaError_t e = cudaMalloc((void**)&ptr, n * sizeof(T));
+    const size_t bytes = n * sizeof(T);
+    if (bytes >= kCacheMinBytes) {
+      size_t c = 0;
+      if (void* p = device_cache_take(bytes, &c)) {
+        ptr = static_cast<T*>(p);
+        count = n;
+        cap = c;
+        return TT_OK;
+      }
+    }
+    cudaError_t e = cudaMalloc((void**)&ptr, bytes);
+    if (e == cudaErrorMemoryAllocation && device_cache_bytes() > 0) {
+      cudaGetLastError();
+      device_cache_trim();
+      e = cudaMalloc((void**)&ptr, bytes);
+    }
     if (e != cudaSuccess) {
       ptr = nullptr;
       cudaGetLastError();
-      set_error("device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed: " +
-                cudaGetErrorString(e));
+      set_error("device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
       return e == cudaErrorMemoryAllocation ? TT_ERR_NOMEM : TT_ERR_CUDA;
     }
     count = n;
+    cap = bytes;
     return TT_OK;
   }
   int upload(const T* h, size_t n, cudaStream_t s) {

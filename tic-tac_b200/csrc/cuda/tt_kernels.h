@@ -54,8 +54,11 @@ int resolvent_device_tables(int Na, int Nq, int Np, const int32_t* e_off, const 
                             const double* d_E, int nE, double* d_G, cudaStream_t st);
 
 // Dense A (n x n, row-major FP64) = C^T (2 P123) (V C); solve_faddeev.cpp:4-181.
-// d_B is an n x n FP64 scratch of the product 2 P123 (V C).
-int build_A_device(const DeviceLayout& L, const DeviceCSR& P, double* d_B, double* d_A, cudaStream_t st);
+// d_aoff: the table of alpha_offsets_device for P.
+int build_A_device(const DeviceLayout& L, const DeviceCSR& P, const int32_t* d_aoff, double* d_A, cudaStream_t st);
+// d_aoff[r (Nalpha + 1) + a]: first nonzero of CSR row r with column >= a Nq Np,
+// relative to rowptr[r] (n (Nalpha + 1) int32).
+int alpha_offsets_device(const DeviceLayout& L, const DeviceCSR& P, int32_t* d_aoff, cudaStream_t st);
 
 // L = 1 - A diag(G), complex, row-major; T = double2 (complex128) or float2 (complex64).
 template <typename T>
@@ -80,10 +83,14 @@ int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_te
 // blocked: the panel in 32-column steps, each followed by its rank-32 update
 // (otherwise recursive halving of the panel and of the U12 solve).
 // panel: the outer panel width (a multiple of 32 up to 512; 0 = 512 for
-// complex64, 128 for complex128).
+// complex64, 128 for complex128).  inv_block: in the tensor-core modes a block
+// row is solved through the explicit inverses of unit-lower diagonal blocks of
+// at most this many rows (a multiple of 32 up to 512; 0 = 128), larger blocks
+// by halving with tensor-core updates between the halves.
 template <typename T>
 int lu_factor_batched_device(T* const* d_L, int B, int n, int32_t* const* d_ipiv, cudaStream_t st,
-                             int use_tensor_cores, int* info, bool blocked = false, int panel = 0);
+                             int use_tensor_cores, int* info, bool blocked = false, int panel = 0,
+                             int inv_block = 0);
 // Row permutation of the interchange sequence ipiv (host, once per factorisation).
 int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cudaStream_t st);
 // Inverted diagonal blocks of one LU factor (unit lower and upper) and their

@@ -164,6 +164,7 @@ int ChannelSolver::set_P_device(DeviceCSR&& P) {
     return TT_ERR_BADARG;
   }
   P_ = std::move(P);
+  aoff_.release();
   return TT_OK;
 }
 
@@ -171,6 +172,7 @@ int ChannelSolver::set_P_host_csr(const int64_t* rowptr, const int32_t* col, con
                                   cudaStream_t st) {
   P_.n = n;
   P_.nnz = nnz;
+  aoff_.release();
   TT_TRY(P_.rowptr.upload(rowptr, (size_t)n + 1, st));
   TT_TRY(P_.col.upload(col, (size_t)std::max<int64_t>(nnz, 0), st));
   TT_TRY(P_.val.upload(val, (size_t)std::max<int64_t>(nnz, 0), st));
@@ -179,15 +181,18 @@ int ChannelSolver::set_P_host_csr(const int64_t* rowptr, const int32_t* col, con
 
 int ChannelSolver::set_P_host_csc(const double* val, const int32_t* row, const uint64_t* colptr, int64_t nnz,
                                   cudaStream_t st) {
+  aoff_.release();
   return csc_to_csr_device(val, row, colptr, nnz, n, P_, st);
 }
 
 int ChannelSolver::build_A(cudaStream_t st, double* ms) {
   auto t0 = std::chrono::steady_clock::now();
   TT_TRY(A_.alloc((size_t)n * n));
-  DevBuf<double> B;
-  TT_TRY(B.alloc((size_t)n * n));
-  TT_TRY(build_A_device(L_, P_, B.ptr, A_.ptr, st));
+  if (!aoff_.ptr && n > 0) {
+    TT_TRY(aoff_.alloc((size_t)n * (L_.Nalpha + 1)));
+    TT_TRY(alpha_offsets_device(L_, P_, aoff_.ptr, st));
+  }
+  TT_TRY(build_A_device(L_, P_, aoff_.ptr, A_.ptr, st));
   TT_CUDA_TRY(cudaStreamSynchronize(st));
   if (ms) *ms = ms_since(t0);
   return TT_OK;
@@ -506,6 +511,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
   if (opt.mixed && nE > 1 && opt.energy_batch > 1) {
     size_t free_b = 0, total_b = 0;
     TT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    free_b += device_cache_bytes();  // cached blocks are freed when an allocation needs them
     const size_t per = (size_t)n * n * sizeof(float2), reserve = (size_t)2 << 30;
     const size_t fit = free_b > reserve + per ? (free_b - reserve) / per : 1;
     B = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>((size_t)nE, std::min(opt.energy_batch, 4)), fit));
@@ -567,7 +573,8 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       r.ms_form += ms_since(t0);
       t0 = std::chrono::steady_clock::now();
       TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, product, info, opt.panel_blocked,
-                                              opt.panel_width ? opt.panel_width : tuned_panel_width(n, product)));
+                                              opt.panel_width ? opt.panel_width : tuned_panel_width(n, product),
+                                              opt.inverse_block));
       r.ms_factor += ms_since(t0);
     } else {
       TT_TRY(form_L_device<double2>(A_.ptr, G_.ptr + (size_t)2 * n * g0, n, L64.ptr, st));

@@ -62,6 +62,10 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
     } else if (key == "panel_width") {
       rp.panel_width = std::stoi(value);
       if (rp.panel_width < 0 || rp.panel_width > 512 || rp.panel_width % 32) return bad("panel_width (0 or 32..512)");
+    } else if (key == "inverse_block") {
+      rp.inverse_block = std::stoi(value);
+      if (rp.inverse_block < 0 || rp.inverse_block > 512 || rp.inverse_block % 32)
+        return bad("inverse_block (0 or 32..512)");
     } else if (key == "panel_order") {
       if (value == "blocked") rp.panel_blocked = true;
       else if (value == "recursive") rp.panel_blocked = false;

@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = (
     "tt_profile_read", "tt_solve_faddeev_adjoint", "tt_run_solve_adjoint", "tt_run_num_lecs", "tt_run_lec_derivative",
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
     "tt_run_solve_energies", "tt_profile_select", "tt_run_adjoint_forward", "tt_run_adjoint_backward",
-    "tt_run_swp_derivative", "tt_run_set_solve_option",
+    "tt_run_swp_derivative", "tt_run_set_solve_option", "tt_release_cached_device_memory",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
@@ -548,7 +548,7 @@ class Run:
         return dVu, dVc[:self.host_array(4).size]
 
     def set_solve_option(self, key, value):
-        """Change a solve option (tc_product, panel_width, panel_order, energy_batch, refine_tol,
+        """Change a solve option (tc_product, panel_width, panel_order, inverse_block, energy_batch, refine_tol,
         refine_max_iter) for the next solves."""
         _check(self.lib.tt_run_set_solve_option(self._h, str(key).encode(), str(value).encode()))
 

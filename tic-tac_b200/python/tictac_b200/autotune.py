@@ -25,7 +25,7 @@ HEADER = os.path.normpath(os.path.join(os.path.dirname(__file__), "..", "..", "c
 
 def time_widths(run, chans, energies, widths, product, reps):
     """{n: {width: median ms}} of build_A + mixed solve per channel."""
-    run.set_solve_option("tc_product", product)
+    run.set_solve_option("tc_product", {v: k for k, v in PRODUCTS.items()}[product])
     out = {}
     for c in chans:
         n = run.channel_info(c)["n"]
