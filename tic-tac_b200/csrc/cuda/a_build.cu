@@ -25,7 +25,7 @@ namespace tt {
 namespace {
 
 constexpr int AB_THREADS = 256;
-constexpr int AB_COLS = 128;  // columns of A per chunk: QW = AB_COLS / Np values of q'
+constexpr int AB_COLS = 64;  // columns of A per chunk: QW = AB_COLS / Np values of q'
 
 __device__ __forceinline__ int64_t first_col_at_least(const int32_t* __restrict__ col, int64_t lo, int64_t hi,
                                                       int32_t key) {
@@ -48,10 +48,31 @@ __global__ void k_alpha_offsets(int n, int Na, int NqNp, const int64_t* __restri
   aoff[tid] = (int32_t)(first_col_at_least(col, lo, hi, a * NqNp) - lo);
 }
 
-// One CTA per (row block R = ar Nq + q, column partial wave ac); MAXH >= Np / 2.
-// Dynamic shared memory: Ct [2][Np][Np], T [2 Np][QW Np] (doubles), cursors [2 Np][2] (int64).
-template <int MAXH>
-__global__ void __launch_bounds__(AB_THREADS) k_abuild(int Na, int Nq, int Np, const int64_t* __restrict__ rowptr,
+// Shared-memory layout of k_abuild for Np and the staging depth CAP.
+struct AbLayout {
+  int QW, CW, RT2;
+  size_t ct, t, start, end, base, scol, sval, bytes;
+  __host__ __device__ AbLayout(int Np, int cap) {
+    QW = AB_COLS / Np > 0 ? AB_COLS / Np : 1;
+    CW = QW * Np;
+    RT2 = 2 * Np * 2;  // (T row, coupled column wave) pairs
+    ct = 0;                                          // double [2][Np][Np]
+    t = ct + sizeof(double) * 2 * Np * Np;           // double [2 Np][CW]
+    start = t + sizeof(double) * 2 * Np * CW;        // int64 [RT2]: cursor
+    end = start + sizeof(int64_t) * RT2;             // int64 [RT2]: end of the range
+    base = end + sizeof(int64_t) * RT2;              // int64 [RT2]: index of the first staged nonzero
+    sval = base + sizeof(int64_t) * RT2;             // double [RT2][CAP]
+    scol = sval + sizeof(double) * RT2 * cap;        // int32 [RT2][CAP]
+    bytes = scol + sizeof(int32_t) * RT2 * cap;
+  }
+};
+
+// One CTA per (row block R = ar Nq + q, column partial wave ac).  MAXH >= Np / 4
+// (thread (g, c) of the contraction computes rows pr = g + 4 h of column c);
+// CAP nonzeros of every (T row, coupled aj) range are staged in shared memory
+// and refilled by the owning warp when a range runs past them.
+template <int MAXH, int CAP>
+__global__ void __launch_bounds__(AB_THREADS, 2) k_abuild(int Na, int Nq, int Np, const int64_t* __restrict__ rowptr,
                                                        const int32_t* __restrict__ col,
                                                        const double* __restrict__ val,
                                                        const int32_t* __restrict__ aoff,
@@ -63,12 +84,17 @@ __global__ void __launch_bounds__(AB_THREADS) k_abuild(int Na, int Nq, int Np, c
                                                        const int32_t* __restrict__ blk_dim,
                                                        const double* __restrict__ Cm,
                                                        const double* __restrict__ VC, double* __restrict__ A) {
-  extern __shared__ double ab_smem[];
+  extern __shared__ __align__(16) unsigned char ab_raw[];
+  const AbLayout ly(Np, CAP);
+  double* sCt = reinterpret_cast<double*>(ab_raw + ly.ct);       // [t][pr][pi]
+  double* sT = reinterpret_cast<double*>(ab_raw + ly.t);         // [t Np + pi][c]
+  int64_t* sCur = reinterpret_cast<int64_t*>(ab_raw + ly.start);  // [rr 2 + t2]
+  int64_t* sEnd = reinterpret_cast<int64_t*>(ab_raw + ly.end);
+  int64_t* sBase = reinterpret_cast<int64_t*>(ab_raw + ly.base);
+  double* sVal = reinterpret_cast<double*>(ab_raw + ly.sval);    // [rr 2 + t2][CAP]
+  int32_t* sCol = reinterpret_cast<int32_t*>(ab_raw + ly.scol);
   const int n = Na * Nq * Np, NqNp = Nq * Np;
-  const int QW = max(1, AB_COLS / Np), CW = QW * Np;
-  double* sCt = ab_smem;                      // [t][pr][pi]
-  double* sT = sCt + 2 * Np * Np;             // [t Np + pi][c]
-  int64_t* sCur = reinterpret_cast<int64_t*>(sT + 2 * Np * CW);  // [t Np + pi][t2]
+  const int QW = ly.QW, CW = ly.CW;
   const int R = blockIdx.x, ac = blockIdx.y;
   const int ar = R / Nq, q = R % Nq;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -85,20 +111,33 @@ __global__ void __launch_bounds__(AB_THREADS) k_abuild(int Na, int Nq, int Np, c
       sCt[i] = Cb[(size_t)(part[ai] * Np + pi) * dimb + part_r * Np + pr];
     }
   }
-  // cursors: each T row's position in the P123 row, per coupled column partial wave aj
+  // the range of every (T row, coupled aj) in its P123 row
   for (int i = tid; i < RT * 2; i += AB_THREADS) {
     const int rr = i >> 1, t2 = i & 1;
-    int64_t e = 0;
+    int64_t e0 = 0, e1 = 0;
     if (t2 < ncc) {
       const int ai = cpl[cr0 + rr / Np], pi = rr % Np, aj = cpl[cc0 + t2];
       const int r = (ai * Nq + q) * Np + pi;
-      e = rowptr[r] + aoff[(size_t)r * (Na + 1) + aj];
+      const int64_t rp = rowptr[r];
+      e0 = rp + aoff[(size_t)r * (Na + 1) + aj];
+      e1 = rp + aoff[(size_t)r * (Na + 1) + aj + 1];
     }
-    sCur[i] = e;
+    sCur[i] = e0;
+    sEnd[i] = e1;
+    sBase[i] = e0;
+  }
+  __syncthreads();
+  // the first CAP nonzeros of every range
+  for (int i = tid; i < RT * 2 * CAP; i += AB_THREADS) {
+    const int pr2 = i / CAP, k = i % CAP;
+    const int64_t e = sBase[pr2] + k;
+    const bool in = e < sEnd[pr2];
+    sCol[i] = in ? col[e] : INT_MAX;
+    sVal[i] = in ? val[e] : 0.0;
   }
   const int bc = blk[ac], dimc = blk_dim[bc], part_c = part[ac];
   const double* VCb = VC + blk_off[bc];
-  const int half = tid >> 7, c = tid & 127;
+  const int g = tid >> 6, c = tid & 63;  // contraction: 4 row groups x 64 columns
   for (int q0 = 0; q0 < Nq; q0 += QW) {
     const int cw = min(QW, Nq - q0) * Np;  // columns of this chunk
     __syncthreads();
@@ -106,42 +145,43 @@ __global__ void __launch_bounds__(AB_THREADS) k_abuild(int Na, int Nq, int Np, c
     __syncthreads();
     // ---- T chunk: one warp per T row (warp-private rows: no atomics)
     for (int rr = warp; rr < RT; rr += AB_THREADS / 32) {
-      const int ai = cpl[cr0 + rr / Np], pi = rr % Np;
-      const int r = (ai * Nq + q) * Np + pi;
       double* Trow = sT + (size_t)rr * CW;
       for (int t2 = 0; t2 < ncc; t2++) {
+        const int pr2 = rr * 2 + t2;
         const int aj = cpl[cc0 + t2], part_j = part[aj];
-        const int64_t e_end = rowptr[r] + aoff[(size_t)r * (Na + 1) + aj + 1];
         const int32_t lim = aj * NqNp + min(q0 + QW, Nq) * Np;  // first column past the chunk
-        const int32_t base = aj * NqNp + q0 * Np;
-        int64_t e = sCur[rr * 2 + t2];
-        bool done = e >= e_end;
-        while (!done) {
-          // 32 nonzeros per coalesced load, then applied one by one from registers
-          const int64_t el = e + lane;
-          const int32_t cl = el < e_end ? col[el] : INT_MAX;
-          const double vl = el < e_end ? val[el] : 0.0;
-          int used = 0;
-          for (int i = 0; i < 32; i++) {
-            const int32_t cj = __shfl_sync(0xffffffffu, cl, i);
-            if (cj >= lim) {  // past the chunk (or the end of the aj range): uniform over the warp
-              done = true;
-              break;
+        const int32_t cbase = aj * NqNp + q0 * Np;
+        const int64_t e_end = sEnd[pr2];
+        int64_t e = sCur[pr2], eb = sBase[pr2];
+        while (e < e_end) {
+          if (e - eb >= CAP) {
+            // past the staged nonzeros: the next CAP of this range
+            __syncwarp();
+            for (int k = lane; k < CAP; k += 32) {
+              const int64_t ek = e + k;
+              const bool in = ek < e_end;
+              sCol[pr2 * CAP + k] = in ? col[ek] : INT_MAX;
+              sVal[pr2 * CAP + k] = in ? val[ek] : 0.0;
             }
-            const double v = 2.0 * __shfl_sync(0xffffffffu, vl, i);
-            const int rel = cj - base, qq = rel / Np, pj = rel % Np;
-            const double* vrow = VCb + (size_t)(part_j * Np + pj) * dimc + part_c * Np;
-            for (int pc = lane; pc < Np; pc += 32) Trow[qq * Np + pc] += v * vrow[pc];
-            used++;
+            eb = e;
+            __syncwarp();
           }
-          e += used;
-          if (e >= e_end) done = true;
+          const int32_t cj = sCol[pr2 * CAP + (int)(e - eb)];
+          if (cj >= lim) break;
+          const double v = 2.0 * sVal[pr2 * CAP + (int)(e - eb)];
+          const int rel = cj - cbase, qq = rel / Np, pj = rel % Np;
+          const double* vrow = VCb + (size_t)(part_j * Np + pj) * dimc + part_c * Np;
+          for (int pc = lane; pc < Np; pc += 32) Trow[qq * Np + pc] += v * vrow[pc];
+          e++;
         }
-        if (lane == 0) sCur[rr * 2 + t2] = e;
+        if (lane == 0) {
+          sCur[pr2] = e;
+          sBase[pr2] = eb;
+        }
       }
     }
     __syncthreads();
-    // ---- A chunk: thread (half, c) computes rows pr = half + 2h of column c
+    // ---- A chunk: thread (g, c) computes rows pr = g + 4 h of column c
     if (c < cw) {
       double acc[MAXH];
 #pragma unroll
@@ -152,24 +192,19 @@ __global__ void __launch_bounds__(AB_THREADS) k_abuild(int Na, int Nq, int Np, c
           const double tv = sT[(size_t)(t * Np + pi) * CW + c];
 #pragma unroll
           for (int h = 0; h < MAXH; h++) {
-            const int pr = 2 * h + half;
-            if (2 * h < Np) acc[h] += Ct[min(pr, Np - 1) * Np + pi] * tv;
+            const int pr = g + 4 * h;
+            if (4 * h < Np) acc[h] += Ct[min(pr, Np - 1) * Np + pi] * tv;
           }
         }
       }
       double* Acol = A + (size_t)R * Np * n + (size_t)(ac * Nq + q0) * Np + c;
 #pragma unroll
       for (int h = 0; h < MAXH; h++) {
-        const int pr = 2 * h + half;
+        const int pr = g + 4 * h;
         if (pr < Np) __stcs(Acol + (size_t)pr * n, acc[h]);
       }
     }
   }
-}
-
-size_t abuild_smem(int Np) {
-  const int CW = std::max(1, AB_COLS / Np) * Np;
-  return (size_t)(2 * Np * Np + 2 * Np * CW) * sizeof(double) + (size_t)2 * Np * 2 * sizeof(int64_t);
 }
 
 }  // namespace
@@ -195,18 +230,19 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, const int32_t* d_a
   const double kcpl = L.Nalpha ? (double)L.cpl.count / L.Nalpha : 0.0;
   ProfScope prof(TT_PROF_A_BUILD, st, 2.0 * kcpl * L.Np * ((double)P.nnz + (double)n * n),
                  12.0 * kcpl * (double)P.nnz + 8.0 * (double)n * n);
-  const size_t smem = abuild_smem(L.Np);
   dim3 grid(L.Nalpha * L.Nq, L.Nalpha);
   if (L.Np <= 32) {
-    TT_TRY(smem_limit_once((const void*)k_abuild<16>, (int)smem));
-    k_abuild<16><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr, d_aoff,
-                                                 L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr, L.blk_off.ptr,
-                                                 L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
+    const size_t smem = AbLayout(L.Np, 32).bytes;
+    TT_TRY(smem_limit_once((const void*)k_abuild<8, 32>, (int)smem));
+    k_abuild<8, 32><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
+                                                    d_aoff, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
+                                                    L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
   } else {
-    TT_TRY(smem_limit_once((const void*)k_abuild<32>, (int)smem));
-    k_abuild<32><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr, d_aoff,
-                                                 L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr, L.blk_off.ptr,
-                                                 L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
+    const size_t smem = AbLayout(L.Np, 16).bytes;
+    TT_TRY(smem_limit_once((const void*)k_abuild<16, 16>, (int)smem));
+    k_abuild<16, 16><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
+                                                     d_aoff, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
+                                                     L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
   }
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());

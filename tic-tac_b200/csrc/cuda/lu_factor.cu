@@ -443,8 +443,9 @@ __global__ void __launch_bounds__(SP_THREADS) k_subpanel_smem(SubpanelBatch<T> b
 // k_inv_diag32 inverts the 32 x 32 diagonal blocks (one CTA each), then per
 // level s = 64, 128, .. every pair of inverted s/2 blocks is joined,
 //   [X11 0; X21 X22] with X21 = -X22 (L21 X11),
-// one CTA per 32 x 32 tile of X21 (k_inv_join), all pairs of a level in one
-// launch.  Entries above the diagonal are written as zero.
+// first T = L21 X11, then X21 = -X22 T, one CTA per 32 x 32 tile
+// (k_inv_join_t, k_inv_join_x), all pairs of a level in the same two
+// launches.  Entries above the diagonal are written as zero.
 constexpr int INV_MAX = 512;
 template <typename T>
 __device__ __forceinline__ void cfma_sub(T& acc, T a, T b) {
@@ -495,53 +496,62 @@ __global__ void __launch_bounds__(256) k_inv_diag32(const T* __restrict__ A, int
 }
 
 // Level s: pair p joins the blocks [p s, p s + s/2) and [p s + s/2, p s + s)
-// (the second may be shorter at the end of w).  CTA (tile ty, tx, pair p)
-// computes X21[ty][tx] = -sum_m X22[ty][m] (L21 X11)[m][tx] over the 32-row
-// tiles m of the second block.
+// (the second may be shorter at the end of w) in two launches of one CTA per
+// 32 x 32 tile (ty: tile row of block 2, tx: tile column of block 1):
+//   k_inv_join_t:  Tp = L21 X11          (X11 lower: k from the tile's column)
+//   k_inv_join_x:  X21 = -X22 Tp         (X22 lower: m up to the tile's row)
+// Tp is the pair's h x h scratch at T + p h h.
 template <typename T>
-__global__ void __launch_bounds__(256) k_inv_join(const T* __restrict__ A, int n, int r0, int w, int s,
-                                                  T* __restrict__ X) {
-  extern __shared__ unsigned char join_raw[];
-  T(*sT)[33] = reinterpret_cast<T(*)[33]>(join_raw);  // (L21 X11) column tile, up to s/2 rows
+__global__ void __launch_bounds__(256) k_inv_join_t(const T* __restrict__ A, int n, int r0, int w, int s,
+                                                    const T* __restrict__ X, T* __restrict__ Tsc) {
   __shared__ T sa[32][33];
   __shared__ T sb[32][33];
   const int h = s / 2;
   const int p = blockIdx.z, base = p * s;
   const int h2 = min(h, w - base - h);  // rows of the second block
-  if (h2 <= 0) return;
-  const int ty = blockIdx.y, tx = blockIdx.x;  // tile row within block 2, tile column within block 1
-  if (ty * 32 >= h2) return;
+  const int ty = blockIdx.y, tx = blockIdx.x;
+  if (h2 <= 0 || ty * 32 >= h2) return;
   const int tid = threadIdx.x, row = tid >> 3, cq = (tid & 7) * 4;
-  const int c0 = base + tx * 32;  // columns of X11 (block 1)
-  // sT[m][c] = sum_k L21[m][k] X11[k][c] for all rows m of block 2 (k over block 1; X11 lower: k >= c)
-  for (int m0 = 0; m0 < h2; m0 += 32) {
-    T acc[4];
+  const int c0 = base + tx * 32;  // columns of X11
+  T acc[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) acc[q].x = acc[q].y = 0;
-    for (int k0 = tx * 32; k0 < h; k0 += 32) {
-      __syncthreads();
-      for (int t = tid; t < 1024; t += 256) {
-        const int i = t >> 5, j = t & 31;
-        T a, b;
-        a.x = a.y = b.x = b.y = 0;
-        if (m0 + i < h2) a = A[(size_t)(r0 + base + h + m0 + i) * n + r0 + base + k0 + j];
-        b = X[(size_t)(base + k0 + i) * w + c0 + j];
-        sa[i][j] = a;
-        sb[i][j] = b;
-      }
-      __syncthreads();
-#pragma unroll 8
-      for (int kk = 0; kk < 32; kk++) {
-        const T a = sa[row][kk];
-#pragma unroll
-        for (int q = 0; q < 4; q++) cfma_add(acc[q], a, sb[kk][cq + q]);
-      }
+  for (int q = 0; q < 4; q++) acc[q].x = acc[q].y = 0;
+  for (int k0 = tx * 32; k0 < h; k0 += 32) {
+    __syncthreads();
+    for (int t = tid; t < 1024; t += 256) {
+      const int i = t >> 5, j = t & 31;
+      T a;
+      a.x = a.y = 0;
+      if (ty * 32 + i < h2) a = A[(size_t)(r0 + base + h + ty * 32 + i) * n + r0 + base + k0 + j];
+      sa[i][j] = a;
+      sb[i][j] = X[(size_t)(base + k0 + i) * w + c0 + j];
     }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < 32; kk++) {
+      const T a = sa[row][kk];
 #pragma unroll
-    for (int q = 0; q < 4; q++) sT[m0 + row][cq + q] = acc[q];
+      for (int q = 0; q < 4; q++) cfma_add(acc[q], a, sb[kk][cq + q]);
+    }
   }
-  __syncthreads();
-  // X21[ty][tx] = -sum_m X22[ty rows][m] sT[m][.]  (X22 lower: m <= row)
+  if (ty * 32 + row < h2) {
+    T* Tp = Tsc + (size_t)p * h * h;
+#pragma unroll
+    for (int q = 0; q < 4; q++) Tp[(size_t)(ty * 32 + row) * h + tx * 32 + cq + q] = acc[q];
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv_join_x(int w, int s, T* __restrict__ X, const T* __restrict__ Tsc) {
+  __shared__ T sa[32][33];
+  __shared__ T sb[32][33];
+  const int h = s / 2;
+  const int p = blockIdx.z, base = p * s;
+  const int h2 = min(h, w - base - h);
+  const int ty = blockIdx.y, tx = blockIdx.x;
+  if (h2 <= 0 || ty * 32 >= h2) return;
+  const int tid = threadIdx.x, row = tid >> 3, cq = (tid & 7) * 4;
+  const T* Tp = Tsc + (size_t)p * h * h;
   T acc[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) acc[q].x = acc[q].y = 0;
@@ -549,21 +559,23 @@ __global__ void __launch_bounds__(256) k_inv_join(const T* __restrict__ A, int n
     __syncthreads();
     for (int t = tid; t < 1024; t += 256) {
       const int i = t >> 5, j = t & 31;
-      T a;
-      a.x = a.y = 0;
+      T a, b;
+      a.x = a.y = b.x = b.y = 0;
       if (ty * 32 + i < h2 && m0 + j < h2) a = X[(size_t)(base + h + ty * 32 + i) * w + base + h + m0 + j];
+      if (m0 + i < h2) b = Tp[(size_t)(m0 + i) * h + tx * 32 + j];
       sa[i][j] = a;
+      sb[i][j] = b;
     }
     __syncthreads();
 #pragma unroll 8
     for (int kk = 0; kk < 32; kk++) {
       const T a = sa[row][kk];
 #pragma unroll
-      for (int q = 0; q < 4; q++) cfma_sub(acc[q], a, sT[m0 + kk][cq + q]);
+      for (int q = 0; q < 4; q++) cfma_sub(acc[q], a, sb[kk][cq + q]);
     }
   }
-  const int gr = base + h + ty * 32 + row;
   if (ty * 32 + row < h2) {
+    const int gr = base + h + ty * 32 + row, c0 = base + tx * 32;
 #pragma unroll
     for (int q = 0; q < 4; q++) X[(size_t)gr * w + c0 + cq + q] = acc[q];
   }
@@ -725,8 +737,9 @@ int laswp2(T* A, int n, const int32_t* ipiv, int p0, int p1, int a0, int a1, int
   return TT_OK;
 }
 
+// Tsc: scratch of at least w * w / 2 elements
 template <typename T>
-int inv_unit_lower(const T* A, int n, int r0, int w, T* X, cudaStream_t st) {
+int inv_unit_lower(const T* A, int n, int r0, int w, T* X, T* Tsc, cudaStream_t st) {
   if (w <= 0) return TT_OK;
   if (w > INV_MAX || w % 32 != 0) {
     set_error("unit-lower inverse of a block of " + std::to_string(w) + " rows (multiples of 32 up to " +
@@ -740,9 +753,10 @@ int inv_unit_lower(const T* A, int n, int r0, int w, T* X, cudaStream_t st) {
   for (int s = 64; s / 2 < w; s *= 2) {
     const int h = s / 2;
     dim3 grid(h / 32, h / 32, (w + s - 1) / s);
-    const int smem = h * 33 * (int)sizeof(T);
-    TT_TRY(smem_limit_once((const void*)k_inv_join<T>, smem));
-    k_inv_join<T><<<grid, 256, smem, st>>>(A, n, r0, w, s, X);
+    k_inv_join_t<T><<<grid, 256, 0, st>>>(A, n, r0, w, s, X, Tsc);
+    count_launch();
+    TT_CUDA_TRY(cudaGetLastError());
+    k_inv_join_x<T><<<grid, 256, 0, st>>>(w, s, X, Tsc);
     count_launch();
     TT_CUDA_TRY(cudaGetLastError());
   }
@@ -867,14 +881,18 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   // the tensor-core modes solve a block row with the explicit inverse of its
   // unit-lower block: X = L^{-1} once, then U = X A in one product
   const bool inv_solve = (mode == TC_TF32 || mode == TC_BF16X3);
-  DevBuf<T> Xinv;
-  if (inv_solve) TT_TRY(Xinv.alloc((size_t)std::min(NB, IVB) * std::min(NB, IVB)));
+  DevBuf<T> Xinv, Tinv;
+  if (inv_solve) {
+    const size_t wmax = (size_t)std::min(NB, IVB);
+    TT_TRY(Xinv.alloc(wmax * wmax));
+    TT_TRY(Tinv.alloc(wmax * wmax / 2));
+  }
   // rows [r0, r0 + h) of columns [cb, ce) <- L^{-1} of them, L the unit-lower h x h block at (r0, r0):
   // halves recursively, so that most of the work is one update of depth h / 2
   std::function<int(T*, int, int, int, int)> trsm_rec = [&](T* A, int r0, int h, int cb, int ce) -> int {
     if (h <= IB) return trsm_blk(A, n, r0, h, cb, ce, st);
     if (inv_solve && h % 32 == 0 && h <= IVB) {
-      TT_TRY(inv_unit_lower(A, n, r0, h, Xinv.ptr, st));
+      TT_TRY(inv_unit_lower(A, n, r0, h, Xinv.ptr, Tinv.ptr, st));
       return tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)r0 * n + cb, n,
                           reinterpret_cast<const float2*>(Xinv.ptr), h,
                           reinterpret_cast<const float2*>(A) + (size_t)r0 * n + cb, n, h, ce - cb, h, st, 1);

@@ -351,6 +351,7 @@ __global__ void k_onshell_pick(const double2* __restrict__ x, const double2* __r
 int resolvent_device(const DeviceLayout& L, const double* d_E, int nE, double* d_G, cudaStream_t st) {
   const size_t total = (size_t)L.n * nE;
   if (total == 0) return TT_OK;
+  ProfScope prof(TT_PROF_VECTOR, st, 0.0, 16.0 * (double)total);
   k_resolvent<<<ceil_div(total, 256), 256, 0, st>>>(L.Nalpha, L.Nq, L.Np, L.e_off.ptr, L.e_swp.ptr, L.q_WP.ptr, d_E,
                                                     nE, reinterpret_cast<double2*>(d_G));
   count_launch();
@@ -393,6 +394,7 @@ template int form_L_device<double2>(const double*, const double*, int, double2*,
 template int form_L_device<float2>(const double*, const double*, int, float2*, cudaStream_t);
 
 int gather_rhs_device(const double* d_A, int n, const int32_t* d_cols, int nrhs, double* d_b, cudaStream_t st) {
+  ProfScope prof(TT_PROF_VECTOR, st, 0.0, 24.0 * (double)n * nrhs);
   k_gather_rhs<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(d_A, n, d_cols, nrhs, reinterpret_cast<double2*>(d_b));
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
@@ -401,6 +403,7 @@ int gather_rhs_device(const double* d_A, int n, const int32_t* d_cols, int nrhs,
 
 int hadamard_device(const double* d_G, const int32_t* d_rhs_e, int n, const double* d_x, int nrhs, double* d_y,
                     cudaStream_t st) {
+  ProfScope prof(TT_PROF_VECTOR, st, 6.0 * (double)n * nrhs, 48.0 * (double)n * nrhs);
   k_hadamard<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_G), d_rhs_e, n,
                                                              reinterpret_cast<const double2*>(d_x), nrhs,
                                                              reinterpret_cast<double2*>(d_y));
@@ -451,6 +454,7 @@ int axpy_norms_device(double* d_x, const double* d_d, int n, int nrhs, double* h
   DevBuf<unsigned long long> mx;
   TT_TRY(mx.alloc(words));
   TT_CUDA_TRY(cudaMemsetAsync(mx.ptr, 0, sizeof(unsigned long long) * 2 * nrhs, st));
+  ProfScope prof(TT_PROF_VECTOR, st, 4.0 * (double)n * nrhs, 48.0 * (double)n * nrhs);
   k_axpy_norm<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<double2*>(d_x),
                                                               reinterpret_cast<const double2*>(d_d), n, nrhs, mx.ptr,
                                                               mx.ptr + nrhs);

@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = (
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
-                   "subst_prep", "simt_update", "tc_panel", "fp64_update")
+                   "subst_prep", "simt_update", "tc_panel", "fp64_update", "vector")
 
 
 class TicTacError(RuntimeError):
