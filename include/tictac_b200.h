@@ -260,7 +260,10 @@ unsigned long long tt_kernel_launches(void);
 #define TT_PROF_TC_PANEL 11
 /*   FP64_UPDATE C -= L U of the complex128 factorisation on the FP64 tensor cores (DMMA): 8 M N K flops */
 #define TT_PROF_FP64_UPDATE 12
-#define TT_PROF_COUNT 13
+/*   VECTOR      O(n k) kernels of the solve: resolvents, right-hand sides, G o x,
+ *               the refinement's axpy and norms (bytes read + written) */
+#define TT_PROF_VECTOR 13
+#define TT_PROF_COUNT 14
 typedef struct tt_kernel_profile {
   unsigned long long launches;
   double ms;
@@ -303,7 +306,7 @@ typedef struct tt_run tt_run;
 int tt_run_create(tt_run** run, int nopt, const char* const* opts);
 void tt_run_destroy(tt_run* run);
 /* Change one option of the linear solve (tc_product, panel_width, panel_order,
- * inverse_block, energy_batch, refine_tol, refine_max_iter) for the run's next solves; the
+ * inverse_block, cta_pairs, energy_batch, refine_tol, refine_max_iter) for the run's next solves; the
  * states, grids and built operators stay.  Other keys: TT_ERR_BADARG. */
 int tt_run_set_solve_option(tt_run* run, const char* key, const char* value);
 

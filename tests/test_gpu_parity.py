@@ -318,11 +318,15 @@ def test_panel_widths_agree(product):
     for c in range(run.num_channels):
         U64, _ = run.solve(c, tt.PRECISION_FP64)
         # panel widths, and the largest unit-lower block solved by its explicit inverse
-        for w, ib in ((32, 0), (96, 0), (256, 0), (512, 0), (512, 32), (512, 256), (512, 512)):
+        # and the updates on single CTAs or on CTA pairs (256-row tiles)
+        for w, ib, pairs in ((32, 0, 0), (96, 0, 0), (256, 0, 0), (512, 0, 0), (512, 32, 0), (512, 128, 0),
+                             (512, 0, 1), (256, 128, 1)):
             run.set_solve_option("panel_width", w)
             run.set_solve_option("inverse_block", ib)
+            run.set_solve_option("cta_pairs", "true" if pairs else "false")
             U, rep = run.solve(c, tt.PRECISION_MIXED)
-            assert rel_elem(U, U64) <= 1e-10, (c, w, ib, rep)
+            assert rel_elem(U, U64) <= 1e-10, (c, w, ib, pairs, rep)
         run.set_solve_option("panel_width", 0)
         run.set_solve_option("inverse_block", 0)
+        run.set_solve_option("cta_pairs", "false")
     run.close()

@@ -394,6 +394,271 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   }
 }
 
+// ---- CTA pairs (cta_group::2)
+//
+// Two CTAs of a cluster compute a 256 x 128 complex tile: each holds its 128
+// L rows (A) and one half of the 256 real B rows, the first CTA the re-rows and
+// the second the im-rows, and the first CTA issues one M = 256, N = 256 MMA per
+// k step that reads both halves of A and of B from the two shared memories; the
+// accumulator rows of each CTA land in its own TMEM (re in columns [0,128), im
+// in [128,256), as in the single-CTA kernel).  Per CTA a stage is a 128-row A
+// tile and 128 B rows, a third less operand traffic per flop than the single
+// CTA's 128 + 256 rows, and five stages fit instead of four.
+//
+// Barriers: both CTAs' copies of a stage complete on the first CTA's full[s]
+// (expect_tx of both CTAs' bytes there); the MMA's commit arrives on empty[s]
+// of both CTAs; acc_full is committed to both; each CTA's epilogue warps arrive
+// on the first CTA's acc_empty.  The copies are plain (no multicast) loads.
+template <int MODE>
+struct PairCfg {
+  static constexpr int A_TILE = Cfg<MODE>::A_TILE;            // 128 rows
+  static constexpr int B_CTA = Cfg<MODE>::B_TILE / 2;         // 128 of the 256 real B rows
+  static constexpr int PART = A_TILE + B_CTA;
+  static constexpr int STAGE = Cfg<MODE>::PARTS * PART;       // 32 KB
+  static constexpr int STAGES = 5;
+};
+
+template <int MODE>
+__host__ __device__ constexpr uint32_t idesc_pair() {
+  constexpr uint32_t ab = (MODE == TC_TF32) ? 2u : 1u;
+  return (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)((2 * BN) >> 3) << 17) | ((uint32_t)((2 * BM) >> 4) << 24);
+}
+
+template <int MODE>
+__device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  constexpr uint32_t id = idesc_pair<MODE>();
+  if constexpr (MODE == TC_TF32) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
+            tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(id), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z),
+        "r"(z));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
+            tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(id), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z),
+        "r"(z));
+  }
+}
+// commit of the pair's MMAs: one arrival on the barrier at this offset in both CTAs
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+  const uint16_t both = 3;
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::
+                   "r"(smem_u32(bar)),
+               "h"(both)
+               : "memory");
+}
+// shared::cluster address of this CTA's variable at `p` in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// 2D tile copy into this CTA's shared memory completing on an mbarrier of the
+// pair's first CTA (cluster address); not a multicast copy
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t cluster_bar, int x,
+                                                 int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(cluster_bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    k_lu_update_tc2_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                         float2* __restrict__ C, int ldc, int M, int N, int K, int a_plane, int store, int* err) {
+  using CF = Cfg<MODE>;
+  using PC = PairCfg<MODE>;
+  constexpr int STAGES_P = PC::STAGES;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float2* epi_stage = (float2*)(smem + STAGES_P * PC::STAGE);
+  uint64_t* full = (uint64_t*)(smem + STAGES_P * PC::STAGE + EPI_WARPS * EPI_STAGE_BYTES);
+  uint64_t* empty = full + STAGES_P;
+  uint64_t* acc_full = empty + STAGES_P;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* fin = acc_empty + 2;  // completion of every MMA the first CTA issued
+  uint32_t* tmem_base_slot = (uint32_t*)(fin + 1);
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  uint32_t rank;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const bool lead = rank == 0;
+  const int kchunks = K / KCC;
+  TileSched sched{(M + 2 * BM - 1) / (2 * BM), (N + BN - 1) / BN, 8};
+  const int ntiles = sched.tiles_m * sched.tiles_n;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES_P; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 2 * EPI_WARPS);  // one arrival per epilogue warp of both CTAs
+    }
+    mbar_init(fin, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_base_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  // both CTAs' barriers exist before either signals the other
+  tc_fence_before();
+  cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_base_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs)
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int t = pair; t < ntiles && ok; t += npairs) {
+        int tm, tn;
+        sched.coords(t, tm, tn);
+        for (int kc = 0; kc < kchunks && ok; kc++, it++) {
+          const int s = it % STAGES_P;
+          const uint32_t ph = (uint32_t)(it / STAGES_P) & 1u;
+          if (it >= STAGES_P && !mbar_wait(&empty[s], ph ^ 1u, err, 1)) {
+            ok = false;
+            break;
+          }
+          unsigned char* st = smem + s * PC::STAGE;
+          if (lead) mbar_expect_tx(&full[s], 2 * PC::STAGE);
+          const uint32_t bar = cluster_addr(&full[s], 0);
+          const int x = kc * 2 * KCC;
+#pragma unroll
+          for (int p = 0; p < CF::PARTS; p++) {
+            unsigned char* a = st + p * PC::PART;
+            tma_load_2d_pair(a, &tmA, bar, x, p * a_plane + tm * 2 * BM + (int)rank * BM);
+            tma_load_2d_pair(a + PC::A_TILE, &tmB, bar, x, p * 2 * N + (int)rank * N + tn * BN);
+          }
+        }
+      }
+      // the first CTA waits (bounded) until every issued copy of both CTAs has
+      // landed; the second is held by the closing cluster barrier meanwhile
+      if (lead)
+        for (int j = (it > STAGES_P ? it - STAGES_P : 0); j < it; j++)
+          mbar_wait(&full[j % STAGES_P], (uint32_t)(j / STAGES_P) & 1u, err, 5);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (first CTA only)
+    if (lead && lane == 0) {
+      const int ta[3] = {0, 0, 1};
+      const int tb[3] = {0, 1, 0};
+      int it = 0, local = 0;
+      bool ok = true;
+      for (int t = pair; t < ntiles && ok; t += npairs, local++) {
+        const int ab = local & 1;
+        const uint32_t aph = (uint32_t)(local >> 1) & 1u;
+        if (local >= 2 && !mbar_wait(&acc_empty[ab], aph ^ 1u, err, 2)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + ab * (2 * BN);
+        for (int kc = 0; kc < kchunks; kc++, it++) {
+          const int s = it % STAGES_P;
+          const uint32_t ph = (uint32_t)(it / STAGES_P) & 1u;
+          if (!mbar_wait(&full[s], ph, err, 3)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t s0 = smem_u32(smem + s * PC::STAGE);
+#pragma unroll
+          for (int ks = 0; ks < CF::KSTEPS; ks++) {
+#pragma unroll
+            for (int q = 0; q < CF::TERMS; q++) {
+              const uint32_t a0 = s0 + ta[q] * PC::PART;
+              const uint32_t b0 = s0 + tb[q] * PC::PART + PC::A_TILE;
+              umma_pair<MODE>(d, op_desc<MODE>(a0 + ks * 32), op_desc<MODE>(b0 + ks * 32),
+                              (kc == 0 && ks == 0 && q == 0) ? 0u : 1u);
+            }
+          }
+          umma_commit_pair(&empty[s]);
+        }
+        if (!ok) break;
+        umma_commit_pair(&acc_full[ab]);
+      }
+      // no MMA may still read the second CTA's shared memory when the pair
+      // leaves (also after an early exit)
+      umma_commit_pair(fin);
+      mbar_wait(fin, 0, err, 6);
+    }
+  } else {
+    // ---------------- epilogue (warps 2..9 of both CTAs): this CTA's 128 rows
+    const int quarter = warp & 3;
+    const int half = (warp - 2) >> 2;
+    float2* stage = epi_stage + (size_t)(warp - 2) * (32 * 16);
+    const uint32_t lead_acc_empty[2] = {cluster_addr(&acc_empty[0], 0), cluster_addr(&acc_empty[1], 0)};
+    int local = 0;
+    for (int t = pair; t < ntiles; t += npairs, local++) {
+      int tm, tn;
+      sched.coords(t, tm, tn);
+      const int ab = local & 1;
+      const uint32_t aph = (uint32_t)(local >> 1) & 1u;
+      const int row0 = tm * 2 * BM + (int)rank * BM + quarter * 32;
+      float2 cv[16];
+      if (!store) load_c_chunk(C, ldc, M, N, row0, tn * BN + half * (BN / 2), lane, cv);
+      if (!mbar_wait(&acc_full[ab], aph, err, 4)) break;
+      tc_fence_after();
+      const uint32_t lane_addr = tmem_base + ((uint32_t)(quarter * 32) << 16) + ab * (2 * BN);
+#pragma unroll 1
+      for (int cc = 0; cc < BN / 2; cc += 16) {
+        const int col = half * (BN / 2) + cc;
+        const int gcol0 = tn * BN + col;
+        if (cc > 0 && !store) load_c_chunk(C, ldc, M, N, row0, gcol0, lane, cv);
+        float re[16], im[16];
+        tmem_ld16(lane_addr + col, re);
+        tmem_ld16(lane_addr + BN + col, im);
+#pragma unroll
+        for (int j = 0; j < 16; j++) stage[lane * 16 + (j ^ (lane & 15))] = make_float2(re[j], im[j]);
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int idx = i * 32 + lane, r = idx >> 4, c = idx & 15;
+          const int grow = row0 + r, gcol = gcol0 + c;
+          const float2 a = stage[r * 16 + (c ^ (r & 15))];
+          if (grow < M && gcol < N)
+            C[(size_t)grow * ldc + gcol] = store ? a : make_float2(cv[i].x - a.x, cv[i].y - a.y);
+        }
+        __syncwarp();
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(lead_acc_empty[ab]);
+    }
+  }
+  __syncwarp();
+  // neither CTA leaves while the other may still read its shared memory or
+  // signal its barriers
+  tc_fence_before();
+  cluster_sync();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+  }
+}
+
 // ---- operand packing
 
 // L rows as [M][2K] reals.  TF32: one fp32 plane (used when the matrix itself
@@ -488,6 +753,15 @@ struct TC2Workspace {
   DevBuf<int> err;
 };
 
+// CTA-pair kernel for updates of more than 128 rows (tc2_set_pairs)
+thread_local bool g_tc2_pairs = false;
+
+int current_device_index() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+
 TC2Workspace& workspace2() {
   static thread_local TC2Workspace ws;
   return ws;
@@ -533,13 +807,42 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
                      tc2::BM));
   TT_TRY(make_map2(&mB, MODE, ws.WB.ptr, (uint64_t)CF::PARTS * 2 * N, (uint64_t)2 * K, (uint64_t)2 * K * esz,
                    tc2::BN));
-  const size_t smem = (size_t)tc2::STAGES * CF::STAGE + tc2::EPI_WARPS * tc2::EPI_STAGE_BYTES + 1024 + 128;
-  TT_TRY(smem_limit_once((const void*)tc2::k_lu_update_tc2<MODE>, (int)smem));
-  const int tiles = ((M + tc2::BM - 1) / tc2::BM) * ((N + tc2::BN - 1) / tc2::BN);
-  const int grid = std::min(tiles, device_sm_count());
-  {
-    ProfScope prof(K >= 256 ? TT_PROF_TC_UPDATE : TT_PROF_TC_PANEL, st, 8.0 * M * N * K,
-                   16.0 * M * N + 8.0 * ((double)M + N) * K);
+  ProfScope prof(K >= 256 ? TT_PROF_TC_UPDATE : TT_PROF_TC_PANEL, st, 8.0 * M * N * K,
+                 16.0 * M * N + 8.0 * ((double)M + N) * K);
+  if (g_tc2_pairs && M > tc2::BM) {
+    // CTA pairs on 256-row tiles, as many pairs as can be resident at once
+    using PC = tc2::PairCfg<MODE>;
+    const size_t smem = (size_t)PC::STAGES * PC::STAGE + tc2::EPI_WARPS * tc2::EPI_STAGE_BYTES + 1024 + 128;
+    const void* kfn = (const void*)tc2::k_lu_update_tc2_pair<MODE>;
+    TT_TRY(smem_limit_once(kfn, (int)smem));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(tc2::NUM_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    static int max_pairs[2][16] = {};
+    int& mp = max_pairs[MODE == TC_TF32 ? 0 : 1][current_device_index() & 15];
+    if (mp == 0) {
+      cfg.gridDim = dim3(2 * (device_sm_count() / 2));
+      int clusters = 0;
+      TT_CUDA_TRY(cudaOccupancyMaxActiveClusters(&clusters, kfn, &cfg));
+      mp = std::max(1, clusters);
+    }
+    const int tiles = ((M + 2 * tc2::BM - 1) / (2 * tc2::BM)) * ((N + tc2::BN - 1) / tc2::BN);
+    cfg.gridDim = dim3(2 * std::min(tiles, mp));
+    TT_CUDA_TRY(cudaLaunchKernelEx(&cfg, tc2::k_lu_update_tc2_pair<MODE>, mA, mB, C, ldc, M, N, K, M, store,
+                                   ws.err.ptr));
+  } else {
+    const size_t smem = (size_t)tc2::STAGES * CF::STAGE + tc2::EPI_WARPS * tc2::EPI_STAGE_BYTES + 1024 + 128;
+    TT_TRY(smem_limit_once((const void*)tc2::k_lu_update_tc2<MODE>, (int)smem));
+    const int tiles = ((M + tc2::BM - 1) / tc2::BM) * ((N + tc2::BN - 1) / tc2::BN);
+    const int grid = std::min(tiles, device_sm_count());
     tc2::k_lu_update_tc2<MODE><<<grid, tc2::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, M, store,
                                                                      ws.err.ptr);
   }
@@ -549,6 +852,8 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
 }
 
 }  // namespace
+
+void tc2_set_pairs(bool on) { g_tc2_pairs = on; }
 
 void* tc2_b_workspace(int mode, int N, int K, int* status) {
   TC2Workspace& ws = workspace2();

@@ -792,7 +792,7 @@ int panel_gemm_sub(int mode, T* C, int ldc, const T* L, int ldl, const T* U, int
 
 template <typename T>
 int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, cudaStream_t st, int use_tc,
-                             int* info, bool blocked_order, int panel, int inv_block) {
+                             int* info, bool blocked_order, int panel, int inv_block, bool cta_pairs) {
   const int mode = use_tc;
   const bool tc = mode != 0;
   if (mode < 0 || mode > TC_BF16X3) {
@@ -815,7 +815,12 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     set_error("inverse block " + std::to_string(inv_block) + " (a multiple of 32 up to 512)");
     return TT_ERR_BADARG;
   }
-  const int IVB = inv_block ? inv_block : 128;
+  const int IVB = inv_block ? inv_block : INV_MAX;
+  // the update kernel's tile shape for this factorisation (restored on return)
+  struct PairScope {
+    explicit PairScope(bool on) { tc2_set_pairs(on); }
+    ~PairScope() { tc2_set_pairs(false); }
+  } pair_scope(cta_pairs);
   const int NB = panel ? panel : (sizeof(T) == sizeof(float2)) ? 512 : 128;
   const int G = device_sm_count();
   DevBuf<double> sval;
@@ -1004,9 +1009,9 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   return TT_OK;
 }
 template int lu_factor_batched_device<double2>(double2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                               bool, int, int);
+                                               bool, int, int, bool);
 template int lu_factor_batched_device<float2>(float2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                              bool, int, int);
+                                              bool, int, int, bool);
 
 template <typename T>
 int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {

@@ -24,6 +24,9 @@ constexpr int TC_BF16X3 = 3;         // gemm_tc2.cu: real-row form, N = 256, BF1
 // prepacked: U's operand planes are already in the workspace (tc2_b_workspace).
 int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
                  cudaStream_t st, int store = 0, bool prepacked = false);
+// Updates of more than 128 rows on CTA pairs (cta_group::2, 256-row tiles) on
+// this host thread's next tc2_gemm_sub calls.
+void tc2_set_pairs(bool on);
 // The B-operand workspace of tc2_gemm_sub, grown to an N-column, K-deep operand.
 void* tc2_b_workspace(int mode, int N, int K, int* status);
 int tc2_check_error(cudaStream_t st);

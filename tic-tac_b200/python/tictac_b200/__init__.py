@@ -548,8 +548,8 @@ class Run:
         return dVu, dVc[:self.host_array(4).size]
 
     def set_solve_option(self, key, value):
-        """Change a solve option (tc_product, panel_width, panel_order, inverse_block, energy_batch, refine_tol,
-        refine_max_iter) for the next solves."""
+        """Change a solve option (tc_product, panel_width, panel_order, inverse_block, cta_pairs, energy_batch,
+        refine_tol, refine_max_iter) for the next solves."""
         _check(self.lib.tt_run_set_solve_option(self._h, str(key).encode(), str(value).encode()))
 
     def release(self, chn):
