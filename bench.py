@@ -254,6 +254,7 @@ def run_ours(args, world, rank, local, pg):
     cfg["panel_width"] = args.panel_width
     cfg["inverse_block"] = args.inverse_block
     cfg["cta_pairs"] = "true" if args.cta_pairs else "false"
+    cfg["mid_panel"] = args.mid_panel
     prec = tt.PRECISION_MIXED if args.precision == "mixed" else tt.PRECISION_FP64
     t_setup = time.perf_counter()
     run = tt.Run(**cfg)
@@ -535,7 +536,8 @@ def main():
     ap.add_argument("--panel-order", choices=["recursive", "blocked"], default="blocked",
                     help="LU panels by recursive halving or in 32-column steps")
     ap.add_argument("--panel-width", type=int, default=0, help="LU panel width (0: the library's table)")
-    ap.add_argument("--cta-pairs", type=int, default=0, help="tensor-core updates on CTA pairs (cta_group::2)")
+    ap.add_argument("--cta-pairs", type=int, default=1, help="tensor-core updates on CTA pairs (cta_group::2)")
+    ap.add_argument("--mid-panel", type=int, default=0, help="blocked panels in mid-panels of this many columns")
     ap.add_argument("--inverse-block", type=int, default=0,
                     help="largest unit-lower block solved through its explicit inverse (0: the library's default)")
     ap.add_argument("--breakdown", type=int, default=1,

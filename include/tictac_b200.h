@@ -306,8 +306,8 @@ typedef struct tt_run tt_run;
 int tt_run_create(tt_run** run, int nopt, const char* const* opts);
 void tt_run_destroy(tt_run* run);
 /* Change one option of the linear solve (tc_product, panel_width, panel_order,
- * inverse_block, cta_pairs, energy_batch, refine_tol, refine_max_iter) for the run's next solves; the
- * states, grids and built operators stay.  Other keys: TT_ERR_BADARG. */
+ * inverse_block, cta_pairs, mid_panel, energy_batch, refine_tol, refine_max_iter) for the run's next
+ * solves; the states, grids and built operators stay.  Other keys: TT_ERR_BADARG. */
 int tt_run_set_solve_option(tt_run* run, const char* key, const char* value);
 
 /* Counts and per-channel facts. */

@@ -131,6 +131,8 @@ def test_ragged_block_sizes_against_oracle(Np, Nq):
         rows = np.repeat(np.arange(len(rowptr) - 1, dtype=np.int32), np.diff(rowptr))
         G_o = np.stack([oracle.resolvent(lay, pw.shape[0], Nq, Np, run.host_array(2), e + run.E_bound) for e in E_com])
         A_o = oracle.build_A(lay, pw.shape[0], Nq, Np, rows, col, val)
+        run.build_A(c)  # odd Np: chunks of 7 (63 columns) or 5 (55) q' values, unaligned rows
+        assert rel(run.A(c), A_o) <= 1e-12, c
         U_o = oracle.dense_solve(A_o, G_o, q_idx, oracle.deuterons(pw), Nq, Np)
         for prec in PRECISIONS:
             U, rep = run.solve(c, prec)
@@ -319,14 +321,16 @@ def test_panel_widths_agree(product):
         U64, _ = run.solve(c, tt.PRECISION_FP64)
         # panel widths, and the largest unit-lower block solved by its explicit inverse
         # and the updates on single CTAs or on CTA pairs (256-row tiles)
-        for w, ib, pairs in ((32, 0, 0), (96, 0, 0), (256, 0, 0), (512, 0, 0), (512, 32, 0), (512, 128, 0),
-                             (512, 0, 1), (256, 128, 1)):
+        # and panels in mid-panels of 64 or 128 columns
+        for w, ib, pairs, mid in ((32, 0, 0, 0), (96, 0, 0, 0), (256, 0, 0, 0), (512, 0, 0, 0), (512, 32, 0, 0),
+                                  (512, 128, 0, 0), (512, 0, 1, 0), (256, 128, 1, 0), (512, 0, 0, 128),
+                                  (512, 0, 1, 128), (384, 0, 0, 64), (512, 32, 0, 96)):
             run.set_solve_option("panel_width", w)
             run.set_solve_option("inverse_block", ib)
             run.set_solve_option("cta_pairs", "true" if pairs else "false")
+            run.set_solve_option("mid_panel", mid)
             U, rep = run.solve(c, tt.PRECISION_MIXED)
-            assert rel_elem(U, U64) <= 1e-10, (c, w, ib, pairs, rep)
-        run.set_solve_option("panel_width", 0)
-        run.set_solve_option("inverse_block", 0)
-        run.set_solve_option("cta_pairs", "false")
+            assert rel_elem(U, U64) <= 1e-10, (c, w, ib, pairs, mid, rep)
+        for k, v in (("panel_width", 0), ("inverse_block", 0), ("cta_pairs", "false"), ("mid_panel", 0)):
+            run.set_solve_option(k, v)
     run.close()

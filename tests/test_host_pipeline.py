@@ -82,7 +82,8 @@ def test_solve_options_on_a_run():
             tt.Run(panel_width=v, **opts)
     run = tt.Run(**opts)
     for k, v in (("panel_width", 384), ("tc_product", "bf16x3"), ("panel_order", "recursive"), ("energy_batch", 2),
-                 ("refine_tol", 1e-11), ("refine_max_iter", 30), ("inverse_block", 256), ("cta_pairs", "true")):
+                 ("refine_tol", 1e-11), ("refine_max_iter", 30), ("inverse_block", 256), ("cta_pairs", "true"),
+                 ("mid_panel", 128)):
         run.set_solve_option(k, v)
     with pytest.raises(tt.TicTacError, match="panel_width"):
         run.set_solve_option("panel_width", 48)

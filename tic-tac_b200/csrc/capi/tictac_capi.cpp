@@ -116,6 +116,7 @@ SolveOptions options_of(const RunParams& rp, int precision) {
   o.panel_width = rp.panel_width;
   o.inverse_block = rp.inverse_block;
   o.cta_pairs = rp.cta_pairs;
+  o.mid_panel = rp.mid_panel;
   return o;
 }
 
@@ -406,7 +407,7 @@ int tt_release_cached_device_memory(void) {
 int tt_run_set_solve_option(tt_run* run, const char* key, const char* value) {
   if (!run || !key || !value) return fail(TT_ERR_BADARG, "null run, key or value");
   static const char* const kSolveKeys[] = {"tc_product", "panel_width", "panel_order", "energy_batch",
-                                           "refine_tol", "refine_max_iter", "inverse_block", "cta_pairs"};
+                                           "refine_tol", "refine_max_iter", "inverse_block", "cta_pairs", "mid_panel"};
   bool ok = false;
   for (const char* k : kSolveKeys) ok = ok || std::strcmp(k, key) == 0;
   if (!ok) return fail(TT_ERR_BADARG, std::string("not a solve option: ") + key);

@@ -67,11 +67,11 @@ struct AbLayout {
   }
 };
 
-// One CTA per (row block R = ar Nq + q, column partial wave ac).  MAXH >= Np / 4
-// (thread (g, c) of the contraction computes rows pr = g + 4 h of column c);
-// CAP nonzeros of every (T row, coupled aj) range are staged in shared memory
-// and refilled by the owning warp when a range runs past them.
-template <int MAXH, int CAP>
+// One CTA per (row block R = ar Nq + q, column partial wave ac).  MT = number
+// of 8-row tiles of Np (4 for Np <= 32, 8 for Np <= 64; the 64 chunk columns
+// are 8 tiles); CAP nonzeros of every (T row, coupled aj) range are staged in
+// shared memory and refilled by the owning warp when a range runs past them.
+template <int MT, int CAP>
 __global__ void __launch_bounds__(AB_THREADS, 2) k_abuild(int Na, int Nq, int Np, const int64_t* __restrict__ rowptr,
                                                        const int32_t* __restrict__ col,
                                                        const double* __restrict__ val,
@@ -137,7 +137,6 @@ __global__ void __launch_bounds__(AB_THREADS, 2) k_abuild(int Na, int Nq, int Np
   }
   const int bc = blk[ac], dimc = blk_dim[bc], part_c = part[ac];
   const double* VCb = VC + blk_off[bc];
-  const int g = tid >> 6, c = tid & 63;  // contraction: 4 row groups x 64 columns
   for (int q0 = 0; q0 < Nq; q0 += QW) {
     const int cw = min(QW, Nq - q0) * Np;  // columns of this chunk
     __syncthreads();
@@ -181,27 +180,41 @@ __global__ void __launch_bounds__(AB_THREADS, 2) k_abuild(int Na, int Nq, int Np
       }
     }
     __syncthreads();
-    // ---- A chunk: thread (g, c) computes rows pr = g + 4 h of column c
-    if (c < cw) {
-      double acc[MAXH];
+    // ---- A chunk on the FP64 tensor cores: (Np x RT) Ct times (RT x cw) T as
+    // 8 x 8 tiles (mma m8n8k4); warp w owns row tile w % MT and MT column tiles
+    {
+      const int gid = lane >> 2, tig = lane & 3;
+      const int mt = warp % MT, nt0 = (warp / MT) * MT;
+      const int row = mt * 8 + gid;
+      double acc[MT][2];
 #pragma unroll
-      for (int h = 0; h < MAXH; h++) acc[h] = 0.0;
-      for (int t = 0; t < ncr; t++) {
-        const double* Ct = sCt + t * Np * Np;
-        for (int pi = 0; pi < Np; pi++) {
-          const double tv = sT[(size_t)(t * Np + pi) * CW + c];
+      for (int j = 0; j < MT; j++) acc[j][0] = acc[j][1] = 0.0;
+      for (int k0 = 0; k0 < RT; k0 += 4) {
+        const int k = k0 + tig, t = k / Np, pi = k - t * Np;
+        const bool kin = k < RT;
+        const double a = (kin && row < Np) ? sCt[(t * Np + row) * Np + pi] : 0.0;
 #pragma unroll
-          for (int h = 0; h < MAXH; h++) {
-            const int pr = g + 4 * h;
-            if (4 * h < Np) acc[h] += Ct[min(pr, Np - 1) * Np + pi] * tv;
-          }
+        for (int j = 0; j < MT; j++) {
+          const int col = (nt0 + j) * 8 + gid;
+          const double b = (kin && col < CW) ? sT[(size_t)k * CW + col] : 0.0;
+          asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                       : "+d"(acc[j][0]), "+d"(acc[j][1])
+                       : "d"(a), "d"(b));
         }
       }
-      double* Acol = A + (size_t)R * Np * n + (size_t)(ac * Nq + q0) * Np + c;
+      if (row < Np) {
+        double* Arow = A + ((size_t)R * Np + row) * n + (size_t)(ac * Nq + q0) * Np;
 #pragma unroll
-      for (int h = 0; h < MAXH; h++) {
-        const int pr = g + 4 * h;
-        if (pr < Np) __stcs(Acol + (size_t)pr * n, acc[h]);
+        for (int j = 0; j < MT; j++) {
+          const int col = (nt0 + j) * 8 + 2 * tig;
+          double* p = Arow + col;
+          if (col + 1 < cw && ((uintptr_t)p & 15) == 0) {
+            __stcs(reinterpret_cast<double2*>(p), make_double2(acc[j][0], acc[j][1]));
+          } else {
+            if (col < cw) __stcs(p, acc[j][0]);
+            if (col + 1 < cw) __stcs(p + 1, acc[j][1]);
+          }
+        }
       }
     }
   }
@@ -233,14 +246,14 @@ int build_A_device(const DeviceLayout& L, const DeviceCSR& P, const int32_t* d_a
   dim3 grid(L.Nalpha * L.Nq, L.Nalpha);
   if (L.Np <= 32) {
     const size_t smem = AbLayout(L.Np, 32).bytes;
-    TT_TRY(smem_limit_once((const void*)k_abuild<8, 32>, (int)smem));
-    k_abuild<8, 32><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
+    TT_TRY(smem_limit_once((const void*)k_abuild<4, 32>, (int)smem));
+    k_abuild<4, 32><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
                                                     d_aoff, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
                                                     L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
   } else {
     const size_t smem = AbLayout(L.Np, 16).bytes;
-    TT_TRY(smem_limit_once((const void*)k_abuild<16, 16>, (int)smem));
-    k_abuild<16, 16><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
+    TT_TRY(smem_limit_once((const void*)k_abuild<8, 16>, (int)smem));
+    k_abuild<8, 16><<<grid, AB_THREADS, smem, st>>>(L.Nalpha, L.Nq, L.Np, P.rowptr.ptr, P.col.ptr, P.val.ptr,
                                                      d_aoff, L.blk.ptr, L.part.ptr, L.cpl_off.ptr, L.cpl.ptr,
                                                      L.blk_off.ptr, L.blk_dim.ptr, L.C.ptr, L.VC.ptr, d_A);
   }

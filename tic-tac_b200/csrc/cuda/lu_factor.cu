@@ -792,7 +792,7 @@ int panel_gemm_sub(int mode, T* C, int ldc, const T* L, int ldl, const T* U, int
 
 template <typename T>
 int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, cudaStream_t st, int use_tc,
-                             int* info, bool blocked_order, int panel, int inv_block, bool cta_pairs) {
+                             int* info, bool blocked_order, int panel, int inv_block, bool cta_pairs, int mid) {
   const int mode = use_tc;
   const bool tc = mode != 0;
   if (mode < 0 || mode > TC_BF16X3) {
@@ -809,6 +809,10 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   }
   if (panel < 0 || panel > INV_MAX || panel % IB != 0) {
     set_error("panel width " + std::to_string(panel) + " (a multiple of 32 up to 512)");
+    return TT_ERR_BADARG;
+  }
+  if (mid < 0 || mid % IB != 0) {
+    set_error("mid-panel width " + std::to_string(mid) + " (0 or a multiple of 32)");
     return TT_ERR_BADARG;
   }
   if (inv_block < 0 || inv_block > INV_MAX || inv_block % IB != 0) {
@@ -946,29 +950,43 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
       }
       continue;
     }
-    // ---- panel [k, k+kb) in sub-panels of IB columns
-    for (int j0 = k; j0 < k + kb; j0 += IB) {
-      const int w = std::min(IB, k + kb - j0);
-      TT_TRY(leaf(j0, w, k, k + kb));
-      for (int b = 0; b < B; b++) {
-        T* A = As[b];
-        const int right = k + kb - (j0 + w);
-        if (right > 0 && inv_solve && w % 16 == 0) {
-          // the solved block row is written straight into the update's operand planes
-          int ws = TT_OK;
-          void* WB = tc2_b_workspace(mode, right, w, &ws);
-          TT_TRY(ws);
-          TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st, mode, WB));
-          TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)(j0 + w) * n + (j0 + w), n,
-                              reinterpret_cast<const float2*>(A) + (size_t)(j0 + w) * n + j0, n,
-                              reinterpret_cast<const float2*>(A) + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right,
-                              w, st, 0, true));
-        } else if (right > 0) {
-          TT_TRY(trsm_blk(A, n, j0, w, j0 + w, k + kb, st));
-          TT_TRY(panel_gemm_sub(mode, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
-                                A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
+    // ---- panel [k, k+kb) in mid-panels of MB columns (MB = kb: one level),
+    // each in sub-panels of IB columns updated within the mid-panel, then the
+    // mid-panel's U block row and the update of the panel's columns right of it
+    const int MB = (mid > 0 && mid < kb) ? mid : kb;
+    for (int m0 = k; m0 < k + kb; m0 += MB) {
+      const int mw = std::min(MB, k + kb - m0);
+      for (int j0 = m0; j0 < m0 + mw; j0 += IB) {
+        const int w = std::min(IB, m0 + mw - j0);
+        TT_TRY(leaf(j0, w, k, k + kb));
+        for (int b = 0; b < B; b++) {
+          T* A = As[b];
+          const int right = m0 + mw - (j0 + w);
+          if (right > 0 && inv_solve && w % 16 == 0) {
+            // the solved block row is written straight into the update's operand planes
+            int ws = TT_OK;
+            void* WB = tc2_b_workspace(mode, right, w, &ws);
+            TT_TRY(ws);
+            TT_TRY(trsm_blk(A, n, j0, w, j0 + w, m0 + mw, st, mode, WB));
+            TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)(j0 + w) * n + (j0 + w), n,
+                                reinterpret_cast<const float2*>(A) + (size_t)(j0 + w) * n + j0, n,
+                                reinterpret_cast<const float2*>(A) + (size_t)j0 * n + (j0 + w), n, n - j0 - w,
+                                right, w, st, 0, true));
+          } else if (right > 0) {
+            TT_TRY(trsm_blk(A, n, j0, w, j0 + w, m0 + mw, st));
+            TT_TRY(panel_gemm_sub(mode, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
+                                  A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
+          }
         }
       }
+      const int right_out = k + kb - (m0 + mw);
+      if (right_out > 0)
+        for (int b = 0; b < B; b++) {
+          T* A = As[b];
+          TT_TRY(trsm_rec(A, m0, mw, m0 + mw, k + kb));
+          TT_TRY(panel_gemm_sub(mode, A + (size_t)(m0 + mw) * n + (m0 + mw), n, A + (size_t)(m0 + mw) * n + m0, n,
+                                A + (size_t)m0 * n + (m0 + mw), n, n - m0 - mw, right_out, mw, st));
+        }
     }
     for (int b = 0; b < B; b++) {
       T* A = As[b];
@@ -1009,9 +1027,9 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   return TT_OK;
 }
 template int lu_factor_batched_device<double2>(double2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                               bool, int, int, bool);
+                                               bool, int, int, bool, int);
 template int lu_factor_batched_device<float2>(float2* const*, int, int, int32_t* const*, cudaStream_t, int, int*,
-                                              bool, int, int, bool);
+                                              bool, int, int, bool, int);
 
 template <typename T>
 int lu_factor_device(T* A, int n, int32_t* ipiv, cudaStream_t st, int use_tc, int* info) {

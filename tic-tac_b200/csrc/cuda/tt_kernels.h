@@ -87,11 +87,14 @@ int lu_factor_device(T* d_L, int n, int32_t* d_ipiv, cudaStream_t st, int use_te
 // row is solved through the explicit inverses of unit-lower diagonal blocks of
 // at most this many rows (a multiple of 32 up to 512; 0 = 512), larger blocks
 // by halving with tensor-core updates between the halves.  cta_pairs: the
-// tensor-core updates run on CTA pairs (256-row tiles, cta_group::2).
+// tensor-core updates run on CTA pairs (256-row tiles, cta_group::2).  mid: the
+// blocked panel in mid-panels of this many columns (a multiple of 32; 0 = one
+// level): sub-panel updates stay inside the mid-panel and the rest of the
+// panel is updated once per mid-panel, with depth mid.
 template <typename T>
 int lu_factor_batched_device(T* const* d_L, int B, int n, int32_t* const* d_ipiv, cudaStream_t st,
                              int use_tensor_cores, int* info, bool blocked = false, int panel = 0,
-                             int inv_block = 0, bool cta_pairs = false);
+                             int inv_block = 0, bool cta_pairs = false, int mid = 0);
 // Row permutation of the interchange sequence ipiv (host, once per factorisation).
 int lu_permutation(const int32_t* d_ipiv, int n, std::vector<int32_t>& perm, cudaStream_t st);
 // Inverted diagonal blocks of one LU factor (unit lower and upper) and their

@@ -574,7 +574,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       t0 = std::chrono::steady_clock::now();
       TT_TRY(lu_factor_batched_device<float2>(Ls, nb, n, ps, st, product, info, opt.panel_blocked,
                                               opt.panel_width ? opt.panel_width : tuned_panel_width(n, product),
-                                              opt.inverse_block, opt.cta_pairs));
+                                              opt.inverse_block, opt.cta_pairs, opt.mid_panel));
       r.ms_factor += ms_since(t0);
     } else {
       TT_TRY(form_L_device<double2>(A_.ptr, G_.ptr + (size_t)2 * n * g0, n, L64.ptr, st));

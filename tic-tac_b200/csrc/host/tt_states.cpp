@@ -66,6 +66,9 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       rp.inverse_block = std::stoi(value);
       if (rp.inverse_block < 0 || rp.inverse_block > 512 || rp.inverse_block % 32)
         return bad("inverse_block (0 or 32..512)");
+    } else if (key == "mid_panel") {
+      rp.mid_panel = std::stoi(value);
+      if (rp.mid_panel < 0 || rp.mid_panel > 512 || rp.mid_panel % 32) return bad("mid_panel (0 or 32..512)");
     } else if (key == "cta_pairs") {
       if (!parse_bool(value, rp.cta_pairs)) return bad("cta_pairs (true or false)");
     } else if (key == "panel_order") {
