@@ -267,7 +267,16 @@ def run_ours(args, world, rank, local, pg):
     plans = shard.plan([infos_all[c]["n"] for c in all_chans], nE, world, group=group)
     mine = {all_chans[i]: js for i, js in plans[rank].items()}
     infos = [infos_all[c] for c in all_chans]
-    nnz = {c: run.build_P123(c) for c in mine}  # resident for the whole run
+    # P123 of this rank's channels, built once on the device and resident for the
+    # whole run (setup, not part of a step): device time per channel
+    nnz, p123_ms = {}, {}
+    for c in mine:
+        run.timer_start()
+        nnz[c] = run.build_P123(c)
+        p123_ms[c] = run.timer_stop()
+    p123_stage = {"ms_total": round(sum(p123_ms.values()), 1), "nnz_total": int(sum(nnz.values())),
+                  "per_channel": {str(c): {"n": infos_all[c]["n"], "nnz": int(nnz[c]), "ms": round(p123_ms[c], 1)}
+                                  for c in mine}}
     t_setup = time.perf_counter() - t_setup
 
     phases = {}  # per channel: the solve report's phase times of the latest step
@@ -439,7 +448,7 @@ def run_ours(args, world, rank, local, pg):
         run.release_A(c)
     return dict(value=value, ms_step=ms_step, clocks=clk.summary(), roofline=roofline, kernels=kernels, e2e=e2e,
                 infos=infos, nE=nE, nnz=nnz, t_setup=t_setup, times=times, launches=launches, fp64=fp64,
-                lab=lab, plan=plans, U_all=U_all, step_phases=step_phases)
+                lab=lab, plan=plans, U_all=U_all, step_phases=step_phases, p123=p123_stage)
 
 
 # Np = Nq of the reference's timed sample: channel 0 of the workload's basis at
@@ -537,7 +546,8 @@ def main():
                     help="LU panels by recursive halving or in 32-column steps")
     ap.add_argument("--panel-width", type=int, default=0, help="LU panel width (0: the library's table)")
     ap.add_argument("--cta-pairs", type=int, default=1, help="tensor-core updates on CTA pairs (cta_group::2)")
-    ap.add_argument("--mid-panel", type=int, default=0, help="blocked panels in mid-panels of this many columns")
+    ap.add_argument("--mid-panel", type=int, default=128,
+                    help="blocked panels in mid-panels of this many columns (0: one level)")
     ap.add_argument("--inverse-block", type=int, default=0,
                     help="largest unit-lower block solved through its explicit inverse (0: the library's default)")
     ap.add_argument("--breakdown", type=int, default=1,
@@ -636,6 +646,7 @@ def main():
                "channel_solves_per_s": round(len(r["infos"]) * r["nE"] / (r["ms_step"] * 1e-3), 4),
                "kernels": r["kernels"], "fp64_comparison": fp, "setup_s": round(r["t_setup"], 3),
                "timed_steps_ms": [round(t, 1) for t in r["times"]],
+               "p123_build": r["p123"],
                "last_timed_step_phases_ms": r["step_phases"],
                "U_gathered": {"channels": len(r["U_all"]), "energies": r["nE"],
                               "layout": "U[d' nd nE + d nE + j] per channel on rank 0"}}

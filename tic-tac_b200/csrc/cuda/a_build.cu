@@ -136,6 +136,7 @@ __global__ void __launch_bounds__(AB_THREADS, 2) k_abuild(int Na, int Nq, int Np
     sVal[i] = in ? val[e] : 0.0;
   }
   const int bc = blk[ac], dimc = blk_dim[bc], part_c = part[ac];
+  const float rNp = 1.0f / (float)Np, hNp = 0.5f / (float)Np;
   const double* VCb = VC + blk_off[bc];
   for (int q0 = 0; q0 < Nq; q0 += QW) {
     const int cw = min(QW, Nq - q0) * Np;  // columns of this chunk
@@ -148,6 +149,7 @@ __global__ void __launch_bounds__(AB_THREADS, 2) k_abuild(int Na, int Nq, int Np
       for (int t2 = 0; t2 < ncc; t2++) {
         const int pr2 = rr * 2 + t2;
         const int aj = cpl[cc0 + t2], part_j = part[aj];
+        const double* VCj = VCb + (size_t)part_j * Np * dimc + part_c * Np;  // row pj of VC(aj -> ac): + pj dimc
         const int32_t lim = aj * NqNp + min(q0 + QW, Nq) * Np;  // first column past the chunk
         const int32_t cbase = aj * NqNp + q0 * Np;
         const int64_t e_end = sEnd[pr2];
@@ -168,8 +170,10 @@ __global__ void __launch_bounds__(AB_THREADS, 2) k_abuild(int Na, int Nq, int Np
           const int32_t cj = sCol[pr2 * CAP + (int)(e - eb)];
           if (cj >= lim) break;
           const double v = 2.0 * sVal[pr2 * CAP + (int)(e - eb)];
-          const int rel = cj - cbase, qq = rel / Np, pj = rel % Np;
-          const double* vrow = VCb + (size_t)(part_j * Np + pj) * dimc + part_c * Np;
+          // rel / Np by a float reciprocal: rel < QW Np <= 64 + Np, so the
+          // product's error (< 2^-17) is far below the 0.5 / Np margin
+          const int rel = cj - cbase, qq = (int)((float)rel * rNp + hNp), pj = rel - qq * Np;
+          const double* vrow = VCj + (size_t)pj * dimc;
           for (int pc = lane; pc < Np; pc += 32) Trow[qq * Np + pc] += v * vrow[pc];
           e++;
         }

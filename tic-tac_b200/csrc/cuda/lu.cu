@@ -257,10 +257,26 @@ __device__ __forceinline__ C butterfly16(C (&acc)[16], int lane) {
   return acc[0] + __shfl_xor_sync(0xffffffffu, acc[0], 1);
 }
 
+// Up to kMaxSweeps factors swept in one cooperative launch: the grid splits
+// into B equal groups, each with its own lead CTA and owners, sharing every
+// grid barrier.
+constexpr int kMaxSweeps = 4;
+template <typename T>
+struct TrsvBatch {
+  const T* LU[kMaxSweeps];
+  const T* inv[kMaxSweeps];
+  const T* Mp[kMaxSweeps];
+  double2* x[kMaxSweeps];
+  int B;
+};
+
 template <typename T, bool UPPER>
-__global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(const T* __restrict__ LU, const T* __restrict__ inv,
-                                                         const T* __restrict__ Mp, int n, double2* __restrict__ x,
-                                                         int kn, int own_max) {
+__global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(TrsvBatch<T> bt, int n, int kn, int own_max) {
+  const int Gb = gridDim.x / bt.B, grp = blockIdx.x / Gb, local = blockIdx.x - grp * Gb;
+  const T* __restrict__ LU = bt.LU[grp];
+  const T* __restrict__ inv = bt.inv[grp];
+  const T* __restrict__ Mp = bt.Mp[grp];
+  double2* __restrict__ x = bt.x[grp];
   using C = typename CT<T>::R;
   constexpr int TILE = TSB * TLD;
   cg::grid_group grid = cg::this_grid();
@@ -272,8 +288,8 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(const T* __restrict__ 
   __shared__ T bsh[RHS][TSB];  // CTA 0: published rows of the block being solved
   __shared__ T ysh[RHS][TSB];  // CTA 0: its solution
   const int nb = (n + TSB - 1) / TSB;
-  const int G = gridDim.x;  // >= 2
-  const bool lead = blockIdx.x == 0;
+  const int G = Gb;  // this factor's CTAs, >= 2
+  const bool lead = local == 0;
   auto blk = [&](int q) { return UPPER ? nb - 1 - q : q; };
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   auto ld_x = [&](int k, int r) -> T {
@@ -317,7 +333,7 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) k_trsv(const T* __restrict__ 
   };
 
   // owners: slots j of block q = 2 + me + j (G-1)
-  const int me = (int)blockIdx.x - 1;
+  const int me = local - 1;
   auto first_slot = [&](int s) { return s > me ? (s - me + (G - 1) - 1) / (G - 1) : 0; };
   auto live = [&](int j) { return j < own_max && 2 + me + j * (G - 1) < nb; };
 
@@ -498,19 +514,31 @@ int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st, b
 template int lu_trsv_prepare<double2>(const double2*, int, TrsvBlocks<double2>&, cudaStream_t, bool);
 template int lu_trsv_prepare<float2>(const float2*, int, TrsvBlocks<float2>&, cudaStream_t, bool);
 
-// forward then backward substitution sweep over x [k][n] in place
+// forward then backward substitution sweeps over x_b [k][n] in place for the
+// B factors of a batch (one cooperative launch per sweep for all of them)
 template <typename T>
-int trsv_sweeps(const T* d_LU, int n, const TrsvBlocks<T>& blk, double2* x, int nrhs, cudaStream_t st) {
-  if (blk.n != n || !blk.invL.ptr) {
-    set_error("triangular solve called without the inverted diagonal blocks of this factor");
+int trsv_sweeps_batched(int B, const T* const* d_LU, int n, const TrsvBlocks<T>* const* blk, double2* const* x,
+                        int nrhs, cudaStream_t st) {
+  if (B < 1 || B > kMaxSweeps) {
+    set_error("substitution batch of " + std::to_string(B) + " factors (1.." + std::to_string(kMaxSweeps) + ")");
     return TT_ERR_BADARG;
   }
-  const int G = std::max(2, device_sm_count());
+  for (int b = 0; b < B; b++)
+    if (blk[b]->n != n || !blk[b]->invL.ptr) {
+      set_error("triangular solve called without the inverted diagonal blocks of this factor");
+      return TT_ERR_BADARG;
+    }
+  const int Gb = std::max(2, device_sm_count() / B);
   const int nb = (n + TSB - 1) / TSB;
-  int own_max = std::max(1, (nb - 2 + (G - 1) - 1) / (G - 1));
+  int own_max = std::max(1, (nb - 2 + (Gb - 1) - 1) / (Gb - 1));
   const size_t smem = (size_t)2 * TSB * TLD * sizeof(T) + (size_t)own_max * RHS * TSB * sizeof(T);
   constexpr size_t kMaxSmem = 212 * 1024;  // + up to 12 KB static, within the 227 KB per CTA
   if (smem > kMaxSmem) {
+    if (B > 1) {
+      // fewer owners per factor would not hold their rows: one factor at a time
+      for (int b = 0; b < B; b++) TT_TRY(trsv_sweeps_batched<T>(1, d_LU + b, n, blk + b, x + b, nrhs, st));
+      return TT_OK;
+    }
     set_error("triangular solve: n = " + std::to_string(n) + " needs " + std::to_string(smem) +
               " bytes of shared memory per CTA (limit " + std::to_string(kMaxSmem) + ")");
     return TT_ERR_UNSUPPORTED;
@@ -519,22 +547,54 @@ int trsv_sweeps(const T* d_LU, int n, const TrsvBlocks<T>& blk, double2* x, int 
   TT_TRY(smem_limit_once((const void*)k_trsv<T, true>, (int)kMaxSmem));
   for (int k0 = 0; k0 < nrhs; k0 += RHS) {
     int kn = std::min(RHS, nrhs - k0);
-    double2* xk = x + (size_t)k0 * n;
-    const T* LUp = d_LU;
+    TrsvBatch<T> bl{}, bu{};
+    bl.B = bu.B = B;
+    for (int b = 0; b < B; b++) {
+      bl.LU[b] = bu.LU[b] = d_LU[b];
+      bl.inv[b] = blk[b]->invL.ptr;
+      bu.inv[b] = blk[b]->invU.ptr;
+      bl.Mp[b] = blk[b]->mL.ptr;
+      bu.Mp[b] = blk[b]->mU.ptr;
+      bl.x[b] = bu.x[b] = x[b] + (size_t)k0 * n;
+    }
     int nn = n;
-    const T* invL = blk.invL.ptr;
-    const T* invU = blk.invU.ptr;
-    const T* mL = blk.mL.ptr;
-    const T* mU = blk.mU.ptr;
-    void* argsL[] = {&LUp, &invL, &mL, &nn, &xk, &kn, &own_max};
-    TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trsv<T, false>, dim3(G), dim3(TRSV_THREADS), argsL, smem, st));
+    void* argsL[] = {&bl, &nn, &kn, &own_max};
+    TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trsv<T, false>, dim3(Gb * B), dim3(TRSV_THREADS), argsL, smem,
+                                            st));
     count_launch();
-    void* argsU[] = {&LUp, &invU, &mU, &nn, &xk, &kn, &own_max};
-    TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trsv<T, true>, dim3(G), dim3(TRSV_THREADS), argsU, smem, st));
+    void* argsU[] = {&bu, &nn, &kn, &own_max};
+    TT_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_trsv<T, true>, dim3(Gb * B), dim3(TRSV_THREADS), argsU, smem,
+                                            st));
     count_launch();
   }
   return TT_OK;
 }
+
+template <typename T>
+int trsv_sweeps(const T* d_LU, int n, const TrsvBlocks<T>& blk, double2* x, int nrhs, cudaStream_t st) {
+  const TrsvBlocks<T>* pb = &blk;
+  return trsv_sweeps_batched<T>(1, &d_LU, n, &pb, &x, nrhs, st);
+}
+
+template <typename T>
+int lu_solve_batched_device(int B, const T* const* d_LU, int n, const TrsvBlocks<T>* const* blk,
+                            const int32_t* const* d_perm, double* const* d_x, double* d_tmp, int nrhs,
+                            cudaStream_t st) {
+  if (n <= 0 || nrhs <= 0 || B <= 0) return TT_OK;
+  ProfScope prof(TT_PROF_TRSV, st, 8.0 * n * (double)n * nrhs * B, (double)n * n * sizeof(T) * B);
+  double2* xs[kMaxSweeps];
+  for (int b = 0; b < B; b++) {
+    TT_CUDA_TRY(cudaMemcpyAsync(d_tmp, d_x[b], sizeof(double2) * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, st));
+    xs[b] = reinterpret_cast<double2*>(d_x[b]);
+    k_permute<<<ceil_div((size_t)n * nrhs, 256), 256, 0, st>>>(reinterpret_cast<const double2*>(d_tmp), d_perm[b],
+                                                              n, nrhs, xs[b]);
+    count_launch();
+    TT_CUDA_TRY(cudaGetLastError());
+  }
+  return trsv_sweeps_batched<T>(B, d_LU, n, blk, xs, nrhs, st);
+}
+template int lu_solve_batched_device<float2>(int, const float2* const*, int, const TrsvBlocks<float2>* const*,
+                                             const int32_t* const*, double* const*, double*, int, cudaStream_t);
 
 template <typename T>
 int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_t* d_perm, double* d_x,

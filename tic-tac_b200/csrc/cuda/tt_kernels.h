@@ -115,6 +115,12 @@ int lu_trsv_prepare(const T* d_LU, int n, TrsvBlocks<T>& blk, cudaStream_t st, b
 template <typename T>
 int lu_solve_device(const T* d_LU, int n, const TrsvBlocks<T>& blk, const int32_t* d_perm, double* d_x,
                     double* d_tmp, int nrhs, cudaStream_t st);
+// The same for B <= 4 factors of order n at once (their substitution sweeps
+// share each cooperative launch and grid barrier): x_b with factor b.
+template <typename T>
+int lu_solve_batched_device(int B, const T* const* d_LU, int n, const TrsvBlocks<T>* const* blk,
+                            const int32_t* const* d_perm, double* const* d_x, double* d_tmp, int nrhs,
+                            cudaStream_t st);
 
 // Solve (P^T L U)^T x = b, i.e. transposed systems of the same factor, for
 // nrhs complex128 columns [k][n] in place: d_LUt is the transpose of the

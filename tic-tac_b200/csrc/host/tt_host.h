@@ -62,7 +62,7 @@ struct RunParams {
   int panel_width = 0;         // complex64 LU panel width, 0 = the tuning table's choice
   int inverse_block = 0;       // explicit unit-lower inverses up to this many rows, 0 = 512
   bool cta_pairs = true;       // tensor-core updates on CTA pairs
-  int mid_panel = 0;           // blocked panels in mid-panels of this many columns, 0 = one level
+  int mid_panel = 128;         // blocked panels in mid-panels of this many columns, 0 = one level
   bool adjoint_total = true;   // run-handle adjoint: total derivative (basis and resolvent move with V)
   std::vector<double> lab_energies; // set directly or read from energy_input_file
   // additive offsets to the potential's low-energy constants, in the model's

@@ -609,18 +609,34 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
     t0 = std::chrono::steady_clock::now();
     TT_TRY(gather_rhs_device(A_.ptr, n, cols.ptr, nb * nd, b.ptr, st));
     TT_CUDA_TRY(cudaMemcpyAsync(x.ptr, b.ptr, sizeof(double) * vec * nb, cudaMemcpyDeviceToDevice, st));
+    // the group's complex64 factors solved together (one sweep launch for all)
+    auto solve_group = [&](const std::vector<int>& qs, double* v) -> int {
+      const float2* F[4];
+      const TrsvBlocks<float2>* TB[4];
+      const int32_t* PD[4];
+      double* X[4];
+      for (size_t i = 0; i < qs.size(); i++) {
+        F[i] = factor_of(qs[i]);
+        TB[i] = &tb32[qs[i]];
+        PD[i] = perm_d[qs[i]].ptr;
+        X[i] = v + vec * qs[i];
+      }
+      return lu_solve_batched_device<float2>((int)qs.size(), F, n, TB, PD, X, tmp.ptr, nd, st);
+    };
+    std::vector<int> all_q;
     for (int q = 0; q < nb; q++) {
       std::vector<int32_t> perm;
       TT_TRY(lu_permutation(ipiv_all.ptr + (size_t)q * n, n, perm, st));
       TT_TRY(perm_d[q].upload(perm, st));
       if (opt.mixed) {
         TT_TRY(lu_trsv_prepare<float2>(factor_of(q), n, tb32[q], st));
-        TT_TRY(lu_solve_device<float2>(factor_of(q), n, tb32[q], perm_d[q].ptr, x.ptr + vec * q, tmp.ptr, nd, st));
+        all_q.push_back(q);
       } else {
         TT_TRY(lu_trsv_prepare<double2>(L64.ptr, n, tb64, st));
         TT_TRY(lu_solve_device<double2>(L64.ptr, n, tb64, perm_d[q].ptr, x.ptr + vec * q, tmp.ptr, nd, st));
       }
     }
+    if (opt.mixed) TT_TRY(solve_group(all_q, x.ptr));
     TT_CUDA_TRY(cudaStreamSynchronize(st));
     r.ms_solve += ms_since(t0);
     if (opt.mixed) {
@@ -644,10 +660,12 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       for (int it = 1; it <= max_it && left > 0; it++) {
         TT_TRY(hadamard_device(Gg, rhs_e.ptr, n, x.ptr, nb * nd, y.ptr, st));
         TT_TRY(residual_multi_device(A_.ptr, n, y.ptr, b.ptr, x.ptr, nb * nd, res.ptr, st));
+        std::vector<int> active;
+        for (int q = 0; q < nb; q++)
+          if (!done[q]) active.push_back(q);
+        TT_TRY(solve_group(active, res.ptr));
         for (int q = 0; q < nb; q++) {
           if (done[q]) continue;
-          TT_TRY(lu_solve_device<float2>(factor_of(q), n, tb32[q], perm_d[q].ptr, res.ptr + vec * q, tmp.ptr, nd,
-                                         st));
           TT_TRY(axpy_norms_device(x.ptr + vec * q, res.ptr + vec * q, n, nd, ratio.data(), st,
                                    cols.ptr + (size_t)q * nd, nd, ratio.data() + nd));
           worst[q] = refine_error_estimate(ratio, prev[q], it > 1);

@@ -34,7 +34,7 @@ struct SolveOptions {
   int panel_width = 0;        // complex64 LU panel width (0: the tuning table's choice for n, else 512)
   int inverse_block = 0;      // unit-lower blocks solved by explicit inverse up to this size (0: 512)
   bool cta_pairs = true;      // tensor-core updates on CTA pairs (cta_group::2, 256-row tiles)
-  int mid_panel = 0;          // blocked panels in mid-panels of this many columns (0: one level)
+  int mid_panel = 128;        // blocked panels in mid-panels of this many columns (0: one level)
   int tc_product = 2;        // product mode of the tensor-core updates: 1 BF16x3 with N = 128 tiles,
                              // 2 TF32 (a group whose refinement does not converge is factored
                              // again with 3), 3 BF16x3 (real-row form, N = 256)
