@@ -458,10 +458,20 @@ __device__ __forceinline__ void cfma_add(T& acc, T a, T b) {
   acc.y += a.x * b.y + a.y * b.x;
 }
 
+// Matrices whose unit-lower blocks are inverted in the same launches: block
+// (blockIdx.y for the diagonal blocks, blockIdx.z / pairs for the joins)
+// picks matrix b, whose inverse is X + b w w and join scratch T + b w w / 2.
 template <typename T>
-__global__ void __launch_bounds__(256) k_inv_diag32(const T* __restrict__ A, int n, int r0, int w, T* __restrict__ X) {
+struct InvBatch {
+  const T* A[4];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv_diag32(InvBatch<T> ib, int n, int r0, int w, T* __restrict__ X) {
   __shared__ T sL[32][33];
   __shared__ T sX[32][33];
+  const T* __restrict__ A = ib.A[blockIdx.y];
+  X += (size_t)blockIdx.y * w * w;
   const int i0 = blockIdx.x * 32, hi = min(32, w - i0);
   for (int t = threadIdx.x; t < 32 * 32; t += 256) {
     const int i = t >> 5, j = t & 31;
@@ -502,12 +512,16 @@ __global__ void __launch_bounds__(256) k_inv_diag32(const T* __restrict__ A, int
 //   k_inv_join_x:  X21 = -X22 Tp         (X22 lower: m up to the tile's row)
 // Tp is the pair's h x h scratch at T + p h h.
 template <typename T>
-__global__ void __launch_bounds__(256) k_inv_join_t(const T* __restrict__ A, int n, int r0, int w, int s,
+__global__ void __launch_bounds__(256) k_inv_join_t(InvBatch<T> ib, int n, int r0, int w, int s,
                                                     const T* __restrict__ X, T* __restrict__ Tsc) {
   __shared__ T sa[32][33];
   __shared__ T sb[32][33];
   const int h = s / 2;
-  const int p = blockIdx.z, base = p * s;
+  const int pairs = (w + s - 1) / s, mb = blockIdx.z / pairs;
+  const int p = blockIdx.z - mb * pairs, base = p * s;
+  const T* __restrict__ A = ib.A[mb];
+  X += (size_t)mb * w * w;
+  Tsc += (size_t)mb * w * w / 2;
   const int h2 = min(h, w - base - h);  // rows of the second block
   const int ty = blockIdx.y, tx = blockIdx.x;
   if (h2 <= 0 || ty * 32 >= h2) return;
@@ -546,7 +560,10 @@ __global__ void __launch_bounds__(256) k_inv_join_x(int w, int s, T* __restrict_
   __shared__ T sa[32][33];
   __shared__ T sb[32][33];
   const int h = s / 2;
-  const int p = blockIdx.z, base = p * s;
+  const int pairs = (w + s - 1) / s, mb = blockIdx.z / pairs;
+  const int p = blockIdx.z - mb * pairs, base = p * s;
+  X += (size_t)mb * w * w;
+  Tsc += (size_t)mb * w * w / 2;
   const int h2 = min(h, w - base - h);
   const int ty = blockIdx.y, tx = blockIdx.x;
   if (h2 <= 0 || ty * 32 >= h2) return;
@@ -737,23 +754,26 @@ int laswp2(T* A, int n, const int32_t* ipiv, int p0, int p1, int a0, int a1, int
   return TT_OK;
 }
 
-// Tsc: scratch of at least w * w / 2 elements
+// X: B w w elements (inverse of matrix b at X + b w w, ld w); Tsc: scratch of
+// at least B w w / 2 elements.  B <= 4.
 template <typename T>
-int inv_unit_lower(const T* A, int n, int r0, int w, T* X, T* Tsc, cudaStream_t st) {
+int inv_unit_lower(const T* const* As, int B, int n, int r0, int w, T* X, T* Tsc, cudaStream_t st) {
   if (w <= 0) return TT_OK;
+  InvBatch<T> ib{};
+  for (int b = 0; b < B; b++) ib.A[b] = As[b];
   if (w > INV_MAX || w % 32 != 0) {
     set_error("unit-lower inverse of a block of " + std::to_string(w) + " rows (multiples of 32 up to " +
               std::to_string(INV_MAX) + ")");
     return TT_ERR_BADARG;
   }
-  ProfScope prof(TT_PROF_PANEL_TRSM, st, 8.0 / 6.0 * w * (double)w * w, 2.0 * w * (double)w * sizeof(T));
-  k_inv_diag32<T><<<w / 32, 256, 0, st>>>(A, n, r0, w, X);
+  ProfScope prof(TT_PROF_PANEL_TRSM, st, 8.0 / 6.0 * w * (double)w * w * B, 2.0 * w * (double)w * sizeof(T) * B);
+  k_inv_diag32<T><<<dim3(w / 32, B), 256, 0, st>>>(ib, n, r0, w, X);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   for (int s = 64; s / 2 < w; s *= 2) {
     const int h = s / 2;
-    dim3 grid(h / 32, h / 32, (w + s - 1) / s);
-    k_inv_join_t<T><<<grid, 256, 0, st>>>(A, n, r0, w, s, X, Tsc);
+    dim3 grid(h / 32, h / 32, ((w + s - 1) / s) * B);
+    k_inv_join_t<T><<<grid, 256, 0, st>>>(ib, n, r0, w, s, X, Tsc);
     count_launch();
     TT_CUDA_TRY(cudaGetLastError());
     k_inv_join_x<T><<<grid, 256, 0, st>>>(w, s, X, Tsc);
@@ -893,15 +913,16 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
   DevBuf<T> Xinv, Tinv;
   if (inv_solve) {
     const size_t wmax = (size_t)std::min(NB, IVB);
-    TT_TRY(Xinv.alloc(wmax * wmax));
-    TT_TRY(Tinv.alloc(wmax * wmax / 2));
+    TT_TRY(Xinv.alloc(wmax * wmax * B));
+    TT_TRY(Tinv.alloc(wmax * wmax * B / 2));
   }
   // rows [r0, r0 + h) of columns [cb, ce) <- L^{-1} of them, L the unit-lower h x h block at (r0, r0):
   // halves recursively, so that most of the work is one update of depth h / 2
   std::function<int(T*, int, int, int, int)> trsm_rec = [&](T* A, int r0, int h, int cb, int ce) -> int {
     if (h <= IB) return trsm_blk(A, n, r0, h, cb, ce, st);
     if (inv_solve && h % 32 == 0 && h <= IVB) {
-      TT_TRY(inv_unit_lower(A, n, r0, h, Xinv.ptr, Tinv.ptr, st));
+      const T* A1 = A;
+      TT_TRY(inv_unit_lower(&A1, 1, n, r0, h, Xinv.ptr, Tinv.ptr, st));
       return tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)r0 * n + cb, n,
                           reinterpret_cast<const float2*>(Xinv.ptr), h,
                           reinterpret_cast<const float2*>(A) + (size_t)r0 * n + cb, n, h, ce - cb, h, st, 1);
@@ -911,6 +932,22 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     TT_TRY(panel_gemm_sub(mode, A + (size_t)(r0 + h1) * n + cb, n, A + (size_t)(r0 + h1) * n + r0, n,
                           A + (size_t)r0 * n + cb, n, h - h1, ce - cb, h1, st));
     return trsm_rec(A, r0 + h1, h - h1, cb, ce);
+  };
+  // trsm_rec of the same block in all B matrices: one set of inverse launches
+  // for all of them when the block is solved through its explicit inverse
+  auto trsm_all = [&](int r0, int h, int cb, int ce) -> int {
+    if (!(inv_solve && h > IB && h % 32 == 0 && h <= IVB)) {
+      for (int b = 0; b < B; b++) TT_TRY(trsm_rec(As[b], r0, h, cb, ce));
+      return TT_OK;
+    }
+    const T* Ac[kMaxBatch];
+    for (int b = 0; b < B; b++) Ac[b] = As[b];
+    TT_TRY(inv_unit_lower(Ac, B, n, r0, h, Xinv.ptr, Tinv.ptr, st));
+    for (int b = 0; b < B; b++)
+      TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(As[b]) + (size_t)r0 * n + cb, n,
+                          reinterpret_cast<const float2*>(Xinv.ptr + (size_t)b * h * h), h,
+                          reinterpret_cast<const float2*>(As[b]) + (size_t)r0 * n + cb, n, h, ce - cb, h, st, 1));
+    return TT_OK;
   };
   // columns [c0, c0 + w) of the panel [k, k + kb) factored by recursive halving:
   // left half, its U block and the update of the right half (depth w / 2), right half
@@ -980,25 +1017,24 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
         }
       }
       const int right_out = k + kb - (m0 + mw);
-      if (right_out > 0)
+      if (right_out > 0) {
+        TT_TRY(trsm_all(m0, mw, m0 + mw, k + kb));
         for (int b = 0; b < B; b++) {
           T* A = As[b];
-          TT_TRY(trsm_rec(A, m0, mw, m0 + mw, k + kb));
           TT_TRY(panel_gemm_sub(mode, A + (size_t)(m0 + mw) * n + (m0 + mw), n, A + (size_t)(m0 + mw) * n + m0, n,
                                 A + (size_t)m0 * n + (m0 + mw), n, n - m0 - mw, right_out, mw, st));
         }
+      }
     }
+    // ---- interchanges outside the panel; U12 = L11^{-1} A12 with the
+    // explicit inverse in the tensor-core modes (all matrices together)
+    for (int b = 0; b < B; b++) TT_TRY(laswp2(As[b], n, ipivs[b], k, k + kb, 0, k, k + kb, n, st));
+    if (rest > 0 && inv_solve) TT_TRY(trsm_all(k, kb, k + kb, n));
     for (int b = 0; b < B; b++) {
       T* A = As[b];
-      const int32_t* ipiv = ipivs[b];
-      // ---- interchanges outside the panel
-      TT_TRY(laswp2(A, n, ipiv, k, k + kb, 0, k, k + kb, n, st));
       if (rest <= 0) continue;
-      // ---- U12 = L11^{-1} A12: with the explicit inverse in the tensor-core
-      // modes, else blocked by IB
-      if (inv_solve) {
-        TT_TRY(trsm_rec(A, k, kb, k + kb, n));
-      } else for (int i0 = k; i0 < k + kb; i0 += IB) {
+      // ---- U12 blocked by IB without tensor cores
+      if (!inv_solve) for (int i0 = k; i0 < k + kb; i0 += IB) {
         const int wi = std::min(IB, k + kb - i0);
         TT_TRY(trsm_blk(A, n, i0, wi, k + kb, n, st));
         const int below = k + kb - (i0 + wi);

@@ -9,7 +9,7 @@
 // of fragments and issues 64 DMMAs:
 //   Re += Lr Ur + Li (-Ui),   Im += Lr Ui + Li Ur
 // The next k tile is read from global memory into registers while the current
-// one is multiplied.
+// one is multiplied, then stored into the second shared-memory buffer.
 #include <algorithm>
 
 #include "tt_kernels.h"
@@ -21,7 +21,7 @@ namespace dmma {
 constexpr int BM = 64, BN = 128, BK = 16;
 constexpr int AS = BM + 4;  // shared-memory stride of the L planes [BK][AS]
 constexpr int BS = BN + 4;  // and of the U planes [BK][BS]
-constexpr int SMEM_BYTES = (2 * BK * AS + 2 * BK * BS) * 8;
+constexpr int SMEM_BYTES = 2 * (2 * BK * AS + 2 * BK * BS) * 8;  // two buffers
 
 __device__ __forceinline__ void mma884(double (&d)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -32,11 +32,10 @@ __device__ __forceinline__ void mma884(double (&d)[2], double a, double b) {
 __global__ void __launch_bounds__(256) k_zgemm_dmma(double2* __restrict__ C, int ldc, const double2* __restrict__ L,
                                                     int ldl, const double2* __restrict__ U, int ldu, int M, int N,
                                                     int K) {
+  // two buffers of the re/im planes: the next k tile is stored into one while
+  // the other is multiplied, one barrier per k tile
   extern __shared__ double dsm[];
-  double* sAr = dsm;
-  double* sAi = sAr + BK * AS;
-  double* sBr = sAi + BK * AS;
-  double* sBi = sBr + BK * BS;
+  constexpr int BUF = 2 * BK * AS + 2 * BK * BS;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int gid = lane >> 2, tig = lane & 3;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -63,7 +62,11 @@ __global__ void __launch_bounds__(256) k_zgemm_dmma(double2* __restrict__ C, int
       rb[e] = (gk < K && gc < N) ? __ldg(&U[(size_t)gk * ldu + gc]) : make_double2(0.0, 0.0);
     }
   };
-  auto store = [&]() {
+  auto store = [&](int buf) {
+    double* sAr = dsm + buf * BUF;
+    double* sAi = sAr + BK * AS;
+    double* sBr = sAi + BK * AS;
+    double* sBi = sBr + BK * BS;
 #pragma unroll
     for (int e = 0; e < 4; e++) {
       const int idx = tid + 256 * e, r = idx >> 4, c = idx & 15;
@@ -79,11 +82,16 @@ __global__ void __launch_bounds__(256) k_zgemm_dmma(double2* __restrict__ C, int
   };
 
   load(0);
-  store();
+  store(0);
   __syncthreads();
+  int buf = 0;
   for (int k0 = 0; k0 < K; k0 += BK) {
     const bool more = k0 + BK < K;
     if (more) load(k0 + BK);
+    const double* sAr = dsm + buf * BUF;
+    const double* sAi = sAr + BK * AS;
+    const double* sBr = sAi + BK * AS;
+    const double* sBi = sBr + BK * BS;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
       double ar[4], ai[4], br[4], bi[4], nbi[4];
@@ -108,11 +116,10 @@ __global__ void __launch_bounds__(256) k_zgemm_dmma(double2* __restrict__ C, int
           mma884(acci[i][j], ai[i], br[j]);
         }
     }
+    // the other buffer was last read before the previous barrier
+    if (more) store(buf ^ 1);
     __syncthreads();
-    if (more) {
-      store();
-      __syncthreads();
-    }
+    buf ^= 1;
   }
 #pragma unroll
   for (int i = 0; i < 4; i++) {
