@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 
 #include "tc2_pack.cuh"
 #include "tt_kernels.h"
@@ -221,14 +222,25 @@ __device__ __forceinline__ void load_c_chunk(const float2* __restrict__ C, int l
   }
 }
 
+// Up to kBatch products of the same shape in one launch: matrix b's L is read
+// through A[b], its U planes are rows [b PARTS 2N, (b + 1) PARTS 2N) of the B
+// operand, its output is C[b]; the tiles of all of them share the persistent
+// grid (tile t of matrix t / tiles-per-matrix).
+constexpr int kBatch = 4;
+struct Ops {
+  CUtensorMap A[kBatch];
+  float2* C[kBatch];
+  int nb;
+};
+
 // tmA: L as [rows][2K] reals (TF32: the matrix itself or a packed copy; BF16X3:
 // hi plane rows [0, M), lo plane rows [a_plane, a_plane + M)).  tmB: U as
 // [2N][2K] reals per plane (re-rows [0, N), im-rows [N, 2N); BF16X3: lo plane
 // at row offset 2N).  K complex depth, a multiple of KCC.
 template <int MODE>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
-    k_lu_update_tc2(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                    float2* __restrict__ C, int ldc, int M, int N, int K, int a_plane, int store, int* err) {
+    k_lu_update_tc2(const __grid_constant__ Ops ops, const __grid_constant__ CUtensorMap tmB, int ldc, int M, int N,
+                    int K, int a_plane, int store, int* err) {
   using CF = Cfg<MODE>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int kchunks = K / KCC;
   TileSched sched{(M + BM - 1) / BM, (N + BN - 1) / BN, 16};
-  const int ntiles = sched.tiles_m * sched.tiles_n;
+  const int per = sched.tiles_m * sched.tiles_n, ntiles = per * ops.nb;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
@@ -272,7 +284,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       bool ok = true;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         int tm, tn;
-        sched.coords(t, tm, tn);
+        const int mb = t / per;
+        sched.coords(t - mb * per, tm, tn);
+        const int brow = mb * CF::PARTS * 2 * N;
         for (int kc = 0; kc < kchunks && ok; kc++, it++) {
           const int s = it % STAGES;
           const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
@@ -286,9 +300,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 #pragma unroll
           for (int p = 0; p < CF::PARTS; p++) {
             unsigned char* a = st + p * (CF::A_TILE + CF::B_TILE);
-            tma_load_2d(a, &tmA, &full[s], x, p * a_plane + tm * BM);
-            tma_load_2d(a + CF::A_TILE, &tmB, &full[s], x, p * 2 * N + tn * BN);
-            tma_load_2d(a + CF::A_TILE + CF::B_TILE / 2, &tmB, &full[s], x, p * 2 * N + N + tn * BN);
+            tma_load_2d(a, &ops.A[mb], &full[s], x, p * a_plane + tm * BM);
+            tma_load_2d(a + CF::A_TILE, &tmB, &full[s], x, brow + p * 2 * N + tn * BN);
+            tma_load_2d(a + CF::A_TILE + CF::B_TILE / 2, &tmB, &full[s], x, brow + p * 2 * N + N + tn * BN);
           }
         }
       }
@@ -348,7 +362,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     int local = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, local++) {
       int tm, tn;
-      sched.coords(t, tm, tn);
+      const int mb = t / per;
+      sched.coords(t - mb * per, tm, tn);
+      float2* __restrict__ C = ops.C[mb];
       const int ab = local & 1;
       const uint32_t aph = (uint32_t)(local >> 1) & 1u;
       const int row0 = tm * BM + quarter * 32;
@@ -479,8 +495,8 @@ __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* m
 
 template <int MODE>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
-    k_lu_update_tc2_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                         float2* __restrict__ C, int ldc, int M, int N, int K, int a_plane, int store, int* err) {
+    k_lu_update_tc2_pair(const __grid_constant__ Ops ops, const __grid_constant__ CUtensorMap tmB, int ldc, int M,
+                         int N, int K, int a_plane, int store, int* err) {
   using CF = Cfg<MODE>;
   using PC = PairCfg<MODE>;
   constexpr int STAGES_P = PC::STAGES;
@@ -501,7 +517,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   const bool lead = rank == 0;
   const int kchunks = K / KCC;
   TileSched sched{(M + 2 * BM - 1) / (2 * BM), (N + BN - 1) / BN, 8};
-  const int ntiles = sched.tiles_m * sched.tiles_n;
+  const int per = sched.tiles_m * sched.tiles_n, ntiles = per * ops.nb;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES_P; s++) {
@@ -533,7 +549,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       bool ok = true;
       for (int t = pair; t < ntiles && ok; t += npairs) {
         int tm, tn;
-        sched.coords(t, tm, tn);
+        const int mb = t / per;
+        sched.coords(t - mb * per, tm, tn);
+        const int brow = mb * CF::PARTS * 2 * N;
         for (int kc = 0; kc < kchunks && ok; kc++, it++) {
           const int s = it % STAGES_P;
           const uint32_t ph = (uint32_t)(it / STAGES_P) & 1u;
@@ -548,8 +566,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 #pragma unroll
           for (int p = 0; p < CF::PARTS; p++) {
             unsigned char* a = st + p * PC::PART;
-            tma_load_2d_pair(a, &tmA, bar, x, p * a_plane + tm * 2 * BM + (int)rank * BM);
-            tma_load_2d_pair(a + PC::A_TILE, &tmB, bar, x, p * 2 * N + (int)rank * N + tn * BN);
+            tma_load_2d_pair(a, &ops.A[mb], bar, x, p * a_plane + tm * 2 * BM + (int)rank * BM);
+            tma_load_2d_pair(a + PC::A_TILE, &tmB, bar, x, brow + p * 2 * N + (int)rank * N + tn * BN);
           }
         }
       }
@@ -613,7 +631,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     int local = 0;
     for (int t = pair; t < ntiles; t += npairs, local++) {
       int tm, tn;
-      sched.coords(t, tm, tn);
+      const int mb = t / per;
+      sched.coords(t - mb * per, tm, tn);
+      float2* __restrict__ C = ops.C[mb];
       const int ab = local & 1;
       const uint32_t aph = (uint32_t)(local >> 1) & 1u;
       const int row0 = tm * 2 * BM + (int)rank * BM + quarter * 32;
@@ -768,47 +788,70 @@ TC2Workspace& workspace2() {
 }
 
 template <int MODE>
-int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, int ldu, int M, int N, int K,
-               cudaStream_t st, int store, bool prepacked) {
+int launch_tc2(int nb, float2* const* C, int ldc, const float2* const* L, int ldl, const float2* const* U, int ldu,
+               int M, int N, int K, cudaStream_t st, int store, bool prepacked) {
   using CF = tc2::Cfg<MODE>;
+  if (nb < 1 || nb > tc2::kBatch) {
+    set_error("tensor-core update batch of " + std::to_string(nb) + " products (1.." + std::to_string(tc2::kBatch) +
+              ")");
+    return TT_ERR_BADARG;
+  }
   TC2Workspace& ws = workspace2();
   const size_t esz = (MODE == TC_TF32) ? 4 : 2;
   // the matrix itself is the TF32 A operand when TMA can address it: 16-byte
   // aligned base and row pitch (the panel's x offsets are multiples of 32 reals)
-  const bool direct_A = MODE == TC_TF32 && ((uintptr_t)L % 16 == 0) && ((size_t)ldl * 8 % 16 == 0);
-  const size_t needA = direct_A ? 0 : (size_t)CF::PARTS * M * 2 * K * esz;
-  const size_t needB = (size_t)CF::PARTS * 2 * N * 2 * K * esz;
+  bool direct_A = MODE == TC_TF32 && ((size_t)ldl * 8 % 16 == 0);
+  for (int b = 0; b < nb; b++) direct_A = direct_A && ((uintptr_t)L[b] % 16 == 0);
+  const size_t planeA = (size_t)CF::PARTS * M * 2 * K * esz, planeB = (size_t)CF::PARTS * 2 * N * 2 * K * esz;
+  const size_t needA = direct_A ? 0 : planeA * nb;
+  const size_t needB = planeB * nb;
   if (needA > ws.WA.count) TT_TRY(ws.WA.alloc(needA));
-  if (needB > ws.WB.count) TT_TRY(ws.WB.alloc(needB));
+  if (needB > ws.WB.count) {
+    if (prepacked) {
+      set_error("tensor-core update: prepacked operand planes larger than the workspace");
+      return TT_ERR_BADARG;
+    }
+    TT_TRY(ws.WB.alloc(needB));
+  }
   if (!ws.err.ptr) {
     TT_TRY(ws.err.alloc(1));
     TT_CUDA_TRY(cudaMemsetAsync(ws.err.ptr, 0, sizeof(int), st));
   }
   {
     ProfScope prof(TT_PROF_OPERANDS, st, 0.0,
-                   8.0 * (direct_A ? 0.0 : (double)M) * K + (double)needA + 8.0 * N * K + (double)needB);
-    if (!direct_A) {
-      tc2::k_pack_A<MODE><<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L, ldl, M, K, ws.WA.ptr);
-      count_launch();
-      TT_CUDA_TRY(cudaGetLastError());
-    }
-    if (!prepacked) {
-      dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
-      tc2::k_pack_B<MODE><<<gs, 256, 0, st>>>(U, ldu, K, N, ws.WB.ptr);
-      count_launch();
-      TT_CUDA_TRY(cudaGetLastError());
+                   nb * (8.0 * (direct_A ? 0.0 : (double)M) * K + (double)(needA / nb) +
+                         (prepacked ? 0.0 : 8.0 * N * K + (double)planeB)));
+    for (int b = 0; b < nb; b++) {
+      if (!direct_A) {
+        tc2::k_pack_A<MODE><<<ceil_div((size_t)M * K, 256), 256, 0, st>>>(L[b], ldl, M, K, ws.WA.ptr + planeA * b);
+        count_launch();
+        TT_CUDA_TRY(cudaGetLastError());
+      }
+      if (!prepacked) {
+        dim3 gs(ceil_div(N, 32), ceil_div(K, 32));
+        tc2::k_pack_B<MODE><<<gs, 256, 0, st>>>(U[b], ldu, K, N, ws.WB.ptr + planeB * b);
+        count_launch();
+        TT_CUDA_TRY(cudaGetLastError());
+      }
     }
   }
-  CUtensorMap mA, mB;
-  if (direct_A)
-    TT_TRY(make_map2(&mA, MODE, const_cast<float2*>(L), (uint64_t)M, (uint64_t)2 * K, (uint64_t)ldl * 8, tc2::BM));
-  else
-    TT_TRY(make_map2(&mA, MODE, ws.WA.ptr, (uint64_t)CF::PARTS * M, (uint64_t)2 * K, (uint64_t)2 * K * esz,
-                     tc2::BM));
-  TT_TRY(make_map2(&mB, MODE, ws.WB.ptr, (uint64_t)CF::PARTS * 2 * N, (uint64_t)2 * K, (uint64_t)2 * K * esz,
+  tc2::Ops ops;
+  std::memset(&ops, 0, sizeof(ops));
+  ops.nb = nb;
+  for (int b = 0; b < nb; b++) {
+    ops.C[b] = C[b];
+    if (direct_A)
+      TT_TRY(make_map2(&ops.A[b], MODE, const_cast<float2*>(L[b]), (uint64_t)M, (uint64_t)2 * K, (uint64_t)ldl * 8,
+                       tc2::BM));
+    else
+      TT_TRY(make_map2(&ops.A[b], MODE, ws.WA.ptr + planeA * b, (uint64_t)CF::PARTS * M, (uint64_t)2 * K,
+                       (uint64_t)2 * K * esz, tc2::BM));
+  }
+  CUtensorMap mB;
+  TT_TRY(make_map2(&mB, MODE, ws.WB.ptr, (uint64_t)nb * CF::PARTS * 2 * N, (uint64_t)2 * K, (uint64_t)2 * K * esz,
                    tc2::BN));
-  ProfScope prof(K >= 256 ? TT_PROF_TC_UPDATE : TT_PROF_TC_PANEL, st, 8.0 * M * N * K,
-                 16.0 * M * N + 8.0 * ((double)M + N) * K);
+  ProfScope prof(K >= 256 ? TT_PROF_TC_UPDATE : TT_PROF_TC_PANEL, st, 8.0 * M * N * K * nb,
+                 nb * (16.0 * M * N + 8.0 * ((double)M + N) * K));
   if (g_tc2_pairs && M > tc2::BM) {
     // CTA pairs on 256-row tiles, as many pairs as can be resident at once
     using PC = tc2::PairCfg<MODE>;
@@ -834,17 +877,16 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
       TT_CUDA_TRY(cudaOccupancyMaxActiveClusters(&clusters, kfn, &cfg));
       mp = std::max(1, clusters);
     }
-    const int tiles = ((M + 2 * tc2::BM - 1) / (2 * tc2::BM)) * ((N + tc2::BN - 1) / tc2::BN);
+    const int tiles = nb * ((M + 2 * tc2::BM - 1) / (2 * tc2::BM)) * ((N + tc2::BN - 1) / tc2::BN);
     cfg.gridDim = dim3(2 * std::min(tiles, mp));
-    TT_CUDA_TRY(cudaLaunchKernelEx(&cfg, tc2::k_lu_update_tc2_pair<MODE>, mA, mB, C, ldc, M, N, K, M, store,
+    TT_CUDA_TRY(cudaLaunchKernelEx(&cfg, tc2::k_lu_update_tc2_pair<MODE>, ops, mB, ldc, M, N, K, M, store,
                                    ws.err.ptr));
   } else {
     const size_t smem = (size_t)tc2::STAGES * CF::STAGE + tc2::EPI_WARPS * tc2::EPI_STAGE_BYTES + 1024 + 128;
     TT_TRY(smem_limit_once((const void*)tc2::k_lu_update_tc2<MODE>, (int)smem));
-    const int tiles = ((M + tc2::BM - 1) / tc2::BM) * ((N + tc2::BN - 1) / tc2::BN);
+    const int tiles = nb * ((M + tc2::BM - 1) / tc2::BM) * ((N + tc2::BN - 1) / tc2::BN);
     const int grid = std::min(tiles, device_sm_count());
-    tc2::k_lu_update_tc2<MODE><<<grid, tc2::NUM_THREADS, smem, st>>>(mA, mB, C, ldc, M, N, K, M, store,
-                                                                     ws.err.ptr);
+    tc2::k_lu_update_tc2<MODE><<<grid, tc2::NUM_THREADS, smem, st>>>(ops, mB, ldc, M, N, K, M, store, ws.err.ptr);
   }
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
@@ -855,10 +897,15 @@ int launch_tc2(float2* C, int ldc, const float2* L, int ldl, const float2* U, in
 
 void tc2_set_pairs(bool on) { g_tc2_pairs = on; }
 
-void* tc2_b_workspace(int mode, int N, int K, int* status) {
+size_t tc2_b_plane_bytes(int mode, int N, int K) {
+  const size_t esz = (mode == TC_TF32) ? 4 : 2, parts = (mode == TC_TF32) ? 1 : 2;
+  return parts * 2 * (size_t)N * 2 * K * esz;
+}
+
+void* tc2_b_workspace(int mode, int N, int K, int* status, int nb) {
   TC2Workspace& ws = workspace2();
   const size_t esz = (mode == TC_TF32) ? 4 : 2, parts = (mode == TC_TF32) ? 1 : 2;
-  const size_t need = parts * 2 * (size_t)N * 2 * K * esz;
+  const size_t need = parts * 2 * (size_t)N * 2 * K * esz * nb;
   *status = TT_OK;
   if (need > ws.WB.count) *status = ws.WB.alloc(need);
   return *status == TT_OK ? ws.WB.ptr : nullptr;
@@ -871,8 +918,19 @@ int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const f
     set_error("tensor-core update needs K to be a multiple of 16");
     return TT_ERR_BADARG;
   }
-  if (mode == TC_TF32) return launch_tc2<TC_TF32>(C, ldc, L, ldl, U, ldu, M, N, K, st, store, prepacked);
-  if (mode == TC_BF16X3) return launch_tc2<TC_BF16X3>(C, ldc, L, ldl, U, ldu, M, N, K, st, store, prepacked);
+  return tc2_gemm_sub_batched(mode, 1, &C, ldc, &L, ldl, &U, ldu, M, N, K, st, store, prepacked);
+}
+
+int tc2_gemm_sub_batched(int mode, int nb, float2* const* C, int ldc, const float2* const* L, int ldl,
+                         const float2* const* U, int ldu, int M, int N, int K, cudaStream_t st, int store,
+                         bool prepacked) {
+  if (M <= 0 || N <= 0 || K <= 0 || nb <= 0) return TT_OK;
+  if (K % tc2::KCC != 0) {
+    set_error("tensor-core update needs K to be a multiple of 16");
+    return TT_ERR_BADARG;
+  }
+  if (mode == TC_TF32) return launch_tc2<TC_TF32>(nb, C, ldc, L, ldl, U, ldu, M, N, K, st, store, prepacked);
+  if (mode == TC_BF16X3) return launch_tc2<TC_BF16X3>(nb, C, ldc, L, ldl, U, ldu, M, N, K, st, store, prepacked);
   set_error("unknown tensor-core product mode " + std::to_string(mode));
   return TT_ERR_BADARG;
 }

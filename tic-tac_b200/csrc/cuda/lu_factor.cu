@@ -943,10 +943,38 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
     const T* Ac[kMaxBatch];
     for (int b = 0; b < B; b++) Ac[b] = As[b];
     TT_TRY(inv_unit_lower(Ac, B, n, r0, h, Xinv.ptr, Tinv.ptr, st));
-    for (int b = 0; b < B; b++)
-      TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(As[b]) + (size_t)r0 * n + cb, n,
-                          reinterpret_cast<const float2*>(Xinv.ptr + (size_t)b * h * h), h,
-                          reinterpret_cast<const float2*>(As[b]) + (size_t)r0 * n + cb, n, h, ce - cb, h, st, 1));
+    float2* Cs[kMaxBatch];
+    const float2* Ls[kMaxBatch];
+    const float2* Us[kMaxBatch];
+    for (int b = 0; b < B; b++) {
+      Cs[b] = reinterpret_cast<float2*>(As[b]) + (size_t)r0 * n + cb;
+      Ls[b] = reinterpret_cast<const float2*>(Xinv.ptr + (size_t)b * h * h);
+      Us[b] = Cs[b];
+    }
+    return tc2_gemm_sub_batched(mode, B, Cs, n, Ls, h, Us, n, h, ce - cb, h, st, 1);
+  };
+  // C -= L U at the same offsets of all B matrices (row/column offsets of C,
+  // L and U given as (row, col) pairs): one batched tensor-core launch in the
+  // real-row modes, else one update per matrix
+  auto gemm_all = [&](int cr, int cc, int lr, int lc, int ur, int uc, int M, int N, int K) -> int {
+    if (M <= 0 || N <= 0 || K <= 0) return TT_OK;
+    if ((mode == TC_TF32 || mode == TC_BF16X3) && K % 16 == 0) {
+      float2* Cs[kMaxBatch];
+      const float2* Ls[kMaxBatch];
+      const float2* Us[kMaxBatch];
+      for (int b = 0; b < B; b++) {
+        float2* A = reinterpret_cast<float2*>(As[b]);
+        Cs[b] = A + (size_t)cr * n + cc;
+        Ls[b] = A + (size_t)lr * n + lc;
+        Us[b] = A + (size_t)ur * n + uc;
+      }
+      return tc2_gemm_sub_batched(mode, B, Cs, n, Ls, n, Us, n, M, N, K, st);
+    }
+    for (int b = 0; b < B; b++) {
+      T* A = As[b];
+      TT_TRY(panel_gemm_sub(mode, A + (size_t)cr * n + cc, n, A + (size_t)lr * n + lc, n, A + (size_t)ur * n + uc, n,
+                            M, N, K, st));
+    }
     return TT_OK;
   };
   // columns [c0, c0 + w) of the panel [k, k + kb) factored by recursive halving:
@@ -996,20 +1024,28 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
       for (int j0 = m0; j0 < m0 + mw; j0 += IB) {
         const int w = std::min(IB, m0 + mw - j0);
         TT_TRY(leaf(j0, w, k, k + kb));
-        for (int b = 0; b < B; b++) {
-          T* A = As[b];
-          const int right = m0 + mw - (j0 + w);
-          if (right > 0 && inv_solve && w % 16 == 0) {
-            // the solved block row is written straight into the update's operand planes
-            int ws = TT_OK;
-            void* WB = tc2_b_workspace(mode, right, w, &ws);
-            TT_TRY(ws);
-            TT_TRY(trsm_blk(A, n, j0, w, j0 + w, m0 + mw, st, mode, WB));
-            TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)(j0 + w) * n + (j0 + w), n,
-                                reinterpret_cast<const float2*>(A) + (size_t)(j0 + w) * n + j0, n,
-                                reinterpret_cast<const float2*>(A) + (size_t)j0 * n + (j0 + w), n, n - j0 - w,
-                                right, w, st, 0, true));
-          } else if (right > 0) {
+        const int right = m0 + mw - (j0 + w);
+        if (right > 0 && inv_solve && w % 16 == 0) {
+          // the solved block rows are written straight into the update's
+          // operand planes, then one update for all matrices
+          int ws = TT_OK;
+          unsigned char* WB = static_cast<unsigned char*>(tc2_b_workspace(mode, right, w, &ws, B));
+          TT_TRY(ws);
+          const size_t plane = tc2_b_plane_bytes(mode, right, w);
+          float2* Cs[kMaxBatch];
+          const float2* Ls[kMaxBatch];
+          const float2* Us[kMaxBatch];
+          for (int b = 0; b < B; b++) {
+            float2* A = reinterpret_cast<float2*>(As[b]);
+            TT_TRY(trsm_blk(As[b], n, j0, w, j0 + w, m0 + mw, st, mode, WB + plane * b));
+            Cs[b] = A + (size_t)(j0 + w) * n + (j0 + w);
+            Ls[b] = A + (size_t)(j0 + w) * n + j0;
+            Us[b] = A + (size_t)j0 * n + (j0 + w);
+          }
+          TT_TRY(tc2_gemm_sub_batched(mode, B, Cs, n, Ls, n, Us, n, n - j0 - w, right, w, st, 0, true));
+        } else if (right > 0) {
+          for (int b = 0; b < B; b++) {
+            T* A = As[b];
             TT_TRY(trsm_blk(A, n, j0, w, j0 + w, m0 + mw, st));
             TT_TRY(panel_gemm_sub(mode, A + (size_t)(j0 + w) * n + (j0 + w), n, A + (size_t)(j0 + w) * n + j0, n,
                                   A + (size_t)j0 * n + (j0 + w), n, n - j0 - w, right, w, st));
@@ -1019,11 +1055,7 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
       const int right_out = k + kb - (m0 + mw);
       if (right_out > 0) {
         TT_TRY(trsm_all(m0, mw, m0 + mw, k + kb));
-        for (int b = 0; b < B; b++) {
-          T* A = As[b];
-          TT_TRY(panel_gemm_sub(mode, A + (size_t)(m0 + mw) * n + (m0 + mw), n, A + (size_t)(m0 + mw) * n + m0, n,
-                                A + (size_t)m0 * n + (m0 + mw), n, n - m0 - mw, right_out, mw, st));
-        }
+        TT_TRY(gemm_all(m0 + mw, m0 + mw, m0 + mw, m0, m0, m0 + mw, n - m0 - mw, right_out, mw));
       }
     }
     // ---- interchanges outside the panel; U12 = L11^{-1} A12 with the
@@ -1042,17 +1074,15 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
           TT_TRY(panel_gemm_sub(mode, A + (size_t)(i0 + wi) * n + (k + kb), n, A + (size_t)(i0 + wi) * n + i0, n,
                                 A + (size_t)i0 * n + (k + kb), n, below, rest, wi, st));
       }
-      // ---- trailing update
+      // ---- trailing update (the real-row modes: below, all matrices in one launch)
       if (mode == TC_LEGACY_BF16X3)
         TT_TRY(lu_update_tc(reinterpret_cast<float2*>(A), n, k, kb, st));
-      else if (tc)
-        TT_TRY(tc2_gemm_sub(mode, reinterpret_cast<float2*>(A) + (size_t)(k + kb) * n + (k + kb), n,
-                            reinterpret_cast<const float2*>(A) + (size_t)(k + kb) * n + k, n,
-                            reinterpret_cast<const float2*>(A) + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
-      else
+      else if (!tc)
         TT_TRY(gemm_sub(A + (size_t)(k + kb) * n + (k + kb), n, A + (size_t)(k + kb) * n + k, n,
                         A + (size_t)k * n + (k + kb), n, rest, rest, kb, st));
     }
+    if (rest > 0 && (mode == TC_TF32 || mode == TC_BF16X3))
+      TT_TRY(gemm_all(k + kb, k + kb, k + kb, k, k, k + kb, rest, rest, kb));
   }
   if (mode == TC_LEGACY_BF16X3) TT_TRY(tc_check_error(st));
   if (mode == TC_TF32 || mode == TC_BF16X3) TT_TRY(tc2_check_error(st));

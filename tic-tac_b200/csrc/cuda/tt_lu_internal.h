@@ -27,8 +27,17 @@ int tc2_gemm_sub(int mode, float2* C, int ldc, const float2* L, int ldl, const f
 // Updates of more than 128 rows on CTA pairs (cta_group::2, 256-row tiles) on
 // this host thread's next tc2_gemm_sub calls.
 void tc2_set_pairs(bool on);
-// The B-operand workspace of tc2_gemm_sub, grown to an N-column, K-deep operand.
-void* tc2_b_workspace(int mode, int N, int K, int* status);
+// The same for nb <= 4 products of one shape in one launch (the tiles of all
+// of them share the persistent grid): C[b] -= L[b] U[b].
+int tc2_gemm_sub_batched(int mode, int nb, float2* const* C, int ldc, const float2* const* L, int ldl,
+                         const float2* const* U, int ldu, int M, int N, int K, cudaStream_t st, int store = 0,
+                         bool prepacked = false);
+// The B-operand workspace of tc2_gemm_sub(_batched), grown to nb N-column,
+// K-deep operands; product b's planes start nb-th of the way in (b times the
+// size of one operand's planes).
+void* tc2_b_workspace(int mode, int N, int K, int* status, int nb = 1);
+// Bytes of one N-column, K-deep operand's planes in that workspace.
+size_t tc2_b_plane_bytes(int mode, int N, int K);
 int tc2_check_error(cudaStream_t st);
 // C[M x N] -= L[M x K] U[K x N], complex128, on the FP64 tensor cores (zgemm_dmma.cu).
 int zgemm_sub_dmma(double2* C, int ldc, const double2* L, int ldl, const double2* U, int ldu, int M, int N, int K,
