@@ -111,8 +111,13 @@ class ClockSampler:
                 for k, nm in enumerate(names):
                     if s[5 + k].lower() == "active":
                         reasons.add(nm)
+        pw = [float(s[3]) for s in self.samples if len(s) >= 9 and s[3].replace(".", "").isdigit()]
+        capped = [s[8].lower() == "active" for s in self.samples if len(s) >= 9]
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "sm_mhz_p10_p90": [float(np.percentile(sm, 10)), float(np.percentile(sm, 90))] if sm else None,
+                "power_w_median": float(np.median(pw)) if pw else None,
+                "power_cap_share": round(sum(capped) / len(capped), 3) if capped else None}
 
 
 def dist_setup():
@@ -150,13 +155,13 @@ def step_flops(ns, nE):
     return sum(nE * 8.0 / 3.0 * float(n) ** 3 for n in ns)
 
 
-# DRAM traffic of the tensor-core update per algorithmic byte (C read + written
-# as complex64, L and U panels read once): dram__bytes_read.sum +
-# dram__bytes_write.sum over 16 M N + 8 (M + N) K for two launches (M = N = 7536
-# and 7280, K = 256) of an ncu capture of the n = 9072 channel
-# (926.4 / 939.5 MB and 861.2 / 877.8 MB); traffic grows with the tile count, so
-# the ratio scales the bench's mean launch to a per-launch traffic figure.
-TC_TRAFFIC_PER_ALGO_BYTE = 0.984
+# DRAM traffic of the tensor-core update (CTA pairs, TF32) per algorithmic byte
+# (C read + written as complex64, L and U panels read once):
+# dram__bytes_read.sum + dram__bytes_write.sum over 16 M N + 8 (M + N) K for
+# the first trailing update of the n = 9072 channel (M = N = 8560, K = 512) in
+# an ncu capture: (974.5 + 560.5) MB / 1242.5 MB; traffic grows with the tile
+# count, so the ratio scales the bench's mean launch to a per-launch figure.
+TC_TRAFFIC_PER_ALGO_BYTE = 1.235
 
 
 # Tensor work per algorithmic complex flop of each product and the kernel
@@ -182,6 +187,11 @@ def roofline_of(kern, timed_ms, ms_step, ns, nE, product="bf16x3"):
                              "gbs": round(k["bytes"] / (k["ms"] * 1e-3) / 1e9, 1) if k["ms"] else None}
     # launch gaps and kernels outside the classes: the rest of the timed region
     kernels["unattributed"] = {"share_of_timed": round(1.0 - sum(k["ms"] for k in kern.values()) / timed_ms, 4)}
+    if ms_step != timed_ms:
+        # the breakdown step records an event pair around every launch class, which
+        # slows the host's launch stream; against a plain timed step:
+        kernels["unattributed"]["share_of_plain_step"] = round(
+            max(0.0, 1.0 - sum(k["ms"] for k in kern.values()) / ms_step), 4)
     dom = max(kern, key=lambda nm: kern[nm]["ms"])
     k = kern[dom]
     if k["launches"] == 0:
@@ -320,7 +330,7 @@ def run_ours(args, world, rank, local, pg):
         run.timer_start()
         one_step()
         t_bd = run.timer_stop()
-        _, kernels = roofline_of(tt.profile_end(), t_bd, t_bd, items, 1, args.tc_product)
+        _, kernels = roofline_of(tt.profile_end(), t_bd, float(np.mean(times)), items, 1, args.tc_product)
         kernels["step_ms"] = round(t_bd, 1)
         kernels["per_channel_phases_ms"] = {str(c): phases[c] for c in mine}
     # U of every (channel, energy) gathered on rank 0 in the reference's layout
