@@ -154,8 +154,8 @@ int tt_calculate_resolvent_array_in_SWP_basis(tt_complex* G, double E, const tt_
  *   each part rounded up to 256,
  * and larger inputs are rejected with TT_ERR_UNSUPPORTED before any device work.
  * The first call on each device looks up the scratch address with
- * cudaGetSymbolAddress (that device current) and loads the module there:
- * make it before any stream capture.  Nothing has to be zeroed beforehand;
+ * cudaGetSymbolAddress (that device current) and loads the module there.
+ * Nothing has to be zeroed beforehand;
  * every call rewrites the tables it reads.  Calls that overlap in time on one
  * device (other streams or host threads) share the scratch and race:
  * serialise them.  Returns when the work is queued on `stream`; a call first
