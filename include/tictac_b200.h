@@ -224,6 +224,8 @@ int tt_device_count(int* count);
  * of GB cost milliseconds each); this returns the current device's cached
  * blocks to the driver.  tt_run_destroy does the same. */
 int tt_release_cached_device_memory(void);
+/* Bytes of those blocks currently held for the current device. */
+int tt_cached_device_memory(size_t* bytes);
 /* Kernels launched by this library since load (diagnostic). */
 unsigned long long tt_kernel_launches(void);
 

@@ -404,6 +404,12 @@ int tt_release_cached_device_memory(void) {
   return TT_OK;
 }
 
+int tt_cached_device_memory(size_t* bytes) {
+  if (!bytes) return fail(TT_ERR_BADARG, "null bytes");
+  *bytes = device_cache_bytes();
+  return TT_OK;
+}
+
 int tt_run_set_solve_option(tt_run* run, const char* key, const char* value) {
   if (!run || !key || !value) return fail(TT_ERR_BADARG, "null run, key or value");
   static const char* const kSolveKeys[] = {"tc_product", "panel_width", "panel_order", "energy_batch",

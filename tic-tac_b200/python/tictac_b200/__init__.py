@@ -42,6 +42,7 @@ EXPORTED_SYMBOLS = (
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
     "tt_run_solve_energies", "tt_profile_select", "tt_run_adjoint_forward", "tt_run_adjoint_backward",
     "tt_run_swp_derivative", "tt_run_set_solve_option", "tt_release_cached_device_memory",
+    "tt_cached_device_memory",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
@@ -132,6 +133,17 @@ def device_count() -> int:
     n = c_int(0)
     rc = lib.tt_device_count(byref(n))
     return n.value if rc == TT_OK else 0
+
+
+def cached_device_memory() -> int:
+    """Bytes of released device blocks the library holds for reuse on the current device."""
+    v = c_size_t()
+    _check(load().tt_cached_device_memory(byref(v)))
+    return v.value
+
+
+def release_cached_device_memory() -> None:
+    _check(load().tt_release_cached_device_memory())
 
 
 def kernel_launches() -> int:
