@@ -174,7 +174,7 @@ PRODUCTS = {
 }
 
 
-def roofline_of(kern, timed_ms, ms_step, ns, nE, product="bf16x3"):
+def roofline_of(kern, timed_ms, ms_step, ns, nE, product="bf16x3", pairs=True):
     """Roofline of the dominant kernel class over the timed region: algorithmic
     flops (or bytes) per launch over the CUDA-event time per launch."""
     hbm, tf_burst, tf_sust, peak_kind = load_peaks()
@@ -202,6 +202,9 @@ def roofline_of(kern, timed_ms, ms_step, ns, nE, product="bf16x3"):
         # product's cost factor; the kernel runs inside a seconds-long step,
         # so the sustained figure
         factor, kname = PRODUCTS[product]
+        if pairs:
+            kname = kname.replace("k_lu_update_tc2<", "k_lu_update_tc2_pair<").replace(
+                " on tcgen05)", " on tcgen05, CTA pairs)")
         achieved = k["flops"] / k["launches"] / per_launch_s / 1e12
         peak = tf_sust / factor
         traffic = None
@@ -322,7 +325,8 @@ def run_ours(args, world, rank, local, pg):
     energies_per_step = nE  # every channel at every on-shell energy of the scan, over all ranks
     value = energies_per_step / (ms_step * 1e-3)
     items = [infos_all[c]["n"] for c, js in mine.items() for _ in js]
-    roofline, _ = roofline_of(kern, float(np.sum(times)), float(np.mean(times)), items, 1, args.tc_product)
+    roofline, _ = roofline_of(kern, float(np.sum(times)), float(np.mean(times)), items, 1, args.tc_product,
+                              bool(args.cta_pairs))
     # breakdown: one more step with every kernel class timed (not part of the value)
     kernels = None
     if args.breakdown:
@@ -330,7 +334,8 @@ def run_ours(args, world, rank, local, pg):
         run.timer_start()
         one_step()
         t_bd = run.timer_stop()
-        _, kernels = roofline_of(tt.profile_end(), t_bd, float(np.mean(times)), items, 1, args.tc_product)
+        _, kernels = roofline_of(tt.profile_end(), t_bd, float(np.mean(times)), items, 1, args.tc_product,
+                                 bool(args.cta_pairs))
         kernels["step_ms"] = round(t_bd, 1)
         kernels["per_channel_phases_ms"] = {str(c): phases[c] for c in mine}
     # U of every (channel, energy) gathered on rank 0 in the reference's layout
@@ -369,7 +374,7 @@ def run_ours(args, world, rank, local, pg):
             deut = [a for a in range(len(pwt)) if tuple(pwt[a, :4]) == (0, 1, 1, 0)]
             host.append((G, val[order].copy(), rows[order].copy(), colptr, tt.PW(pwt, cfg["J_2N_max"]), deut,
                          q_idx[js]))
-            run.release(c)
+            run.release_A(c)  # A and G; P123 stays resident for the FP64 comparison below
         # inputs live in pinned host memory, as a caller streaming channels would keep them
         import torch
 
