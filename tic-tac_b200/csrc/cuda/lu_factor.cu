@@ -621,11 +621,22 @@ __global__ void k_laswp2(T* __restrict__ A, int n, const int32_t* __restrict__ i
 // X <- L^{-1} X, L the w x w unit-lower block at (r0, r0), X = rows [r0, r0+w) of columns [cb, ce).
 // With pack_mode (complex64 only), X is also written as the packed B operand
 // of the real-row tensor-core update that follows (w deep, ce - cb columns).
+// The matrices of a batch whose same 32-row block is solved in one launch
+// (blockIdx.y = matrix); matrix b's operand planes start at WB + b plane.
 template <typename T>
-__global__ void __launch_bounds__(256) k_trsm_blk(T* __restrict__ A, int n, int r0, int w, int cb, int ce,
-                                                  int pack_mode, void* __restrict__ WB) {
+struct TrsmBatch {
+  T* A[4];
+  unsigned char* WB;
+  size_t plane;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsm_blk(TrsmBatch<T> tb, int n, int r0, int w, int cb, int ce,
+                                                  int pack_mode) {
   __shared__ T sL[IB][IB + 1];
   __shared__ T sX[IB][33];
+  T* __restrict__ A = tb.A[blockIdx.y];
+  void* __restrict__ WB = tb.WB ? tb.WB + tb.plane * blockIdx.y : nullptr;
   const int c0 = cb + blockIdx.x * 32;
   for (int t = threadIdx.x; t < w * w; t += blockDim.x) sL[t / w][t % w] = A[(size_t)(r0 + t / w) * n + r0 + t % w];
   for (int t = threadIdx.x; t < w * 32; t += blockDim.x) {
@@ -783,14 +794,27 @@ int inv_unit_lower(const T* const* As, int B, int n, int r0, int w, T* X, T* Tsc
   return TT_OK;
 }
 
+// the same block of B <= 4 matrices (pack_mode: matrix b's solved rows also
+// go to its operand planes at WB + b plane)
 template <typename T>
-int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st, int pack_mode = 0, void* WB = nullptr) {
+int trsm_blk_batched(T* const* As, int B, int n, int r0, int w, int cb, int ce, cudaStream_t st, int pack_mode = 0,
+                     unsigned char* WB = nullptr, size_t plane = 0) {
   if (ce <= cb) return TT_OK;
-  ProfScope prof(TT_PROF_PANEL_TRSM, st, 4.0 * w * w * (double)(ce - cb), 2.0 * w * (double)(ce - cb) * sizeof(T));
-  k_trsm_blk<T><<<ceil_div(ce - cb, 32), 256, 0, st>>>(A, n, r0, w, cb, ce, pack_mode, WB);
+  ProfScope prof(TT_PROF_PANEL_TRSM, st, 4.0 * w * w * (double)(ce - cb) * B,
+                 2.0 * w * (double)(ce - cb) * sizeof(T) * B);
+  TrsmBatch<T> tb{};
+  for (int b = 0; b < B; b++) tb.A[b] = As[b];
+  tb.WB = WB;
+  tb.plane = plane;
+  k_trsm_blk<T><<<dim3(ceil_div(ce - cb, 32), B), 256, 0, st>>>(tb, n, r0, w, cb, ce, pack_mode);
   count_launch();
   TT_CUDA_TRY(cudaGetLastError());
   return TT_OK;
+}
+
+template <typename T>
+int trsm_blk(T* A, int n, int r0, int w, int cb, int ce, cudaStream_t st) {
+  return trsm_blk_batched<T>(&A, 1, n, r0, w, cb, ce, st);
 }
 
 // C -= L U on the tensor cores in the factorisation's product mode when K is
@@ -1035,9 +1059,9 @@ int lu_factor_batched_device(T* const* As, int B, int n, int32_t* const* ipivs, 
           float2* Cs[kMaxBatch];
           const float2* Ls[kMaxBatch];
           const float2* Us[kMaxBatch];
+          TT_TRY(trsm_blk_batched<T>(As, B, n, j0, w, j0 + w, m0 + mw, st, mode, WB, plane));
           for (int b = 0; b < B; b++) {
             float2* A = reinterpret_cast<float2*>(As[b]);
-            TT_TRY(trsm_blk(As[b], n, j0, w, j0 + w, m0 + mw, st, mode, WB + plane * b));
             Cs[b] = A + (size_t)(j0 + w) * n + (j0 + w);
             Ls[b] = A + (size_t)(j0 + w) * n + j0;
             Us[b] = A + (size_t)j0 * n + (j0 + w);
