@@ -29,7 +29,7 @@
 //               coalesced C -= acc store
 // Every mbarrier wait is bounded in time; on expiry the kernel records an
 // error code, drains its own copies in flight, frees TMEM and returns.
-// No TMA load here uses cluster multicast.
+// Every TMA copy here lands in the shared memory of the CTA that issues it.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 // Barriers: both CTAs' copies of a stage complete on the first CTA's full[s]
 // (expect_tx of both CTAs' bytes there); the MMA's commit arrives on empty[s]
 // of both CTAs; acc_full is committed to both; each CTA's epilogue warps arrive
-// on the first CTA's acc_empty.  The copies are plain (no multicast) loads.
+// on the first CTA's acc_empty.  Each copy lands in its issuing CTA only.
 template <int MODE>
 struct PairCfg {
   static constexpr int A_TILE = Cfg<MODE>::A_TILE;            // 128 rows
@@ -483,7 +483,7 @@ __device__ __forceinline__ void cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 // 2D tile copy into this CTA's shared memory completing on an mbarrier of the
-// pair's first CTA (cluster address); not a multicast copy
+// pair's first CTA (cluster address); one destination CTA
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t cluster_bar, int x,
                                                  int y) {
   asm volatile(
