@@ -53,12 +53,14 @@ struct ProfScope {
 // cudaFree of tens of GB take 5-35 ms each.  A cached block serves a request
 // of at most its size and at least two thirds of it.  Releasing a block waits
 // for the device, as cudaFree does, so a block is idle when it is handed out
-// again.  Cached blocks are freed when an allocation would otherwise fail, by
-// device_cache_trim(), and by tt_run_destroy / tt_release_cached_device_memory.
+// again.  When an allocation would otherwise fail, cached blocks are freed
+// one at a time, the longest-held first, until it succeeds; device_cache_trim(),
+// tt_run_destroy and tt_release_cached_device_memory free all of them.
 constexpr size_t kCacheMinBytes = size_t(256) << 20;
 void* device_cache_take(size_t bytes, size_t* capacity);
 void device_cache_give(void* p, size_t capacity);
 size_t device_cache_bytes();  // cached on the current device
+size_t device_cache_evict_one();  // frees the longest-held block; its bytes (0: none)
 void device_cache_trim();     // frees the current device's cached blocks
 
 // Owning device buffer.  alloc() reports NOMEM through the status path instead
@@ -112,9 +114,8 @@ struct DevBuf {
       }
     }
     cudaError_t e = cudaMalloc((void**)&ptr, bytes);
-    if (e == cudaErrorMemoryAllocation && device_cache_bytes() > 0) {
+    while (e == cudaErrorMemoryAllocation && device_cache_evict_one() > 0) {
       cudaGetLastError();
-      device_cache_trim();
       e = cudaMalloc((void**)&ptr, bytes);
     }
     if (e != cudaSuccess) {

@@ -58,6 +58,19 @@ size_t device_cache_bytes() {
   return s;
 }
 
+size_t device_cache_evict_one() {
+  std::pair<void*, size_t> b{nullptr, 0};
+  {
+    std::lock_guard<std::mutex> lk(cache_mu());
+    auto& v = cache()[current_device()];
+    if (v.empty()) return 0;
+    b = v.front();  // the block released longest ago
+    v.erase(v.begin());
+  }
+  cudaFree(b.first);
+  return b.second;
+}
+
 void device_cache_trim() {
   std::vector<std::pair<void*, size_t>> v;
   {
