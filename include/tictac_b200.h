@@ -93,6 +93,17 @@ typedef struct tt_os_indexing {
   int num_deuteron_states;
 } tt_os_indexing;
 
+/* Breakup indexing, the include_breakup_channels fields of
+ * channel_os_indexing (CPP/type_defs.h:82-84) as find_on_shell_bins fills
+ * them (CPP/run_organizer.cpp:134-339): the cells of energy j are
+ * q_com_BU_idx_array[j] .. q_com_BU_idx_array[j+1]-1, cell b is
+ * (alpha, q bin, p bin) = alphapq_idx_array[3b .. 3b+2]. */
+typedef struct tt_bu_indexing {
+  int num_BU_chns;
+  const int* q_com_BU_idx_array; /* [num_T_lab + 1] */
+  const int* alphapq_idx_array;  /* [3 num_BU_chns] */
+} tt_bu_indexing;
+
 /* The run_params fields (CPP/type_defs.h:87-123) the three functions read,
  * plus the precision controls of this implementation. */
 typedef struct tt_run_params {
@@ -175,6 +186,22 @@ int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double*
                                const size_t* P123_colptr_csc, size_t P123_nnz, const double* V_WP_unco,
                                const double* V_WP_coup, const tt_swp_states* swp, const tt_os_indexing* os,
                                const tt_pw_states* pw, const tt_run_params* rp, tt_solve_report* report);
+
+/* solve_faddeev_equations with its breakup output U_BU (CPP/solve_faddeev.h:25-38
+ * with include_breakup_channels=true): U as tt_solve_faddeev_equations, and
+ * U_BU[d*num_BU_chns + b] (caller allocates nd*num_BU_chns) for deuteron state
+ * d and breakup cell b of bu, read off the on-shell rows of A (G A)^n at the
+ * cell's column and Pade-resummed with the elastic criteria
+ * (CPP/solve_faddeev.cpp:867-890, 1176-1205, 1299-1407).  The reference
+ * computes breakup amplitudes on its Pade path only: rp->precision must be
+ * TT_PRECISION_PADE, else TT_ERR_UNSUPPORTED.  A cell outside the grid (the
+ * neighbour of an edge cell, bin -1 or N) gets NaN; the reference reads a
+ * neighbouring element of its row storage there. */
+int tt_solve_faddeev_equations_breakup(tt_complex* U, tt_complex* U_BU, const tt_bu_indexing* bu, const tt_complex* G,
+                                       const double* P123_val, const int* P123_row, const size_t* P123_colptr_csc,
+                                       size_t P123_nnz, const double* V_WP_unco, const double* V_WP_coup,
+                                       const tt_swp_states* swp, const tt_os_indexing* os, const tt_pw_states* pw,
+                                       const tt_run_params* rp, tt_solve_report* report);
 
 /* Adjoint of tt_solve_faddeev_equations (no counterpart in the reference):
  * besides U, the derivatives dU/dtheta_k for n_theta perturbations of the
@@ -410,6 +437,25 @@ int tt_run_get_host_array(const tt_run* run, int chn, int which, void* buf, size
 
 /* U-matrix text table in the reference's format (disk_io_routines.cpp:759-913). */
 int tt_run_write_U_table(const tt_run* run, int chn, const tt_complex* U, const char* path);
+
+/* Breakup cells of channel chn for the run's energies (the
+ * include_breakup_channels part of find_on_shell_bins,
+ * CPP/run_organizer.cpp:134-339; located at tt_run_create when the run was
+ * made with include_breakup_channels=true, else on this call).  *num_cells
+ * always; start[num_energies + 1] and cells[3 num_cells] = (alpha, q bin,
+ * p bin) in the reference's order when not NULL.  Host work only. */
+int tt_run_breakup_cells(const tt_run* run, int chn, int* num_cells, int* start, int* cells);
+
+/* Pade solve (TT_PRECISION_PADE) of all the run's energies of channel chn
+ * with the breakup amplitudes: U as tt_run_solve, U_BU[d*num_cells + b] as
+ * tt_solve_faddeev_equations_breakup (caller allocates nd*num_cells). */
+int tt_run_solve_breakup(tt_run* run, int chn, tt_complex* U, tt_complex* U_BU, tt_solve_report* report);
+
+/* Breakup U-matrix text table in the reference's format
+ * (restructure_breakup_data + store_U_BU_matrix_elements_txt,
+ * disk_io_routines.cpp:341-706); boundaries of a cell outside the grid are
+ * written as nan.  Host work only. */
+int tt_run_write_U_BU_table(const tt_run* run, int chn, const tt_complex* U_BU, const char* path);
 
 #ifdef __cplusplus
 }

@@ -235,3 +235,139 @@ def pade_solve(A, G, q_idx, deut, Nq, Np):
                 conv[e] = True
                 best[e] = idx_best
     return np.array([pa[e, best[e]] for e in range(nel)])
+
+
+# ---------------------------------------------------------------------------
+# Breakup amplitudes (include_breakup_channels=true).  The reference locates,
+# per on-shell energy, the (alpha, q, p) wave-packet cells whose energy range
+# holds E_com, plus three neighbours chosen by the quadrant of the cell that
+# E_com falls in (find_on_shell_bins, CPP/run_organizer.cpp:134-339), and
+# reads their amplitudes off the same on-shell rows of A (G A)^n as the
+# elastic ones, each Pade-resummed with the elastic criteria
+# (CPP/solve_faddeev.cpp:867-890, 1176-1205, 1299-1407).
+
+M_P, M_N = 938.272, 939.565
+
+
+def mu1_free():
+    """kinetic_conversion.cpp:16-19"""
+    M12 = M_P + M_N
+    return M_N * M12 / (M_N + M12)
+
+
+def breakup_cells(Na, Np, Nq, q_WP, e_swp, e_off, E_com, E_bound):
+    """start[nE+1] and cells[num][3] = (alpha, q, p) in the reference's order.
+    Neighbour bins may lie outside 0..N-1 at the grid's edge, as there."""
+    start, cells = [0], []
+    mu = mu1_free()
+    for E in E_com:
+        if E + E_bound < 0:
+            start.append(len(cells))
+            continue
+        found = False
+        for a in range(Na):
+            e = e_swp[e_off[a]:e_off[a] + Np + 1]
+            for qi in range(Nq):
+                Eql = 0.5 * (q_WP[qi] * q_WP[qi]) / mu
+                Equ = 0.5 * (q_WP[qi + 1] * q_WP[qi + 1]) / mu
+                for pi in range(Np):
+                    Epl, Epu = e[pi], e[pi + 1]
+                    Ecl, Ecu = Epl + Eql, Epu + Equ
+                    if not (Ecl <= E <= Ecu and Epl >= 0 and Epu >= 0):
+                        continue
+                    found = True
+                    cells.append((a, qi, pi))
+                    Ep, Eq = 0.5 * (Epu + Epl), 0.5 * (Equ + Eql)
+                    if Eq + Ep <= E <= Ecu:
+                        pr, qr = (pi, pi + 1), (qi, qi + 1)
+                    elif Eq + Epl <= E <= Ep + Equ:
+                        pr, qr = (pi - 1, pi), (qi, qi + 1)
+                    elif Ecl <= E <= Eq + Ep:
+                        pr, qr = (pi - 1, pi), (qi - 1, qi)
+                    elif Eql + Ep <= E <= Epu + Eq:
+                        pr, qr = (pi, pi + 1), (qi - 1, qi)
+                    else:
+                        continue
+                    for p2 in range(pr[0], pr[1] + 1):
+                        for q2 in range(qr[0], qr[1] + 1):
+                            if p2 != pi or q2 != qi:
+                                cells.append((a, q2, p2))
+        if not found:
+            raise ValueError(f"on-shell energy {E} outside the WP state space")
+        start.append(len(cells))
+    return np.array(start, dtype=np.int32), np.array(cells, dtype=np.int32).reshape(-1, 3)
+
+
+def pade_solve_breakup(A, G, q_idx, deut, Nq, Np, start, cells):
+    """pade_solve plus the breakup amplitudes U_BU[d * num + b] of the cells
+    (NaN for a cell outside the grid).  Also returns whether the reference's
+    loop test (solve_faddeev.cpp:921: stop when elastic + breakup elements
+    converged equal the number of elastic elements) would stop it with
+    elements still open, where the reference then reads an unset index."""
+    n = A.shape[0]
+    Na = n // (Nq * Np)
+    G = np.asarray(G, dtype=np.complex128).reshape(len(q_idx), n)
+    nE, nd, nb = len(q_idx), len(deut), len(cells)
+    rows = [deut[d] * Nq * Np + q_idx[j] * Np for d in range(nd) for j in range(nE)]
+    R = A[rows, :].astype(np.complex128)
+    e_of = np.zeros(nb, dtype=int)
+    for j in range(nE):
+        e_of[start[j]:start[j + 1]] = j
+    inside = [(0 <= c[0] < Na and 0 <= c[1] < Nq and 0 <= c[2] < Np) for c in cells]
+    # element list: elastic (d', d, j) first, then breakup (d, b) over in-grid cells
+    pick = [(dr * nE + j, deut[dc] * Nq * Np + q_idx[j] * Np) for dr in range(nd) for dc in range(nd)
+            for j in range(nE)]
+    nel_el = len(pick)
+    bu_el = []
+    for d in range(nd):
+        for b in range(nb):
+            if inside[b]:
+                a, q, p = (int(x) for x in cells[b])
+                bu_el.append(d * nb + b)
+                pick.append((d * nE + e_of[b], a * Nq * Np + q * Np + p))
+    nel = len(pick)
+    a = np.zeros((nel, 2 * NM_MAX + 1), dtype=np.complex128)
+    pa = np.zeros((nel, NM_MAX + 1), dtype=np.complex128)
+    conv = np.zeros(nel, dtype=bool)
+    best = np.zeros(nel, dtype=int)
+    early_stop = False
+
+    def extract(nterm):
+        for e in range(nel):
+            if not conv[e]:
+                a[e, nterm] = R[pick[e][0], pick[e][1]]
+
+    extract(0)
+    for NM in range(NM_MAX + 1):
+        if conv.all():
+            break
+        if conv.sum() == nel_el and nb:
+            early_stop = True
+        for nterm in (2 * NM - 1, 2 * NM):
+            if nterm <= 0:
+                continue
+            for dr in range(nd):
+                for j in range(nE):
+                    R[dr * nE + j] = (R[dr * nE + j] * G[j]) @ A
+            extract(nterm)
+        for e in range(nel):
+            if conv[e]:
+                continue
+            pa[e, NM] = pade_approximant(a[e], NM, NM)
+            idx_best, min_diff = 0, 1.0
+            for prev in range(NM):
+                d = abs(pa[e, prev] - pa[e, prev - 1])
+                if min_diff > d > 1e-15:
+                    idx_best, min_diff = prev, d
+            d = abs(pa[e, NM] - pa[e, NM - 1])
+            if min_diff > d > 1e-15:
+                idx_best, min_diff = NM, d
+            if NM == NM_MAX or NM - idx_best > 4 or min_diff < 1e-6 * abs(pa[e, idx_best]) or min_diff < 1e-7:
+                conv[e] = True
+                best[e] = idx_best
+    U = np.array([pa[e, best[e]] for e in range(nel_el)])
+    U_BU = np.full(nd * nb, np.nan + 1j * np.nan)
+    for k, slot in enumerate(bu_el):
+        e = nel_el + k
+        U_BU[slot] = pa[e, best[e]]
+    return U, U_BU, early_stop

@@ -5,6 +5,8 @@
 //
 //   tictac_ref dump <outdir> [--solver=reference|replica|pade] key=value ...
 //   tictac_ref time <outdir> [--channel=k] [--sample_cols=m] [--repeat=r] key=value ...
+//
+// --channel=k also restricts dump to channel k.
 //   tictac_ref info <outdir> key=value ...
 //
 // time: the dense solve of the selected channel (A columns once, then per
@@ -36,6 +38,7 @@
 #include "General_functions/matrix_routines.h"
 #include "Interactions/potential_model.h"
 #include "constants.h"
+#include "disk_io_routines.h"
 #include "make_permutation_matrix.h"
 #include "make_potential_matrix.h"
 #include "make_pw_symm_states.h"
@@ -217,7 +220,7 @@ int main(int argc, char** argv) {
   meta << "E_bound " << swp.E_bound << "\nn_chn " << pw.N_chn_3N << "\n";
 
   for (int chn = 0; chn < pw.N_chn_3N; chn++) {
-    if (mode == "time" && time_channel >= 0 && chn != time_channel) continue;
+    if ((mode == "time" || mode == "dump") && time_channel >= 0 && chn != time_channel) continue;
     pw_3N_statespace sub = substates(pw, chn);
     const size_t n = (size_t)sub.Nalpha * Nq * Np;
     std::vector<int> pwtab;
@@ -274,8 +277,21 @@ int main(int argc, char** argv) {
 
     std::vector<cdouble> U(nE * nd * nd + 1);
     if (mode == "dump" && (solver == "reference" || solver == "pade")) {
-      solve_faddeev_equations(U.data(), nullptr, G.data(), val, row, colptr.data(), nnz, Vu.data(), Vc.data(), swp, os,
-                              sub, "_ref", rp);
+      // include_breakup_channels=true: the breakup cells find_on_shell_bins
+      // located (run_organizer.cpp:136-339) and their Pade amplitudes
+      // (solve_faddeev.cpp:867-890, 1176-1205, 1299-1407), U_BU[d*num_BU + b];
+      // main.cpp:416-419 allocates num_T_lab * num_BU, the larger size is taken here
+      std::vector<cdouble> U_BU;
+      const size_t nbu = rp.include_breakup_channels ? (size_t)os.num_BU_chns : 0;
+      if (rp.include_breakup_channels) U_BU.assign(std::max(nE, nd) * nbu + 1, cdouble(0.0, 0.0));
+      solve_faddeev_equations(U.data(), rp.include_breakup_channels ? U_BU.data() : nullptr, G.data(), val, row,
+                              colptr.data(), nnz, Vu.data(), Vc.data(), swp, os, sub, "_ref", rp);
+      if (rp.include_breakup_channels) {
+        dump("bu_start" + tag, os.q_com_BU_idx_array, nE + 1);
+        dump("bu_cells" + tag, os.alphapq_idx_array, 3 * nbu);
+        dump("U_BU" + tag, U_BU.data(), nd * nbu);
+        store_U_BU_matrix_elements_txt(U_BU.data(), cfg, os, rp, fwp, swp, sub, g_out + "/U_BU" + tag + ".txt");
+      }
     } else {
       // the dense solver's steps (solve_faddeev.cpp:305-438) without its text dumps
       double** CT = new double*[sub.Nalpha * sub.Nalpha];
@@ -351,6 +367,7 @@ int main(int argc, char** argv) {
       delete[] VC;
     }
     dump("U" + tag, U.data(), nE * nd * nd);
+    meta.flush();
     delete[] val;
     delete[] row;
     delete[] col;

@@ -9,7 +9,8 @@ resolvents, on-shell U) into one .npz per case.
     make -C oracle ref && python tests/golden/make_golden.py [--pade | --large]
 
 (--pade regenerates only the Pade fixtures <case>_pade.npz; --large only the
-summary fixtures of the bench-sized cases, <case>.npz with U and checksums.)
+summary fixtures of the bench-sized cases, <case>.npz with U and checksums;
+--breakup only the breakup fixtures <case>_breakup.npz.)
 
 Test infrastructure only; the product never reads these files.
 """
@@ -172,12 +173,50 @@ def run_large(name, opts):
         print(name, "channels", len(meta["channels"]), "n", [ch["n"] for ch in meta["channels"]],
               "nnz", [ch["nnz"] for ch in meta["channels"]])
 
+# Breakup channels (include_breakup_channels=true, Pade path): per channel the
+# cells find_on_shell_bins located (bu_start, bu_cells), their amplitudes
+# U_BU[d * num + b], the elastic U of the same run and, for the channels named
+# in "tables", the reference's own breakup table text.  Channel 3 of
+# lo_j1_J3_n8 is left out: there the reference's Pade loop stops when the
+# elastic plus breakup elements converged equal the number of elastic elements
+# (CPP/solve_faddeev.cpp:921) with elastic elements still open, and reads an
+# unset approximant index for them (the run ends in a segmentation fault).
+BREAKUP_CASES = {
+    "mt_swave_n16": dict(channels=[0], tables=[0]),
+    "lo_j1_J3_n8": dict(channels=[0, 1, 2], tables=[0]),
+}
+
+
+def run_breakup(name, opts, channels, tables):
+    data = {"channels": np.array(channels, dtype=np.int32)}
+    for c in channels:
+        with tempfile.TemporaryDirectory() as out:
+            args = [REF_BIN, "dump", out, "--solver=pade", f"--channel={c}", "include_breakup_channels=true"] + \
+                [f"{k}={v}" for k, v in opts.items()]
+            subprocess.run(args, check=True, cwd=out, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 4)))
+            t = f"_c{c}"
+            data["bu_start" + t] = np.fromfile(os.path.join(out, f"bu_start{t}.bin"), dtype=np.int32)
+            data["bu_cells" + t] = np.fromfile(os.path.join(out, f"bu_cells{t}.bin"), dtype=np.int32).reshape(-1, 3)
+            data["U_BU" + t] = np.fromfile(os.path.join(out, f"U_BU{t}.bin"), dtype=np.complex128)
+            data["U_pade" + t] = np.fromfile(os.path.join(out, f"U{t}.bin"), dtype=np.complex128)
+            if c in tables:
+                with open(os.path.join(out, f"U_BU{t}.txt")) as f:
+                    data["table" + t] = np.array(f.read())
+    np.savez_compressed(os.path.join(HERE, f"{name}_breakup.npz"), **data)
+    print(name, "breakup channels", channels, "cells", [len(data[f"bu_cells_c{c}"]) for c in channels])
+
+
 if __name__ == "__main__":
     if not os.path.exists(REF_BIN):
         sys.exit(f"{REF_BIN} missing: run `make -C oracle ref` first")
     if "--large" in sys.argv:
         for name, opts in LARGE_CASES.items():
             run_large(name, opts)
+        sys.exit(0)
+    if "--breakup" in sys.argv:
+        for name, sel in BREAKUP_CASES.items():
+            run_breakup(name, CASES[name], **sel)
         sys.exit(0)
     only_pade = "--pade" in sys.argv
     for name, opts in CASES.items():

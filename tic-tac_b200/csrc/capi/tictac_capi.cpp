@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../cuda/tt_kernels.h"
+#include "../host/tt_breakup.h"
 #include "../host/tt_h5.h"
 #include "../host/tt_host.h"
 #include "../host/tt_math.h"
@@ -157,8 +158,18 @@ int dvc_blocks(const RunParams& rp, const PWChannel& ch, const SWPStates& w, int
 int dropin_solve(tt_complex* U, tt_complex* dU, int n_theta, const double* dVu, const double* dVc,
                  const tt_complex* G, const double* P_val, const int* P_row, const size_t* P_colptr, size_t P_nnz,
                  const double* V_unco, const double* V_coup, const tt_swp_states* swp, const tt_os_indexing* os,
-                 const tt_pw_states* pw, const tt_run_params* rpp, tt_solve_report* report) {
+                 const tt_pw_states* pw, const tt_run_params* rpp, tt_solve_report* report,
+                 const tt_bu_indexing* bui = nullptr, tt_complex* U_BU = nullptr) {
   if (!U || !G || !P_colptr || !swp || !os || !pw || !rpp) return fail(TT_ERR_BADARG, "null argument");
+  BreakupCells cells;
+  if (bui) {
+    if (rpp->precision != TT_PRECISION_PADE)
+      return fail(TT_ERR_UNSUPPORTED, "breakup amplitudes come from the Pade path (TT_PRECISION_PADE), as in the reference");
+    if (bui->num_BU_chns < 0 || !bui->q_com_BU_idx_array || (bui->num_BU_chns > 0 && (!bui->alphapq_idx_array || !U_BU)))
+      return fail(TT_ERR_BADARG, "null or negative breakup indexing");
+    cells.start.assign(bui->q_com_BU_idx_array, bui->q_com_BU_idx_array + os->num_T_lab + 1);
+    cells.cells.assign(bui->alphapq_idx_array, bui->alphapq_idx_array + (size_t)3 * bui->num_BU_chns);
+  }
   if (P_nnz && (!P_val || !P_row)) return fail(TT_ERR_BADARG, "null P123 arrays");
   if (n_theta < 0 || (n_theta > 0 && (!dU || !dVu || (swp->num_2N_coup_states && !dVc))))
     return fail(TT_ERR_BADARG, "null or negative adjoint arguments");
@@ -209,11 +220,17 @@ int dropin_solve(tt_complex* U, tt_complex* dU, int n_theta, const double* dVu, 
     adj.vc_count = per;
     adj.dU = &dUh;
   }
-  s = cs.solve(q_idx, deut, options_of(rp, rpp->precision), Uh, &rep, st, n_theta > 0 ? &adj : nullptr);
+  std::vector<double> UBh;
+  BreakupRequest bq;
+  bq.cells = &cells;
+  bq.U_BU = &UBh;
+  s = cs.solve(q_idx, deut, options_of(rp, rpp->precision), Uh, &rep, st, n_theta > 0 ? &adj : nullptr,
+               bui ? &bq : nullptr);
   fill_report(rep, msA, report);
   if (s != TT_OK) return s;
   std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
   if (n_theta > 0) std::memcpy(dU, dUh.data(), sizeof(double) * dUh.size());
+  if (bui && !UBh.empty()) std::memcpy(U_BU, UBh.data(), sizeof(double) * UBh.size());
   return TT_OK;
 }
 
@@ -226,6 +243,7 @@ struct tt_run {
   std::vector<double> V_unco, V_coup;
   SWPStates swp;
   OnShell os;
+  std::vector<BreakupCells> bu;  // per channel, when include_breakup_channels=true
   std::vector<ChannelState> chn;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -366,6 +384,16 @@ int tt_solve_faddeev_equations(tt_complex* U, const tt_complex* G, const double*
                       rpp, report);
 }
 
+int tt_solve_faddeev_equations_breakup(tt_complex* U, tt_complex* U_BU, const tt_bu_indexing* bu, const tt_complex* G,
+                                       const double* P_val, const int* P_row, const size_t* P_colptr, size_t P_nnz,
+                                       const double* V_unco, const double* V_coup, const tt_swp_states* swp,
+                                       const tt_os_indexing* os, const tt_pw_states* pw, const tt_run_params* rp,
+                                       tt_solve_report* report) {
+  if (!bu) return fail(TT_ERR_BADARG, "null breakup indexing");
+  return dropin_solve(U, nullptr, 0, nullptr, nullptr, G, P_val, P_row, P_colptr, P_nnz, V_unco, V_coup, swp, os, pw,
+                      rp, report, bu, U_BU);
+}
+
 int tt_solve_faddeev_adjoint(tt_complex* U, tt_complex* dU, int n_theta, const double* dVu, const double* dVc,
                              const tt_complex* G, const double* P_val, const int* P_row, const size_t* P_colptr,
                              size_t P_nnz, const double* V_unco, const double* V_coup, const tt_swp_states* swp,
@@ -394,6 +422,12 @@ int tt_run_create(tt_run** out, int nopt, const char* const* opts) {
   if (!potential_matrices(r->rp, r->fwp, r->pw, r->V_unco, r->V_coup, &err)) return fail(TT_ERR_BADARG, err);
   if (!make_swp_states(r->rp, r->fwp, r->pw, r->V_unco, r->V_coup, r->swp, &err)) return fail(TT_ERR_BADARG, err);
   if (!find_on_shell_bins(r->rp, r->swp, r->os, &err)) return fail(TT_ERR_BADARG, err);
+  if (r->rp.include_breakup_channels) {  // located with the elastic bins, as in the reference
+    r->bu.resize(r->pw.N_chn_3N);
+    for (int c = 0; c < r->pw.N_chn_3N; c++)
+      if (!find_breakup_cells(r->rp, channel_view(r->pw, c), r->swp, r->os.E_com, r->bu[c], &err))
+        return fail(TT_ERR_BADARG, err);
+  }
   r->chn.resize(r->pw.N_chn_3N);
   *out = r.release();
   return TT_OK;
@@ -928,6 +962,82 @@ int tt_run_write_U_table(const tt_run* run, int chn, const tt_complex* U, const 
   return TT_OK;
 }
 
+
+// ---- breakup channels ----
+
+// the channel's breakup cells: those located at creation, else located now
+static int run_breakup_cells(const tt_run* run, int chn, BreakupCells& out, const BreakupCells** cells) {
+  if (!run->bu.empty()) {
+    *cells = &run->bu[chn];
+    return TT_OK;
+  }
+  std::string err;
+  if (!find_breakup_cells(run->rp, channel_view(run->pw, chn), run->swp, run->os.E_com, out, &err))
+    return fail(TT_ERR_BADARG, err);
+  *cells = &out;
+  return TT_OK;
+}
+
+int tt_run_breakup_cells(const tt_run* run, int chn, int* num_cells, int* start, int* cells) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!num_cells) return fail(TT_ERR_BADARG, "null num_cells");
+  BreakupCells local;
+  const BreakupCells* bu = nullptr;
+  TT_TRY(run_breakup_cells(run, chn, local, &bu));
+  *num_cells = bu->count();
+  if (start) std::memcpy(start, bu->start.data(), sizeof(int) * bu->start.size());
+  if (cells) std::memcpy(cells, bu->cells.data(), sizeof(int) * bu->cells.size());
+  return TT_OK;
+}
+
+int tt_run_solve_breakup(tt_run* run, int chn, tt_complex* U, tt_complex* U_BU, tt_solve_report* report) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!U || !U_BU) return fail(TT_ERR_BADARG, "null U or U_BU");
+  BreakupCells local;
+  const BreakupCells* bu = nullptr;
+  TT_TRY(run_breakup_cells(run, chn, local, &bu));
+  double msA = 0;
+  if (!run->chn[chn].have_A) TT_TRY(tt_run_build_A(run, chn, &msA));
+  if (!run->chn[chn].have_G) TT_TRY(tt_run_build_resolvent(run, chn));
+  const std::vector<int> deut = deuteron_indices(channel_view(run->pw, chn));
+  std::vector<double> Uh, UBh;
+  BreakupRequest bq;
+  bq.cells = bu;
+  bq.U_BU = &UBh;
+  SolveReport rep;
+  s = run->chn[chn].solver->solve(run->os.q_com_idx, deut, options_of(run->rp, TT_PRECISION_PADE), Uh, &rep,
+                                  run_stream(run), nullptr, &bq);
+  fill_report(rep, msA, report);
+  if (s != TT_OK) return s;
+  std::memcpy(U, Uh.data(), sizeof(double) * Uh.size());
+  if (!UBh.empty()) std::memcpy(U_BU, UBh.data(), sizeof(double) * UBh.size());
+  return TT_OK;
+}
+
+int tt_run_write_U_BU_table(const tt_run* run, int chn, const tt_complex* U_BU, const char* path) {
+  int s = check_chn(run, chn);
+  if (s) return s;
+  if (!path) return fail(TT_ERR_BADARG, "null path");
+  BreakupCells local;
+  const BreakupCells* bu = nullptr;
+  TT_TRY(run_breakup_cells(run, chn, local, &bu));
+  BreakupTableInput in;
+  in.rp = &run->rp;
+  in.ch = channel_view(run->pw, chn);
+  in.swp = &run->swp;
+  in.os = &run->os;
+  in.deut = deuteron_indices(in.ch);
+  in.bu = bu;
+  if (!U_BU && !in.deut.empty() && bu->count() > 0) return fail(TT_ERR_BADARG, "null U_BU");
+  in.U_BU = reinterpret_cast<const double*>(U_BU);
+  std::ofstream f(path);
+  if (!f) return fail(TT_ERR_IO, std::string("cannot open ") + path);
+  std::string err;
+  if (!write_breakup_table(f, in, &err)) return fail(TT_ERR_BADARG, err);
+  return f ? TT_OK : fail(TT_ERR_IO, std::string("write failed: ") + path);
+}
 
 // ---- P123 files in the reference's HDF5 layout ----
 

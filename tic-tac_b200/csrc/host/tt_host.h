@@ -5,6 +5,7 @@
 // device stages depends on them bit-for-bit, so each function restates the
 // reference routine it cites with the same arithmetic.
 #pragma once
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -46,6 +47,7 @@ struct RunParams {
   bool solve_dense = false;
   bool production_run = true;
   bool swave_only = false;          // the reference's commented-out s-wave filter (make_pw_symm_states.cpp:176-179)
+  bool include_breakup_channels = false;  // breakup cells located per channel, amplitudes from the Pade solve
   std::string potential_model = "LO_internal";
   std::string energy_input_file = "lab_energies.txt";
   std::string output_folder = "Output";
@@ -152,8 +154,30 @@ struct OnShell {
 bool find_on_shell_bins(const RunParams& rp, const SWPStates& swp, OnShell& os, std::string* err);
 std::vector<int> deuteron_indices(const PWChannel& ch);
 
+// Breakup on-shell cells of one channel (the include_breakup_channels part of
+// find_on_shell_bins, CPP/run_organizer.cpp:134-339): for every on-shell
+// energy at or above the breakup threshold (E_com + E_bound >= 0), each
+// (alpha, q, p) wave-packet cell whose energy range [e_p + E_q, e_{p+1} +
+// E_{q+1}] (E_q = q^2 / (2 mu1_free)) holds E_com with both p boundaries
+// >= 0, followed by the three neighbours on the side of the cell's quadrant
+// that holds E_com.  The order and the repeats are the reference's; a
+// neighbour of an edge cell can lie outside the grid (bin -1 or N).
+struct BreakupCells {
+  std::vector<int32_t> start;  // [nE + 1]: energy j owns cells start[j] .. start[j+1]-1
+  std::vector<int32_t> cells;  // 3 per cell: alpha, q bin, p bin
+  int count() const { return (int)(cells.size() / 3); }
+  bool inside(int b, int Nalpha, int Nq, int Np) const {
+    const int32_t* c = &cells[(size_t)3 * b];
+    return c[0] >= 0 && c[0] < Nalpha && c[1] >= 0 && c[1] < Nq && c[2] >= 0 && c[2] < Np;
+  }
+};
+bool find_breakup_cells(const RunParams& rp, const PWChannel& ch, const SWPStates& swp,
+                        const std::vector<double>& E_com, BreakupCells& bu, std::string* err);
+
 // Kinematics, CPP/General_functions/kinetic_conversion.cpp:5-54.
 double mu1(double Eb);
+double mu1_free();
+double com_energy_to_com_p_momentum(double Ep);
 double com_momentum_to_lab_energy(double q_com, double Eb);
 double lab_energy_to_com_momentum(double T_lab, double Eb);
 double com_energy_to_com_q_momentum(double E_com);

@@ -272,12 +272,27 @@ cd pade_approximant(const cd* a, int N, int M, cd z) {
 // reference's criteria (N = 14; no better difference in the last 4 orders;
 // smallest difference of consecutive approximants < 1e-6 |best| or < 1e-7).
 int ChannelSolver::solve_pade(const std::vector<int>& q_idx, const std::vector<int>& deut, std::vector<double>& U,
-                              SolveReport& r, cudaStream_t st) {
+                              SolveReport& r, cudaStream_t st, const BreakupRequest* bu) {
   constexpr int NM_MAX = 14, NTERMS = 2 * NM_MAX + 1;
   auto t0 = std::chrono::steady_clock::now();
   const int nE = (int)q_idx.size(), nd = (int)deut.size();
   const int Nq = L_.Nq, Np = L_.Np;
-  const int nrows = nd * nE, nel = nd * nd * nE;
+  const int nrows = nd * nE, nel_el = nd * nd * nE;
+  // breakup elements (d, cell) of the cells inside the grid follow the
+  // elastic ones; bu_slot maps them to U_BU's [d][cell] index
+  const BreakupCells* cells = bu ? bu->cells : nullptr;
+  const int nb = cells ? cells->count() : 0;
+  std::vector<int32_t> bu_row, bu_col, bu_slot;
+  for (int d = 0; d < nd && nb; d++)
+    for (int j = 0; j < nE; j++)
+      for (int b = cells->start[j]; b < cells->start[j + 1]; b++) {
+        if (!cells->inside(b, L_.Nalpha, Nq, Np)) continue;
+        const int32_t* c = &cells->cells[(size_t)3 * b];
+        bu_row.push_back(d * nE + j);
+        bu_col.push_back(c[0] * Nq * Np + c[1] * Np + c[2]);
+        bu_slot.push_back(d * nb + b);
+      }
+  const int nel = nel_el + (int)bu_slot.size();
   std::vector<int32_t> rows(nrows), erow(nrows), prow(nel), pcol(nel);
   for (int d = 0; d < nd; d++)
     for (int j = 0; j < nE; j++) {
@@ -291,6 +306,15 @@ int ChannelSolver::solve_pade(const std::vector<int>& q_idx, const std::vector<i
         prow[e] = dr * nE + j;
         pcol[e] = deut[dc] * Nq * Np + q_idx[j] * Np;
       }
+  for (size_t k = 0; k < bu_slot.size(); k++) {
+    prow[nel_el + k] = bu_row[k];
+    pcol[nel_el + k] = bu_col[k];
+  }
+  for (int e = 0; e < nel; e++)  // every picked element inside the on-shell rows of R
+    if (prow[e] < 0 || prow[e] >= nrows || pcol[e] < 0 || pcol[e] >= n) {
+      set_error("Pade element outside the on-shell rows");
+      return TT_ERR_BADARG;
+    }
   DevBuf<int32_t> d_rows, d_erow, d_prow, d_pcol;
   DevBuf<double> R, V, picked;
   TT_TRY(d_rows.upload(rows, st));
@@ -354,8 +378,9 @@ int ChannelSolver::solve_pade(const std::vector<int>& q_idx, const std::vector<i
   }
   for (int e = 0; e < nel; e++) {
     const cd v = pa[(size_t)e * (NM_MAX + 1) + best[e]];
-    U[2 * e + 0] = v.real();
-    U[2 * e + 1] = v.imag();
+    double* out = e < nel_el ? &U[2 * (size_t)e] : &(*bu->U_BU)[2 * (size_t)bu_slot[e - nel_el]];
+    out[0] = v.real();
+    out[1] = v.imag();
   }
   r.ms_solve += ms_since(t0);
   r.refine_iters = top;           // highest [N/N] order formed
@@ -466,8 +491,27 @@ int ChannelSolver::adjoint_energy(int j, int nE, int nd, const double* Gj, const
 }
 
 int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
-                         std::vector<double>& U, SolveReport* rep, cudaStream_t st, const AdjointRequest* adj) {
+                         std::vector<double>& U, SolveReport* rep, cudaStream_t st, const AdjointRequest* adj,
+                         const BreakupRequest* bu) {
   const int nE = (int)q_idx.size(), nd = (int)deut.size();
+  if (bu) {
+    if (!opt.pade) {
+      set_error("breakup amplitudes come from the Pade path, as in the reference");
+      return TT_ERR_UNSUPPORTED;
+    }
+    const BreakupCells* c = bu->cells;
+    if (!c || !bu->U_BU || c->start.size() != (size_t)nE + 1 || c->cells.size() % 3 || c->start[0] != 0 ||
+        c->start[nE] != c->count()) {
+      set_error("breakup cells do not match the solve's energies");
+      return TT_ERR_BADARG;
+    }
+    for (int j = 0; j < nE; j++)
+      if (c->start[j + 1] < c->start[j]) {
+        set_error("breakup cell offsets decrease");
+        return TT_ERR_BADARG;
+      }
+    bu->U_BU->assign((size_t)2 * nd * c->count(), std::nan(""));
+  }
   if (nE != nE_) {
     set_error("number of on-shell bins does not match the resolvent energies");
     return TT_ERR_BADARG;
@@ -499,7 +543,7 @@ int ChannelSolver::solve(const std::vector<int>& q_idx, const std::vector<int>& 
       set_error("the adjoint needs the LU path; the Pade series has no stored factors");
       return TT_ERR_UNSUPPORTED;
     }
-    const int s = solve_pade(q_idx, deut, U, r, st);
+    const int s = solve_pade(q_idx, deut, U, r, st, bu);
     if (rep) *rep = r;
     return s;
   }

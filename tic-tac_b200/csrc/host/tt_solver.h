@@ -77,6 +77,16 @@ struct AdjointRequest {
   double dlnmu1_dEb = 0;
 };
 
+// Breakup amplitudes wanted from a Pade solve (the reference computes them on
+// that path only, CPP/solve_faddeev.cpp:867-890, 1176-1205, 1299-1407): the
+// on-shell rows of A (G A)^n read at each cell's column alpha Nq Np + q Np + p
+// and resummed with the elastic criteria.  U_BU receives [nd][cells]
+// interleaved complex; a cell outside the grid gets NaN.
+struct BreakupRequest {
+  const BreakupCells* cells = nullptr;  // the cells of the solve's energies
+  std::vector<double>* U_BU = nullptr;
+};
+
 class ChannelSolver {
  public:
   int n = 0;
@@ -92,7 +102,7 @@ class ChannelSolver {
   // U[d'*nd*nE + d*nE + j] for each on-shell q bin j and deuteron states
   int solve(const std::vector<int>& q_idx, const std::vector<int>& deut, const SolveOptions& opt,
             std::vector<double>& U_interleaved, SolveReport* rep, cudaStream_t st,
-            const AdjointRequest* adj = nullptr);
+            const AdjointRequest* adj = nullptr, const BreakupRequest* bu = nullptr);
   // Adjoint of the last solve(keep_factors) from the factors it kept:
   // dU/dtheta of adj for its energies.  TT_ERR_UNSUPPORTED when nothing was
   // kept (the energies' factors did not fit at once): the caller then runs
@@ -114,7 +124,7 @@ class ChannelSolver {
 
  private:
   int solve_pade(const std::vector<int>& q_idx, const std::vector<int>& deut, std::vector<double>& U,
-                 SolveReport& r, cudaStream_t st);
+                 SolveReport& r, cudaStream_t st, const BreakupRequest* bu);
   int adjoint_energy(int j, int nE, int nd, const double* Gj, const int32_t* d_rows, const int32_t* d_perm,
                      double* tmp, const double* x, const SolveOptions& opt, void* F,
                      TrsvBlocks<float2>& tbT32, TrsvBlocks<double2>& tbT64, double* lam, double* yT, double* rT,

@@ -44,6 +44,9 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
     else if (key == "solve_dense") { if (!parse_bool(value, rp.solve_dense)) return bad("solve_dense"); }
     else if (key == "production_run") { if (!parse_bool(value, rp.production_run)) return bad("production_run"); }
     else if (key == "swave_only") { if (!parse_bool(value, rp.swave_only)) return bad("swave_only"); }
+    else if (key == "include_breakup_channels") {
+      if (!parse_bool(value, rp.include_breakup_channels)) return bad("include_breakup_channels");
+    }
     else if (key == "potential_model") rp.potential_model = value;
     else if (key == "energy_input_file") rp.energy_input_file = value;
     else if (key == "output_folder") rp.output_folder = value;
@@ -95,7 +98,7 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       std::string tok;
       while (std::getline(ss, tok, ',')) if (!tok.empty()) rp.lec_offsets.push_back(std::stod(tok));
     } else if (key == "subfolder" || key == "P123_omp_num_threads" || key == "P123_recovery" ||
-               key == "include_breakup_channels" || key == "parameter_walk" || key == "parameter_file" ||
+               key == "parameter_walk" || key == "parameter_file" ||
                key == "PSI_start" || key == "PSI_end" || key == "p_grid_filename" || key == "q_grid_filename") {
       // accepted for argument-surface compatibility; no effect on this path
     } else {

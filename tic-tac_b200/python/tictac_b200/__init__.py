@@ -42,7 +42,8 @@ EXPORTED_SYMBOLS = (
     "tt_store_P123_h5", "tt_read_P123_h5", "tt_P123_h5_filename", "tt_run_store_P123_h5", "tt_run_load_P123_h5",
     "tt_run_solve_energies", "tt_profile_select", "tt_run_adjoint_forward", "tt_run_adjoint_backward",
     "tt_run_swp_derivative", "tt_run_set_solve_option", "tt_release_cached_device_memory",
-    "tt_cached_device_memory",
+    "tt_cached_device_memory", "tt_solve_faddeev_equations_breakup", "tt_run_breakup_cells", "tt_run_solve_breakup",
+    "tt_run_write_U_BU_table",
 )
 
 PROFILE_CLASSES = ("tc_update", "subpanel", "trsv", "residual", "a_build", "panel_trsm", "operands", "laswp", "form_L",
@@ -76,6 +77,10 @@ class tt_swp_states(ctypes.Structure):
 class tt_os_indexing(ctypes.Structure):
     _fields_ = [("num_T_lab", c_int), ("q_com_idx_array", POINTER(c_int)), ("deuteron_idx_array", POINTER(c_int)),
                 ("num_deuteron_states", c_int)]
+
+
+class tt_bu_indexing(ctypes.Structure):
+    _fields_ = [("num_BU_chns", c_int), ("q_com_BU_idx_array", POINTER(c_int)), ("alphapq_idx_array", POINTER(c_int))]
 
 
 class tt_run_params(ctypes.Structure):
@@ -349,6 +354,37 @@ def solve_faddeev(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q_idx, de
     return U, rep.as_dict()
 
 
+def solve_faddeev_breakup(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q_idx, deut, pw: PW, bu_start, bu_cells,
+                          **rp_kw):
+    """tt_solve_faddeev_equations_breakup (the Pade path): the elastic U and the
+    breakup U_BU[d * num_cells + b] of the cells bu_cells[num][3] = (alpha, q, p),
+    bu_start[nE + 1] their offsets per energy."""
+    lib = load()
+    G = np.ascontiguousarray(G, dtype=np.complex128)
+    Pv = np.ascontiguousarray(P_val, dtype=np.float64)
+    Pr = np.ascontiguousarray(P_row, dtype=np.int32)
+    Pc = np.ascontiguousarray(P_colptr, dtype=np.uint64)
+    Vu = np.ascontiguousarray(V_unco, dtype=np.float64)
+    Vc = np.ascontiguousarray(V_coup if V_coup is not None and len(V_coup) else np.zeros(1), dtype=np.float64)
+    qi = np.ascontiguousarray(q_idx, dtype=np.int32)
+    di = np.ascontiguousarray(deut, dtype=np.int32)
+    st = np.ascontiguousarray(bu_start, dtype=np.int32)
+    cl = np.ascontiguousarray(np.asarray(bu_cells).reshape(-1), dtype=np.int32)
+    num = cl.size // 3
+    cl_buf = cl if cl.size else np.zeros(1, dtype=np.int32)
+    os_ = tt_os_indexing(len(qi), _iptr(qi), _iptr(di), len(di))
+    bu = tt_bu_indexing(num, _iptr(st), _iptr(cl_buf))
+    rp = run_params(precision=PRECISION_PADE, **rp_kw)
+    U = np.zeros(max(len(qi) * len(di) * len(di), 1), dtype=np.complex128)
+    U_BU = np.zeros(max(len(di) * num, 1), dtype=np.complex128)
+    rep = tt_solve_report()
+    _check(lib.tt_solve_faddeev_equations_breakup(
+        U.ctypes.data_as(c_void_p), U_BU.ctypes.data_as(c_void_p), byref(bu), G.ctypes.data_as(c_void_p), _dptr(Pv),
+        _iptr(Pr), Pc.ctypes.data_as(POINTER(c_size_t)), c_size_t(len(Pv)), _dptr(Vu), _dptr(Vc), byref(swp.s),
+        byref(os_), byref(pw.s), byref(rp), byref(rep)))
+    return U[:len(qi) * len(di) * len(di)], U_BU[:len(di) * num], rep.as_dict()
+
+
 def solve_faddeev_adjoint(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q_idx, deut, pw: PW, dV_unco, dV_coup,
                           precision=PRECISION_MIXED, **rp_kw):
     """tt_solve_faddeev_adjoint: U and dU/dtheta_k for the potential derivatives
@@ -593,3 +629,32 @@ class Run:
     def write_U_table(self, chn, U, path):
         U = np.ascontiguousarray(U, dtype=np.complex128)
         _check(self.lib.tt_run_write_U_table(self._h, chn, U.ctypes.data_as(c_void_p), path.encode()))
+
+    def breakup_cells(self, chn):
+        """tt_run_breakup_cells: (start[nE + 1], cells[num][3] = (alpha, q bin, p bin))."""
+        chn = int(chn)
+        num = c_int()
+        _check(self.lib.tt_run_breakup_cells(self._h, chn, byref(num), None, None))
+        start = np.zeros(len(self.energies()[0]) + 1, dtype=np.int32)
+        cells = np.zeros(max(3 * num.value, 1), dtype=np.int32)
+        _check(self.lib.tt_run_breakup_cells(self._h, chn, byref(num), _iptr(start), _iptr(cells)))
+        return start, cells[:3 * num.value].reshape(-1, 3)
+
+    def solve_breakup(self, chn):
+        """tt_run_solve_breakup: the Pade solve's elastic U and breakup U_BU[d * num_cells + b]."""
+        chn = int(chn)
+        nE = len(self.energies()[0])
+        nd = self.channel_info(chn)["n_deuteron"]
+        num = c_int()
+        _check(self.lib.tt_run_breakup_cells(self._h, chn, byref(num), None, None))
+        U = np.zeros(max(nE * nd * nd, 1), dtype=np.complex128)
+        U_BU = np.zeros(max(nd * num.value, 1), dtype=np.complex128)
+        rep = tt_solve_report()
+        _check(self.lib.tt_run_solve_breakup(self._h, chn, U.ctypes.data_as(c_void_p), U_BU.ctypes.data_as(c_void_p),
+                                             byref(rep)))
+        return U[:nE * nd * nd], U_BU[:nd * num.value], rep.as_dict()
+
+    def write_U_BU_table(self, chn, U_BU, path):
+        U_BU = np.ascontiguousarray(U_BU, dtype=np.complex128)
+        _check(self.lib.tt_run_write_U_BU_table(self._h, int(chn), U_BU.ctypes.data_as(c_void_p) if U_BU.size else None,
+                                                os.fsencode(path)))
