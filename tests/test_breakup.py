@@ -45,7 +45,7 @@ def in_grid_mask(cells, nd, Na, Nq, Np):
 def test_oracle_breakup_cells_match_reference(case):
     g, m = load_case(case)
     f = breakup_fixture(case)
-    for c in f["channels"]:
+    for c in map(int, f["channels"]):
         _, st, cells = oracle_cells(g, m, c)
         assert np.array_equal(st, f[f"bu_start_c{c}"])
         assert np.array_equal(cells, f[f"bu_cells_c{c}"])
@@ -58,7 +58,7 @@ def test_oracle_breakup_amplitudes_match_reference(case):
     g, m = load_case(case)
     f = breakup_fixture(case)
     Np, Nq = m["Np"], m["Nq"]
-    for c in f["channels"]:
+    for c in map(int, f["channels"]):
         pw = g[f"pw_c{c}"]
         lay, st, cells = oracle_cells(g, m, c)
         A = oracle.build_A(lay, pw.shape[0], Nq, Np, g[f"p123_row_c{c}"], g[f"p123_col_c{c}"], g[f"p123_val_c{c}"])
@@ -93,7 +93,7 @@ def test_run_breakup_cells_match_reference(case):
     g, m = load_case(case)
     f = breakup_fixture(case)
     run = tt.Run(**m["opts"], include_breakup_channels="true")
-    for c in f["channels"]:
+    for c in map(int, f["channels"]):
         st, cells = run.breakup_cells(c)
         assert np.array_equal(st, f[f"bu_start_c{c}"])
         assert np.array_equal(cells, f[f"bu_cells_c{c}"])
@@ -140,7 +140,7 @@ def test_breakup_table_matches_reference(case):
     g, m = load_case(case)
     f = breakup_fixture(case)
     run = tt.Run(**m["opts"], include_breakup_channels="true")
-    tables = [c for c in f["channels"] if f"table_c{c}" in f]
+    tables = [int(c) for c in f["channels"] if f"table_c{c}" in f]
     assert tables
     for c in tables:
         path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"tt_breakup_table_{case}_{c}.txt")
@@ -195,21 +195,54 @@ def test_breakup_dropin_rejects_dense_precisions():
     assert rc == tt.TT_ERR_UNSUPPORTED
 
 
+def swp_signs(g, m, c, run):
+    """s[alpha, p] = +-1: the sign of the run's SWP eigenvector of state
+    (alpha, p) relative to the reference's.  The reference keeps the signs its
+    LAPACK eigensolver returns; this library makes each eigenvector's largest
+    component positive.  An elastic U element carries the deuteron state's
+    sign twice, a breakup element the deuteron's and the cell's."""
+    pw = g[f"pw_c{c}"]
+    Na, Np = pw.shape[0], m["Np"]
+    ref = oracle.layout(pw, Np, g["V_unco"], g["V_coup"], g["C_unco"], g["C_coup"], g["e_unco"], g["e_coup"],
+                        m["tensor_force"], m["iso"])
+    ours = oracle.layout(pw, Np, run.host_array(3), run.host_array(4), run.host_array(5), run.host_array(6),
+                         run.host_array(7), run.host_array(8), m["tensor_force"], m["iso"])
+    s = np.ones((Na, Np))
+    for a in range(Na):
+        b = ref["blk"][a]
+        d, off = int(ref["blk_dim"][b]), int(ref["blk_off"][b])
+        Cr = ref["C"][off:off + d * d].reshape(d, d)
+        Co = ours["C"][off:off + d * d].reshape(d, d)
+        for p in range(Np):
+            col = int(ref["part"][a]) * Np + p
+            s[a, p] = 1.0 if Cr[:, col] @ Co[:, col] >= 0 else -1.0
+    return s
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", BREAKUP_CASES)
 def test_gpu_breakup_run_matches_reference(case):
     # tt_run_solve_breakup: the Pade solve on the device with the breakup
-    # elements, against the reference's amplitudes at the method's accuracy
+    # elements, against the reference's amplitudes at the method's accuracy,
+    # in the reference's SWP eigenvector signs
     g, m = load_case(case)
     f = breakup_fixture(case)
     run = tt.Run(**m["opts"], include_breakup_channels="true")
-    for c in f["channels"]:
+    for c in map(int, f["channels"]):
         st, cells = run.breakup_cells(c)
         info = run.channel_info(c)
         U, U_BU, rep = run.solve_breakup(c)
-        ok = in_grid_mask(cells, info["n_deuteron"], info["Nalpha"], m["Nq"], m["Np"])
+        nd, nb = info["n_deuteron"], len(cells)
+        ok = in_grid_mask(cells, nd, info["Nalpha"], m["Nq"], m["Np"])
         assert np.all(np.isnan(U_BU[~ok])) and np.all(np.isfinite(U_BU[ok]))
-        assert rel(U_BU[ok], f[f"U_BU_c{c}"][ok]) <= 1e-5, (c, rep)
+        s = swp_signs(g, m, c, run)
+        deut = oracle.deuterons(g[f"pw_c{c}"])
+        sign = np.ones(nd * nb)
+        for d in range(nd):
+            for b in range(nb):
+                if ok[d * nb + b]:
+                    sign[d * nb + b] = s[deut[d], 0] * s[cells[b, 0], cells[b, 2]]
+        assert rel((sign * U_BU)[ok], f[f"U_BU_c{c}"][ok]) <= 1e-5, (c, rep)
         assert rel(U, f[f"U_pade_c{c}"]) <= 1e-5, (c, rep)
     run.close()
 
@@ -224,7 +257,7 @@ def test_gpu_breakup_dropin_matches_reference():
     Np, Nq = m["Np"], m["Nq"]
     swp = tt.SWP(Np, Nq, len(g["e_unco"]) // (Np + 1), len(g["e_coup"]) // (2 * (Np + 1)), float(g["E_bound"]),
                  g["e_unco"], g["e_coup"], g["C_unco"], g["C_coup"], g["q_WP"])
-    for c in f["channels"]:
+    for c in map(int, f["channels"]):
         pwt = g[f"pw_c{c}"]
         n = pwt.shape[0] * Np * Nq
         row, col, val = g[f"p123_row_c{c}"], g[f"p123_col_c{c}"], g[f"p123_val_c{c}"]
