@@ -329,9 +329,13 @@ typedef struct tt_run tt_run;
 
 /* Configure a run from key=value options with the reference's keys and
  * defaults (CPP/set_run_parameters.cpp:76-280, 577-615), e.g.
- * "Np_WP=16", "potential_model=malfliet_tjon", "lab_energies=13".  Builds the
- * partial-wave basis, WP grids, potential matrices, SWP states and on-shell
- * bins on the host (CPP/main.cpp:98-378). */
+ * "Np_WP=16", "potential_model=malfliet_tjon", "lab_energies=13".  An option
+ * without '=' that ends in ".txt" names an input-list file of key=value lines
+ * (CPP/set_run_parameters.cpp:247-279, 641-644); options and files apply in
+ * order, the last setting wins.  Builds the partial-wave basis, WP grids
+ * (Chebyshev, or p_grid_type=custom with the boundaries read from
+ * p_grid_filename / q_grid_filename), potential matrices, SWP states and
+ * on-shell bins on the host (CPP/main.cpp:98-378). */
 int tt_run_create(tt_run** run, int nopt, const char* const* opts);
 void tt_run_destroy(tt_run* run);
 /* Change one option of the linear solve (tc_product, panel_width, panel_order,

@@ -10,7 +10,8 @@ resolvents, on-shell U) into one .npz per case.
 
 (--pade regenerates only the Pade fixtures <case>_pade.npz; --large only the
 summary fixtures of the bench-sized cases, <case>.npz with U and checksums;
---breakup only the breakup fixtures <case>_breakup.npz.)
+--breakup only the breakup fixtures <case>_breakup.npz; --custom-grid only the
+custom-grid fixtures.)
 
 Test infrastructure only; the product never reads these files.
 """
@@ -207,12 +208,64 @@ def run_breakup(name, opts, channels, tables):
     print(name, "breakup channels", channels, "cells", [len(data[f"bu_cells_c{c}"]) for c in channels])
 
 
+# Custom wave-packet grids (p_grid_type=custom, boundaries read from files,
+# CPP/make_wp_states.cpp:46-75, disk_io_routines.cpp:977-994): the boundary
+# files' text is kept in the fixture so that a test can write the same files.
+CUSTOM_GRID_CASES = {
+    "mt_swave_custom_n8": dict(
+        opts=dict(potential_model="malfliet_tjon", swave_only="true", isospin_breaking_1S0="false",
+                  tensor_force="false", J_2N_max=1, two_J_3N_max=1, Np_WP=8, Nq_WP=8, Nphi=16, Nx=16,
+                  lab_energies="13", p_grid_type="custom", q_grid_type="custom"),
+        p=[0.0, 8.0, 20.0, 45.0, 90.0, 160.0, 280.0, 500.0, 1000.0],
+        q=[0.0, 6.5, 17.25, 35.0, 70.0, 125.5, 210.0, 400.0, 900.0]),
+}
+
+
+def run_custom_grid(name, opts, p, q):
+    with tempfile.TemporaryDirectory() as out:
+        texts = {}
+        for key, vals in (("p", p), ("q", q)):
+            texts[key] = "".join(f"{v!r}\n" for v in vals)
+            with open(os.path.join(out, f"{key}_grid.dat"), "w") as f:
+                f.write(texts[key])
+        # not *.txt: the reference's argument parser takes any argument ending in
+        # ".txt" for an input-list file (CPP/set_run_parameters.cpp:641-644)
+        args = [REF_BIN, "dump", out, "--solver=replica", f"p_grid_filename={out}/p_grid.dat",
+                f"q_grid_filename={out}/q_grid.dat"] + [f"{k}={v}" for k, v in opts.items()]
+        subprocess.run(args, check=True, cwd=out, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 4)))
+        meta = read_meta(os.path.join(out, "meta.txt"))
+
+        def rd(fname, dtype):
+            return np.fromfile(os.path.join(out, fname + ".bin"), dtype=dtype)
+
+        data = {"opts": np.array([f"{k}={v}" for k, v in opts.items()]), "p_grid_text": np.array(texts["p"]),
+                "q_grid_text": np.array(texts["q"]), "E_bound": np.array(meta["E_bound"]), "T_lab": meta["T_lab"],
+                "E_com": meta["E_com"], "q_idx": meta["q_idx"], "p_WP": rd("p_WP", np.float64),
+                "q_WP": rd("q_WP", np.float64), "V_unco": rd("V_unco", np.float64),
+                "C_unco": rd("C_unco", np.float64), "e_unco": rd("e_unco", np.float64),
+                "n_chn": np.array(len(meta["channels"]))}
+        for ch in meta["channels"]:
+            t = f"_c{ch['chn']}"
+            data["pw" + t] = rd("pw" + t, np.int32).reshape(-1, 9)
+            data["p123_row" + t] = rd("p123_row" + t, np.int32)
+            data["p123_col" + t] = rd("p123_col" + t, np.int32)
+            data["p123_val" + t] = rd("p123_val" + t, np.float64)
+            data["U" + t] = rd("U" + t, np.complex128)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+        print(name, "custom grids, channels", len(meta["channels"]))
+
+
 if __name__ == "__main__":
     if not os.path.exists(REF_BIN):
         sys.exit(f"{REF_BIN} missing: run `make -C oracle ref` first")
     if "--large" in sys.argv:
         for name, opts in LARGE_CASES.items():
             run_large(name, opts)
+        sys.exit(0)
+    if "--custom-grid" in sys.argv:
+        for name, case in CUSTOM_GRID_CASES.items():
+            run_custom_grid(name, **case)
         sys.exit(0)
     if "--breakup" in sys.argv:
         for name, sel in BREAKUP_CASES.items():

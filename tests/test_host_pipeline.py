@@ -106,3 +106,91 @@ def test_panel_table_rows_and_header():
     # the committed header has the same shape as the rendered one
     src = open(autotune.HEADER).read()
     assert "kPanelWidthTable" in src and "struct PanelWidthRow" in src
+
+
+def write_custom_grids(g, tmp_path):
+    paths = {}
+    for key in ("p", "q"):
+        p = tmp_path / f"{key}_grid.dat"
+        p.write_text(str(g[f"{key}_grid_text"]))
+        paths[f"{key}_grid_filename"] = str(p)
+    return paths
+
+
+def test_custom_grids_match_reference(tmp_path):
+    # p_grid_type=custom: boundaries read from files (CPP/make_wp_states.cpp:46-75,
+    # disk_io_routines.cpp:977-994); the fixture was made by the reference with
+    # the same files.  The host stages reproduce the reference's grids and V bit
+    # for bit, and the oracle chain (P123 -> A -> LU) on them its U
+    import harness as oracle
+    from conftest import load_case as _load, rel_elem
+    g, m = _load("mt_swave_custom_n8")
+    run = tt.Run(**m["opts"], **write_custom_grids(g, tmp_path))
+    assert np.array_equal(run.host_array(1), g["p_WP"])
+    assert np.array_equal(run.host_array(2), g["q_WP"])
+    assert np.array_equal(run.host_array(3), g["V_unco"])
+    assert np.max(np.abs(run.host_array(7) - g["e_unco"])) <= 1e-12 * max(np.max(np.abs(g["e_unco"])), 1.0)
+    T, E, q = run.energies()
+    assert np.array_equal(q, g["q_idx"]) and rel(T, g["T_lab"]) <= 1e-12 and rel(E, g["E_com"]) <= 1e-12
+    pw = run.host_array(0, 0).reshape(-1, 9)
+    assert np.array_equal(pw, g["pw_c0"])
+    r, c, v = oracle.p123(pw, run.host_array(1), run.host_array(2), m["Nphi"], m["Nx"])
+    assert np.array_equal(r, g["p123_row_c0"]) and np.array_equal(c, g["p123_col_c0"])
+    assert rel(v, g["p123_val_c0"]) <= 1e-13
+    lay = oracle.layout(pw, m["Np"], run.host_array(3), run.host_array(4), run.host_array(5), run.host_array(6),
+                        run.host_array(7), run.host_array(8), tensor_force=False, iso=False)
+    Na = pw.shape[0]
+    G = np.stack([oracle.resolvent(lay, Na, m["Nq"], m["Np"], run.host_array(2), e + run.E_bound) for e in E])
+    A = oracle.build_A(lay, Na, m["Nq"], m["Np"], r, c, v)
+    U = oracle.dense_solve(A, G, q, oracle.deuterons(pw), m["Nq"], m["Np"])
+    assert rel_elem(U, g["U_c0"]) <= 1e-10
+    run.close()
+
+
+def test_custom_grid_errors(tmp_path):
+    g, m = load_case("mt_swave_custom_n8")
+    paths = write_custom_grids(g, tmp_path)
+    base = {k: v for k, v in m["opts"].items() if k not in ("p_grid_type", "q_grid_type")}
+    # the q grid is read from its file only when the p grid type is "custom",
+    # as in the reference (make_wp_states.cpp:69)
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(**base, **paths, p_grid_type="chebyshev", q_grid_type="custom")
+    assert "q-momentum gridtype" in str(e.value)
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(**base, **paths, p_grid_type="linear")
+    assert "p-momentum gridtype" in str(e.value)
+    short = tmp_path / "short.dat"
+    short.write_text("0.0\n1.0\n")
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(**base, p_grid_type="custom", q_grid_type="custom", p_grid_filename=str(short),
+               q_grid_filename=paths["q_grid_filename"])
+    assert "mismatch with number of wave-packets" in str(e.value)
+    bad = tmp_path / "bad.dat"
+    bad.write_text("0.0\nx\n" + "1.0\n" * 7)
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(**base, p_grid_type="custom", q_grid_type="custom", p_grid_filename=str(bad),
+               q_grid_filename=paths["q_grid_filename"])
+    assert "Unknown format" in str(e.value)
+
+
+def test_input_list_file(tmp_path):
+    # an argument ending in .txt is an input list of key=value lines, applied in
+    # order with the other options (CPP/set_run_parameters.cpp:247-279, 641-644)
+    g, m = load_case("mt_j2_J1_n8")
+    lst = tmp_path / "run.txt"
+    lines = ["# options of the mt_j2_J1_n8 case", "no delimiter on this line", "Nphi = "]
+    lines += [f"{k}= {v}" for k, v in m["opts"].items()]
+    lst.write_text("\n".join(lines) + "\n")
+    a = tt.Run(str(lst))
+    b = tt.Run(**m["opts"])
+    for which in (1, 2, 3, 7):
+        assert np.array_equal(a.host_array(which), b.host_array(which))
+    assert np.array_equal(a.energies()[2], b.energies()[2])
+    # a later keyword option overrides the list
+    c = tt.Run(str(lst), lab_energies="30")
+    assert len(c.energies()[0]) >= 1 and not np.array_equal(c.energies()[0], a.energies()[0])
+    with pytest.raises(tt.TicTacError) as e:
+        tt.Run(str(tmp_path / "missing.txt"))
+    assert e.value.code == tt.TT_ERR_BADARG
+    for r in (a, b, c):
+        r.close()

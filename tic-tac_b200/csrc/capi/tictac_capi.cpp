@@ -412,6 +412,11 @@ int tt_run_create(tt_run** out, int nopt, const char* const* opts) {
   for (int i = 0; i < nopt; i++) {
     const std::string a = opts[i] ? opts[i] : "";
     const size_t eq = a.find('=');
+    // an input-list file, applied in argument order (CPP/set_run_parameters.cpp:641-644)
+    if (eq == std::string::npos && a.size() > 4 && a.compare(a.size() - 4, 4, ".txt") == 0) {
+      if (!read_input_list(a, r->rp, &err)) return fail(TT_ERR_BADARG, err);
+      continue;
+    }
     if (eq == std::string::npos) return fail(TT_ERR_BADARG, "option without '=': " + a);
     const std::string v = a.substr(eq + 1);
     if (v.empty()) continue;  // the reference skips empty values

@@ -54,6 +54,7 @@ struct RunParams {
   std::string P123_folder = "Output";
   std::string p_grid_type = "chebyshev";
   std::string q_grid_type = "chebyshev";
+  std::string p_grid_filename, q_grid_filename;  // boundaries of a "custom" grid, one per line
   std::string precision = "mixed";  // "fp64" | "mixed"
   int precision_code = 1;           // TT_PRECISION_*
   double refine_tol = 1e-12;
@@ -74,6 +75,10 @@ struct RunParams {
 
 // Sets one key=value option. Returns false (with message) on unknown key or bad value.
 bool set_run_parameter(RunParams& rp, const std::string& key, const std::string& value, std::string* err);
+// Applies an input-list file (read_input_list_and_set_parameters,
+// CPP/set_run_parameters.cpp:247-279): every line "key=value" in order, the
+// value's whitespace removed, lines without '=' and empty values skipped.
+bool read_input_list(const std::string& path, RunParams& rp, std::string* err);
 // Reads whitespace-separated lab energies (disk_io_routines.cpp:80-108).
 bool read_input_energies(const std::string& path, std::vector<double>& out, std::string* err);
 

@@ -2,6 +2,7 @@
 // indexing and kinematics.  See tt_host.h for the reference routine each
 // function restates.
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdlib>
 #include <fstream>
@@ -53,6 +54,8 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
     else if (key == "P123_folder") rp.P123_folder = value;
     else if (key == "p_grid_type") rp.p_grid_type = value;
     else if (key == "q_grid_type") rp.q_grid_type = value;
+    else if (key == "p_grid_filename") rp.p_grid_filename = value;
+    else if (key == "q_grid_filename") rp.q_grid_filename = value;
     else if (key == "precision") {
       if (value != "fp64" && value != "mixed") return bad("precision");
       rp.precision = value;
@@ -99,7 +102,7 @@ bool set_run_parameter(RunParams& rp, const std::string& key, const std::string&
       while (std::getline(ss, tok, ',')) if (!tok.empty()) rp.lec_offsets.push_back(std::stod(tok));
     } else if (key == "subfolder" || key == "P123_omp_num_threads" || key == "P123_recovery" ||
                key == "parameter_walk" || key == "parameter_file" ||
-               key == "PSI_start" || key == "PSI_end" || key == "p_grid_filename" || key == "q_grid_filename") {
+               key == "PSI_start" || key == "PSI_end") {
       // accepted for argument-surface compatibility; no effect on this path
     } else {
       if (err) *err = "unrecognised run option: " + key;
@@ -240,11 +243,69 @@ void chebyshev_boundaries(int n, double* b, double scale, double t) {
   b[0] = 0.0;
 }
 
-bool make_fwp_states(const RunParams& rp, FWPStates& f, std::string* err) {
-  if (rp.p_grid_type != "chebyshev" || rp.q_grid_type != "chebyshev") {
-    if (err) *err = "only chebyshev wave-packet grids are supported";
+bool read_input_list(const std::string& path, RunParams& rp, std::string* err) {
+  std::ifstream in(path);
+  if (!in) {
+    if (err) *err = "cannot open input list " + path;
     return false;
   }
+  std::string line;
+  while (std::getline(in, line)) {
+    const size_t eq = line.find('=');
+    if (eq == std::string::npos) continue;  // lines without '=' are comments
+    const std::string key = line.substr(0, eq);
+    std::string value = line.substr(eq + 1);
+    if (value.find_first_not_of(' ') == std::string::npos) continue;  // empty value: keep the default
+    value.erase(std::remove_if(value.begin(), value.end(), [](unsigned char ch) { return std::isspace(ch); }),
+                value.end());
+    if (!set_run_parameter(rp, key, value, err)) return false;
+  }
+  return true;
+}
+
+// read_WP_boundaries_from_txt (CPP/disk_io_routines.cpp:977-994): one
+// boundary per line (the first number of the line), exactly N + 1 lines
+static bool read_wp_boundaries(const std::string& path, int N, double* out, std::string* err) {
+  std::ifstream in(path);
+  if (!in) {
+    if (err) *err = "cannot open WP-boundary file " + path;
+    return false;
+  }
+  std::string line;
+  int k = 0;
+  while (std::getline(in, line)) {
+    std::istringstream ls(line);
+    double v;
+    if (!(ls >> v)) {
+      if (err) *err = "Unknown format in input WP-boundary file:" + path;
+      return false;
+    }
+    if (k <= N) out[k] = v;
+    k++;
+  }
+  if (k != N + 1) {
+    if (err) *err = "Program mismatch with number of wave-packets in input WP-boundaries file";
+    return false;
+  }
+  return true;
+}
+
+// make_p_bin_grid / make_q_bin_grid (CPP/make_wp_states.cpp:46-75): Chebyshev
+// boundaries or a file; the q grid is read from its file when the P grid
+// type is "custom", as there
+static bool wp_boundaries(const RunParams& rp, bool is_p, int N, double* b, std::string* err) {
+  const std::string& type = is_p ? rp.p_grid_type : rp.q_grid_type;
+  if (type == "chebyshev") {
+    chebyshev_boundaries(N, b, rp.chebyshev_s, rp.chebyshev_t);
+    return true;
+  }
+  if (rp.p_grid_type == "custom")
+    return read_wp_boundaries(is_p ? rp.p_grid_filename : rp.q_grid_filename, N, b, err);
+  if (err) *err = is_p ? "Unknown p-momentum gridtype specified." : "Unknown q-momentum gridtype specified.";
+  return false;
+}
+
+bool make_fwp_states(const RunParams& rp, FWPStates& f, std::string* err) {
   if (rp.Np_WP < 2 || rp.Nq_WP < 2) {
     if (err) *err = "Np_WP and Nq_WP must be >= 2";
     return false;
@@ -258,8 +319,8 @@ bool make_fwp_states(const RunParams& rp, FWPStates& f, std::string* err) {
   const int Nq = rp.midpoint_approx ? f.Nq_WP : f.Nq_per_WP * f.Nq_WP;
   f.p_WP.resize(f.Np_WP + 1);
   f.q_WP.resize(f.Nq_WP + 1);
-  chebyshev_boundaries(f.Np_WP, f.p_WP.data(), rp.chebyshev_s, rp.chebyshev_t);
-  chebyshev_boundaries(f.Nq_WP, f.q_WP.data(), rp.chebyshev_s, rp.chebyshev_t);
+  if (!wp_boundaries(rp, true, f.Np_WP, f.p_WP.data(), err)) return false;
+  if (!wp_boundaries(rp, false, f.Nq_WP, f.q_WP.data(), err)) return false;
   f.p.resize(Np);
   f.q.resize(Nq);
   if (rp.midpoint_approx) {

@@ -417,11 +417,13 @@ def solve_faddeev_adjoint(G, P_val, P_row, P_colptr, V_unco, V_coup, swp: SWP, q
 
 
 class Run:
-    """A configured run (tt_run_*): host state-space setup from key=value options."""
+    """A configured run (tt_run_*): host state-space setup from key=value options
+    (keywords) and input-list files (positional paths ending in .txt, applied
+    first)."""
 
-    def __init__(self, **opts):
+    def __init__(self, *input_lists, **opts):
         lib = load()
-        args = [f"{k}={v}" for k, v in opts.items()]
+        args = [os.fspath(p) for p in input_lists] + [f"{k}={v}" for k, v in opts.items()]
         arr = (c_char_p * len(args))(*[a.encode() for a in args])
         self._h = c_void_p()
         _check(lib.tt_run_create(byref(self._h), len(args), arr))
