@@ -3,6 +3,7 @@
 // U elements (restructure_breakup_data + store_U_BU_matrix_elements_txt,
 // CPP/disk_io_routines.cpp:341-706).  The amplitudes themselves come from
 // the Pade solve on the device (ChannelSolver::solve_pade).
+#include <algorithm>
 #include <cmath>
 #include <iomanip>
 #include <map>
@@ -173,7 +174,9 @@ bool write_breakup_table(std::ostream& f, const BreakupTableInput& in, std::stri
     for (const auto& kv : next_row) last = std::max(last, kv.second);
     rows_at.push_back(last);
   }
-  const int n_rows = rows_at.back(), n_cols = (int)head.size();
+  // rows_at is non-decreasing here (energies ascend, so those below the
+  // threshold come first); the maximum keeps every row index in the table
+  const int n_rows = *std::max_element(rows_at.begin(), rows_at.end()), n_cols = (int)head.size();
   std::vector<double> re((size_t)n_rows * n_cols, 0.0), im((size_t)n_rows * n_cols, 0.0);
   const double nan = std::nan("");
   auto at = [&](int r, int col) -> size_t { return (size_t)r * n_cols + col; };
