@@ -2,10 +2,12 @@
 // the free wave-packet basis and scattering wave packets (SWP).  Each routine
 // restates the reference routine named in tt_host.h with the same arithmetic.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <memory>
 #include <numeric>
+#include <thread>
 
 #include "tt_host.h"
 #include "tt_math.h"
@@ -167,6 +169,100 @@ static double extract_element(int L, int Lp, int J, int S, bool coupled, const d
   return 0;
 }
 
+namespace {
+
+// One 2N matrix of potential_matrices: the (alpha_r, alpha_c) pair that first
+// touches it and how its elements are formed.
+struct VTask {
+  int L_r, L_c, S_r, J_r, T_r;
+  int iso_type;  // 0 np (T = 0), 1 nn/np average (T = 1), 2 / 3 isospin-breaking 1S0 blocks
+  bool via_L, via_T, coupled_matrix, coupled_model;
+  int idx;       // 2N slot in V_coup (coupled_matrix) or V_unco
+};
+
+// Isoscalar potential Vis[6] at (p_in, p_out) for one task
+// (make_potential_matrix.cpp:215-300).
+void isoscalar(Potential& pot, const RunParams& rp, const VTask& t, double p_in, double p_out, double* Vis) {
+  const int Tz_nn = -1, Tz_np = 0;
+  double Vnn[6], Vnp[6];
+  const bool np_only = rp.midpoint_approx ? t.iso_type == 0 : (!t.via_T && t.iso_type == 0);
+  const bool average = rp.midpoint_approx ? t.iso_type == 1 : (!t.via_T && t.iso_type == 1);
+  if (np_only) {
+    pot.V(p_in, p_out, t.coupled_model, t.S_r, t.J_r, t.T_r, Tz_np, Vis);
+  } else if (average) {
+    pot.V(p_in, p_out, t.coupled_model, t.S_r, t.J_r, t.T_r, Tz_nn, Vnn);
+    pot.V(p_in, p_out, t.coupled_model, t.S_r, t.J_r, t.T_r, Tz_np, Vnp);
+    for (int k = 0; k < 6; k++) Vis[k] = (2. / 3) * Vnn[k] + (1. / 3) * Vnp[k];
+  } else {  // the 1S0 block coupled through T_3N
+    pot.V(p_in, p_out, t.coupled_model, t.S_r, t.J_r, t.T_r, Tz_nn, Vnn);
+    pot.V(p_in, p_out, t.coupled_model, t.S_r, t.J_r, t.T_r, Tz_np, Vnp);
+    const double e_nn = extract_element(t.L_r, t.L_c, t.J_r, t.S_r, false, Vnn);
+    const double e_np = extract_element(t.L_r, t.L_c, t.J_r, t.S_r, false, Vnp);
+    Vis[2] = (2. / 3) * e_nn + (1. / 3) * e_np;
+    Vis[3] = (std::sqrt(2) / 3.) * (e_nn - e_np);
+    Vis[4] = (std::sqrt(2) / 3.) * (e_nn - e_np);
+    Vis[5] = (1. / 3) * e_nn + (2. / 3) * e_np;
+  }
+}
+
+// Row br of a task's matrix: every element is a quadrature double sum over
+// the two bins' points (or the bin mid-points), summed in the same order for
+// any thread count, so V does not depend on how rows are shared out.
+void potential_row(Potential& pot, const RunParams& rp, const FWPStates& fwp, const VTask& t, int br,
+                   std::vector<double>& V_unco, std::vector<double>& V_coup) {
+  const int Np = fwp.Np_WP;
+  const double N_r = fwp.norm_p[br];
+  double Vwp[6], Vis[6] = {0, 0, 0, 0, 0, 0};
+  for (int bc = 0; bc < Np; bc++) {
+    const double N_c = fwp.norm_p[bc];
+    for (int k = 0; k < 6; k++) Vwp[k] = 0;
+    if (rp.midpoint_approx) {
+      const double p_in = fwp.p[bc], p_out = fwp.p[br];
+      const double f_in = fwp.fp[bc], f_out = fwp.fp[br];
+      const double d_c = fwp.p_WP[bc + 1] - fwp.p_WP[bc];
+      const double d_r = fwp.p_WP[br + 1] - fwp.p_WP[br];
+      for (int k = 0; k < 6; k++) Vis[k] = 0;
+      isoscalar(pot, rp, t, p_in, p_out, Vis);
+      for (int k = 0; k < 6; k++) Vwp[k] += p_in * p_out * f_in * f_out * d_r * d_c * Vis[k] / (N_r * N_c);
+    } else {
+      const int npw = fwp.Np_per_WP;
+      for (int ir = 0; ir < npw; ir++) {
+        const double p_r = fwp.p[br * npw + ir];
+        const double wp_r = fwp.wp[br * npw + ir];
+        const double wpf_r = fwp.fp[br * npw + ir] * wp_r * p_r;
+        for (int ic = 0; ic < npw; ic++) {
+          const double p_c = fwp.p[bc * npw + ic];
+          const double wp_c = fwp.wp[bc * npw + ic];
+          const double wpf_c = fwp.fp[bc * npw + ic] * wp_c * p_c;
+          const double fac = wpf_r * wpf_c;
+          isoscalar(pot, rp, t, p_c, p_r, Vis);
+          for (int k = 0; k < 6; k++) Vwp[k] += fac * Vis[k] / (N_r * N_c);
+        }
+      }
+    }
+    if (t.coupled_matrix) {
+      double* M = &V_coup[(size_t)t.idx * 4 * Np * Np];
+      const size_t ul = (size_t)br * 2 * Np + bc, ur = ul + Np;
+      const size_t ll = (size_t)(br + Np) * 2 * Np + bc, lr = ll + Np;
+      if (t.via_L) {
+        M[ul] = extract_element(t.J_r - 1, t.J_r - 1, t.J_r, t.S_r, true, Vwp);
+        M[ur] = extract_element(t.J_r - 1, t.J_r + 1, t.J_r, t.S_r, true, Vwp);
+        M[ll] = extract_element(t.J_r + 1, t.J_r - 1, t.J_r, t.S_r, true, Vwp);
+        M[lr] = extract_element(t.J_r + 1, t.J_r + 1, t.J_r, t.S_r, true, Vwp);
+      } else {
+        M[ul] = Vwp[2];
+        M[ur] = Vwp[3];
+        M[ll] = Vwp[4];
+        M[lr] = Vwp[5];
+      }
+    } else {
+      V_unco[(size_t)t.idx * Np * Np + (size_t)br * Np + bc] = extract_element(t.L_r, t.L_c, t.J_r, t.S_r, false, Vwp);
+    }
+  }
+}
+
+}  // namespace
+
 bool potential_matrices(const RunParams& rp, const FWPStates& fwp, const PWStates& pw,
                         std::vector<double>& V_unco, std::vector<double>& V_coup, std::string* err) {
   std::unique_ptr<Potential> pot(make_potential(rp.potential_model, err, rp.lec_offsets));
@@ -176,9 +272,12 @@ bool potential_matrices(const RunParams& rp, const FWPStates& fwp, const PWState
   const int Np = fwp.Np_WP;
   V_unco.assign((size_t)Np * Np * n_unco, 0.0);
   V_coup.assign((size_t)Np * Np * 4 * n_coup, 0.0);
+  // the 2N matrices in the reference's discovery order (every (alpha_r,
+  // alpha_c) pair of equal T, J, S and allowed L; a matrix once), with the
+  // reference's errors in that order (make_potential_matrix.cpp:51-214)
   std::vector<char> done_unco(n_unco, 0), done_coup(n_coup, 0);
+  std::vector<VTask> tasks;
   const bool tf = rp.tensor_force;
-  const int Tz_nn = -1, Tz_np = 0;
   for (int r = 0; r < pw.Nalpha; r++) {
     const int L_r = pw.L_2N[r], S_r = pw.S_2N[r], J_r = pw.J_2N[r], T_r = pw.T_2N[r];
     const int tT_r = pw.two_T_3N[r];
@@ -188,132 +287,58 @@ bool potential_matrices(const RunParams& rp, const FWPStates& fwp, const PWState
       const bool check_L = ((tf && std::abs(L_r - L_c) <= 2) || L_r == L_c);
       if (!(T_r == T_c && J_r == J_c && S_r == S_c && check_L)) continue;
       const bool state_1S0 = (S_r == 0 && J_r == 0 && L_r == 0);
-      int iso_type = -1;
-      if (state_1S0 && tT_r == 3 && tT_c == 3) iso_type = 2;
-      else if ((state_1S0 && (tT_r == 3 && tT_c == 1)) || (tT_r == 1 && tT_c == 3)) iso_type = 3;
-      else if (T_r == 0 && tT_r == tT_c && tT_r == 1) iso_type = 0;
-      else if (T_r == 1 && tT_r == tT_c && tT_r == 1) iso_type = 1;
+      VTask t;
+      t.iso_type = -1;
+      if (state_1S0 && tT_r == 3 && tT_c == 3) t.iso_type = 2;
+      else if ((state_1S0 && (tT_r == 3 && tT_c == 1)) || (tT_r == 1 && tT_c == 3)) t.iso_type = 3;
+      else if (T_r == 0 && tT_r == tT_c && tT_r == 1) t.iso_type = 0;
+      else if (T_r == 1 && tT_r == tT_c && tT_r == 1) t.iso_type = 1;
       else {
         if (err) *err = "Unknown isoscalar-potential encountered in potential-matrix construction";
         return false;
       }
-      const bool via_L = (tf && (L_r != L_c || (L_r == L_c && L_r != J_r && J_r != 0)));
-      const bool via_T = (state_1S0 && rp.isospin_breaking_1S0);
-      if (via_L && via_T) {
+      t.via_L = (tf && (L_r != L_c || (L_r == L_c && L_r != J_r && J_r != 0)));
+      t.via_T = (state_1S0 && rp.isospin_breaking_1S0);
+      if (t.via_L && t.via_T) {
         if (err) *err = "isospin-breaking in coupled channels is not supported";
         return false;
       }
-      const bool coupled_matrix = via_L || via_T;
-      const bool coupled_model = (L_r != L_c || (L_r == L_c && L_r != J_r));
-      int idx_c = 0, idx_u = 0;
-      if (coupled_matrix) idx_c = unique_2N_idx(L_r, S_r, J_r, T_r, true, rp);
-      else idx_u = unique_2N_idx(L_r, S_r, J_r, T_r, false, rp);
-      if (coupled_matrix) {
-        if (done_coup[idx_c]) continue;
-        done_coup[idx_c] = 1;
-      } else {
-        if (done_unco[idx_u]) continue;
-        done_unco[idx_u] = 1;
+      t.coupled_matrix = t.via_L || t.via_T;
+      t.coupled_model = (L_r != L_c || (L_r == L_c && L_r != J_r));
+      t.L_r = L_r;
+      t.L_c = L_c;
+      t.S_r = S_r;
+      t.J_r = J_r;
+      t.T_r = T_r;
+      t.idx = unique_2N_idx(L_r, S_r, J_r, T_r, t.coupled_matrix, rp);
+      std::vector<char>& done = t.coupled_matrix ? done_coup : done_unco;
+      if (t.idx < 0 || t.idx >= (int)done.size()) {
+        if (err) *err = "partial wave maps to a 2N channel outside the potential arrays";
+        return false;
       }
-      double Vwp[6], Vis[6], Vnn[6], Vnp[6];
-      auto isoscalar = [&](double p_in, double p_out) -> bool {
-        if (!rp.midpoint_approx) {
-          if (!via_T && iso_type == 0) {
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_np, Vis);
-          } else if (!via_T && iso_type == 1) {
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_nn, Vnn);
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_np, Vnp);
-            for (int k = 0; k < 6; k++) Vis[k] = (2. / 3) * Vnn[k] + (1. / 3) * Vnp[k];
-          } else if (via_T) {
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_nn, Vnn);
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_np, Vnp);
-            const double e_nn = extract_element(L_r, L_c, J_r, S_r, false, Vnn);
-            const double e_np = extract_element(L_r, L_c, J_r, S_r, false, Vnp);
-            Vis[2] = (2. / 3) * e_nn + (1. / 3) * e_np;
-            Vis[3] = (std::sqrt(2) / 3.) * (e_nn - e_np);
-            Vis[4] = (std::sqrt(2) / 3.) * (e_nn - e_np);
-            Vis[5] = (1. / 3) * e_nn + (2. / 3) * e_np;
-          } else {
-            return false;
-          }
-        } else {
-          if (iso_type == 0) {
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_np, Vis);
-          } else if (iso_type == 1) {
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_nn, Vnn);
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_np, Vnp);
-            for (int k = 0; k < 6; k++) Vis[k] = (2. / 3) * Vnn[k] + (1. / 3) * Vnp[k];
-          } else {
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_nn, Vnn);
-            pot->V(p_in, p_out, coupled_model, S_r, J_r, T_r, Tz_np, Vnp);
-            const double e_nn = extract_element(L_r, L_c, J_r, S_r, false, Vnn);
-            const double e_np = extract_element(L_r, L_c, J_r, S_r, false, Vnp);
-            Vis[2] = (2. / 3) * e_nn + (1. / 3) * e_np;
-            Vis[3] = (std::sqrt(2) / 3.) * (e_nn - e_np);
-            Vis[4] = (std::sqrt(2) / 3.) * (e_nn - e_np);
-            Vis[5] = (1. / 3) * e_nn + (2. / 3) * e_np;
-          }
-        }
-        return true;
-      };
-      for (int br = 0; br < Np; br++) {
-        const double N_r = fwp.norm_p[br];
-        for (int bc = 0; bc < Np; bc++) {
-          const double N_c = fwp.norm_p[bc];
-          for (int k = 0; k < 6; k++) Vwp[k] = 0;
-          if (rp.midpoint_approx) {
-            const double p_in = fwp.p[bc], p_out = fwp.p[br];
-            const double f_in = fwp.fp[bc], f_out = fwp.fp[br];
-            const double d_c = fwp.p_WP[bc + 1] - fwp.p_WP[bc];
-            const double d_r = fwp.p_WP[br + 1] - fwp.p_WP[br];
-            for (int k = 0; k < 6; k++) Vis[k] = 0;
-            if (!isoscalar(p_in, p_out)) {
-              if (err) *err = "Unknown isoscalar potential encountered";
-              return false;
-            }
-            for (int k = 0; k < 6; k++) Vwp[k] += p_in * p_out * f_in * f_out * d_r * d_c * Vis[k] / (N_r * N_c);
-          } else {
-            const int npw = fwp.Np_per_WP;
-            for (int ir = 0; ir < npw; ir++) {
-              const double p_r = fwp.p[br * npw + ir];
-              const double wp_r = fwp.wp[br * npw + ir];
-              const double wpf_r = fwp.fp[br * npw + ir] * wp_r * p_r;
-              for (int ic = 0; ic < npw; ic++) {
-                const double p_c = fwp.p[bc * npw + ic];
-                const double wp_c = fwp.wp[bc * npw + ic];
-                const double wpf_c = fwp.fp[bc * npw + ic] * wp_c * p_c;
-                const double fac = wpf_r * wpf_c;
-                if (!isoscalar(p_c, p_r)) {
-                  if (err) *err = "Unknown isoscalar potential encountered";
-                  return false;
-                }
-                for (int k = 0; k < 6; k++) Vwp[k] += fac * Vis[k] / (N_r * N_c);
-              }
-            }
-          }
-          if (coupled_matrix) {
-            double* M = &V_coup[(size_t)idx_c * 4 * Np * Np];
-            const size_t ul = (size_t)br * 2 * Np + bc, ur = ul + Np;
-            const size_t ll = (size_t)(br + Np) * 2 * Np + bc, lr = ll + Np;
-            if (via_L) {
-              M[ul] = extract_element(J_r - 1, J_r - 1, J_r, S_r, true, Vwp);
-              M[ur] = extract_element(J_r - 1, J_r + 1, J_r, S_r, true, Vwp);
-              M[ll] = extract_element(J_r + 1, J_r - 1, J_r, S_r, true, Vwp);
-              M[lr] = extract_element(J_r + 1, J_r + 1, J_r, S_r, true, Vwp);
-            } else {
-              M[ul] = Vwp[2];
-              M[ur] = Vwp[3];
-              M[ll] = Vwp[4];
-              M[lr] = Vwp[5];
-            }
-          } else {
-            V_unco[(size_t)idx_u * Np * Np + (size_t)br * Np + bc] =
-                extract_element(L_r, L_c, J_r, S_r, false, Vwp);
-          }
-        }
+      if (done[t.idx]) continue;
+      done[t.idx] = 1;
+      // outside the mid-point approximation an isospin-breaking block needs T_3N coupling
+      if (!rp.midpoint_approx && !t.via_T && (t.iso_type == 2 || t.iso_type == 3)) {
+        if (err) *err = "Unknown isoscalar potential encountered";
+        return false;
       }
+      tasks.push_back(t);
     }
   }
+  // rows of all matrices shared out over the host's cores
+  const size_t items = tasks.size() * (size_t)Np;
+  auto work = [&](std::atomic<size_t>* next) {
+    for (size_t it = next->fetch_add(1); it < items; it = next->fetch_add(1))
+      potential_row(*pot, rp, fwp, tasks[it / Np], (int)(it % Np), V_unco, V_coup);
+  };
+  std::atomic<size_t> next{0};
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nthreads = std::min<size_t>({hw, (size_t)64, std::max<size_t>(1, items / 4)});
+  std::vector<std::thread> pool;
+  for (size_t k = 1; k < nthreads; k++) pool.emplace_back(work, &next);
+  work(&next);
+  for (auto& th : pool) th.join();
   return true;
 }
 
