@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <memory>
 #include <numeric>
+#include <system_error>
 #include <thread>
 
 #include "tt_host.h"
@@ -336,7 +337,11 @@ bool potential_matrices(const RunParams& rp, const FWPStates& fwp, const PWState
   const size_t hw = std::max(1u, std::thread::hardware_concurrency());
   const size_t nthreads = std::min<size_t>({hw, (size_t)64, std::max<size_t>(1, items / 4)});
   std::vector<std::thread> pool;
-  for (size_t k = 1; k < nthreads; k++) pool.emplace_back(work, &next);
+  try {
+    for (size_t k = 1; k < nthreads; k++) pool.emplace_back(work, &next);
+  } catch (const std::system_error&) {
+    // fewer threads than asked for: the ones running (and this one) take all rows
+  }
   work(&next);
   for (auto& th : pool) th.join();
   return true;
