@@ -367,6 +367,8 @@ int main(int argc, char** argv) {
       delete[] VC;
     }
     dump("U" + tag, U.data(), nE * nd * nd);
+    if (mode == "dump")  // the reference's own elastic table of this U (disk_io_routines.cpp:759-913)
+      store_U_matrix_elements_txt(U.data(), cfg, os, rp, swp, sub, g_out + "/U_table" + tag + ".txt");
     meta.flush();
     delete[] val;
     delete[] row;

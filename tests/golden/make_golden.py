@@ -11,7 +11,7 @@ resolvents, on-shell U) into one .npz per case.
 (--pade regenerates only the Pade fixtures <case>_pade.npz; --large only the
 summary fixtures of the bench-sized cases, <case>.npz with U and checksums;
 --breakup only the breakup fixtures <case>_breakup.npz; --custom-grid only the
-custom-grid fixtures.)
+custom-grid fixtures; --tables only the elastic U tables <case>_tables.npz.)
 
 Test infrastructure only; the product never reads these files.
 """
@@ -208,6 +208,24 @@ def run_breakup(name, opts, channels, tables):
     print(name, "breakup channels", channels, "cells", [len(data[f"bu_cells_c{c}"]) for c in channels])
 
 
+def run_tables(name, opts):
+    """The reference's elastic U table (store_U_matrix_elements_txt) of every
+    channel of a case, with the U it was written from, as <name>_tables.npz."""
+    with tempfile.TemporaryDirectory() as out:
+        args = [REF_BIN, "dump", out, "--solver=replica"] + [f"{k}={v}" for k, v in opts.items()]
+        subprocess.run(args, check=True, cwd=out, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 4)))
+        meta = read_meta(os.path.join(out, "meta.txt"))
+        data = {}
+        for ch in meta["channels"]:
+            t = f"_c{ch['chn']}"
+            data["U" + t] = np.fromfile(os.path.join(out, f"U{t}.bin"), dtype=np.complex128)
+            with open(os.path.join(out, f"U_table{t}.txt")) as f:
+                data["table" + t] = np.array(f.read())
+        np.savez_compressed(os.path.join(HERE, f"{name}_tables.npz"), **data)
+        print(name, "tables of", len(meta["channels"]), "channels")
+
+
 # Custom wave-packet grids (p_grid_type=custom, boundaries read from files,
 # CPP/make_wp_states.cpp:46-75, disk_io_routines.cpp:977-994): the boundary
 # files' text is kept in the fixture so that a test can write the same files.
@@ -262,6 +280,10 @@ if __name__ == "__main__":
     if "--large" in sys.argv:
         for name, opts in LARGE_CASES.items():
             run_large(name, opts)
+        sys.exit(0)
+    if "--tables" in sys.argv:
+        for name in ("mt_swave_n16", "lo_j1_J3_n8"):
+            run_tables(name, CASES[name])
         sys.exit(0)
     if "--custom-grid" in sys.argv:
         for name, case in CUSTOM_GRID_CASES.items():

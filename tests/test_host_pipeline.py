@@ -194,3 +194,34 @@ def test_input_list_file(tmp_path):
     assert e.value.code == tt.TT_ERR_BADARG
     for r in (a, b, c):
         r.close()
+
+
+@pytest.mark.parametrize("case", ["mt_swave_n16", "lo_j1_J3_n8"])
+def test_u_table_matches_reference_table(case, tmp_path):
+    # tt_run_write_U_table against the reference's own table of the same U
+    # (store_U_matrix_elements_txt, disk_io_routines.cpp:759-913; fixture from
+    # make_golden.py --tables): header lines and U columns identical, T_lab and
+    # E_com within the host set-up's rounding
+    import os
+    from conftest import GOLDEN
+    g, m = load_case(case)
+    t = np.load(os.path.join(GOLDEN, f"{case}_tables.npz"))
+    run = tt.Run(**m["opts"])
+    for c in range(run.num_channels):
+        p = str(tmp_path / f"U_c{c}.txt")
+        run.write_U_table(c, t[f"U_c{c}"], p)
+        ours = open(p).read().split("\n")
+        ref = str(t[f"table_c{c}"]).split("\n")
+        assert len(ours) == len(ref)
+        for a, b in zip(ours, ref):
+            if a.startswith("#") or not a.strip() or a.strip().startswith("U"):
+                assert a == b
+                continue
+            ta, tb = a.split(), b.split()
+            assert len(ta) == len(tb) and len(a) == len(b)
+            for x, y in zip(ta, tb):
+                if x.endswith("j") or "." not in x:
+                    assert x == y
+                else:
+                    assert abs(float(x) - float(y)) <= 1e-13 * abs(float(y))
+    run.close()

@@ -934,6 +934,20 @@ int tt_run_write_U_table(const tt_run* run, int chn, const tt_complex* U, const 
   f << "# Nq:          " << run->fwp.Nq_WP << " \n";
   f << "# Particles:   nd-scattering\n";
   f << "# Deuteron BE: " << run->swp.E_bound << " MeV \n# \n";
+  f << "# Symbol definitions: \n";
+  static const char* const kSymbols[][2] = {
+      {"Uij:", "U-matrix element in MeV with row-idx i and col-idx j (NOTE in wave-packet representation!)"},
+      {"l:", "Spectator nucleon orbital angular momentum"},
+      {"j:", "Spectator nucleon total angular momentum"},
+      {"Tlab:", "Laboratory scattering/kinetic energy"},
+      {"Ecm:", "Centre-of-mass scattering/kinetic energy"},
+      {"q_idx:", "Index of on-shell q-momentum bin correponding to Tlab/Ecm"}};
+  for (const auto& sym : kSymbols) {
+    std::string tag = sym[0];
+    tag.resize(7, ' ');
+    f << "# " << tag << sym[1] << "  \n";
+  }
+  f << "# \n";
   f << "# ################################################################################################### \n";
   f << std::right << std::scientific << std::setprecision(16);
   const char* h1[] = {"Name", "row-idx", "col-idx", "l'", "2*j'", "l", "2*j"};
@@ -947,11 +961,12 @@ int tt_run_write_U_table(const tt_run* run, int chn, const tt_complex* U, const 
         << std::setw(10) << c.L_1N[deut[cc]] << std::setw(10) << c.two_J_1N[deut[cc]] << "\n";
     }
   f << "# ################################################################################################### \n";
-  auto fmt = [](double v) {
-    char b[64];
-    std::snprintf(b, sizeof(b), "%+.16e", v);
-    return std::string(b);
-  };
+  // the second table's header names nine U columns whatever nd is, as there
+  f << "#" << std::setw(24) << "Tlab [MeV]" << std::setw(24) << "Ecm [MeV]" << std::setw(10) << "q_idx";
+  for (int r = 0; r < 3; r++)
+    for (int cc = 0; cc < 3; cc++) f << std::setw(50) << ("U" + std::to_string(r) + std::to_string(cc) + " [MeV]");
+  f << "\n";
+  const auto fmt = signed_scientific;
   for (size_t j = 0; j < nE; j++) {
     f << " " << std::setw(24) << run->os.T_lab[j] << std::setw(24) << run->os.E_com[j] << std::setw(10)
       << run->os.q_com_idx[j];

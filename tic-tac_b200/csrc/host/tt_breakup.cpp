@@ -95,19 +95,13 @@ bool find_breakup_cells(const RunParams& rp, const PWChannel& ch, const SWPState
   return true;
 }
 
-namespace {
-
-// to_string_with_precision_and_sign (CPP/disk_io_routines.cpp:3-12): a "+"
-// in front of values >= 0, then the stream's scientific form
-std::string signed_sci(double v) {
+std::string signed_scientific(double v) {
   std::ostringstream o;
   o.precision(16);
   if (v >= 0) o << "+";
   o << std::scientific << v;
   return o.str();
 }
-
-}  // namespace
 
 bool write_breakup_table(std::ostream& f, const BreakupTableInput& in, std::string* err) {
   const PWChannel& c = in.ch;
@@ -256,7 +250,7 @@ bool write_breakup_table(std::ostream& f, const BreakupTableInput& in, std::stri
     f << " ";
     for (int col = 0; col < n_cols; col++) {
       if (head[col].comp)
-        f << std::right << std::setw(50) << (signed_sci(re[at(r, col)]) + signed_sci(im[at(r, col)]) + "j");
+        f << std::right << std::setw(50) << (signed_scientific(re[at(r, col)]) + signed_scientific(im[at(r, col)]) + "j");
       else
         f << std::right << std::setw(24) << re[at(r, col)];
     }

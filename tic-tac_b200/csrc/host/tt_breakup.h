@@ -1,4 +1,5 @@
-// Breakup U-matrix table of one channel (find_breakup_cells is declared in tt_host.h).
+// The reference's U-matrix text tables: the breakup table of one channel
+// (find_breakup_cells is declared in tt_host.h) and the number format of both.
 #pragma once
 #include <ostream>
 #include <string>
@@ -24,5 +25,10 @@ struct BreakupTableInput {
 // pair (U, the cell's q and p boundaries as momenta).  Boundaries of a cell
 // outside the grid are written as nan.
 bool write_breakup_table(std::ostream& f, const BreakupTableInput& in, std::string* err);
+
+// A U element part as the reference's tables write it
+// (to_string_with_precision_and_sign, CPP/disk_io_routines.cpp:3-12): "+" in
+// front of values >= 0, then 16 digits in scientific form.
+std::string signed_scientific(double v);
 
 }  // namespace tt
