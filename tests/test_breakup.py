@@ -132,7 +132,7 @@ def table_tokens(text):
 
 
 @pytest.mark.parametrize("case", BREAKUP_CASES)
-def test_breakup_table_matches_reference(case):
+def test_breakup_table_matches_reference(case, tmp_path):
     # tt_run_write_U_BU_table given the reference's U_BU: the header and every
     # U token identical, the kinematic columns within rounding of the SWP
     # energies (this library's eigensolver and the reference's LAPACK differ in
@@ -143,11 +143,9 @@ def test_breakup_table_matches_reference(case):
     tables = [int(c) for c in f["channels"] if f"table_c{c}" in f]
     assert tables
     for c in tables:
-        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"tt_breakup_table_{case}_{c}.txt")
+        path = tmp_path / f"U_BU_c{c}.txt"
         run.write_U_BU_table(c, f[f"U_BU_c{c}"], path)
-        with open(path) as fh:
-            ours = fh.read()
-        os.remove(path)
+        ours = path.read_text()
         h1, r1 = table_tokens(ours)
         h2, r2 = table_tokens(str(f[f"table_c{c}"]))
         assert h1 == h2
