@@ -225,3 +225,11 @@ def test_u_table_matches_reference_table(case, tmp_path):
                 else:
                     assert abs(float(x) - float(y)) <= 1e-13 * abs(float(y))
     run.close()
+
+
+def test_parallel_run_needs_channel_index():
+    # set_run_parameters.cpp:666-668
+    opts = dict(potential_model="malfliet_tjon", J_2N_max=1, two_J_3N_max=1, Np_WP=8, Nq_WP=8, lab_energies="10")
+    with pytest.raises(tt.TicTacError, match="channel index"):
+        tt.Run(parallel_run="true", **opts)
+    tt.Run(parallel_run="true", channel_idx=0, **opts).close()
