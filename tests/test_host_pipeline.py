@@ -233,3 +233,6 @@ def test_parallel_run_needs_channel_index():
     with pytest.raises(tt.TicTacError, match="channel index"):
         tt.Run(parallel_run="true", **opts)
     tt.Run(parallel_run="true", channel_idx=0, **opts).close()
+    # main.cpp:162-164
+    with pytest.raises(tt.TicTacError, match="nothing to do"):
+        tt.Run(solve_faddeev="false", calculate_and_store_P123="false", **opts)

@@ -422,9 +422,12 @@ int tt_run_create(tt_run** out, int nopt, const char* const* opts) {
     if (v.empty()) continue;  // the reference skips empty values
     if (!set_run_parameter(r->rp, a.substr(0, eq), v, &err)) return fail(TT_ERR_BADARG, err);
   }
-  // set_run_parameters' consistency check (CPP/set_run_parameters.cpp:666-668)
+  // set_run_parameters' and main's consistency checks (CPP/set_run_parameters.cpp:666-668, main.cpp:162-164)
   if (r->rp.parallel_run && r->rp.channel_idx == -1)
     return fail(TT_ERR_BADARG, "Parallel run specified in input but no channel index (i.e. channel_idx=<int>) given!");
+  if (!r->rp.solve_faddeev && !r->rp.calculate_and_store_P123)
+    return fail(TT_ERR_BADARG,
+                "Both solve_faddeev=false and calculate_and_store_P123==false so code has nothing to do!");
   if (!construct_pw_states(r->rp, r->pw, &err)) return fail(TT_ERR_BADARG, err);
   if (!make_fwp_states(r->rp, r->fwp, &err)) return fail(TT_ERR_BADARG, err);
   if (!potential_matrices(r->rp, r->fwp, r->pw, r->V_unco, r->V_coup, &err)) return fail(TT_ERR_BADARG, err);
